@@ -1,0 +1,176 @@
+/*
+ * sem_b200.h - C ABI of the B200 elastic spectral-element time loop.
+ *
+ * Drop-in replacement for the hot path that SpecFWAT's xfwat_fwd_measure_adj
+ * drives through its SPECFEM interface layer:
+ *
+ *   reference call                                   replaced by
+ *   -----------------------------------------------  -------------------------
+ *   read_mesh_databases_fwat + prepare_GPU (mesh)     sem_prepare_mesh
+ *     src/specfem_interface/read_mesh_databases.f90:91-1396
+ *     src/specfem_interface/prepare_timerun_fwat.f90:120
+ *   prepare_timerun_fwat(ievt)                        sem_prepare_timerun
+ *     src/specfem_interface/prepare_timerun_fwat.f90:29-168
+ *   setup_sources_receivers_fwat(ievt)                sem_set_sources,
+ *     src/specfem_interface/setup_sources_receivers_fwat.f90:29-88
+ *                                                     sem_set_receivers
+ *   iterate_time() (SIMULATION_TYPE 1 / 3)            sem_iterate_time
+ *     called at src/preproc/prepare_fwd.f90:364
+ *   seismograms_d read by read_syn_data               sem_get_seismograms
+ *     src/preproc/syn_data.f90:64-66
+ *   SEM/<sta>.adj written by write_adj, read back as      sem_set_adjoint_sources
+ *   source_adjoint                                    (or sem_measure_l2)
+ *     src/preproc/syn_data.f90:232-251,
+ *     src/specfem_interface/setup_sources_receivers_fwat.f90:487-490
+ *   WaveformMisfit%calc_adjoint_source                sem_measure_l2
+ *     src/preproc/adjoint_sources/waveform_misfit.f90:15-64
+ *   compute_kernels + save_adjoint_kernels            sem_save_adjoint_kernels
+ *     called at src/preproc/prepare_fwd.f90:381
+ *   PostFlow%sum_kernel (cross-event sum)             sem_sum_kernels
+ *     src/postproc/post_processing.f90:108-149
+ *   FinalizeSpecfem / prepare_cleanup_device          sem_release_run,
+ *     src/specfem_interface/specfem_api.f90:298-369    sem_release_mesh
+ *
+ * Conventions
+ *  - Every function returns SEM_OK (0) or a negative sem_status; the reason
+ *    is kept per thread and returned by sem_last_error().  No call aborts
+ *    the process (the reference aborts through exit_MPI).
+ *  - All arrays are caller-owned HOST arrays; the library copies them.
+ *  - Index arrays may be 0- or 1-based (sem_mesh_desc.index_base), so the
+ *    Fortran database arrays can be passed unchanged.
+ *  - Array layouts are the reference's Fortran column-major layouts read as
+ *    C row-major with the indices reversed: ibool(5,5,5,nspec) is
+ *    ibool[nspec][5][5][5] with i fastest; abs_boundary_ijk(3,25,nf) is
+ *    ijk[nf][25][3]; seismograms are [nrec][3][nstep] with components
+ *    (x=East, y=North, z=Up).
+ *  - One run handle per host thread; calls on one handle must not overlap.
+ *    All device work of a run is queued on the run's own CUDA stream.
+ */
+#ifndef SEM_B200_H
+#define SEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SEM_ABI_VERSION 1
+
+typedef enum {
+  SEM_OK = 0,
+  SEM_ERR_ARG = -1,          /* invalid argument or inconsistent sizes      */
+  SEM_ERR_CUDA = -2,         /* CUDA runtime error                          */
+  SEM_ERR_NOMEM = -3,        /* device memory budget or allocation failed   */
+  SEM_ERR_STATE = -4,        /* call out of order (e.g. adjoint w/o forward)*/
+  SEM_ERR_UNSUPPORTED = -5,  /* input outside what this build implements    */
+  SEM_ERR_NUMERIC = -6,      /* non-finite wavefield detected               */
+  SEM_ERR_NODEVICE = -7      /* no usable sm_100 device                      */
+} sem_status;
+
+/* Mesh database of one slice (read_mesh_databases.f90:158-193,455-486,
+ * 766-804).  All elements must be regular (cubes: one xix_regular and one
+ * jacobian_regular); irregular_element_number, when given, must be all <= 0
+ * (SEM_ERR_UNSUPPORTED otherwise). */
+typedef struct {
+  int nspec;
+  int nglob;
+  int index_base;                   /* 0 (C) or 1 (Fortran) for ibool/ijk  */
+  const int *ibool;                 /* [nspec][5][5][5]                    */
+  const float *xstore, *ystore, *zstore;   /* [nglob] metres               */
+  float xix_regular;                /* d xi / d x of the regular elements  */
+  float jacobian_regular;           /* (h/2)^3                             */
+  const int *irregular_element_number;     /* [nspec] or NULL              */
+  const float *kappastore, *mustore, *rhostore;   /* [nspec][125]          */
+  const float *rmass;               /* [nglob] assembled mass (no Stacey)  */
+  const float *rho_vp, *rho_vs;     /* [nspec][125]                        */
+  int num_abs_boundary_faces;
+  const int *abs_boundary_ispec;    /* [nf]                                */
+  const int *abs_boundary_ijk;      /* [nf][25][3]                         */
+  const float *abs_boundary_jacobian2Dw;   /* [nf][25]                     */
+  const float *abs_boundary_normal; /* [nf][25][3]                         */
+} sem_mesh_desc;
+
+/* Run options (prepare_timerun_fwat.f90:29-168 + Par_file switches). */
+typedef enum { SEM_STORE_FP32 = 0, SEM_STORE_FP16 = 1 } sem_store_kind;
+
+typedef struct {
+  int nev;            /* events in this run (1 = plain path)               */
+  int nstep;          /* NSTEP                                             */
+  double dt;          /* DT (s)                                            */
+  int store_kind;     /* sem_store_kind for the Stacey boundary store      */
+  int use_graph;      /* 1: replay the step loop as CUDA graphs            */
+  int graph_steps;    /* steps per captured graph (0 = default 50)         */
+  int max_receivers;  /* receivers per event upper bound (>= 1)            */
+  int check_every;    /* steps between non-finite checks (0 = off)         */
+} sem_run_cfg;
+
+/* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard
+ * CMT frame (r up, theta south, phi east), mapped to x=E, y=N, z=Up as
+ * locate_source_fwat.f90:215-228 does; Ricker wavelet with dominant
+ * frequency f0 centred at 1.2/f0 + tshift (locate_source_fwat.f90:499-506). */
+typedef struct {
+  double x, y, z;             /* metres, z <= 0 is depth                  */
+  double Mrr, Mtt, Mpp, Mrt, Mrp, Mtp;   /* N m                            */
+  double f0;                  /* Hz                                       */
+  double tshift;              /* s                                        */
+} sem_source;
+
+typedef struct sem_mesh_s sem_mesh;
+typedef struct sem_run_s sem_run;
+
+/* Library / device information. */
+int sem_abi_version(void);
+const char *sem_last_error(void);
+int sem_device_info(int *sm_count, long long *hbm_bytes, int *cc_major,
+                    int *cc_minor);
+
+/* Mesh residency: upload a database once; many runs may share it. */
+int sem_prepare_mesh(const sem_mesh_desc *desc, sem_mesh **out);
+int sem_release_mesh(sem_mesh *mesh);
+int sem_mesh_info(const sem_mesh *mesh, int *nspec, int *nglob, int *nfaces,
+                  long long *device_bytes);
+
+/* Per-run device state: mass matrix with the Stacey term for this dt,
+ * wavefields, boundary store, seismogram and kernel buffers. */
+int sem_prepare_timerun(sem_mesh *mesh, const sem_run_cfg *cfg,
+                        sem_run **out);
+int sem_release_run(sem_run *run);
+/* Bytes sem_prepare_timerun would allocate for this cfg with sim types
+ * 1 and 3 (HBM-budget admission). */
+long long sem_run_bytes(const sem_mesh *mesh, const sem_run_cfg *cfg);
+
+/* Sources and receivers (located on the host, nearest element centre). */
+int sem_set_sources(sem_run *run, int nev, const sem_source *src);
+int sem_set_receivers(sem_run *run, int ev, int nrec, const double *xyz);
+
+/* Time loop.  sim_type 1: forward (save_forward=1 keeps the boundary store
+ * and the final state in HBM for a later sim_type 3).  sim_type 3: adjoint
+ * field driven by the adjoint sources plus backward reconstruction with
+ * kernel accumulation.  Asynchronous: returns after queueing. */
+int sem_iterate_time(sem_run *run, int sim_type, int save_forward);
+int sem_synchronize(sem_run *run);
+
+/* Seismograms of event ev: out[nrec][3][nstep] (displacement, m). */
+int sem_get_seismograms(sem_run *run, int ev, float *out);
+/* Adjoint sources of event ev in forward time order, [nrec][3][nstep]. */
+int sem_set_adjoint_sources(sem_run *run, int ev, const double *adj);
+/* L2 waveform misfit on the device in FP64 between the last forward
+ * seismograms of ev and obs[nrec][3][nstep]; sets the adjoint sources of ev
+ * and writes the misfit (sum over receivers and components). */
+int sem_measure_l2(sem_run *run, int ev, const double *obs,
+                   double taper_pct, int taper_type, double *misfit);
+
+/* Kernels of event ev after sim_type 3: out[6][nspec][125] in the order
+ * rho, mu, kappa, rhop, beta, alpha (names of post_processing.f90:417-422). */
+int sem_save_adjoint_kernels(sem_run *run, int ev, double *out);
+/* FP64 sum of the six kernels over all events of the run, same layout. */
+int sem_sum_kernels(sem_run *run, double *out);
+
+/* Device-time of the last sem_iterate_time in milliseconds. */
+int sem_last_loop_ms(sem_run *run, double *ms);
+/* Number of kernel launches queued by the last sem_iterate_time. */
+int sem_last_launch_count(sem_run *run, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEM_B200_H */

@@ -1,0 +1,947 @@
+// Host engine and C ABI (include/sem_b200.h) of the B200 SEM time loop.
+//
+// The reference drives its solver through argument-free Fortran entry
+// points acting on module globals (src/preproc/prepare_fwd.f90:328-368);
+// here the same sequence is a handle API: a resident mesh (the database of
+// read_mesh_databases_fwat), a run (prepare_timerun_fwat: mass matrix with
+// the Stacey term for this dt, wavefields, boundary store), sources and
+// receivers (setup_sources_receivers_fwat), the time loop (iterate_time for
+// SIMULATION_TYPE 1 and 3) and the kernels (save_adjoint_kernels).
+//
+// Device work of a run is queued on the run's stream.  The step loop is
+// either launched step by step or replayed as CUDA graphs of `graph_steps`
+// steps; per-lane step counters live in device memory (LaneDesc::it0) and
+// are advanced by a kernel at the end of each graph, so the graph needs no
+// parameter updates between replays.
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "sem_b200.h"
+#include "sem_internal.cuh"
+
+using namespace sem;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(x)                                                                   \
+  do {                                                                          \
+    cudaError_t e_ = (x);                                                       \
+    if (e_ != cudaSuccess)                                                      \
+      return fail(SEM_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));   \
+  } while (0)
+
+#define CKM(x, what)                                                            \
+  do {                                                                          \
+    cudaError_t e_ = (x);                                                       \
+    if (e_ != cudaSuccess) {                                                    \
+      cudaGetLastError();                                                       \
+      return fail(SEM_ERR_NOMEM, "device allocation of %s failed: %s", what,   \
+                  cudaGetErrorString(e_));                                      \
+    }                                                                           \
+  } while (0)
+
+// ----------------------------------------------------------------------------
+// GLL quadrature of degree 4 (closed form) and Lagrange interpolants
+// ----------------------------------------------------------------------------
+
+struct GllTables {
+  double xi[5], w[5], D[5][5];
+};
+
+const GllTables& gll() {
+  static GllTables t = [] {
+    GllTables g{};
+    const double s = std::sqrt(3.0 / 7.0);
+    const double xi[5] = {-1.0, -s, 0.0, s, 1.0};
+    const double w[5] = {0.1, 49.0 / 90.0, 32.0 / 45.0, 49.0 / 90.0, 0.1};
+    for (int i = 0; i < 5; ++i) {
+      g.xi[i] = xi[i];
+      g.w[i] = w[i];
+    }
+    // D[i][l] = derivative of the l-th Lagrange polynomial at node i:
+    // off-diagonal (pi_i / pi_l) / (x_i - x_l) with pi_m = prod_{n!=m}
+    // (x_m - x_n); diagonal = sum_{n!=i} 1/(x_i - x_n).
+    double pi[5];
+    for (int m = 0; m < 5; ++m) {
+      pi[m] = 1.0;
+      for (int n = 0; n < 5; ++n)
+        if (n != m) pi[m] *= (xi[m] - xi[n]);
+    }
+    for (int i = 0; i < 5; ++i)
+      for (int l = 0; l < 5; ++l) {
+        if (i != l) {
+          g.D[i][l] = pi[i] / (pi[l] * (xi[i] - xi[l]));
+        } else {
+          double sum = 0.0;
+          for (int n = 0; n < 5; ++n)
+            if (n != i) sum += 1.0 / (xi[i] - xi[n]);
+          g.D[i][l] = sum;
+        }
+      }
+    return g;
+  }();
+  return t;
+}
+
+void lagrange_all(double x, double h[5], double hd[5]) {
+  const GllTables& g = gll();
+  for (int a = 0; a < 5; ++a) {
+    double p = 1.0;
+    for (int m = 0; m < 5; ++m)
+      if (m != a) p *= (x - g.xi[m]) / (g.xi[a] - g.xi[m]);
+    h[a] = p;
+    double s = 0.0;
+    for (int m = 0; m < 5; ++m) {
+      if (m == a) continue;
+      double prod = 1.0 / (g.xi[a] - g.xi[m]);
+      for (int n = 0; n < 5; ++n) {
+        if (n == a || n == m) continue;
+        prod *= (x - g.xi[n]) / (g.xi[a] - g.xi[n]);
+      }
+      s += prod;
+    }
+    hd[a] = s;
+  }
+}
+
+double ricker(double t, double f0) {
+  const double a = M_PI * M_PI * f0 * f0;
+  return (1.0 - 2.0 * a * t * t) * std::exp(-a * t * t);
+}
+
+template <typename T>
+struct DevArray {
+  T* p = nullptr;
+  size_t n = 0;
+  DevArray() = default;
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  ~DevArray() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    reset();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+int check_device() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SEM_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) return fail(SEM_ERR_NODEVICE, "%s", cudaGetErrorString(e));
+  if (prop.major != 10)
+    return fail(SEM_ERR_NODEVICE, "device %s is sm_%d%d; this library is built for sm_100a",
+                prop.name, prop.major, prop.minor);
+  return SEM_OK;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------
+// mesh
+// ----------------------------------------------------------------------------
+
+struct sem_mesh_s {
+  int nspec = 0, nglob = 0, nf = 0;
+  float xix = 0.f, jac = 0.f;
+  DevArray<int> ibool;
+  DevArray<float> kappa, mu, rho;
+  DevArray<int> f_iglob;
+  DevArray<float> f_rvp, f_rvs, f_jw, f_n;
+  // host copies used for set-up work
+  std::vector<int> h_ibool;
+  std::vector<float> h_rmass;
+  std::vector<int> h_f_iglob;
+  std::vector<float> h_f_rvp, h_f_rvs, h_f_jw, h_f_n;
+  std::vector<double> centre;  // [nspec][3]
+  std::vector<double> half;    // [nspec][3]
+  int live_runs = 0;
+
+  MeshView view() const {
+    MeshView v{};
+    v.nspec = nspec;
+    v.nglob = nglob;
+    v.nf = nf;
+    v.xix = xix;
+    v.jac = jac;
+    v.ibool = ibool.p;
+    v.kappa = kappa.p;
+    v.mu = mu.p;
+    v.f_iglob = f_iglob.p;
+    v.f_rvp = f_rvp.p;
+    v.f_rvs = f_rvs.p;
+    v.f_jw = f_jw.p;
+    v.f_n = f_n.p;
+    return v;
+  }
+  size_t device_bytes() const {
+    return ibool.bytes() + kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
+           f_rvp.bytes() + f_rvs.bytes() + f_jw.bytes() + f_n.bytes();
+  }
+
+  // Element whose centre is nearest to the point (ties: lowest index), and
+  // the reference coordinates inside it, clamped to [-1, 1].
+  int locate(double px, double py, double pz, double xi3[3]) const {
+    int best = -1;
+    double bd = 1e300;
+    for (int e = 0; e < nspec; ++e) {
+      const double* c = &centre[(size_t)e * 3];
+      const double d =
+          (px - c[0]) * (px - c[0]) + (py - c[1]) * (py - c[1]) + (pz - c[2]) * (pz - c[2]);
+      if (d < bd) {
+        bd = d;
+        best = e;
+      }
+    }
+    const double* c = &centre[(size_t)best * 3];
+    const double* h = &half[(size_t)best * 3];
+    const double p[3] = {px, py, pz};
+    for (int d = 0; d < 3; ++d) {
+      double v = (p[d] - c[d]) / h[d];
+      xi3[d] = v < -1.0 ? -1.0 : (v > 1.0 ? 1.0 : v);
+    }
+    return best;
+  }
+};
+
+// ----------------------------------------------------------------------------
+// run
+// ----------------------------------------------------------------------------
+
+struct sem_run_s {
+  sem_mesh_s* mesh = nullptr;
+  sem_run_cfg cfg{};
+  int nev = 1, nstep = 0, nrec_max = 1;
+  double dt = 0.0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  DevArray<float> minv;
+  DevArray<float> u1, v1, a1, u2, v2, a2;
+  DevArray<LaneDesc> lanes;
+  std::vector<LaneDesc> h_lanes;
+  DevArray<float> stf, srcarr, rec_w, seis, adj;
+  DevArray<int> rec_ispec;
+  DevArray<unsigned char> store;
+  DevArray<float> scale;
+  DevArray<float> k_rho, k_mu, k_kappa;
+  DevArray<double> kout, ksum;
+  DevArray<double> obs, taper, simpw, misfit_rc;
+  DevArray<int> flag;
+  std::vector<int> src_ispec, nrec;
+  std::vector<char> have_src, have_rec, have_adj;
+  bool fwd_saved = false, adj_done = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  double last_ms = 0.0;
+  long long last_launches = 0;
+
+  ~sem_run_s() {
+    for (auto& g : gexec)
+      if (g) cudaGraphExecDestroy(g);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (stream) cudaStreamDestroy(stream);
+    if (mesh) mesh->live_runs--;
+  }
+
+  size_t store_elem() const { return cfg.store_kind == SEM_STORE_FP16 ? 2 : 4; }
+  size_t store_bytes_per_event() const {
+    return (size_t)nstep * mesh->nf * 75 * store_elem();
+  }
+
+  StepArgs args(bool adjoint) const {
+    StepArgs a{};
+    a.m = mesh->view();
+    a.f1 = {u1.p, v1.p, a1.p};
+    a.f2 = adjoint ? Fields{u2.p, v2.p, a2.p} : Fields{nullptr, nullptr, nullptr};
+    a.k = {k_rho.p, k_mu.p, k_kappa.p};
+    a.lanes = lanes.p;
+    a.minv = minv.p;
+    a.nev = nev;
+    a.s = 0;
+    a.dt = (float)dt;
+    a.store_fp16 = cfg.store_kind == SEM_STORE_FP16;
+    a.nrec_max = nrec_max;
+    return a;
+  }
+
+  void fill_lanes(int phase, int save) {
+    h_lanes.assign(nev, LaneDesc{});
+    const size_t ns = (size_t)nstep;
+    for (int e = 0; e < nev; ++e) {
+      LaneDesc& L = h_lanes[e];
+      L.phase = phase;
+      L.it0 = 0;
+      L.nstep = nstep;
+      L.save = save;
+      L.src_ispec = src_ispec[e];
+      L.nrec = nrec[e];
+      L.stf = stf.p + (size_t)e * ns;
+      L.srcarr = srcarr.p + (size_t)e * 375;
+      L.rec_ispec = rec_ispec.p + (size_t)e * nrec_max;
+      L.rec_w = rec_w.p + (size_t)e * nrec_max * 125;
+      L.seis = seis.p + (size_t)e * nrec_max * 3 * ns;
+      L.adj = adj.p + (size_t)e * nrec_max * 3 * ns;
+      L.store = store.p ? store.p + (size_t)e * store_bytes_per_event() : nullptr;
+      L.scale = scale.p ? scale.p + (size_t)e * ns * mesh->nf : nullptr;
+    }
+  }
+};
+
+// ----------------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------------
+
+extern "C" {
+
+int sem_abi_version(void) { return SEM_ABI_VERSION; }
+
+const char* sem_last_error(void) { return g_err.c_str(); }
+
+int sem_device_info(int* sm_count, long long* hbm_bytes, int* cc_major, int* cc_minor) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SEM_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  cudaDeviceProp p;
+  CK(cudaGetDeviceProperties(&p, dev));
+  if (sm_count) *sm_count = p.multiProcessorCount;
+  if (hbm_bytes) *hbm_bytes = (long long)p.totalGlobalMem;
+  if (cc_major) *cc_major = p.major;
+  if (cc_minor) *cc_minor = p.minor;
+  return SEM_OK;
+}
+
+int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
+  if (!d || !out) return fail(SEM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->nspec <= 0 || d->nglob <= 0) return fail(SEM_ERR_ARG, "nspec and nglob must be > 0");
+  if (d->index_base != 0 && d->index_base != 1)
+    return fail(SEM_ERR_ARG, "index_base must be 0 or 1");
+  if (!d->ibool || !d->xstore || !d->ystore || !d->zstore || !d->kappastore || !d->mustore ||
+      !d->rhostore || !d->rmass || !d->rho_vp || !d->rho_vs)
+    return fail(SEM_ERR_ARG, "missing mesh array");
+  const int nf = d->num_abs_boundary_faces;
+  if (nf < 0) return fail(SEM_ERR_ARG, "num_abs_boundary_faces < 0");
+  if (nf > 0 && (!d->abs_boundary_ispec || !d->abs_boundary_ijk ||
+                 !d->abs_boundary_jacobian2Dw || !d->abs_boundary_normal))
+    return fail(SEM_ERR_ARG, "missing absorbing-boundary array");
+  if (!(d->xix_regular > 0.f) || !(d->jacobian_regular > 0.f))
+    return fail(SEM_ERR_ARG, "xix_regular and jacobian_regular must be > 0");
+  if (d->irregular_element_number)
+    for (int e = 0; e < d->nspec; ++e)
+      if (d->irregular_element_number[e] > 0)
+        return fail(SEM_ERR_UNSUPPORTED,
+                    "element %d is irregular; this build implements regular elements only", e);
+  int rc = check_device();
+  if (rc) return rc;
+
+  auto m = new sem_mesh_s();
+  std::unique_ptr<sem_mesh_s> guard(m);
+  m->nspec = d->nspec;
+  m->nglob = d->nglob;
+  m->nf = nf;
+  m->xix = d->xix_regular;
+  m->jac = d->jacobian_regular;
+  const size_t ne = (size_t)d->nspec * NGLL3;
+  m->h_ibool.resize(ne);
+  for (size_t i = 0; i < ne; ++i) {
+    const int g = d->ibool[i] - d->index_base;
+    if (g < 0 || g >= d->nglob)
+      return fail(SEM_ERR_ARG, "ibool[%zu] = %d outside [0, nglob)", i, d->ibool[i]);
+    m->h_ibool[i] = g;
+  }
+  for (size_t i = 0; i < ne; ++i) {
+    const float k = d->kappastore[i], mu = d->mustore[i], r = d->rhostore[i];
+    if (!std::isfinite(k) || !std::isfinite(mu) || !std::isfinite(r) || !(r > 0.f) ||
+        mu < 0.f || !(k > 0.f))
+      return fail(SEM_ERR_ARG, "invalid material at element point %zu", i);
+  }
+  m->h_rmass.assign(d->rmass, d->rmass + d->nglob);
+  for (int g = 0; g < d->nglob; ++g)
+    if (!(m->h_rmass[g] > 0.f) || !std::isfinite(m->h_rmass[g]))
+      return fail(SEM_ERR_ARG, "mass matrix is not positive at point %d", g);
+  // element centres and half widths for locating points
+  m->centre.resize((size_t)d->nspec * 3);
+  m->half.resize((size_t)d->nspec * 3);
+  for (int e = 0; e < d->nspec; ++e) {
+    const int g0 = m->h_ibool[(size_t)e * NGLL3 + 0];
+    const int g7 = m->h_ibool[(size_t)e * NGLL3 + 124];
+    const float* c[3] = {d->xstore, d->ystore, d->zstore};
+    for (int k = 0; k < 3; ++k) {
+      m->centre[(size_t)e * 3 + k] = 0.5 * ((double)c[k][g0] + (double)c[k][g7]);
+      m->half[(size_t)e * 3 + k] = 0.5 * ((double)c[k][g7] - (double)c[k][g0]);
+      if (!(m->half[(size_t)e * 3 + k] > 0.0))
+        return fail(SEM_ERR_ARG, "element %d has non-positive extent along axis %d", e, k);
+    }
+  }
+  // absorbing faces: per face point global index and coefficients
+  m->h_f_iglob.resize((size_t)nf * NGLL2);
+  m->h_f_rvp.resize((size_t)nf * NGLL2);
+  m->h_f_rvs.resize((size_t)nf * NGLL2);
+  m->h_f_jw.resize((size_t)nf * NGLL2);
+  m->h_f_n.resize((size_t)nf * NGLL2 * 3);
+  for (int f = 0; f < nf; ++f) {
+    const int e = d->abs_boundary_ispec[f] - d->index_base;
+    if (e < 0 || e >= d->nspec) return fail(SEM_ERR_ARG, "abs_boundary_ispec[%d] out of range", f);
+    for (int p = 0; p < NGLL2; ++p) {
+      const size_t fp = (size_t)f * NGLL2 + p;
+      int ijk[3];
+      for (int k = 0; k < 3; ++k) {
+        ijk[k] = d->abs_boundary_ijk[fp * 3 + k] - d->index_base;
+        if (ijk[k] < 0 || ijk[k] >= NGLL)
+          return fail(SEM_ERR_ARG, "abs_boundary_ijk of face %d point %d out of range", f, p);
+      }
+      const size_t lp = (size_t)e * NGLL3 + ijk[0] + NGLL * ijk[1] + NGLL2 * ijk[2];
+      m->h_f_iglob[fp] = m->h_ibool[lp];
+      m->h_f_rvp[fp] = d->rho_vp[lp];
+      m->h_f_rvs[fp] = d->rho_vs[lp];
+      m->h_f_jw[fp] = d->abs_boundary_jacobian2Dw[fp];
+      for (int k = 0; k < 3; ++k) m->h_f_n[fp * 3 + k] = d->abs_boundary_normal[fp * 3 + k];
+    }
+  }
+  CKM(m->ibool.alloc(ne), "ibool");
+  CKM(m->kappa.alloc(ne), "kappastore");
+  CKM(m->mu.alloc(ne), "mustore");
+  CKM(m->rho.alloc(ne), "rhostore");
+  CKM(m->f_iglob.alloc((size_t)nf * NGLL2), "face index");
+  CKM(m->f_rvp.alloc((size_t)nf * NGLL2), "face rho_vp");
+  CKM(m->f_rvs.alloc((size_t)nf * NGLL2), "face rho_vs");
+  CKM(m->f_jw.alloc((size_t)nf * NGLL2), "face jacobian2Dw");
+  CKM(m->f_n.alloc((size_t)nf * NGLL2 * 3), "face normal");
+  CK(cudaMemcpy(m->ibool.p, m->h_ibool.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m->kappa.p, d->kappastore, ne * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m->mu.p, d->mustore, ne * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m->rho.p, d->rhostore, ne * sizeof(float), cudaMemcpyHostToDevice));
+  if (nf > 0) {
+    CK(cudaMemcpy(m->f_iglob.p, m->h_f_iglob.data(), m->f_iglob.bytes(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->f_rvp.p, m->h_f_rvp.data(), m->f_rvp.bytes(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->f_rvs.p, m->h_f_rvs.data(), m->f_rvs.bytes(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->f_jw.p, m->h_f_jw.data(), m->f_jw.bytes(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->f_n.p, m->h_f_n.data(), m->f_n.bytes(), cudaMemcpyHostToDevice));
+  }
+  // GLL derivative tables for the element kernel
+  const GllTables& g = gll();
+  float D[25], DWt[25], w[5];
+  for (int i = 0; i < 5; ++i) {
+    w[i] = (float)g.w[i];
+    for (int l = 0; l < 5; ++l) {
+      D[i * 5 + l] = (float)g.D[i][l];
+      DWt[i * 5 + l] = (float)(g.w[l] * g.D[l][i]);
+    }
+  }
+  set_gll_constants(D, DWt, w);
+  CK(cudaGetLastError());
+  *out = guard.release();
+  return SEM_OK;
+}
+
+int sem_release_mesh(sem_mesh* m) {
+  if (!m) return fail(SEM_ERR_ARG, "null mesh");
+  if (m->live_runs > 0) return fail(SEM_ERR_STATE, "mesh still has %d live runs", m->live_runs);
+  delete m;
+  return SEM_OK;
+}
+
+int sem_mesh_info(const sem_mesh* m, int* nspec, int* nglob, int* nfaces,
+                  long long* device_bytes) {
+  if (!m) return fail(SEM_ERR_ARG, "null mesh");
+  if (nspec) *nspec = m->nspec;
+  if (nglob) *nglob = m->nglob;
+  if (nfaces) *nfaces = m->nf;
+  if (device_bytes) *device_bytes = (long long)m->device_bytes();
+  return SEM_OK;
+}
+
+static int validate_cfg(const sem_run_cfg* c) {
+  if (!c) return fail(SEM_ERR_ARG, "null cfg");
+  if (c->nev < 1 || c->nev > 4096) return fail(SEM_ERR_ARG, "nev must be in [1, 4096]");
+  if (c->nstep < 1) return fail(SEM_ERR_ARG, "nstep must be >= 1");
+  if (!(c->dt > 0.0) || !std::isfinite(c->dt)) return fail(SEM_ERR_ARG, "dt must be > 0");
+  if (c->store_kind != SEM_STORE_FP32 && c->store_kind != SEM_STORE_FP16)
+    return fail(SEM_ERR_ARG, "unknown store_kind %d", c->store_kind);
+  if (c->max_receivers < 1 || c->max_receivers > 100000)
+    return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
+  if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
+  return SEM_OK;
+}
+
+long long sem_run_bytes(const sem_mesh* m, const sem_run_cfg* c) {
+  if (!m || validate_cfg(c)) return -1;
+  const size_t ng = m->nglob, ne = (size_t)m->nspec * NGLL3, nev = c->nev, ns = c->nstep;
+  const size_t nr = c->max_receivers;
+  size_t b = ng * 3 * 4;                         // minv
+  b += 6 * ng * 3 * nev * 4;                     // two fields
+  b += nev * (ns + 375) * 4;                     // stf + source arrays
+  b += nev * nr * (4 + 125 * 4);                 // receivers
+  b += 2 * nev * nr * 3 * ns * 4;                // seismograms + adjoint sources
+  b += nev * ns * (size_t)m->nf * 75 * (c->store_kind == SEM_STORE_FP16 ? 2 : 4);
+  if (c->store_kind == SEM_STORE_FP16) b += nev * ns * (size_t)m->nf * 4;
+  b += (ng + 2 * ne) * nev * 4;                  // kernel accumulators
+  b += 2 * 6 * ne * 8;                           // kernel output + sum
+  b += nr * 3 * ns * 8 + 2 * ns * 8 + nr * 3 * 8;  // measurement
+  return (long long)b;
+}
+
+int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
+  if (!m || !out) return fail(SEM_ERR_ARG, "null argument");
+  *out = nullptr;
+  int rc = validate_cfg(c);
+  if (rc) return rc;
+  auto r = new sem_run_s();
+  std::unique_ptr<sem_run_s> guard(r);
+  r->mesh = m;
+  m->live_runs++;
+  r->cfg = *c;
+  if (r->cfg.graph_steps == 0) r->cfg.graph_steps = 50;
+  r->nev = c->nev;
+  r->nstep = c->nstep;
+  r->dt = c->dt;
+  r->nrec_max = c->max_receivers;
+  CK(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&r->e0));
+  CK(cudaEventCreate(&r->e1));
+
+  // 1/(M + dt/2 C): Stacey's diagonal damping folded into the mass so the
+  // absorbing term is implicit in the corrector velocity.
+  const size_t ng = m->nglob;
+  std::vector<double> mx(ng * 3);
+  for (size_t g = 0; g < ng; ++g)
+    for (int k = 0; k < 3; ++k) mx[g * 3 + k] = (double)m->h_rmass[g];
+  for (int f = 0; f < m->nf; ++f)
+    for (int p = 0; p < NGLL2; ++p) {
+      const size_t fp = (size_t)f * NGLL2 + p;
+      const size_t g = (size_t)m->h_f_iglob[fp];
+      const double rvp = m->h_f_rvp[fp], rvs = m->h_f_rvs[fp], jw = m->h_f_jw[fp];
+      for (int k = 0; k < 3; ++k) {
+        const double n = m->h_f_n[fp * 3 + k];
+        mx[g * 3 + k] += 0.5 * c->dt * jw * (rvp * n * n + rvs * (1.0 - n * n));
+      }
+    }
+  std::vector<float> mi(ng * 3);
+  for (size_t i = 0; i < mi.size(); ++i) mi[i] = (float)(1.0 / mx[i]);
+  CKM(r->minv.alloc(ng * 3), "inverse mass");
+  CK(cudaMemcpy(r->minv.p, mi.data(), r->minv.bytes(), cudaMemcpyHostToDevice));
+
+  const size_t nev = r->nev, ns = r->nstep, nr = r->nrec_max, ne = (size_t)m->nspec * NGLL3;
+  const size_t nf3 = ng * 3 * nev;
+  CKM(r->u1.alloc(nf3), "displ");
+  CKM(r->v1.alloc(nf3), "veloc");
+  CKM(r->a1.alloc(nf3), "accel");
+  CKM(r->lanes.alloc(nev), "lane table");
+  CKM(r->stf.alloc(nev * ns), "source time functions");
+  CKM(r->srcarr.alloc(nev * 375), "source arrays");
+  CKM(r->rec_ispec.alloc(nev * nr), "receiver elements");
+  CKM(r->rec_w.alloc(nev * nr * 125), "receiver weights");
+  CKM(r->seis.alloc(nev * nr * 3 * ns), "seismograms");
+  CKM(r->adj.alloc(nev * nr * 3 * ns), "adjoint sources");
+  CK(cudaMemsetAsync(r->seis.p, 0, r->seis.bytes(), r->stream));
+  CK(cudaMemsetAsync(r->adj.p, 0, r->adj.bytes(), r->stream));
+  CKM(r->flag.alloc(1), "flag");
+  (void)ne;
+  r->src_ispec.assign(nev, -1);
+  r->nrec.assign(nev, 0);
+  r->have_src.assign(nev, 0);
+  r->have_rec.assign(nev, 0);
+  r->have_adj.assign(nev, 0);
+  CK(cudaStreamSynchronize(r->stream));
+  *out = guard.release();
+  return SEM_OK;
+}
+
+int sem_release_run(sem_run* r) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  cudaStreamSynchronize(r->stream);
+  delete r;
+  return SEM_OK;
+}
+
+int sem_set_sources(sem_run* r, int nev, const sem_source* src) {
+  if (!r || !src) return fail(SEM_ERR_ARG, "null argument");
+  if (nev != r->nev) return fail(SEM_ERR_ARG, "nev %d != run nev %d", nev, r->nev);
+  const size_t ns = r->nstep;
+  std::vector<float> stf((size_t)nev * ns), sa((size_t)nev * 375);
+  for (int e = 0; e < nev; ++e) {
+    const sem_source& s = src[e];
+    if (!(s.f0 > 0.0) || !std::isfinite(s.x + s.y + s.z))
+      return fail(SEM_ERR_ARG, "source %d: invalid position or f0", e);
+    double xi3[3];
+    const int ispec = r->mesh->locate(s.x, s.y, s.z, xi3);
+    r->src_ispec[e] = ispec;
+    // CMT (r, theta, phi) -> x=E, y=N, z=Up (locate_source_fwat.f90:215-228)
+    const double Mzz = s.Mrr, Myy = s.Mtt, Mxx = s.Mpp;
+    const double Myz = -s.Mrt, Mxz = s.Mrp, Mxy = -s.Mtp;
+    const double M[3][3] = {{Mxx, Mxy, Mxz}, {Mxy, Myy, Myz}, {Mxz, Myz, Mzz}};
+    double hx[5], hxd[5], hy[5], hyd[5], hz[5], hzd[5];
+    lagrange_all(xi3[0], hx, hxd);
+    lagrange_all(xi3[1], hy, hyd);
+    lagrange_all(xi3[2], hz, hzd);
+    const double xix = (double)r->mesh->xix;
+    for (int c = 0; c < 5; ++c)
+      for (int b = 0; b < 5; ++b)
+        for (int a = 0; a < 5; ++a) {
+          const double gr[3] = {xix * hxd[a] * hy[b] * hz[c], xix * hx[a] * hyd[b] * hz[c],
+                                xix * hx[a] * hy[b] * hzd[c]};
+          const int p = a + 5 * b + 25 * c;
+          for (int k = 0; k < 3; ++k)
+            sa[(size_t)e * 375 + p * 3 + k] =
+                (float)(M[k][0] * gr[0] + M[k][1] * gr[1] + M[k][2] * gr[2]);
+        }
+    const double t0 = 1.2 / s.f0 + s.tshift;
+    for (size_t it = 0; it < ns; ++it)
+      stf[(size_t)e * ns + it] = (float)ricker((double)it * r->dt - t0, s.f0);
+    r->have_src[e] = 1;
+  }
+  CK(cudaMemcpyAsync(r->stf.p, stf.data(), r->stf.bytes(), cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->srcarr.p, sa.data(), r->srcarr.bytes(), cudaMemcpyHostToDevice,
+                     r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_set_receivers(sem_run* r, int ev, int nrec, const double* xyz) {
+  if (!r || (!xyz && nrec > 0)) return fail(SEM_ERR_ARG, "null argument");
+  if (nrec < 0 || nrec > r->nrec_max)
+    return fail(SEM_ERR_ARG, "nrec %d outside [0, max_receivers=%d]", nrec, r->nrec_max);
+  if (ev < -1 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  std::vector<int> isp(r->nrec_max, 0);
+  std::vector<float> w((size_t)r->nrec_max * 125, 0.f);
+  for (int k = 0; k < nrec; ++k) {
+    if (!std::isfinite(xyz[k * 3] + xyz[k * 3 + 1] + xyz[k * 3 + 2]))
+      return fail(SEM_ERR_ARG, "receiver %d position is not finite", k);
+    double xi3[3];
+    isp[k] = r->mesh->locate(xyz[k * 3], xyz[k * 3 + 1], xyz[k * 3 + 2], xi3);
+    double hx[5], hy[5], hz[5], d[5];
+    lagrange_all(xi3[0], hx, d);
+    lagrange_all(xi3[1], hy, d);
+    lagrange_all(xi3[2], hz, d);
+    for (int c = 0; c < 5; ++c)
+      for (int b = 0; b < 5; ++b)
+        for (int a = 0; a < 5; ++a)
+          w[(size_t)k * 125 + a + 5 * b + 25 * c] = (float)(hx[a] * hy[b] * hz[c]);
+  }
+  const int e0 = ev < 0 ? 0 : ev, e1 = ev < 0 ? r->nev : ev + 1;
+  for (int e = e0; e < e1; ++e) {
+    CK(cudaMemcpyAsync(r->rec_ispec.p + (size_t)e * r->nrec_max, isp.data(),
+                       isp.size() * sizeof(int), cudaMemcpyHostToDevice, r->stream));
+    CK(cudaMemcpyAsync(r->rec_w.p + (size_t)e * r->nrec_max * 125, w.data(),
+                       w.size() * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    r->nrec[e] = nrec;
+    r->have_rec[e] = 1;
+  }
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+static int ensure_adjoint_buffers(sem_run* r) {
+  const size_t ng = r->mesh->nglob, nev = r->nev, ne = (size_t)r->mesh->nspec * NGLL3;
+  if (!r->u2.p) {
+    CKM(r->u2.alloc(ng * 3 * nev), "backward displ");
+    CKM(r->v2.alloc(ng * 3 * nev), "backward veloc");
+    CKM(r->a2.alloc(ng * 3 * nev), "backward accel");
+  }
+  if (!r->k_rho.p) {
+    CKM(r->k_rho.alloc(ng * nev), "rho kernel");
+    CKM(r->k_mu.alloc(ne * nev), "mu kernel");
+    CKM(r->k_kappa.alloc(ne * nev), "kappa kernel");
+  }
+  return SEM_OK;
+}
+
+static int ensure_store(sem_run* r) {
+  if (r->mesh->nf == 0 || r->store.p) return SEM_OK;
+  CKM(r->store.alloc(r->store_bytes_per_event() * r->nev), "boundary store");
+  if (r->cfg.store_kind == SEM_STORE_FP16)
+    CKM(r->scale.alloc((size_t)r->nev * r->nstep * r->mesh->nf), "boundary store scales");
+  return SEM_OK;
+}
+
+// Queue the step loop of one phase (graphs or per-step launches).
+static int run_loop(sem_run* r, bool adjoint) {
+  long long launches = 0;
+  StepArgs a = r->args(adjoint);
+  CK(cudaEventRecord(r->e0, r->stream));
+  if (r->cfg.use_graph) {
+    const int K = r->cfg.graph_steps;
+    cudaGraphExec_t& gx = r->gexec[adjoint ? 1 : 0];
+    if (!gx) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
+      for (int s = 0; s < K; ++s) {
+        a.s = s;
+        launch_forces(a, adjoint, r->stream);
+        launch_boundary(a, adjoint, r->stream);
+        launch_points(a, r->stream);
+        launch_update(a, adjoint, r->stream);
+      }
+      launch_advance(r->lanes.p, r->nev, K, r->stream);
+      cudaError_t ce = cudaStreamEndCapture(r->stream, &g);
+      if (ce != cudaSuccess) return fail(SEM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&gx, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess)
+        return fail(SEM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+    }
+    const int nlaunch = (r->nstep + K - 1) / K;
+    const int per_step = (r->mesh->nf > 0 ? 4 : 3);
+    for (int g = 0; g < nlaunch; ++g) {
+      CK(cudaGraphLaunch(gx, r->stream));
+      launches += (long long)K * per_step + 1;
+    }
+  } else {
+    for (int s = 0; s < r->nstep; ++s) {
+      a.s = s;
+      launches += launch_forces(a, adjoint, r->stream);
+      launches += launch_boundary(a, adjoint, r->stream);
+      launches += launch_points(a, r->stream);
+      launches += launch_update(a, adjoint, r->stream);
+    }
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(r->e1, r->stream));
+  r->last_launches = launches;
+  return SEM_OK;
+}
+
+int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nev;
+  if (sim_type == 1) {
+    for (int e = 0; e < r->nev; ++e)
+      if (!r->have_src[e] || !r->have_rec[e])
+        return fail(SEM_ERR_STATE, "event %d has no source or receivers", e);
+    if (save_forward) {
+      int rc = ensure_store(r);
+      if (rc) return rc;
+    }
+    CK(cudaMemsetAsync(r->u1.p, 0, n3 * 4, r->stream));
+    CK(cudaMemsetAsync(r->v1.p, 0, n3 * 4, r->stream));
+    CK(cudaMemsetAsync(r->a1.p, 0, n3 * 4, r->stream));
+    r->fill_lanes(PH_FWD, save_forward ? 1 : 0);
+    CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
+                       r->stream));
+    int rc = run_loop(r, false);
+    if (rc) return rc;
+    r->fwd_saved = save_forward != 0;
+    r->adj_done = false;
+  } else if (sim_type == 3) {
+    if (!r->fwd_saved)
+      return fail(SEM_ERR_STATE, "sim_type 3 needs a previous sim_type 1 with save_forward");
+    for (int e = 0; e < r->nev; ++e)
+      if (!r->have_adj[e]) return fail(SEM_ERR_STATE, "event %d has no adjoint sources", e);
+    int rc = ensure_adjoint_buffers(r);
+    if (rc) return rc;
+    // backward field starts from the final forward state; adjoint at rest
+    CK(cudaMemcpyAsync(r->u2.p, r->u1.p, n3 * 4, cudaMemcpyDeviceToDevice, r->stream));
+    CK(cudaMemcpyAsync(r->v2.p, r->v1.p, n3 * 4, cudaMemcpyDeviceToDevice, r->stream));
+    CK(cudaMemcpyAsync(r->a2.p, r->a1.p, n3 * 4, cudaMemcpyDeviceToDevice, r->stream));
+    CK(cudaMemsetAsync(r->u1.p, 0, n3 * 4, r->stream));
+    CK(cudaMemsetAsync(r->v1.p, 0, n3 * 4, r->stream));
+    CK(cudaMemsetAsync(r->a1.p, 0, n3 * 4, r->stream));
+    CK(cudaMemsetAsync(r->k_rho.p, 0, r->k_rho.bytes(), r->stream));
+    CK(cudaMemsetAsync(r->k_mu.p, 0, r->k_mu.bytes(), r->stream));
+    CK(cudaMemsetAsync(r->k_kappa.p, 0, r->k_kappa.bytes(), r->stream));
+    r->fill_lanes(PH_ADJ, 0);
+    CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
+                       r->stream));
+    rc = run_loop(r, true);
+    if (rc) return rc;
+    r->fwd_saved = false;  // the final state has been consumed
+    r->adj_done = true;
+  } else {
+    return fail(SEM_ERR_ARG, "sim_type must be 1 or 3");
+  }
+  if (r->cfg.check_every > 0) {
+    CK(cudaMemsetAsync(r->flag.p, 0, sizeof(int), r->stream));
+    launch_nonfinite(r->u1.p, n3, r->flag.p, r->stream);
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, r->flag.p, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    if (h) return fail(SEM_ERR_NUMERIC, "non-finite wavefield after sim_type %d", sim_type);
+  }
+  return SEM_OK;
+}
+
+int sem_synchronize(sem_run* r) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  CK(cudaStreamSynchronize(r->stream));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, r->e0, r->e1) == cudaSuccess) r->last_ms = ms;
+  cudaGetLastError();
+  return SEM_OK;
+}
+
+int sem_get_seismograms(sem_run* r, int ev, float* out) {
+  if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  const size_t n = (size_t)r->nrec[ev] * 3 * r->nstep;
+  CK(cudaMemcpyAsync(out, r->seis.p + (size_t)ev * r->nrec_max * 3 * r->nstep, n * 4,
+                     cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_set_adjoint_sources(sem_run* r, int ev, const double* adj) {
+  if (!r || !adj) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  const size_t n = (size_t)r->nrec[ev] * 3 * r->nstep;
+  std::vector<float> f(n);
+  for (size_t i = 0; i < n; ++i) f[i] = (float)adj[i];
+  CK(cudaMemcpyAsync(r->adj.p + (size_t)ev * r->nrec_max * 3 * r->nstep, f.data(), n * 4,
+                     cudaMemcpyHostToDevice, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  r->have_adj[ev] = 1;
+  return SEM_OK;
+}
+
+int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int taper_type,
+                   double* misfit) {
+  if (!r || !obs) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  if (taper_pct < 0.0 || taper_pct > 1.0)
+    return fail(SEM_ERR_ARG, "taper_percentage must be in [0, 1]");
+  if (taper_type < 1 || taper_type > 4) return fail(SEM_ERR_ARG, "taper type must be 1..4");
+  const int ns = r->nstep, nr = r->nrec[ev];
+  if (nr == 0) return fail(SEM_ERR_STATE, "event %d has no receivers", ev);
+  // taper weights (src/shared/signal.f90:419-491)
+  std::vector<double> w(ns, 1.0);
+  const int frac = (taper_pct == 0.0 || taper_pct == 1.0) ? (int)(ns * taper_pct / 2.0)
+                                                          : (int)(ns * taper_pct / 2.0 + 0.5);
+  if (frac > 0) {
+    const double den = 2.0 * frac - 1.0;
+    auto tw = [&](double x) {
+      switch (taper_type) {
+        case 1: return 0.5 - 0.5 * std::cos(2.0 * M_PI * x / den);
+        case 2: return 0.54 - 0.46 * std::cos(2.0 * M_PI * x / den);
+        case 3: return std::cos(M_PI * x / den - M_PI / 2.0);
+        default: return 1.0 - std::pow(std::cos(M_PI * x / den), 10.0);
+      }
+    };
+    for (int i = 0; i < frac; ++i) {
+      w[i] *= tw(i);
+      w[ns - frac + i] *= tw(frac + i);
+    }
+  }
+  // Simpson weights of src/shared/utils.f90:1635-1663 (as written there)
+  std::vector<double> sw(ns, 0.0);
+  const double dx = r->dt;
+  if (ns >= 2) {
+    if (ns % 2 == 0) {
+      sw[0] += dx / 3.0;
+      sw[ns - 2] += dx / 3.0;
+      for (int i = 2; i <= ns - 2; i += 2) {  // 1-based loop index
+        sw[i - 1] += 4.0 * dx / 3.0;
+        sw[i] += 2.0 * dx / 3.0;
+      }
+      sw[ns - 2] += 0.5 * dx;
+      sw[ns - 1] += 0.5 * dx;
+    } else {
+      sw[0] += dx / 3.0;
+      sw[ns - 1] += dx / 3.0;
+      for (int i = 2; i <= ns - 1; i += 2) sw[i - 1] += 4.0 * dx / 3.0;
+      for (int i = 3; i <= ns - 2; i += 2) sw[i - 1] += 2.0 * dx / 3.0;
+    }
+  }
+  const size_t nobs = (size_t)nr * 3 * ns;
+  if (r->obs.n < (size_t)r->nrec_max * 3 * ns) {
+    CKM(r->obs.alloc((size_t)r->nrec_max * 3 * ns), "observed data");
+    CKM(r->taper.alloc(ns), "taper");
+    CKM(r->simpw.alloc(ns), "simpson weights");
+    CKM(r->misfit_rc.alloc((size_t)r->nrec_max * 3), "misfits");
+  }
+  CK(cudaMemcpyAsync(r->obs.p, obs, nobs * 8, cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->taper.p, w.data(), ns * 8, cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->simpw.p, sw.data(), ns * 8, cudaMemcpyHostToDevice, r->stream));
+  const size_t off = (size_t)ev * r->nrec_max * 3 * ns;
+  launch_measure_l2(r->seis.p + off, r->obs.p, r->taper.p, r->simpw.p, nr, ns, r->adj.p + off,
+                    r->misfit_rc.p, r->stream);
+  CK(cudaGetLastError());
+  std::vector<double> m((size_t)nr * 3);
+  CK(cudaMemcpyAsync(m.data(), r->misfit_rc.p, m.size() * 8, cudaMemcpyDeviceToHost,
+                     r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  double total = 0.0;
+  for (double v : m) total += v;
+  if (misfit) *misfit = total;
+  r->have_adj[ev] = 1;
+  return SEM_OK;
+}
+
+int sem_save_adjoint_kernels(sem_run* r, int ev, double* out) {
+  if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  if (!r->adj_done) return fail(SEM_ERR_STATE, "no adjoint run has completed");
+  const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+  if (!r->kout.p) CKM(r->kout.alloc(6 * ne), "kernel output");
+  launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p, {r->k_rho.p, r->k_mu.p, r->k_kappa.p},
+                          r->nev, ev, r->kout.p, nullptr, r->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, r->kout.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_sum_kernels(sem_run* r, double* out) {
+  if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (!r->adj_done) return fail(SEM_ERR_STATE, "no adjoint run has completed");
+  const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+  if (!r->ksum.p) CKM(r->ksum.alloc(6 * ne), "kernel sum");
+  CK(cudaMemsetAsync(r->ksum.p, 0, r->ksum.bytes(), r->stream));
+  for (int e = 0; e < r->nev; ++e)
+    launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p,
+                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->nev, e, nullptr,
+                            r->ksum.p, r->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, r->ksum.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_last_loop_ms(sem_run* r, double* ms) {
+  if (!r || !ms) return fail(SEM_ERR_ARG, "null argument");
+  CK(cudaStreamSynchronize(r->stream));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, r->e0, r->e1));
+  *ms = f;
+  return SEM_OK;
+}
+
+int sem_last_launch_count(sem_run* r, long long* count) {
+  if (!r || !count) return fail(SEM_ERR_ARG, "null argument");
+  *count = r->last_launches;
+  return SEM_OK;
+}
+
+}  // extern "C"

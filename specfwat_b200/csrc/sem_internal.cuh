@@ -1,0 +1,102 @@
+// Internal types shared by the CUDA kernels and the host engine.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace sem {
+
+constexpr int NGLL = 5;
+constexpr int NGLL2 = 25;
+constexpr int NGLL3 = 125;
+
+// Phase of an event lane.  A lane is one event's wavefield column in the
+// lane-interleaved layout [point][component][lane].
+enum Phase : int { PH_IDLE = 0, PH_FWD = 1, PH_ADJ = 3 };
+
+// Per-lane state read by every kernel of a step.  `it0` is the step index
+// at graph step s = 0; the kernel's step is it0 + s.  In the adjoint phase
+// the step index is the adjoint iteration j (adjoint source sample
+// nstep-1-j, backward state nstep-1-j).
+struct LaneDesc {
+  int phase;
+  int it0;
+  int nstep;
+  int save;          // forward phase: write the boundary store
+  int src_ispec;
+  int nrec;
+  int pad0, pad1;
+  const float* stf;      // [nstep]      source time function samples
+  const float* srcarr;   // [125][3]     moment tensor : grad(phi_abc)
+  const int* rec_ispec;  // [nrec]
+  const float* rec_w;    // [nrec][125]  Lagrange interpolation weights
+  float* seis;           // [nrec][3][nstep]
+  const float* adj;      // [nrec][3][nstep] adjoint sources, forward time
+  void* store;           // [nstep][nf][25][3] float or half
+  float* scale;          // [nstep][nf] per-face FP16 scale
+};
+
+struct MeshView {
+  int nspec, nglob, nf;
+  float xix, jac;
+  const int* ibool;      // [nspec*125]
+  const float* kappa;    // [nspec*125]
+  const float* mu;       // [nspec*125]
+  const int* f_iglob;    // [nf*25]
+  const float* f_rvp;    // [nf*25] rho*vp at the face point
+  const float* f_rvs;    // [nf*25] rho*vs
+  const float* f_jw;     // [nf*25] jacobian2D * weights
+  const float* f_n;      // [nf*25*3]
+};
+
+struct Fields {
+  float* u;
+  float* v;
+  float* a;
+};
+
+struct KernAcc {
+  float* rho_glob;   // [nglob][nev]
+  float* mu;         // [nspec*125][nev]
+  float* kappa;      // [nspec*125][nev]
+};
+
+struct StepArgs {
+  MeshView m;
+  Fields f1;             // forward field, or adjoint field in PH_ADJ
+  Fields f2;             // backward (reconstructed) field, PH_ADJ only
+  KernAcc k;
+  const LaneDesc* lanes; // [nev]
+  const float* minv;     // [nglob*3] 1/(M + dt/2 C)
+  int nev;
+  int s;                 // graph step
+  float dt;
+  int store_fp16;
+  int nrec_max;
+};
+
+// Launch helpers (defined in sem_kernels.cu).  Each returns the number of
+// kernels launched.
+int launch_forces(const StepArgs& a, bool adj, cudaStream_t st);
+int launch_boundary(const StepArgs& a, bool adj, cudaStream_t st);
+int launch_update(const StepArgs& a, bool adj, cudaStream_t st);
+int launch_points(const StepArgs& a, cudaStream_t st);
+int launch_advance(LaneDesc* lanes, int nev, int k, cudaStream_t st);
+int launch_finalize_kernels(const MeshView& m, const float* rho,
+                            const KernAcc& k, int nev, int lane,
+                            double* out6, double* sum6, cudaStream_t st);
+int launch_measure_l2(const float* seis, const double* obs, const double* taper,
+                      const double* simpw, int nrec, int nstep, float* adj_out,
+                      double* misfit_rc, cudaStream_t st);
+int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, int nev,
+                     int lane, cudaStream_t st);
+int launch_lane_zero(const Fields& f, int nglob, int nev, int lane,
+                     cudaStream_t st);
+int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st);
+
+void set_gll_constants(const float* D, const float* DWt, const float* w);
+
+}  // namespace sem

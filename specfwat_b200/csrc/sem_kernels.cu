@@ -1,0 +1,681 @@
+// CUDA kernels of the elastic SEM time loop (sm_100a).
+//
+// Wavefields use the lane-interleaved layout [point][component][lane]: a
+// lane is one event.  With one event (the plain path) this is the usual
+// point-major xyz layout of the reference's displ(3,NGLOB); with many events
+// consecutive lanes of one point/component are contiguous, so a warp's
+// gather and scatter-add of one point touch whole 32-byte sectors and the
+// element data (ibool, kappa, mu) is read once for all lanes of a block.
+//
+// One step = k_forces (element stiffness + assembly, strain products for
+// the kernels), k_stacey (absorbing traction / boundary store save and
+// replay), k_points (moment-tensor source, receivers, adjoint sources) and
+// k_update (Newmark corrector of this step fused with the predictor of the
+// next, plus the density-kernel product).
+
+#include <cstdio>
+
+#include "sem_internal.cuh"
+
+namespace sem {
+
+__constant__ float c_D[25];    // D[i][l] = l_l'(xi_i), index i*5+l
+__constant__ float c_DWt[25];  // DWt[i][l] = w_l * D[l][i], index i*5+l
+__constant__ float c_w[5];
+
+void set_gll_constants(const float* D, const float* DWt, const float* w) {
+  cudaMemcpyToSymbol(c_D, D, 25 * sizeof(float));
+  cudaMemcpyToSymbol(c_DWt, DWt, 25 * sizeof(float));
+  cudaMemcpyToSymbol(c_w, w, 5 * sizeof(float));
+}
+
+// ---------------------------------------------------------------------------
+// element kernel
+// ---------------------------------------------------------------------------
+
+// Displacement gradient at GLL point (i,j,k) of one lane.  b holds the
+// element's displacement as [c][125][LB]; g[c][d] = d u_c / d x_d.
+template <int LB>
+__device__ __forceinline__ void grad_point(const float* __restrict__ b, int i, int j, int k,
+                                           int lane, const float* __restrict__ sD, float xix,
+                                           float g[3][3]) {
+  float di[5], dj[5], dk[5];
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    di[l] = sD[i * 5 + l];
+    dj[l] = sD[j * 5 + l];
+    dk[l] = sD[k * 5 + l];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float* bc = b + c * NGLL3 * LB;
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      s1 = fmaf(di[l], bc[(l + 5 * j + 25 * k) * LB + lane], s1);
+      s2 = fmaf(dj[l], bc[(i + 5 * l + 25 * k) * LB + lane], s2);
+      s3 = fmaf(dk[l], bc[(i + 5 * j + 25 * l) * LB + lane], s3);
+    }
+    g[c][0] = xix * s1;
+    g[c][1] = xix * s2;
+    g[c][2] = xix * s3;
+  }
+}
+
+// Isotropic stress times jacobian*xix: sig = {xx, yy, zz, xy, xz, yz}.
+__device__ __forceinline__ void stress_point(const float g[3][3], float kap, float mu, float fac,
+                                             float sig[6]) {
+  const float l2m = kap + (4.0f / 3.0f) * mu;
+  const float lam = l2m - 2.0f * mu;
+  sig[0] = fac * (l2m * g[0][0] + lam * (g[1][1] + g[2][2]));
+  sig[1] = fac * (l2m * g[1][1] + lam * (g[0][0] + g[2][2]));
+  sig[2] = fac * (l2m * g[2][2] + lam * (g[0][0] + g[1][1]));
+  sig[3] = fac * (mu * (g[0][1] + g[1][0]));
+  sig[4] = fac * (mu * (g[0][2] + g[2][0]));
+  sig[5] = fac * (mu * (g[1][2] + g[2][1]));
+}
+
+// Weak-form divergence at (i,j,k): f_c = -sum_d w w sum_l DW * sig_{c,d}.
+template <int LB>
+__device__ __forceinline__ void div_point(const float* __restrict__ b, int i, int j, int k,
+                                          int lane, const float* __restrict__ sDWt,
+                                          const float* __restrict__ sw, float f[3]) {
+  const float* Sxx = b;
+  const float* Syy = b + 1 * NGLL3 * LB;
+  const float* Szz = b + 2 * NGLL3 * LB;
+  const float* Sxy = b + 3 * NGLL3 * LB;
+  const float* Sxz = b + 4 * NGLL3 * LB;
+  const float* Syz = b + 5 * NGLL3 * LB;
+  float ax = 0.f, ay = 0.f, az = 0.f, bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f,
+        cz = 0.f;
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    const float wi = sDWt[i * 5 + l], wj = sDWt[j * 5 + l], wk = sDWt[k * 5 + l];
+    const int qi = (l + 5 * j + 25 * k) * LB + lane;
+    const int qj = (i + 5 * l + 25 * k) * LB + lane;
+    const int qk = (i + 5 * j + 25 * l) * LB + lane;
+    ax = fmaf(wi, Sxx[qi], ax);
+    ay = fmaf(wi, Sxy[qi], ay);
+    az = fmaf(wi, Sxz[qi], az);
+    bx = fmaf(wj, Sxy[qj], bx);
+    by = fmaf(wj, Syy[qj], by);
+    bz = fmaf(wj, Syz[qj], bz);
+    cx = fmaf(wk, Sxz[qk], cx);
+    cy = fmaf(wk, Syz[qk], cy);
+    cz = fmaf(wk, Szz[qk], cz);
+  }
+  const float wjk = sw[j] * sw[k], wik = sw[i] * sw[k], wij = sw[i] * sw[j];
+  f[0] = -(wjk * ax + wik * bx + wij * cx);
+  f[1] = -(wjk * ay + wik * by + wij * cy);
+  f[2] = -(wjk * az + wik * bz + wij * cz);
+}
+
+// One block = one element x LB lanes.  ADJ: lanes in the adjoint phase also
+// carry the backward field (f2) and accumulate the mu/kappa kernels.
+template <int LB, int NT, bool ADJ>
+__global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
+  constexpr int G = NT / LB;
+  constexpr int P = (NGLL3 + G - 1) / G;
+  extern __shared__ float sm[];
+  __shared__ int s_ib[NGLL3];
+  __shared__ float s_kap[NGLL3], s_mu[NGLL3];
+  __shared__ float s_D[25], s_DWt[25], s_w[5];
+  float* b1 = sm;
+  float* b2 = sm + 6 * NGLL3 * LB;
+
+  const int e = blockIdx.x;
+  const int lane = threadIdx.x % LB;
+  const int pg = threadIdx.x / LB;
+  const int lg = blockIdx.y * LB + lane;
+  const int nev = A.nev;
+  bool act1 = false, act2 = false, scat2 = false;
+  if (lg < nev) {
+    const LaneDesc* L = A.lanes + lg;
+    const int it = L->it0 + A.s;
+    const int ph = L->phase;
+    if (ph != PH_IDLE && it < L->nstep) {
+      act1 = true;
+      if (ADJ && ph == PH_ADJ) {
+        act2 = true;
+        scat2 = it > 0;
+      }
+    }
+  }
+  if (!__syncthreads_or(act1)) return;
+
+  for (int p = threadIdx.x; p < NGLL3; p += NT) {
+    const size_t ep = (size_t)e * NGLL3 + p;
+    s_ib[p] = A.m.ibool[ep];
+    s_kap[p] = A.m.kappa[ep];
+    s_mu[p] = A.m.mu[ep];
+  }
+  if (threadIdx.x < 25) {
+    s_D[threadIdx.x] = c_D[threadIdx.x];
+    s_DWt[threadIdx.x] = c_DWt[threadIdx.x];
+  }
+  if (threadIdx.x < 5) s_w[threadIdx.x] = c_w[threadIdx.x];
+  __syncthreads();
+
+#pragma unroll
+  for (int t = 0; t < P; ++t) {
+    const int p = pg + t * G;
+    if (p < NGLL3) {
+      const size_t ig = (size_t)s_ib[p];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t q = (ig * 3 + c) * nev + lg;
+        b1[(c * NGLL3 + p) * LB + lane] = act1 ? A.f1.u[q] : 0.f;
+        if (ADJ) b2[(c * NGLL3 + p) * LB + lane] = act2 ? A.f2.u[q] : 0.f;
+      }
+    }
+  }
+  __syncthreads();
+
+  const float xix = A.m.xix;
+  const float fac = A.m.jac * A.m.xix;
+  float sg1[P][6];
+  float sg2[ADJ ? P : 1][6];
+#pragma unroll
+  for (int t = 0; t < P; ++t) {
+    const int p = pg + t * G;
+    if (p < NGLL3) {
+      const int i = p % 5, j = (p / 5) % 5, k = p / 25;
+      float g1[3][3];
+      grad_point<LB>(b1, i, j, k, lane, s_D, xix, g1);
+      stress_point(g1, s_kap[p], s_mu[p], fac, sg1[t]);
+      if (ADJ) {
+        float g2[3][3];
+        grad_point<LB>(b2, i, j, k, lane, s_D, xix, g2);
+        stress_point(g2, s_kap[p], s_mu[p], fac, sg2[t]);
+        if (act2) {
+          // deviatoric strain products (adjoint x backward) and traces
+          const float tr1 = g1[0][0] + g1[1][1] + g1[2][2];
+          const float tr2 = g2[0][0] + g2[1][1] + g2[2][2];
+          const float a_xx = g1[0][0] - tr1 * (1.0f / 3.0f);
+          const float a_yy = g1[1][1] - tr1 * (1.0f / 3.0f);
+          const float b_xx = g2[0][0] - tr2 * (1.0f / 3.0f);
+          const float b_yy = g2[1][1] - tr2 * (1.0f / 3.0f);
+          const float a_xy = 0.5f * (g1[0][1] + g1[1][0]);
+          const float a_xz = 0.5f * (g1[0][2] + g1[2][0]);
+          const float a_yz = 0.5f * (g1[1][2] + g1[2][1]);
+          const float b_xy = 0.5f * (g2[0][1] + g2[1][0]);
+          const float b_xz = 0.5f * (g2[0][2] + g2[2][0]);
+          const float b_yz = 0.5f * (g2[1][2] + g2[2][1]);
+          const float dd = a_xx * b_xx + a_yy * b_yy + (a_xx + a_yy) * (b_xx + b_yy) +
+                           2.0f * (a_xy * b_xy + a_xz * b_xz + a_yz * b_yz);
+          const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
+          A.k.mu[q] += A.dt * dd;
+          A.k.kappa[q] += A.dt * (tr1 * tr2);
+        }
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < P; ++t) {
+    const int p = pg + t * G;
+    if (p < NGLL3) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        b1[(q * NGLL3 + p) * LB + lane] = sg1[t][q];
+        if (ADJ) b2[(q * NGLL3 + p) * LB + lane] = sg2[t][q];
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < P; ++t) {
+    const int p = pg + t * G;
+    if (p < NGLL3) {
+      const int i = p % 5, j = (p / 5) % 5, k = p / 25;
+      const size_t ig = (size_t)s_ib[p];
+      if (act1) {
+        float f[3];
+        div_point<LB>(b1, i, j, k, lane, s_DWt, s_w, f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[(ig * 3 + c) * nev + lg], f[c]);
+      }
+      if (ADJ && scat2) {
+        float f[3];
+        div_point<LB>(b2, i, j, k, lane, s_DWt, s_w, f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[(ig * 3 + c) * nev + lg], f[c]);
+      }
+    }
+  }
+}
+
+template <int LB, int NT, bool ADJ>
+static void forces_cfg(const StepArgs& a, cudaStream_t st) {
+  const size_t shm = (size_t)(ADJ ? 2 : 1) * 6 * NGLL3 * LB * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_forces<LB, NT, ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)shm);
+    attr = true;
+  }
+  dim3 grid(a.m.nspec, (a.nev + LB - 1) / LB);
+  k_forces<LB, NT, ADJ><<<grid, NT, shm, st>>>(a);
+}
+
+int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.nev == 1) {
+    if (adj)
+      forces_cfg<1, 128, true>(a, st);
+    else
+      forces_cfg<1, 128, false>(a, st);
+  } else {
+    if (adj)
+      forces_cfg<8, 256, true>(a, st);
+    else
+      forces_cfg<8, 256, false>(a, st);
+  }
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Stacey absorbing faces: traction, boundary store save / replay
+// ---------------------------------------------------------------------------
+
+// Block of 128 threads = FPB faces x (32 point slots x LBB lanes).
+template <int LBB>
+__global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
+  constexpr int FPB = 128 / (32 * LBB);
+  __shared__ unsigned s_max[FPB * LBB];
+  const int t = threadIdx.x;
+  const int fl = t / (32 * LBB);
+  const int r = t % (32 * LBB);
+  const int lane = r % LBB;
+  const int p = r / LBB;
+  const int f = blockIdx.x * FPB + fl;
+  const int lg = blockIdx.y * LBB + lane;
+  const int nf = A.m.nf;
+  const int nev = A.nev;
+  if (t < FPB * LBB) s_max[t] = 0u;
+  __syncthreads();
+
+  bool absorb = false, save = false, replay = false;
+  int it = 0, nstep = 1;
+  const LaneDesc* L = nullptr;
+  if (lg < nev) {
+    L = A.lanes + lg;
+    it = L->it0 + A.s;
+    nstep = L->nstep;
+    if (L->phase != PH_IDLE && it < nstep) {
+      absorb = true;
+      save = (L->phase == PH_FWD) && L->save;
+      replay = (L->phase == PH_ADJ) && it > 0;
+    }
+  }
+  const bool valid = (f < nf) && (p < NGLL2) && (lg < nev);
+  float sv[3] = {0.f, 0.f, 0.f};
+  size_t ig = 0;
+  if (valid) {
+    const int fp = f * NGLL2 + p;
+    ig = (size_t)A.m.f_iglob[fp];
+    if (absorb) {
+      const float nx = A.m.f_n[fp * 3 + 0], ny = A.m.f_n[fp * 3 + 1], nz = A.m.f_n[fp * 3 + 2];
+      const float vx = A.f1.v[(ig * 3 + 0) * nev + lg];
+      const float vy = A.f1.v[(ig * 3 + 1) * nev + lg];
+      const float vz = A.f1.v[(ig * 3 + 2) * nev + lg];
+      const float vn = vx * nx + vy * ny + vz * nz;
+      const float rvp = A.m.f_rvp[fp], rvs = A.m.f_rvs[fp];
+      const float jw = A.m.f_jw[fp];
+      sv[0] = (rvp * vn * nx + rvs * (vx - vn * nx)) * jw;
+      sv[1] = (rvp * vn * ny + rvs * (vy - vn * ny)) * jw;
+      sv[2] = (rvp * vn * nz + rvs * (vz - vn * nz)) * jw;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[(ig * 3 + c) * nev + lg], -sv[c]);
+      if (save && A.store_fp16) {
+        const float m = fmaxf(fabsf(sv[0]), fmaxf(fabsf(sv[1]), fabsf(sv[2])));
+        atomicMax(&s_max[fl * LBB + lane], __float_as_uint(m));
+      }
+    }
+  }
+  if (A.store_fp16) __syncthreads();
+  if (valid && save) {
+    const size_t base = ((size_t)it * nf + f) * 75 + p * 3;
+    if (A.store_fp16) {
+      const float mx = __uint_as_float(s_max[fl * LBB + lane]);
+      const float inv = mx > 0.f ? 32768.0f / mx : 0.f;
+      __half* st = (__half*)L->store;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) st[base + c] = __float2half_rn(sv[c] * inv);
+      if (p == 0) L->scale[(size_t)it * nf + f] = mx * (1.0f / 32768.0f);
+    } else {
+      float* st = (float*)L->store;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) st[base + c] = sv[c];
+    }
+  }
+  if (valid && replay) {
+    const int n = nstep - 1 - it;
+    const size_t base = ((size_t)n * nf + f) * 75 + p * 3;
+    float val[3];
+    if (A.store_fp16) {
+      const float sc = L->scale[(size_t)n * nf + f];
+      const __half* st = (const __half*)L->store;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) val[c] = __half2float(st[base + c]) * sc;
+    } else {
+      const float* st = (const float*)L->store;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) val[c] = st[base + c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[(ig * 3 + c) * nev + lg], -val[c]);
+  }
+}
+
+int launch_boundary(const StepArgs& a, bool adj, cudaStream_t st) {
+  (void)adj;
+  int n = 0;
+  if (a.m.nf > 0) {
+    if (a.nev == 1) {
+      dim3 grid((a.m.nf + 3) / 4, 1);
+      k_stacey<1><<<grid, 128, 0, st>>>(a);
+    } else if (a.nev == 2) {
+      dim3 grid((a.m.nf + 1) / 2, 1);
+      k_stacey<2><<<grid, 128, 0, st>>>(a);
+    } else {
+      dim3 grid(a.m.nf, (a.nev + 3) / 4);
+      k_stacey<4><<<grid, 128, 0, st>>>(a);
+    }
+    ++n;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// point sources, receivers and adjoint sources
+// ---------------------------------------------------------------------------
+
+// blocks [0, nev): moment-tensor source of one lane (forward field in the
+// forward phase, backward field in the adjoint phase).
+// blocks [nev, ...): one warp per (receiver, lane): record the forward
+// displacement, or inject the adjoint source into the adjoint field.
+__global__ void __launch_bounds__(128) k_points(StepArgs A) {
+  const int nev = A.nev;
+  if ((int)blockIdx.x < nev) {
+    const int lg = blockIdx.x;
+    const LaneDesc* L = A.lanes + lg;
+    const int it = L->it0 + A.s;
+    if (L->phase == PH_IDLE || it >= L->nstep || L->src_ispec < 0) return;
+    float* acc;
+    float s;
+    if (L->phase == PH_FWD) {
+      acc = A.f1.a;
+      s = L->stf[it];
+    } else {
+      if (it == 0) return;
+      acc = A.f2.a;
+      s = L->stf[L->nstep - 1 - it];
+    }
+    const int p = threadIdx.x;
+    if (p < NGLL3) {
+      const size_t ig = (size_t)A.m.ibool[(size_t)L->src_ispec * NGLL3 + p];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        atomicAdd(&acc[(ig * 3 + c) * nev + lg], L->srcarr[p * 3 + c] * s);
+    }
+    return;
+  }
+  const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const int pair = ((int)blockIdx.x - nev) * 4 + warp;
+  const int r = pair / nev, lg = pair - r * nev;
+  if (r >= A.nrec_max) return;
+  const LaneDesc* L = A.lanes + lg;
+  const int it = L->it0 + A.s;
+  if (L->phase == PH_IDLE || it >= L->nstep || r >= L->nrec) return;
+  const int e = L->rec_ispec[r];
+  const float* w = L->rec_w + (size_t)r * NGLL3;
+  if (L->phase == PH_FWD) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int p = ln; p < NGLL3; p += 32) {
+      const size_t ig = (size_t)A.m.ibool[(size_t)e * NGLL3 + p];
+      const float wp = w[p];
+      s0 = fmaf(wp, A.f1.u[(ig * 3 + 0) * nev + lg], s0);
+      s1 = fmaf(wp, A.f1.u[(ig * 3 + 1) * nev + lg], s1);
+      s2 = fmaf(wp, A.f1.u[(ig * 3 + 2) * nev + lg], s2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (ln == 0) {
+      const size_t ns = (size_t)L->nstep;
+      L->seis[((size_t)r * 3 + 0) * ns + it] = s0;
+      L->seis[((size_t)r * 3 + 1) * ns + it] = s1;
+      L->seis[((size_t)r * 3 + 2) * ns + it] = s2;
+    }
+  } else {
+    const size_t ns = (size_t)L->nstep;
+    const int n = L->nstep - 1 - it;
+    const float a0 = L->adj[((size_t)r * 3 + 0) * ns + n];
+    const float a1 = L->adj[((size_t)r * 3 + 1) * ns + n];
+    const float a2 = L->adj[((size_t)r * 3 + 2) * ns + n];
+    for (int p = ln; p < NGLL3; p += 32) {
+      const size_t ig = (size_t)A.m.ibool[(size_t)e * NGLL3 + p];
+      const float wp = w[p];
+      atomicAdd(&A.f1.a[(ig * 3 + 0) * nev + lg], wp * a0);
+      atomicAdd(&A.f1.a[(ig * 3 + 1) * nev + lg], wp * a1);
+      atomicAdd(&A.f1.a[(ig * 3 + 2) * nev + lg], wp * a2);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Newmark corrector (this step) + predictor (next step)
+// ---------------------------------------------------------------------------
+
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_update(StepArgs A) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nev = A.nev;
+  if (idx >= (size_t)A.m.nglob * nev) return;
+  const size_t ig = idx / nev;
+  const int lg = (int)(idx - ig * nev);
+  const LaneDesc* L = A.lanes + lg;
+  const int it = L->it0 + A.s;
+  const int ph = L->phase;
+  if (ph == PH_IDLE || it >= L->nstep) return;
+  const bool pred = it + 1 < L->nstep;
+  const float dt = A.dt, dt2 = 0.5f * A.dt, dtsq2 = 0.5f * A.dt * A.dt;
+  float u[3], v[3], a[3], mi[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const size_t q = (ig * 3 + c) * nev + lg;
+    mi[c] = A.minv[ig * 3 + c];
+    a[c] = A.f1.a[q] * mi[c];
+    v[c] = A.f1.v[q] + dt2 * a[c];
+    u[c] = A.f1.u[q];
+  }
+  if (ADJ && ph == PH_ADJ) {
+    float bu[3], bv[3], ba[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t q = (ig * 3 + c) * nev + lg;
+      bu[c] = A.f2.u[q];
+      bv[c] = A.f2.v[q];
+      ba[c] = A.f2.a[q];
+      if (it > 0) {
+        ba[c] = ba[c] * mi[c];
+        bv[c] = bv[c] - dt2 * ba[c];
+      }
+    }
+    A.k.rho_glob[ig * nev + lg] += dt * (a[0] * bu[0] + a[1] * bu[1] + a[2] * bu[2]);
+    if (pred) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        bu[c] = bu[c] - dt * bv[c] + dtsq2 * ba[c];
+        bv[c] = bv[c] - dt2 * ba[c];
+        ba[c] = 0.f;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t q = (ig * 3 + c) * nev + lg;
+      A.f2.u[q] = bu[c];
+      A.f2.v[q] = bv[c];
+      A.f2.a[q] = ba[c];
+    }
+  }
+  if (pred) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      u[c] = u[c] + dt * v[c] + dtsq2 * a[c];
+      v[c] = v[c] + dt2 * a[c];
+      a[c] = 0.f;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const size_t q = (ig * 3 + c) * nev + lg;
+    A.f1.u[q] = u[c];
+    A.f1.v[q] = v[c];
+    A.f1.a[q] = a[c];
+  }
+}
+
+int launch_update(const StepArgs& a, bool adj, cudaStream_t st) {
+  const size_t n = (size_t)a.m.nglob * a.nev;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (adj)
+    k_update<true><<<blocks, 256, 0, st>>>(a);
+  else
+    k_update<false><<<blocks, 256, 0, st>>>(a);
+  return 1;
+}
+
+int launch_points(const StepArgs& a, cudaStream_t st) {
+  const int blocks = a.nev + (a.nrec_max * a.nev + 3) / 4;
+  k_points<<<blocks, 128, 0, st>>>(a);
+  return 1;
+}
+
+__global__ void k_advance(LaneDesc* lanes, int nev, int k) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l < nev) lanes[l].it0 += k;
+}
+
+int launch_advance(LaneDesc* lanes, int nev, int k, cudaStream_t st) {
+  k_advance<<<(nev + 127) / 128, 128, 0, st>>>(lanes, nev, k);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// kernels: final scaling (FP64) and cross-event FP64 sum
+// ---------------------------------------------------------------------------
+
+__global__ void k_finalize(MeshView m, const float* __restrict__ rho, KernAcc k, int nev, int lane,
+                           double* __restrict__ out6, double* __restrict__ sum6) {
+  const size_t ne = (size_t)m.nspec * NGLL3;
+  const size_t ep = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ep >= ne) return;
+  const double r = rho[ep], mu = m.mu[ep], kap = m.kappa[ep];
+  const double rk = -r * (double)k.rho_glob[(size_t)m.ibool[ep] * nev + lane];
+  const double mk = -2.0 * mu * (double)k.mu[ep * nev + lane];
+  const double kk = -kap * (double)k.kappa[ep * nev + lane];
+  const double v6[6] = {rk, mk, kk, rk + kk + mk, 2.0 * (mk - 4.0 / 3.0 * mu / kap * kk),
+                        2.0 * (1.0 + 4.0 / 3.0 * mu / kap) * kk};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    if (out6) out6[q * ne + ep] = v6[q];
+    if (sum6) sum6[q * ne + ep] += v6[q];
+  }
+}
+
+int launch_finalize_kernels(const MeshView& m, const float* rho, const KernAcc& k, int nev,
+                            int lane, double* out6, double* sum6, cudaStream_t st) {
+  const size_t ne = (size_t)m.nspec * NGLL3;
+  k_finalize<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, rho, k, nev, lane, out6, sum6);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// L2 waveform misfit and adjoint source in FP64
+// ---------------------------------------------------------------------------
+
+// One block per (receiver, component) series.
+__global__ void __launch_bounds__(256) k_measure_l2(const float* __restrict__ seis,
+                                                    const double* __restrict__ obs,
+                                                    const double* __restrict__ taper,
+                                                    const double* __restrict__ simpw, int nstep,
+                                                    float* __restrict__ adj,
+                                                    double* __restrict__ misfit_rc) {
+  __shared__ double red[256];
+  const size_t base = (size_t)blockIdx.x * nstep;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nstep; i += blockDim.x) {
+    const double w = taper[i];
+    const double r = (double)seis[base + i] * w - obs[base + i] * w;
+    adj[base + i] = (float)(r * w);
+    acc += simpw[i] * r * r;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) misfit_rc[blockIdx.x] = 0.5 * red[0];
+}
+
+int launch_measure_l2(const float* seis, const double* obs, const double* taper,
+                      const double* simpw, int nrec, int nstep, float* adj_out,
+                      double* misfit_rc, cudaStream_t st) {
+  k_measure_l2<<<nrec * 3, 256, 0, st>>>(seis, obs, taper, simpw, nstep, adj_out, misfit_rc);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// lane utilities (phase transitions) and health check
+// ---------------------------------------------------------------------------
+
+__global__ void k_lane_copy(Fields s, Fields d, int nglob, int nev, int lane) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nglob * 3) return;
+  const size_t q = i * nev + lane;
+  d.u[q] = s.u[q];
+  d.v[q] = s.v[q];
+  d.a[q] = s.a[q];
+}
+
+__global__ void k_lane_zero(Fields f, int nglob, int nev, int lane) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nglob * 3) return;
+  const size_t q = i * nev + lane;
+  f.u[q] = 0.f;
+  f.v[q] = 0.f;
+  f.a[q] = 0.f;
+}
+
+int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, int nev, int lane,
+                     cudaStream_t st) {
+  const size_t n = (size_t)nglob * 3;
+  k_lane_copy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, dst, nglob, nev, lane);
+  return 1;
+}
+
+int launch_lane_zero(const Fields& f, int nglob, int nev, int lane, cudaStream_t st) {
+  const size_t n = (size_t)nglob * 3;
+  k_lane_zero<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f, nglob, nev, lane);
+  return 1;
+}
+
+__global__ void k_nonfinite(const float* __restrict__ u, size_t n, int* flag) {
+  bool bad = false;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    bad |= !isfinite(u[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st) {
+  k_nonfinite<<<148 * 4, 256, 0, st>>>(u, n, flag);
+  return 1;
+}
+
+}  // namespace sem

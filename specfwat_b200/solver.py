@@ -1,0 +1,239 @@
+"""Host-side mirror of the reference's per-event driver over the C ABI.
+
+The reference runs one event as (``src/preproc/prepare_fwd.f90:297-384``)::
+
+    run_simulation(1)   InitSpecfem, setup_sources_receivers_fwat,
+                        prepare_timerun_fwat, iterate_time, FinalizeSpecfem
+    measure_adj         seismograms -> misfit + adjoint sources (SEM/*.adj)
+    run_simulation(3)   same chain with SIMULATION_TYPE=3
+    postproc_adjoint    save_adjoint_kernels
+
+:class:`Mesh` is the resident database (``read_mesh_databases_fwat`` +
+``prepare_GPU``); :class:`Simulation` is one run (``prepare_timerun_fwat``)
+with methods named after the reference entry points; :class:`PrepareFWD`
+strings them together per run mode (``src/shared/config.f90:52-56``).  All
+arrays stay on the device between the forward and adjoint runs: the
+boundary store and the final forward state (``absorb_field.bin`` and
+``save_forward_arrays.bin`` in the reference) are never written out.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+FORWARD_ONLY, FORWARD_MEASADJ, FORWARD_ADJOINT = 1, 2, 3   # config.f90:52-56
+KERNEL_NAMES = ("rho", "mu", "kappa", "rhop", "beta", "alpha")
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+class Mesh:
+    """A mesh database resident in device memory."""
+
+    def __init__(self, db, index_base: int = 0):
+        L = _lib.load()
+        self.db = db
+        k = dict(
+            ibool=np.ascontiguousarray(db.ibool.reshape(-1) + index_base, np.int32),
+            x=np.ascontiguousarray(db.xstore, np.float32),
+            y=np.ascontiguousarray(db.ystore, np.float32),
+            z=np.ascontiguousarray(db.zstore, np.float32),
+            kappa=np.ascontiguousarray(db.kappa.reshape(-1), np.float32),
+            mu=np.ascontiguousarray(db.mu.reshape(-1), np.float32),
+            rho=np.ascontiguousarray(db.rho.reshape(-1), np.float32),
+            rmass=np.ascontiguousarray(db.rmass, np.float32),
+            rho_vp=np.ascontiguousarray(db.rho_vp.reshape(-1), np.float32),
+            rho_vs=np.ascontiguousarray(db.rho_vs.reshape(-1), np.float32),
+            f_ispec=np.ascontiguousarray(db.abs_ispec + index_base, np.int32),
+            f_ijk=np.ascontiguousarray(db.abs_ijk.reshape(-1) + index_base, np.int32),
+            f_jw=np.ascontiguousarray(db.abs_jw.reshape(-1), np.float32),
+            f_n=np.ascontiguousarray(db.abs_normal.reshape(-1), np.float32),
+        )
+        f, i = C.c_float, C.c_int
+        desc = _lib.MeshDesc(
+            db.nspec, db.nglob, index_base, _p(k["ibool"], i), _p(k["x"], f),
+            _p(k["y"], f), _p(k["z"], f), db.xix_regular, db.jacobian_regular,
+            None, _p(k["kappa"], f), _p(k["mu"], f), _p(k["rho"], f),
+            _p(k["rmass"], f), _p(k["rho_vp"], f), _p(k["rho_vs"], f),
+            db.nfaces, _p(k["f_ispec"], i), _p(k["f_ijk"], i), _p(k["f_jw"], f),
+            _p(k["f_n"], f))
+        h = C.c_void_p()
+        check(L.sem_prepare_mesh(C.byref(desc), C.byref(h)))
+        self._h = h
+        self.nspec, self.nglob, self.nfaces = db.nspec, db.nglob, db.nfaces
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_bytes(self) -> int:
+        b = C.c_longlong()
+        check(_lib.load().sem_mesh_info(self._h, None, None, None, C.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            check(_lib.load().sem_release_mesh(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_source(x, y, z, mt: Sequence[float], f0: float, tshift=0.0):
+    """CMT-convention source: ``mt`` = (Mrr, Mtt, Mpp, Mrt, Mrp, Mtp)."""
+    return _lib.Source(float(x), float(y), float(z), *[float(m) for m in mt],
+                       float(f0), float(tshift))
+
+
+class Simulation:
+    """One run: ``nev`` events sharing a mesh, ``nstep`` steps of ``dt``.
+
+    ``nev == 1`` is the plain one-event-per-launch path; ``nev > 1`` runs all
+    events in the same kernels with lane-interleaved wavefields.
+    """
+
+    def __init__(self, mesh: Mesh, nstep: int, dt: float, nev: int = 1,
+                 store: str = "fp32", use_graph: bool = False,
+                 graph_steps: int = 50, max_receivers: int = 128,
+                 check_every: int = 0):
+        L = _lib.load()
+        self.mesh = mesh
+        self.nstep, self.dt, self.nev = nstep, dt, nev
+        kind = {"fp32": _lib.SEM_STORE_FP32, "fp16": _lib.SEM_STORE_FP16}[store]
+        self.cfg = _lib.RunCfg(nev, nstep, dt, kind, int(use_graph),
+                               graph_steps, max_receivers, check_every)
+        h = C.c_void_p()
+        check(L.sem_prepare_timerun(mesh.handle, C.byref(self.cfg), C.byref(h)))
+        self._h = h
+        self.nrec = [0] * nev
+
+    # setup_sources_receivers_fwat
+    def set_sources(self, sources: Iterable):
+        src = list(sources)
+        arr = (_lib.Source * len(src))(*src)
+        check(_lib.load().sem_set_sources(self._h, len(src), arr))
+
+    def set_receivers(self, xyz, ev: int = -1):
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        check(_lib.load().sem_set_receivers(self._h, ev, xyz.shape[0],
+                                            xyz.ctypes.data))
+        for e in (range(self.nev) if ev < 0 else [ev]):
+            self.nrec[e] = xyz.shape[0]
+
+    # iterate_time
+    def iterate_time(self, sim_type: int = 1, save_forward: bool = False,
+                     synchronize: bool = True):
+        check(_lib.load().sem_iterate_time(self._h, sim_type, int(save_forward)))
+        if synchronize:
+            self.synchronize()
+
+    def synchronize(self):
+        check(_lib.load().sem_synchronize(self._h))
+
+    def seismograms(self, ev: int = 0) -> np.ndarray:
+        out = np.zeros((self.nrec[ev], 3, self.nstep), np.float32)
+        check(_lib.load().sem_get_seismograms(self._h, ev, out.ctypes.data))
+        return out
+
+    def set_adjoint_sources(self, ev: int, adj):
+        adj = np.ascontiguousarray(adj, np.float64)
+        assert adj.shape == (self.nrec[ev], 3, self.nstep)
+        check(_lib.load().sem_set_adjoint_sources(self._h, ev, adj.ctypes.data))
+
+    def measure_l2(self, ev: int, obs, taper_pct=0.05, taper_type=1) -> float:
+        obs = np.ascontiguousarray(obs, np.float64)
+        assert obs.shape == (self.nrec[ev], 3, self.nstep)
+        m = C.c_double()
+        check(_lib.load().sem_measure_l2(self._h, ev, obs.ctypes.data,
+                                         float(taper_pct), int(taper_type),
+                                         C.byref(m)))
+        return m.value
+
+    # save_adjoint_kernels
+    def save_adjoint_kernels(self, ev: int = 0) -> np.ndarray:
+        out = np.zeros((6, self.mesh.nspec, 5, 5, 5), np.float64)
+        check(_lib.load().sem_save_adjoint_kernels(self._h, ev, out.ctypes.data))
+        return out
+
+    def sum_kernels(self) -> np.ndarray:
+        out = np.zeros((6, self.mesh.nspec, 5, 5, 5), np.float64)
+        check(_lib.load().sem_sum_kernels(self._h, out.ctypes.data))
+        return out
+
+    def loop_ms(self) -> float:
+        ms = C.c_double()
+        check(_lib.load().sem_last_loop_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        check(_lib.load().sem_last_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            check(_lib.load().sem_release_run(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PrepareFWD:
+    """Per-event driver in the shape of the reference's ``PrepareFWD``
+    (``src/preproc/prepare_fwd.f90:28-35,297-384``): forward run, L2
+    measurement against observed data, adjoint run, kernels.
+
+    All ``nev`` events of one call share the mesh and run together.
+    """
+
+    def __init__(self, mesh: Mesh, nstep: int, dt: float, nev: int = 1,
+                 store: str = "fp32", use_graph: bool = False,
+                 graph_steps: int = 50, max_receivers: int = 128,
+                 taper_pct: float = 0.05, taper_type: int = 1):
+        self.sim = Simulation(mesh, nstep, dt, nev=nev, store=store,
+                              use_graph=use_graph, graph_steps=graph_steps,
+                              max_receivers=max_receivers)
+        self.taper_pct, self.taper_type = taper_pct, taper_type
+        self.misfits = np.zeros(nev)
+
+    def setup(self, sources, receivers):
+        self.sim.set_sources(sources)
+        if isinstance(receivers, (list, tuple)):
+            for e, r in enumerate(receivers):
+                self.sim.set_receivers(r, e)
+        else:
+            self.sim.set_receivers(receivers)
+
+    def simulation(self, obs: Optional[Sequence[np.ndarray]] = None,
+                   run_mode: int = FORWARD_ADJOINT):
+        """Run one pass for all events.  ``obs[ev]`` are observed
+        seismograms [nrec, 3, nstep] (needed for run modes >= 2)."""
+        sim = self.sim
+        sim.iterate_time(1, save_forward=run_mode == FORWARD_ADJOINT,
+                         synchronize=False)
+        if run_mode == FORWARD_ONLY:
+            sim.synchronize()
+            return
+        for ev in range(sim.nev):
+            self.misfits[ev] = sim.measure_l2(ev, obs[ev], self.taper_pct,
+                                              self.taper_type)
+        if run_mode == FORWARD_ADJOINT:
+            sim.iterate_time(3, synchronize=True)
+
+    def close(self):
+        self.sim.close()

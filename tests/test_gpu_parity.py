@@ -1,0 +1,186 @@
+"""Parity of the CUDA solver (through the C ABI) with the CPU oracle.
+
+Tolerances: seismograms within relative L2 1e-4 of the FP32 oracle run,
+event kernels within relative L2 1e-3; errors against the FP64 oracle run
+are asserted at the same bounds.  Runs need a B200.
+"""
+import numpy as np
+import pytest
+
+from specfwat_b200 import database as D
+from specfwat_b200 import solver as S
+from oracle.oracle import Oracle, l2_adjoint_source
+
+pytestmark = pytest.mark.gpu
+
+SEIS_TOL = 1e-4
+KERN_TOL = 1e-3
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def small():
+    db = D.build("small")
+    rec = D.surface_receivers(db.box, 5)
+    mt = D.random_moment_tensor(np.random.default_rng(1234))
+    return db, rec, mt
+
+
+def test_forward_plain_matches_oracle(gpu, small):
+    db, rec, mt = small
+    nstep, dt = 400, 0.02
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec))
+    sim.set_sources([S.make_source(20000., 20000., -10000., mt, 1.0)])
+    sim.set_receivers(rec)
+    sim.iterate_time(1)
+    g = sim.seismograms(0)
+    src = Oracle.source(20000., 20000., -10000., mt, 1.0)
+    o32 = Oracle(db, precision=4).forward(dt, nstep, src, rec)
+    o64 = Oracle(db, precision=8).forward(dt, nstep, src, rec)
+    assert np.abs(g).max() > 1e-4
+    assert rel_l2(g, o32) < SEIS_TOL
+    assert rel_l2(g, o64) < SEIS_TOL
+
+
+def test_forward_one_based_indices(gpu, small):
+    db, rec, mt = small
+    nstep, dt = 100, 0.02
+    out = []
+    for base in (0, 1):
+        mesh = S.Mesh(db, index_base=base)
+        sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec))
+        sim.set_sources([S.make_source(20000., 20000., -10000., mt, 1.0)])
+        sim.set_receivers(rec)
+        sim.iterate_time(1)
+        out.append(sim.seismograms(0))
+        sim.close()
+        mesh.close()
+    assert rel_l2(out[1], out[0]) < 1e-6
+
+
+@pytest.fixture(scope="module")
+def mini_adjoint():
+    """Forward on the background model, 'observed' data on the model with
+    a vs anomaly (oracle FP64), L2 adjoint sources, kernels."""
+    box = D.BoxSpec(8, 8, 6)
+    db = D.make_box(box)
+    vp, vs, rho = D.background_model(db, seed=7)
+    db = db.with_model(vp, vs, rho)
+    vs_obs = D.gaussian_vs_anomaly(db, vs, radius=6000.0, depth=12000.0)
+    db_obs = db.with_model(vp, vs_obs, rho)
+    rec = D.surface_receivers(box, 4)
+    mt = D.random_moment_tensor(np.random.default_rng(5))
+    src_xyz = (16000., 16000., -14000.)
+    nstep, dt = 500, 0.02
+    src = Oracle.source(*src_xyz, mt, 1.0)
+    obs = Oracle(db_obs, precision=8).forward(dt, nstep, src, rec)
+    return db, rec, mt, src_xyz, nstep, dt, obs
+
+
+def test_adjoint_kernels_match_oracle(gpu, mini_adjoint):
+    db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec))
+    sim.set_sources([S.make_source(*sxyz, mt, 1.0)])
+    sim.set_receivers(rec)
+    sim.iterate_time(1, save_forward=True)
+    syn = sim.seismograms(0)
+    misfit = sim.measure_l2(0, obs, 0.05, 1)
+    sim.iterate_time(3)
+    kg = sim.save_adjoint_kernels(0)
+
+    src = Oracle.source(*sxyz, mt, 1.0)
+    res = {}
+    for prec in (4, 8):
+        o = Oracle(db, precision=prec)
+        osyn = o.forward(dt, nstep, src, rec, save_forward=True)
+        om, oadj = l2_adjoint_source(osyn, obs, dt, 0.05, 1)
+        res[prec] = (osyn, om.sum(), o.adjoint(rec, oadj))
+    assert rel_l2(syn, res[4][0]) < SEIS_TOL
+    assert abs(misfit - res[8][1]) / res[8][1] < 1e-3
+    for q, name in enumerate(S.KERNEL_NAMES[:3]):
+        e32 = rel_l2(kg[q], res[4][2][q])
+        e64 = rel_l2(kg[q], res[8][2][q])
+        assert e32 < KERN_TOL, (name, e32)
+        assert e64 < KERN_TOL, (name, e64)
+
+
+def test_batched_equals_plain(gpu, small):
+    db, rec, _ = small
+    nstep, dt, nev = 200, 0.02, 5
+    rng = np.random.default_rng(99)
+    srcs = [S.make_source(rng.uniform(8e3, 32e3), rng.uniform(8e3, 32e3),
+                          -rng.uniform(5e3, 30e3), D.random_moment_tensor(rng),
+                          rng.uniform(0.5, 1.5)) for _ in range(nev)]
+    mesh = S.Mesh(db)
+    b = S.Simulation(mesh, nstep, dt, nev=nev, max_receivers=len(rec))
+    b.set_sources(srcs)
+    b.set_receivers(rec)
+    b.iterate_time(1)
+    for e in range(nev):
+        p = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec))
+        p.set_sources([srcs[e]])
+        p.set_receivers(rec)
+        p.iterate_time(1)
+        assert rel_l2(b.seismograms(e), p.seismograms(0)) < 1e-5
+        p.close()
+
+
+def test_graph_equals_stepwise(gpu, small):
+    db, rec, mt = small
+    nstep, dt = 130, 0.02   # not a multiple of graph_steps
+    mesh = S.Mesh(db)
+    out = []
+    for g in (False, True):
+        sim = S.Simulation(mesh, nstep, dt, use_graph=g, graph_steps=50,
+                           max_receivers=len(rec))
+        sim.set_sources([S.make_source(20000., 20000., -10000., mt, 1.0)])
+        sim.set_receivers(rec)
+        sim.iterate_time(1)
+        out.append(sim.seismograms(0))
+        sim.close()
+    assert rel_l2(out[1], out[0]) < 1e-6
+
+
+def test_batched_adjoint_fp16_store(gpu, mini_adjoint):
+    db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
+    mesh = S.Mesh(db)
+    kern = {}
+    for store in ("fp32", "fp16"):
+        sim = S.Simulation(mesh, nstep, dt, nev=2, store=store, use_graph=True,
+                           max_receivers=len(rec))
+        sim.set_sources([S.make_source(*sxyz, mt, 1.0)] * 2)
+        sim.set_receivers(rec)
+        sim.iterate_time(1, save_forward=True)
+        for e in range(2):
+            sim.measure_l2(e, obs)
+        sim.iterate_time(3)
+        kern[store] = sim.sum_kernels()
+        k0 = sim.save_adjoint_kernels(0)
+        k1 = sim.save_adjoint_kernels(1)
+        assert rel_l2(k0[:3], k1[:3]) < 1e-5
+        assert rel_l2(kern[store][:3], 2 * k0[:3]) < 1e-5
+        sim.close()
+    for q in range(3):
+        assert rel_l2(kern["fp16"][q], kern["fp32"][q]) < 5e-3
+
+
+def test_state_errors(gpu, small):
+    db, rec, mt = small
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, 10, 0.02, max_receivers=len(rec))
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.iterate_time(1)
+    assert ei.value.code == -4
+    sim.set_sources([S.make_source(20000., 20000., -10000., mt, 1.0)])
+    sim.set_receivers(rec)
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.iterate_time(3)
+    assert ei.value.code == -4
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.set_receivers(np.zeros((len(rec) + 1, 3)))
+    assert ei.value.code == -1
