@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Benchmark: forward+adjoint events/hour of the elastic SEM hot path.
+
+Workload (one "step" = one batch of events through the whole hot path):
+the 40x40x20-element box (160x160x80 km, 2,099,601 GLL points, NGLL=5),
+background model vp/vs/rho = 6000/3464/2700 x (1 + 0.05 g) with a seeded
+8 km Gaussian random field g, "observed" data from the same model plus a
++10% Gaussian vs anomaly (radius 15 km, depth 30 km) computed once before
+timing, 100 surface receivers (10x10), NSTEP 4000, dt 0.02 s.  Each event:
+forward run saving the Stacey boundary store, FP64 L2 waveform misfit and
+adjoint sources on the device, adjoint + backward run with rho/mu/kappa
+kernel accumulation, FP64 cross-event kernel sum.  Events have seeded
+random moment tensors, depths 5-40 km and Ricker f0 in 0.5-1.5 Hz.
+
+Lines printed (rank 0, one JSON line):
+  value   events/hour of the batched path (events of a batch share every
+          launch; FP16 per-face-scaled boundary store; CUDA graphs), device
+          resident inputs, CUDA-event timed, max over ranks
+  e2e     the same through the public API from pinned host buffers: sources
+          and receivers set from the host, observed data H2D, kernels and
+          seismograms D2H inside the timed region
+  plain   one event per launch (FP32 boundary store, step-by-step launches)
+`--impl reference` times the CPU restatement of the path (OpenMP, all host
+threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("fwd+adj events/hour batched+served vs plain per-event on 1 B200; "
+          "p50/p99 latency")
+WORKLOAD = ("medium box 40x40x20 el over 160x160x80 km (2,099,601 GLL pts), "
+            "NSTEP 4000, dt 0.02 s, 100 surface receivers, fwd + L2 adjoint "
+            "source + adjoint/backward with rho/mu/kappa kernels")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--events", type=int, default=32)
+    p.add_argument("--nstep", type=int, default=4000)
+    p.add_argument("--mesh", default="medium")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=1)
+    p.add_argument("--store", default="fp16", choices=["fp16", "fp32"])
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def make_workload(mesh_name, nev, seed):
+    from specfwat_b200 import database as D
+    db = D.build(mesh_name, seed=1234)
+    vp, vs, rho = D.background_model(db, seed=1234)
+    db_obs = db.with_model(vp, D.gaussian_vs_anomaly(db, vs), rho)
+    rec = D.surface_receivers(db.box, 10)
+    rng = np.random.default_rng(seed)
+    box = db.box
+    events = []
+    for _ in range(nev):
+        x = rng.uniform(0.15, 0.85) * box.lx
+        y = rng.uniform(0.15, 0.85) * box.ly
+        z = -rng.uniform(5000.0, 40000.0)
+        events.append((x, y, z, D.random_moment_tensor(rng),
+                       rng.uniform(0.5, 1.5)))
+    return db, db_obs, rec, events
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: CPU restatement of the path
+# ---------------------------------------------------------------------------
+
+def cpu_sample(db, db_obs, rec, ev, nstep_full, sample_steps, dt=0.02):
+    """FP32 oracle (OpenMP, all host threads): sample_steps forward (saving
+    the boundary store) + sample_steps adjoint/backward steps, extrapolated
+    to nstep_full.  Returns (seconds per event, threads)."""
+    from oracle.oracle import Oracle, l2_adjoint_source
+    nth = os.cpu_count() or 1
+    x, y, z, mt, f0 = ev
+    o = Oracle(db, precision=4, nthreads=nth)
+    src = Oracle.source(x, y, z, mt, f0)
+    t0 = time.perf_counter()
+    syn = o.forward(dt, sample_steps, src, rec, save_forward=True)
+    _, adj = l2_adjoint_source(syn, np.zeros_like(syn), dt)
+    o.adjoint(rec, adj)
+    t = time.perf_counter() - t0
+    return t * nstep_full / sample_steps, nth
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    db, db_obs, rec, events = make_workload(args.mesh, 1, 4321)
+    sample = 40
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        s, nth = cpu_sample(db, db_obs, rec, events[0], args.nstep, sample)
+        if i >= args.warmup:
+            per_step.append(s)
+    sec = float(np.mean(per_step))
+    v = 3600.0 / sec
+    cb = {"value": v, "unit": "events/hour", "cores": nth, "kind": "port",
+          "sample": f"{sample} forward + {sample} adjoint/backward steps of one "
+                    f"event, extrapolated to NSTEP {args.nstep}"}
+    line = {"metric": METRIC, "value": v, "unit": "events/hour",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "events_per_step": 1,
+                       "reference_solver": "unavailable on this box (SPECFEM3D "
+                       "submodule absent); the CPU restatement of the path is timed"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "events/hour", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def algorithmic_bytes(nspec, nglob, nev, adjoint):
+    """Per-launch algorithmic bytes of the element (forces) kernel: element
+    data once (ibool, kappa, mu: 1,500 B per element), per event the
+    displacement gather (12 B/point) and the acceleration read-modify-write
+    (24 B/point); adjoint launches carry two fields and the mu/kappa kernel
+    read-modify-write (16 B per element point)."""
+    b = nspec * 1500 + nglob * nev * 36
+    if adjoint:
+        b += nglob * nev * 36 + nspec * 125 * nev * 16
+    return b
+
+
+def run_ours(args):
+    import torch
+    from specfwat_b200 import solver as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    E, NS, dt = args.events, args.nstep, 0.02
+
+    db, db_obs, rec, events = make_workload(args.mesh, E, 1000 + rank)
+    srcs = [S.make_source(x, y, z, mt, f0) for (x, y, z, mt, f0) in events]
+
+    # observed data (synthetic, before timing): batched forward on the
+    # anomaly model
+    mesh_obs = S.Mesh(db_obs)
+    so = S.Simulation(mesh_obs, NS, dt, nev=E, use_graph=True,
+                      max_receivers=len(rec))
+    so.set_sources(srcs)
+    so.set_receivers(rec)
+    so.iterate_time(1)
+    obs = [so.seismograms(e).astype(np.float64) for e in range(E)]
+    so.close()
+    mesh_obs.close()
+
+    mesh = S.Mesh(db)
+    result = {}
+
+    # ---- plain path: one event per launch --------------------------------
+    if not args.no_plain:
+        sp = S.Simulation(mesh, NS, dt, nev=1, store="fp32", use_graph=False,
+                          max_receivers=len(rec))
+        sp.set_stream(stream.cuda_stream)
+        sp.set_sources([srcs[0]])
+        sp.set_receivers(rec)
+        sp.set_observed(0, obs[0])
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        for rep in range(2):   # first pass warms up
+            torch.cuda.synchronize()
+            t0.record(stream)
+            sp.iterate_time(1, save_forward=True, synchronize=False)
+            sp.measure_l2_resident(0)
+            sp.iterate_time(3, synchronize=False)
+            t1.record(stream)
+            torch.cuda.synchronize()
+        plain_ms = t0.elapsed_time(t1)
+        fms = sp.time_kernels(1, 20)
+        ams = sp.time_kernels(3, 20)
+        sp.close()
+        result["plain"] = {
+            "events_per_hour": 3600e3 / plain_ms, "ms_per_event": plain_ms,
+            "store": "fp32", "graphs": False,
+            "kernel_ms_fwd": dict(zip(("forces", "stacey", "points", "update"), fms)),
+            "kernel_ms_adj": dict(zip(("forces", "stacey", "points", "update"), ams)),
+        }
+
+    # ---- batched path ------------------------------------------------------
+    sb = S.Simulation(mesh, NS, dt, nev=E, store=args.store, use_graph=True,
+                      graph_steps=50, max_receivers=len(rec))
+    sb.set_stream(stream.cuda_stream)
+    sb.set_sources(srcs)
+    sb.set_receivers(rec)
+    for e in range(E):
+        sb.set_observed(e, obs[e])
+    ne = db.nspec * 125
+    ksum = torch.zeros((6, ne), dtype=torch.float64, device=dev)
+    launches_per_step = [0]
+
+    def step():
+        n = 0
+        sb.iterate_time(1, save_forward=True, synchronize=False)
+        n += sb.launch_count()
+        for e in range(E):
+            sb.measure_l2_resident(e)
+        n += E
+        sb.iterate_time(3, synchronize=False)
+        n += sb.launch_count()
+        sb.sum_kernels_device(ksum.data_ptr())
+        n += E
+        if dist is not None:
+            dist.all_reduce(ksum[:3])
+        launches_per_step[0] = n
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    if dist is not None:
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_per_step = ms / args.steps
+    value = E * world * args.steps / (ms / 1e3) * 3600.0
+
+    # kernel timing for the roofline (same run, further steps)
+    fms = sb.time_kernels(1, 20)
+    ams = sb.time_kernels(3, 20)
+
+    # ---- end to end through the public API from pinned host buffers -------
+    pin_obs = [torch.from_numpy(o).pin_memory() for o in obs]
+    pin_k = torch.empty((6, db.nspec, 5, 5, 5), dtype=torch.float64).pin_memory()
+    pin_seis = torch.empty((E, len(rec), 3, NS), dtype=torch.float32).pin_memory()
+    h2d = sum(o.numel() * 8 for o in pin_obs)
+    d2h = pin_k.numel() * 8 + pin_seis.numel() * 4
+    e2e_ms = []
+    for _ in range(max(1, args.e2e_steps)):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        sb.set_sources(srcs)
+        sb.set_receivers(rec)
+        sb.iterate_time(1, save_forward=True, synchronize=False)
+        for e in range(E):
+            sb.measure_l2(e, pin_obs[e].numpy())
+        sb.iterate_time(3, synchronize=False)
+        for e in range(E):
+            sb.seismograms(e, out=pin_seis[e].numpy())
+        kout = pin_k.numpy()
+        sb.sum_kernels(out=kout)
+        if dist is not None:
+            kt = torch.from_numpy(kout[:3]).to(dev)
+            dist.all_reduce(kt)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - w0) * 1e3)
+    e2e = float(np.mean(e2e_ms))
+    if dist is not None:
+        tt = torch.tensor([e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = float(tt.item())
+    sb.close()
+
+    nglob = db.nglob
+    adj_bytes = algorithmic_bytes(db.nspec, nglob, E, True)
+    fwd_bytes = algorithmic_bytes(db.nspec, nglob, E, False)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    achieved = adj_bytes / (ams[0] * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            tr = json.load(f)
+        key = f"forces_adj_{args.mesh}_nev{E}"
+        if key in tr:
+            traffic = tr[key]["dram_bytes_per_launch"]
+    except Exception:
+        pass
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        sec, nth = cpu_sample(db, db_obs, rec, events[0], NS, 20)
+        cpu = {"value": 3600.0 / sec, "unit": "events/hour", "cores": nth,
+               "kind": "port",
+               "sample": f"20 forward + 20 adjoint/backward steps of one event "
+                         f"(FP32 CPU restatement, OpenMP), extrapolated to NSTEP {NS}"}
+
+    flops_evt_step = 29750 * db.nspec
+    line = {
+        "metric": METRIC, "value": value, "unit": "events/hour",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "events_per_step": E,
+                   "path": f"batched: {E} events per launch, {args.store} "
+                           "per-face-scaled boundary store, CUDA graphs of 50 steps",
+                   "l2": "inputs larger than L2 (per event 151 MB of wavefields "
+                         "+ 2.9 GB boundary store)",
+                   "parallelism": f"events sharded over {world} GPU(s), FP64 "
+                                  "kernel-sum all-reduce per step"},
+        "batched": {"events_per_hour": value, "ms_per_event": ms_per_step / E,
+                    "kernel_ms_fwd": dict(zip(("forces", "stacey", "points",
+                                               "update"), fms)),
+                    "kernel_ms_adj": dict(zip(("forces", "stacey", "points",
+                                               "update"), ams))},
+        "roofline": {"kernel": "k_forces (adjoint+backward, batched)",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": peak_src, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": adj_bytes,
+                     "fwd_achieved": fwd_bytes / (fms[0] * 1e-3) / 1e9,
+                     "fp32_tflops_adj": 2 * flops_evt_step * E / (ams[0] * 1e-3) / 1e12},
+        "e2e": {"value": E * world / (e2e / 1e3) * 3600.0, "unit": "events/hour",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e},
+        "gpu_launches": launches_per_step[0] * args.steps,
+        "clocks": clk,
+    }
+    if "plain" in result:
+        line["plain"] = result["plain"]
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -165,6 +165,23 @@ int sem_save_adjoint_kernels(sem_run *run, int ev, double *out);
 /* FP64 sum of the six kernels over all events of the run, same layout. */
 int sem_sum_kernels(sem_run *run, double *out);
 
+/* Observed data of event ev kept in device memory, [nrec][3][nstep]; a
+ * later sem_measure_l2 with obs == NULL uses it (no host transfer). */
+int sem_set_observed(sem_run *run, int ev, const double *obs);
+
+/* Queue all work of the run on the caller's CUDA stream (a cudaStream_t
+ * passed as void*; NULL restores the run's own stream). */
+int sem_set_stream(sem_run *run, void *stream);
+
+/* FP64 sum of the six kernels over all events into DEVICE memory
+ * dev_out[6][nspec][125] (e.g. a buffer handed to a collective). */
+int sem_sum_kernels_device(sem_run *run, double *dev_out);
+
+/* Average device time in ms of each kernel of one step - forces, stacey,
+ * points, update - measured with CUDA events over nsteps further steps of
+ * the current state (sim_type 1 or 3 kernels).  Advances the wavefields. */
+int sem_time_kernels(sem_run *run, int sim_type, int nsteps, double *ms4);
+
 /* Device-time of the last sem_iterate_time in milliseconds. */
 int sem_last_loop_ms(sem_run *run, double *ms);
 /* Number of kernel launches queued by the last sem_iterate_time. */

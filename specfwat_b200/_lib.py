@@ -28,7 +28,8 @@ EXPORTS = (
     "sem_set_sources", "sem_set_receivers", "sem_iterate_time",
     "sem_synchronize", "sem_get_seismograms", "sem_set_adjoint_sources",
     "sem_measure_l2", "sem_save_adjoint_kernels", "sem_sum_kernels",
-    "sem_last_loop_ms", "sem_last_launch_count",
+    "sem_last_loop_ms", "sem_last_launch_count", "sem_set_observed",
+    "sem_set_stream", "sem_sum_kernels_device", "sem_time_kernels",
 )
 
 
@@ -108,6 +109,10 @@ def load():
         "sem_sum_kernels": (C.c_int, [vp, fp]),
         "sem_last_loop_ms": (C.c_int, [vp, C.POINTER(C.c_double)]),
         "sem_last_launch_count": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+        "sem_set_observed": (C.c_int, [vp, ip, fp]),
+        "sem_set_stream": (C.c_int, [vp, vp]),
+        "sem_sum_kernels_device": (C.c_int, [vp, vp]),
+        "sem_time_kernels": (C.c_int, [vp, ip, ip, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -244,7 +244,8 @@ struct sem_run_s {
   sem_run_cfg cfg{};
   int nev = 1, nstep = 0, nrec_max = 1;
   double dt = 0.0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream work is queued on
+  cudaStream_t own_stream = nullptr;  // the run's own stream
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   DevArray<float> minv;
   DevArray<float> u1, v1, a1, u2, v2, a2;
@@ -256,7 +257,9 @@ struct sem_run_s {
   DevArray<float> scale;
   DevArray<float> k_rho, k_mu, k_kappa;
   DevArray<double> kout, ksum;
-  DevArray<double> obs, taper, simpw, misfit_rc;
+  DevArray<double> obs, taper, simpw, misfit_rc, obs_ev;
+  double taper_pct_cached = -1.0;
+  int taper_type_cached = -1;
   DevArray<int> flag;
   std::vector<int> src_ispec, nrec;
   std::vector<char> have_src, have_rec, have_adj;
@@ -270,7 +273,7 @@ struct sem_run_s {
       if (g) cudaGraphExecDestroy(g);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    if (stream) cudaStreamDestroy(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
     if (mesh) mesh->live_runs--;
   }
 
@@ -530,7 +533,8 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   r->nstep = c->nstep;
   r->dt = c->dt;
   r->nrec_max = c->max_receivers;
-  CK(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&r->own_stream, cudaStreamNonBlocking));
+  r->stream = r->own_stream;
   CK(cudaEventCreate(&r->e0));
   CK(cudaEventCreate(&r->e1));
 
@@ -826,16 +830,16 @@ int sem_set_adjoint_sources(sem_run* r, int ev, const double* adj) {
   return SEM_OK;
 }
 
-int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int taper_type,
-                   double* misfit) {
-  if (!r || !obs) return fail(SEM_ERR_ARG, "null argument");
-  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
-  if (taper_pct < 0.0 || taper_pct > 1.0)
-    return fail(SEM_ERR_ARG, "taper_percentage must be in [0, 1]");
-  if (taper_type < 1 || taper_type > 4) return fail(SEM_ERR_ARG, "taper type must be 1..4");
-  const int ns = r->nstep, nr = r->nrec[ev];
-  if (nr == 0) return fail(SEM_ERR_STATE, "event %d has no receivers", ev);
-  // taper weights (src/shared/signal.f90:419-491)
+// Taper (src/shared/signal.f90:419-491) and Simpson weights
+// (src/shared/utils.f90:1635-1663, as written there) for nstep samples.
+static int prepare_measure(sem_run* r, double taper_pct, int taper_type) {
+  const int ns = r->nstep;
+  if (!r->taper.p) {
+    CKM(r->taper.alloc(ns), "taper");
+    CKM(r->simpw.alloc(ns), "simpson weights");
+    CKM(r->misfit_rc.alloc((size_t)r->nrec_max * 3), "misfits");
+  }
+  if (taper_pct == r->taper_pct_cached && taper_type == r->taper_type_cached) return SEM_OK;
   std::vector<double> w(ns, 1.0);
   const int frac = (taper_pct == 0.0 || taper_pct == 1.0) ? (int)(ns * taper_pct / 2.0)
                                                           : (int)(ns * taper_pct / 2.0 + 0.5);
@@ -854,7 +858,8 @@ int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int 
       w[ns - frac + i] *= tw(frac + i);
     }
   }
-  // Simpson weights of src/shared/utils.f90:1635-1663 (as written there)
+  // The even-count branch weights sample n-1 (1-based) by 1 + 2: the
+  // initial sum holds y(n-1) and the loop adds 2 y(i+1) up to i+1 = n-1.
   std::vector<double> sw(ns, 0.0);
   const double dx = r->dt;
   if (ns >= 2) {
@@ -874,28 +879,61 @@ int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int 
       for (int i = 3; i <= ns - 2; i += 2) sw[i - 1] += 2.0 * dx / 3.0;
     }
   }
-  const size_t nobs = (size_t)nr * 3 * ns;
-  if (r->obs.n < (size_t)r->nrec_max * 3 * ns) {
-    CKM(r->obs.alloc((size_t)r->nrec_max * 3 * ns), "observed data");
-    CKM(r->taper.alloc(ns), "taper");
-    CKM(r->simpw.alloc(ns), "simpson weights");
-    CKM(r->misfit_rc.alloc((size_t)r->nrec_max * 3), "misfits");
-  }
-  CK(cudaMemcpyAsync(r->obs.p, obs, nobs * 8, cudaMemcpyHostToDevice, r->stream));
   CK(cudaMemcpyAsync(r->taper.p, w.data(), ns * 8, cudaMemcpyHostToDevice, r->stream));
   CK(cudaMemcpyAsync(r->simpw.p, sw.data(), ns * 8, cudaMemcpyHostToDevice, r->stream));
-  const size_t off = (size_t)ev * r->nrec_max * 3 * ns;
-  launch_measure_l2(r->seis.p + off, r->obs.p, r->taper.p, r->simpw.p, nr, ns, r->adj.p + off,
+  CK(cudaStreamSynchronize(r->stream));
+  r->taper_pct_cached = taper_pct;
+  r->taper_type_cached = taper_type;
+  return SEM_OK;
+}
+
+int sem_set_observed(sem_run* r, int ev, const double* obs) {
+  if (!r || !obs) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  const size_t per = (size_t)r->nrec_max * 3 * r->nstep;
+  if (!r->obs_ev.p) CKM(r->obs_ev.alloc(per * r->nev), "observed data");
+  CK(cudaMemcpyAsync(r->obs_ev.p + per * ev, obs, (size_t)r->nrec[ev] * 3 * r->nstep * 8,
+                     cudaMemcpyHostToDevice, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int taper_type,
+                   double* misfit) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  if (!(taper_pct >= 0.0 && taper_pct <= 1.0))
+    return fail(SEM_ERR_ARG, "taper_percentage must be in [0, 1]");
+  if (taper_type < 1 || taper_type > 4) return fail(SEM_ERR_ARG, "taper type must be 1..4");
+  const int ns = r->nstep, nr = r->nrec[ev];
+  if (nr == 0) return fail(SEM_ERR_STATE, "event %d has no receivers", ev);
+  if (!obs && !r->obs_ev.p) return fail(SEM_ERR_STATE, "no observed data for event %d", ev);
+  int rc = prepare_measure(r, taper_pct, taper_type);
+  if (rc) return rc;
+  const size_t per = (size_t)r->nrec_max * 3 * ns;
+  const double* dobs;
+  if (obs) {
+    if (!r->obs.p) CKM(r->obs.alloc(per), "observed data");
+    CK(cudaMemcpyAsync(r->obs.p, obs, (size_t)nr * 3 * ns * 8, cudaMemcpyHostToDevice,
+                       r->stream));
+    dobs = r->obs.p;
+  } else {
+    dobs = r->obs_ev.p + per * ev;
+  }
+  const size_t off = (size_t)ev * per;
+  launch_measure_l2(r->seis.p + off, dobs, r->taper.p, r->simpw.p, nr, ns, r->adj.p + off,
                     r->misfit_rc.p, r->stream);
   CK(cudaGetLastError());
-  std::vector<double> m((size_t)nr * 3);
-  CK(cudaMemcpyAsync(m.data(), r->misfit_rc.p, m.size() * 8, cudaMemcpyDeviceToHost,
-                     r->stream));
-  CK(cudaStreamSynchronize(r->stream));
-  double total = 0.0;
-  for (double v : m) total += v;
-  if (misfit) *misfit = total;
   r->have_adj[ev] = 1;
+  if (misfit) {
+    std::vector<double> m((size_t)nr * 3);
+    CK(cudaMemcpyAsync(m.data(), r->misfit_rc.p, m.size() * 8, cudaMemcpyDeviceToHost,
+                       r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    double total = 0.0;
+    for (double v : m) total += v;
+    *misfit = total;
+  }
   return SEM_OK;
 }
 
@@ -926,6 +964,74 @@ int sem_sum_kernels(sem_run* r, double* out) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, r->ksum.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
   CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_sum_kernels_device(sem_run* r, double* dev_out) {
+  if (!r || !dev_out) return fail(SEM_ERR_ARG, "null argument");
+  if (!r->adj_done) return fail(SEM_ERR_STATE, "no adjoint run has completed");
+  const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+  CK(cudaMemsetAsync(dev_out, 0, 6 * ne * 8, r->stream));
+  for (int e = 0; e < r->nev; ++e)
+    launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p,
+                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->nev, e, nullptr, dev_out,
+                            r->stream);
+  CK(cudaGetLastError());
+  return SEM_OK;
+}
+
+int sem_set_stream(sem_run* r, void* stream) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  CK(cudaStreamSynchronize(r->stream));
+  r->stream = stream ? (cudaStream_t)stream : r->own_stream;
+  return SEM_OK;
+}
+
+int sem_time_kernels(sem_run* r, int sim_type, int nsteps, double* ms4) {
+  if (!r || !ms4) return fail(SEM_ERR_ARG, "null argument");
+  if (sim_type != 1 && sim_type != 3) return fail(SEM_ERR_ARG, "sim_type must be 1 or 3");
+  if (nsteps < 1 || nsteps >= r->nstep) return fail(SEM_ERR_ARG, "nsteps must be in [1, nstep)");
+  const bool adj = sim_type == 3;
+  if (adj && (!r->u2.p || !r->k_rho.p))
+    return fail(SEM_ERR_STATE, "sim_type 3 timing needs a completed adjoint run");
+  if (!adj && !r->have_src[0]) return fail(SEM_ERR_STATE, "sources not set");
+  if (r->mesh->nf > 0 && !r->store.p) {
+    int rc = ensure_store(r);
+    if (rc) return rc;
+  }
+  // lanes at step 1 so that every kernel does its full work (backward
+  // scatter, store replay and source are skipped at step 0)
+  r->fill_lanes(adj ? PH_ADJ : PH_FWD, adj ? 0 : 1);
+  for (auto& L : r->h_lanes) L.it0 = 1;
+  CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
+                     r->stream));
+  std::vector<cudaEvent_t> ev(5 * nsteps);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  StepArgs a = r->args(adj);
+  for (int s = 0; s < nsteps; ++s) {
+    a.s = s;
+    cudaEvent_t* E = &ev[5 * s];
+    CK(cudaEventRecord(E[0], r->stream));
+    launch_forces(a, adj, r->stream);
+    CK(cudaEventRecord(E[1], r->stream));
+    launch_boundary(a, adj, r->stream);
+    CK(cudaEventRecord(E[2], r->stream));
+    launch_points(a, r->stream);
+    CK(cudaEventRecord(E[3], r->stream));
+    launch_update(a, adj, r->stream);
+    CK(cudaEventRecord(E[4], r->stream));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(r->stream));
+  double acc[4] = {0, 0, 0, 0};
+  for (int s = 0; s < nsteps; ++s)
+    for (int k = 0; k < 4; ++k) {
+      float f = 0.f;
+      CK(cudaEventElapsedTime(&f, ev[5 * s + k], ev[5 * s + k + 1]));
+      acc[k] += f;
+    }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < 4; ++k) ms4[k] = acc[k] / nsteps;
   return SEM_OK;
 }
 

@@ -259,7 +259,7 @@ def gaussian_random_field(box: BoxSpec, corr_len: float, seed: int,
     K2 = (k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2
           + kz[None, None, :] ** 2)
     filt = np.exp(-K2 * corr_len * corr_len / 8.0)
-    field = np.fft.irfftn(np.fft.rfftn(noise) * filt, s=n)
+    field = np.fft.irfftn(np.fft.rfftn(noise) * filt, s=n, axes=(0, 1, 2))
     i0 = int(round(pad / spacing))
     nb = [int(math.ceil(L / spacing)) + 1 for L in (box.lx, box.ly, box.lz)]
     g = field[i0:i0 + nb[0], i0:i0 + nb[1], i0:i0 + nb[2]]

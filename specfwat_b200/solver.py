@@ -141,8 +141,11 @@ class Simulation:
     def synchronize(self):
         check(_lib.load().sem_synchronize(self._h))
 
-    def seismograms(self, ev: int = 0) -> np.ndarray:
-        out = np.zeros((self.nrec[ev], 3, self.nstep), np.float32)
+    def seismograms(self, ev: int = 0, out=None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.nrec[ev], 3, self.nstep), np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous
+        assert out.size == self.nrec[ev] * 3 * self.nstep
         check(_lib.load().sem_get_seismograms(self._h, ev, out.ctypes.data))
         return out
 
@@ -160,14 +163,50 @@ class Simulation:
                                          C.byref(m)))
         return m.value
 
+    def set_observed(self, ev: int, obs):
+        """Keep observed data of ``ev`` in device memory for measure_l2."""
+        obs = np.ascontiguousarray(obs, np.float64)
+        assert obs.shape == (self.nrec[ev], 3, self.nstep)
+        check(_lib.load().sem_set_observed(self._h, ev, obs.ctypes.data))
+
+    def measure_l2_resident(self, ev: int, taper_pct=0.05, taper_type=1,
+                            want_misfit=False):
+        """L2 measurement against the device-resident observed data."""
+        m = C.c_double()
+        check(_lib.load().sem_measure_l2(
+            self._h, ev, None, float(taper_pct), int(taper_type),
+            C.byref(m) if want_misfit else None))
+        return m.value if want_misfit else None
+
+    def set_stream(self, stream_handle: int):
+        """Queue the run's device work on a caller CUDA stream (handle as an
+        integer, e.g. ``torch.cuda.current_stream().cuda_stream``)."""
+        check(_lib.load().sem_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def sum_kernels_device(self, dev_ptr: int):
+        """FP64 cross-event kernel sum into device memory [6, nspec, 125]."""
+        check(_lib.load().sem_sum_kernels_device(self._h, C.c_void_p(dev_ptr)))
+
+    def time_kernels(self, sim_type: int, nsteps: int):
+        """Average ms of (forces, stacey, points, update) over nsteps steps."""
+        ms = (C.c_double * 4)()
+        check(_lib.load().sem_time_kernels(self._h, sim_type, nsteps, ms))
+        return list(ms)
+
     # save_adjoint_kernels
-    def save_adjoint_kernels(self, ev: int = 0) -> np.ndarray:
-        out = np.zeros((6, self.mesh.nspec, 5, 5, 5), np.float64)
+    def save_adjoint_kernels(self, ev: int = 0, out=None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((6, self.mesh.nspec, 5, 5, 5), np.float64)
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        assert out.size == 6 * self.mesh.nspec * 125
         check(_lib.load().sem_save_adjoint_kernels(self._h, ev, out.ctypes.data))
         return out
 
-    def sum_kernels(self) -> np.ndarray:
-        out = np.zeros((6, self.mesh.nspec, 5, 5, 5), np.float64)
+    def sum_kernels(self, out=None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((6, self.mesh.nspec, 5, 5, 5), np.float64)
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        assert out.size == 6 * self.mesh.nspec * 125
         check(_lib.load().sem_sum_kernels(self._h, out.ctypes.data))
         return out
 
