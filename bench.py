@@ -224,7 +224,12 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):
+        return _run_ours(args, torch, S, dist, world, rank, local, dev, stream)
+
+
+def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
     E, NS, dt = args.events, args.nstep, 0.02
 
     db, db_obs, rec, events = make_workload(args.mesh, E, 1000 + rank)

@@ -101,6 +101,8 @@ typedef struct {
   int graph_steps;    /* steps per captured graph (0 = default 50)         */
   int max_receivers;  /* receivers per event upper bound (>= 1)            */
   int check_every;    /* steps between non-finite checks (0 = off)         */
+  int kernel_variant; /* element kernel: 0 default, 1 thread-per-point,
+                         2 pencil decomposition                            */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard

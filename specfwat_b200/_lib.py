@@ -62,7 +62,7 @@ class RunCfg(C.Structure):
     _fields_ = [("nev", C.c_int), ("nstep", C.c_int), ("dt", C.c_double),
                 ("store_kind", C.c_int), ("use_graph", C.c_int),
                 ("graph_steps", C.c_int), ("max_receivers", C.c_int),
-                ("check_every", C.c_int)]
+                ("check_every", C.c_int), ("kernel_variant", C.c_int)]
 
 
 class Source(C.Structure):

@@ -76,6 +76,7 @@ struct StepArgs {
   float dt;
   int store_fp16;
   int nrec_max;
+  int variant;           // element kernel: 0 thread-per-point, 1 pencil
 };
 
 // Launch helpers (defined in sem_kernels.cu).  Each returns the number of

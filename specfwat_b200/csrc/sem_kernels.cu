@@ -245,6 +245,385 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// element kernel, pencil decomposition
+// ---------------------------------------------------------------------------
+//
+// Each element is worked by 25 "pencil" threads per lane.  Thread t takes
+// three roles: owner of the xi-pencil (j,k) = (t%5, t/5), of the eta-pencil
+// (i,k) and of the gamma-pencil (i,j).  Along its own pencil every
+// contraction is register-local with the GLL matrices as immediates; the
+// other two directions are exchanged through shared memory, so one element
+// costs about 235 shared accesses per pencil thread instead of the ~130 per
+// GLL point of a thread-per-point kernel (~3x fewer per element).
+//
+//   gather        u -> U                      (cooperative, coalesced)
+//   eta/gamma     U -> d_eta, d_gamma -> A
+//   xi            U, A -> gradient -> stress -> B (sigma for eta/gamma),
+//                 f_xi in registers, strain products (adjoint)
+//   eta/gamma     B -> f_eta, f_gamma -> A
+//   xi            A + f_xi -> scatter-add into accel
+
+// D[i][l] = l_l'(xi_i) and DWt[i][l] = w_l D[l][i] for the GLL nodes
+// (-1, -sqrt(3/7), 0, sqrt(3/7), 1): double-precision values rounded to
+// float, identical to the host-built tables.  Only ever indexed with
+// compile-time constants (fully unrolled loops), so they fold to immediates.
+__device__ __forceinline__ float gD(int i, int l) {
+  constexpr float t[25] = {
+      -5.0f, 6.7565024887242409f, -2.6666666666666674f, 1.410164177942427f, -0.5f,
+      -1.2409902530309822f, -4.4408920985006262e-16f, 1.7457431218879393f,
+      -0.76376261582597327f, 0.25900974696901707f,
+      0.37499999999999989f, -1.3365845776954535f, 0.0f, 1.3365845776954532f,
+      -0.37499999999999989f,
+      -0.25900974696901713f, 0.76376261582597349f, -1.7457431218879396f,
+      4.4408920985006262e-16f, 1.2409902530309824f,
+      0.5f, -1.4101641779424272f, 2.6666666666666674f, -6.75650248872424f, 5.0f};
+  return t[i * 5 + l];
+}
+__device__ __forceinline__ float gDWt(int i, int l) {
+  constexpr float t[25] = {
+      -0.5f, -0.67565024887242353f, 0.26666666666666661f, -0.14101641779424265f,
+      0.050000000000000003f,
+      0.67565024887242409f, -2.4178190314058963e-16f, -0.95046014413898916f,
+      0.41582631306080775f, -0.14101641779424273f,
+      -0.26666666666666677f, 0.95046014413898916f, 0.0f, -0.95046014413898927f,
+      0.26666666666666677f,
+      0.1410164177942427f, -0.41582631306080764f, 0.95046014413898905f,
+      2.4178190314058963e-16f, -0.67565024887242409f,
+      -0.050000000000000003f, 0.14101641779424262f, -0.26666666666666661f,
+      0.67565024887242375f, 0.5f};
+  return t[i * 5 + l];
+}
+__device__ __forceinline__ float gW(int i) {
+  constexpr float t[5] = {0.10000000000000001f, 0.5444444444444444f, 0.71111111111111114f,
+                          0.5444444444444444f, 0.10000000000000001f};
+  return t[i];
+}
+
+// shared floats per (field, element, lane): U/B region then A region
+constexpr int PR_U = 640;  // >= 625 (B: 5 sigma components)
+constexpr int PR_A = 768;  // >= 750 (6 derivative / divergence components)
+constexpr int PR_F = PR_U + PR_A;
+
+template <int LB>
+struct PencilBuf {
+  float* base;  // this (field, element) block, lane offset applied
+  __device__ __forceinline__ float& U(int c, int p) const { return base[(c * 125 + p) * LB]; }
+  __device__ __forceinline__ float& B(int q, int p) const { return base[(q * 125 + p) * LB]; }
+  __device__ __forceinline__ float& Ar(int q, int p) const {
+    return base[(PR_U + q * 125 + p) * LB];
+  }
+};
+
+// eta / gamma derivative roles of thread t (pencils (i,k) and (i,j)).
+template <int LB>
+__device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t, float xix) {
+  const int pi = t % 5, pq = t / 5;
+  // eta-pencil (i = pi, k = pq): d/d eta at (pi, j, pq)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float v[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) v[l] = b.U(c, pi + 5 * l + 25 * pq);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      float s = 0.f;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) s = fmaf(gD(j, l), v[l], s);
+      b.Ar(c, pi + 5 * j + 25 * pq) = xix * s;
+    }
+  }
+  // gamma-pencil (i = pi, j = pq): d/d gamma at (pi, pq, k)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float v[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) v[l] = b.U(c, pi + 5 * pq + 25 * l);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      float s = 0.f;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) s = fmaf(gD(k, l), v[l], s);
+      b.Ar(3 + c, pi + 5 * pq + 25 * k) = xix * s;
+    }
+  }
+}
+
+// xi role of thread t: full gradient on its xi-pencil (j,k) = (t%5, t/5).
+// g[i][c][d] = d u_c / d x_d at (i, j, k).
+template <int LB>
+__device__ __forceinline__ void pencil_grad_xi(const PencilBuf<LB>& b, int t, float xix,
+                                               float g[5][3][3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float v[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) v[l] = b.U(c, l + 5 * t);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      float s = 0.f;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) s = fmaf(gD(i, l), v[l], s);
+      g[i][c][0] = xix * s;
+      g[i][c][1] = b.Ar(c, i + 5 * t);
+      g[i][c][2] = b.Ar(3 + c, i + 5 * t);
+    }
+  }
+}
+
+// Stress on the xi-pencil, sigma components for the other roles into B
+// (xy, yy, yz, xz, zz) and the xi part of the divergence in registers.
+template <int LB>
+__device__ __forceinline__ void pencil_stress(const PencilBuf<LB>& b, int t, const float g[5][3][3],
+                                              const float* s_kap, const float* s_mu, float fac,
+                                              float fx[5][3]) {
+  float sxx[5], sxy[5], sxz[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    float sig[6];
+    stress_point(g[i], s_kap[p], s_mu[p], fac, sig);
+    sxx[i] = sig[0];
+    sxy[i] = sig[3];
+    sxz[i] = sig[4];
+    b.B(0, p) = sig[3];  // xy
+    b.B(1, p) = sig[1];  // yy
+    b.B(2, p) = sig[5];  // yz
+    b.B(3, p) = sig[4];  // xz
+    b.B(4, p) = sig[2];  // zz
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      ax = fmaf(gDWt(i, l), sxx[l], ax);
+      ay = fmaf(gDWt(i, l), sxy[l], ay);
+      az = fmaf(gDWt(i, l), sxz[l], az);
+    }
+    fx[i][0] = ax;
+    fx[i][1] = ay;
+    fx[i][2] = az;
+  }
+}
+
+// eta / gamma divergence roles: B -> A.
+template <int LB>
+__device__ __forceinline__ void pencil_div_eg(const PencilBuf<LB>& b, int t) {
+  const int pi = t % 5, pq = t / 5;
+  {  // eta-pencil (i = pi, k = pq): sigma_{c,y} = (xy, yy, yz) = B0, B1, B2
+    float v[3][5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      const int p = pi + 5 * l + 25 * pq;
+      v[0][l] = b.B(0, p);
+      v[1][l] = b.B(1, p);
+      v[2][l] = b.B(2, p);
+    }
+#pragma unroll
+    for (int j = 0; j < 5; ++j)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float s = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) s = fmaf(gDWt(j, l), v[c][l], s);
+        b.Ar(c, pi + 5 * j + 25 * pq) = s;
+      }
+  }
+  {  // gamma-pencil (i = pi, j = pq): sigma_{c,z} = (xz, yz, zz) = B3, B2, B4
+    float v[3][5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      const int p = pi + 5 * pq + 25 * l;
+      v[0][l] = b.B(3, p);
+      v[1][l] = b.B(2, p);
+      v[2][l] = b.B(4, p);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float s = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) s = fmaf(gDWt(k, l), v[c][l], s);
+        b.Ar(3 + c, pi + 5 * pq + 25 * k) = s;
+      }
+  }
+}
+
+// xi role: total force on the xi-pencil and scatter-add.
+template <int LB>
+__device__ __forceinline__ void pencil_scatter(const PencilBuf<LB>& b, int t, const float fx[5][3],
+                                               const int* s_ib, float* acc, int nev, int lg) {
+  const int pj = t % 5, pk = t / 5;
+  float wj = 0.f, wk = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q == pj) wj = gW(q);
+    if (q == pk) wk = gW(q);
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    const size_t ig = (size_t)s_ib[p];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float f = -(wj * wk * fx[i][c] + gW(i) * wk * b.Ar(c, p) + gW(i) * wj * b.Ar(3 + c, p));
+      atomicAdd(&acc[(ig * 3 + c) * nev + lg], f);
+    }
+  }
+}
+
+template <int LB, int EPB, bool ADJ>
+__global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
+  constexpr int NT = EPB * 25 * LB;
+  constexpr int NF = ADJ ? 2 : 1;
+  extern __shared__ float sm[];
+  __shared__ int s_ib[EPB * NGLL3];
+  __shared__ float s_kap[EPB * NGLL3], s_mu[EPB * NGLL3];
+  __shared__ unsigned char s_act[2][LB];
+
+  const int tid = threadIdx.x;
+  const int lane = tid % LB;
+  const int t = (tid / LB) % 25;
+  const int el = tid / (25 * LB);
+  const int e = blockIdx.x * EPB + el;
+  const int lg = blockIdx.y * LB + lane;
+  const int nev = A.nev;
+
+  bool any = false;
+  if (tid < LB) {
+    bool a1 = false, a2 = false;
+    const int l2 = blockIdx.y * LB + tid;
+    if (l2 < nev) {
+      const LaneDesc* L = A.lanes + l2;
+      const int it = L->it0 + A.s;
+      if (L->phase != PH_IDLE && it < L->nstep) {
+        a1 = true;
+        // at it == 0 of the adjoint phase the backward strain is still
+        // needed (kernels); only its scatter is skipped
+        a2 = ADJ && L->phase == PH_ADJ;
+      }
+    }
+    s_act[0][tid] = a1;
+    s_act[1][tid] = a2;
+    any = a1;
+  }
+  if (!__syncthreads_or(any)) return;
+  bool scat2 = false;
+  if (ADJ && lg < nev) {
+    const LaneDesc* L = A.lanes + lg;
+    scat2 = s_act[1][lane] && (L->it0 + A.s) > 0;
+  }
+
+  for (int idx = tid; idx < EPB * NGLL3; idx += NT) {
+    const int e2 = blockIdx.x * EPB + idx / NGLL3;
+    if (e2 < A.m.nspec) {
+      const size_t ep = (size_t)blockIdx.x * EPB * NGLL3 + idx;
+      s_ib[idx] = A.m.ibool[ep];
+      s_kap[idx] = A.m.kappa[ep];
+      s_mu[idx] = A.m.mu[ep];
+    } else {
+      s_ib[idx] = -1;
+      s_kap[idx] = 0.f;
+      s_mu[idx] = 0.f;
+    }
+  }
+  __syncthreads();
+  // cooperative gather of the displacement of every (field, element, lane)
+#pragma unroll 1
+  for (int f = 0; f < NF; ++f) {
+    const float* src = f == 0 ? A.f1.u : A.f2.u;
+    for (int idx = tid; idx < EPB * NGLL3 * 3 * LB; idx += NT) {
+      const int ln = idx % LB;
+      const int r = idx / LB;
+      const int c = r % 3;
+      const int r2 = r / 3;
+      const int p = r2 % NGLL3;
+      const int e2 = r2 / NGLL3;
+      const int ig = s_ib[e2 * NGLL3 + p];
+      const int l2 = blockIdx.y * LB + ln;
+      float v = 0.f;
+      if (ig >= 0 && s_act[f][ln]) v = src[((size_t)ig * 3 + c) * nev + l2];
+      sm[((f * EPB + e2) * PR_F + c * NGLL3 + p) * LB + ln] = v;
+    }
+  }
+  __syncthreads();
+
+  const float xix = A.m.xix, fac = A.m.jac * A.m.xix;
+  PencilBuf<LB> b1{sm + ((0 * EPB + el) * PR_F) * LB + lane};
+  PencilBuf<LB> b2{sm + ((1 * EPB + el) * PR_F) * LB + lane};
+  pencil_grad_eg<LB>(b1, t, xix);
+  if (ADJ) pencil_grad_eg<LB>(b2, t, xix);
+  __syncthreads();
+
+  const float* kap = s_kap + el * NGLL3;
+  const float* mu = s_mu + el * NGLL3;
+  float fx1[5][3], fx2[ADJ ? 5 : 1][3];
+  if (ADJ) {
+    float g2[5][3][3];
+    pencil_grad_xi<LB>(b2, t, xix, g2);
+    float e2v[5][6];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const float tr = g2[i][0][0] + g2[i][1][1] + g2[i][2][2];
+      e2v[i][0] = g2[i][0][0] - tr * (1.0f / 3.0f);
+      e2v[i][1] = g2[i][1][1] - tr * (1.0f / 3.0f);
+      e2v[i][2] = 0.5f * (g2[i][0][1] + g2[i][1][0]);
+      e2v[i][3] = 0.5f * (g2[i][0][2] + g2[i][2][0]);
+      e2v[i][4] = 0.5f * (g2[i][1][2] + g2[i][2][1]);
+      e2v[i][5] = tr;
+    }
+    pencil_stress<LB>(b2, t, g2, kap, mu, fac, fx2);
+    float g1[5][3][3];
+    pencil_grad_xi<LB>(b1, t, xix, g1);
+    if (s_act[1][lane] && e < A.m.nspec) {
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const float tr1 = g1[i][0][0] + g1[i][1][1] + g1[i][2][2];
+        const float a_xx = g1[i][0][0] - tr1 * (1.0f / 3.0f);
+        const float a_yy = g1[i][1][1] - tr1 * (1.0f / 3.0f);
+        const float a_xy = 0.5f * (g1[i][0][1] + g1[i][1][0]);
+        const float a_xz = 0.5f * (g1[i][0][2] + g1[i][2][0]);
+        const float a_yz = 0.5f * (g1[i][1][2] + g1[i][2][1]);
+        const float* bv = e2v[i];
+        const float dd = a_xx * bv[0] + a_yy * bv[1] + (a_xx + a_yy) * (bv[0] + bv[1]) +
+                         2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
+        const size_t q = ((size_t)e * NGLL3 + i + 5 * t) * nev + lg;
+        A.k.mu[q] += A.dt * dd;
+        A.k.kappa[q] += A.dt * (tr1 * bv[5]);
+      }
+    }
+    pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
+  } else {
+    float g1[5][3][3];
+    pencil_grad_xi<LB>(b1, t, xix, g1);
+    pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
+  }
+  __syncthreads();
+  pencil_div_eg<LB>(b1, t);
+  if (ADJ) pencil_div_eg<LB>(b2, t);
+  __syncthreads();
+  if (e < A.m.nspec) {
+    const int* ib = s_ib + el * NGLL3;
+    if (s_act[0][lane]) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, nev, lg);
+    if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, nev, lg);
+  }
+}
+
+template <int LB, int EPB, bool ADJ>
+static void forces_pencil_cfg(const StepArgs& a, cudaStream_t st) {
+  const size_t shm = (size_t)(ADJ ? 2 : 1) * EPB * PR_F * LB * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_forces_pencil<LB, EPB, ADJ>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    attr = true;
+  }
+  dim3 grid((a.m.nspec + EPB - 1) / EPB, (a.nev + LB - 1) / LB);
+  k_forces_pencil<LB, EPB, ADJ><<<grid, EPB * 25 * LB, shm, st>>>(a);
+}
+
 template <int LB, int NT, bool ADJ>
 static void forces_cfg(const StepArgs& a, cudaStream_t st) {
   const size_t shm = (size_t)(ADJ ? 2 : 1) * 6 * NGLL3 * LB * sizeof(float);
@@ -259,6 +638,25 @@ static void forces_cfg(const StepArgs& a, cudaStream_t st) {
 }
 
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.variant == 1) {
+    if (a.nev == 1) {
+      if (adj)
+        forces_pencil_cfg<1, 5, true>(a, st);
+      else
+        forces_pencil_cfg<1, 5, false>(a, st);
+    } else if (a.nev <= 4) {
+      if (adj)
+        forces_pencil_cfg<4, 1, true>(a, st);
+      else
+        forces_pencil_cfg<4, 1, false>(a, st);
+    } else {
+      if (adj)
+        forces_pencil_cfg<8, 1, true>(a, st);
+      else
+        forces_pencil_cfg<8, 1, false>(a, st);
+    }
+    return 1;
+  }
   if (a.nev == 1) {
     if (adj)
       forces_cfg<1, 128, true>(a, st);

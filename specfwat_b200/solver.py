@@ -106,13 +106,14 @@ class Simulation:
     def __init__(self, mesh: Mesh, nstep: int, dt: float, nev: int = 1,
                  store: str = "fp32", use_graph: bool = False,
                  graph_steps: int = 50, max_receivers: int = 128,
-                 check_every: int = 0):
+                 check_every: int = 0, kernel_variant: int = 0):
         L = _lib.load()
         self.mesh = mesh
         self.nstep, self.dt, self.nev = nstep, dt, nev
         kind = {"fp32": _lib.SEM_STORE_FP32, "fp16": _lib.SEM_STORE_FP16}[store]
         self.cfg = _lib.RunCfg(nev, nstep, dt, kind, int(use_graph),
-                               graph_steps, max_receivers, check_every)
+                               graph_steps, max_receivers, check_every,
+                               kernel_variant)
         h = C.c_void_p()
         check(L.sem_prepare_timerun(mesh.handle, C.byref(self.cfg), C.byref(h)))
         self._h = h

@@ -29,11 +29,13 @@ def small():
     return db, rec, mt
 
 
-def test_forward_plain_matches_oracle(gpu, small):
+@pytest.mark.parametrize("variant", [1, 2])
+def test_forward_plain_matches_oracle(gpu, small, variant):
     db, rec, mt = small
     nstep, dt = 400, 0.02
     mesh = S.Mesh(db)
-    sim = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec))
+    sim = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec),
+                       kernel_variant=variant)
     sim.set_sources([S.make_source(20000., 20000., -10000., mt, 1.0)])
     sim.set_receivers(rec)
     sim.iterate_time(1)
@@ -81,10 +83,12 @@ def mini_adjoint():
     return db, rec, mt, src_xyz, nstep, dt, obs
 
 
-def test_adjoint_kernels_match_oracle(gpu, mini_adjoint):
+@pytest.mark.parametrize("variant", [1, 2])
+def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
-    sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec))
+    sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec),
+                       kernel_variant=variant)
     sim.set_sources([S.make_source(*sxyz, mt, 1.0)])
     sim.set_receivers(rec)
     sim.iterate_time(1, save_forward=True)
@@ -109,20 +113,23 @@ def test_adjoint_kernels_match_oracle(gpu, mini_adjoint):
         assert e64 < KERN_TOL, (name, e64)
 
 
-def test_batched_equals_plain(gpu, small):
+@pytest.mark.parametrize("variant,nev", [(1, 5), (2, 3), (2, 11)])
+def test_batched_equals_plain(gpu, small, variant, nev):
     db, rec, _ = small
-    nstep, dt, nev = 200, 0.02, 5
+    nstep, dt = 200, 0.02
     rng = np.random.default_rng(99)
     srcs = [S.make_source(rng.uniform(8e3, 32e3), rng.uniform(8e3, 32e3),
                           -rng.uniform(5e3, 30e3), D.random_moment_tensor(rng),
                           rng.uniform(0.5, 1.5)) for _ in range(nev)]
     mesh = S.Mesh(db)
-    b = S.Simulation(mesh, nstep, dt, nev=nev, max_receivers=len(rec))
+    b = S.Simulation(mesh, nstep, dt, nev=nev, max_receivers=len(rec),
+                     kernel_variant=variant)
     b.set_sources(srcs)
     b.set_receivers(rec)
     b.iterate_time(1)
     for e in range(nev):
-        p = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec))
+        p = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec),
+                         kernel_variant=1)
         p.set_sources([srcs[e]])
         p.set_receivers(rec)
         p.iterate_time(1)
@@ -146,24 +153,25 @@ def test_graph_equals_stepwise(gpu, small):
     assert rel_l2(out[1], out[0]) < 1e-5
 
 
-def test_batched_adjoint_fp16_store(gpu, mini_adjoint):
+@pytest.mark.parametrize("nev", [2, 9])
+def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
     kern = {}
     for store in ("fp32", "fp16"):
-        sim = S.Simulation(mesh, nstep, dt, nev=2, store=store, use_graph=True,
+        sim = S.Simulation(mesh, nstep, dt, nev=nev, store=store, use_graph=True,
                            max_receivers=len(rec))
-        sim.set_sources([S.make_source(*sxyz, mt, 1.0)] * 2)
+        sim.set_sources([S.make_source(*sxyz, mt, 1.0)] * nev)
         sim.set_receivers(rec)
         sim.iterate_time(1, save_forward=True)
-        for e in range(2):
+        for e in range(nev):
             sim.measure_l2(e, obs)
         sim.iterate_time(3)
         kern[store] = sim.sum_kernels()
         k0 = sim.save_adjoint_kernels(0)
-        k1 = sim.save_adjoint_kernels(1)
+        k1 = sim.save_adjoint_kernels(nev - 1)
         assert rel_l2(k0[:3], k1[:3]) < 1e-5
-        assert rel_l2(kern[store][:3], 2 * k0[:3]) < 1e-5
+        assert rel_l2(kern[store][:3], nev * k0[:3]) < 1e-5
         sim.close()
     for q in range(3):
         assert rel_l2(kern["fp16"][q], kern["fp32"][q]) < 5e-3
