@@ -102,7 +102,8 @@ typedef struct {
   int max_receivers;  /* receivers per event upper bound (>= 1)            */
   int check_every;    /* steps between non-finite checks (0 = off)         */
   int kernel_variant; /* element kernel: 0 default, 1 thread-per-point,
-                         2 pencil decomposition                            */
+                         2 pencil decomposition, 3 pencil, persistent and
+                         cp.async-pipelined                                */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard

@@ -295,7 +295,8 @@ struct sem_run_s {
     a.dt = (float)dt;
     a.store_fp16 = cfg.store_kind == SEM_STORE_FP16;
     a.nrec_max = nrec_max;
-    a.variant = cfg.kernel_variant == 1 ? 0 : 1;
+    // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined
+    a.variant = cfg.kernel_variant == 1 ? 0 : cfg.kernel_variant == 2 ? 1 : 2;
     return a;
   }
 
@@ -499,8 +500,8 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->max_receivers < 1 || c->max_receivers > 100000)
     return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
-  if (c->kernel_variant < 0 || c->kernel_variant > 2)
-    return fail(SEM_ERR_ARG, "kernel_variant must be 0, 1 or 2");
+  if (c->kernel_variant < 0 || c->kernel_variant > 3)
+    return fail(SEM_ERR_ARG, "kernel_variant must be 0..3");
   return SEM_OK;
 }
 

@@ -307,12 +307,11 @@ constexpr int PR_F = PR_U + PR_A;
 
 template <int LB>
 struct PencilBuf {
-  float* base;  // this (field, element) block, lane offset applied
-  __device__ __forceinline__ float& U(int c, int p) const { return base[(c * 125 + p) * LB]; }
-  __device__ __forceinline__ float& B(int q, int p) const { return base[(q * 125 + p) * LB]; }
-  __device__ __forceinline__ float& Ar(int q, int p) const {
-    return base[(PR_U + q * 125 + p) * LB];
-  }
+  float* ub;  // U/B region of this (field, element), lane offset applied
+  float* ab;  // A region
+  __device__ __forceinline__ float& U(int c, int p) const { return ub[(c * 125 + p) * LB]; }
+  __device__ __forceinline__ float& B(int q, int p) const { return ub[(q * 125 + p) * LB]; }
+  __device__ __forceinline__ float& Ar(int q, int p) const { return ab[(q * 125 + p) * LB]; }
 };
 
 // eta / gamma derivative roles of thread t (pencils (i,k) and (i,j)).
@@ -551,8 +550,10 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   __syncthreads();
 
   const float xix = A.m.xix, fac = A.m.jac * A.m.xix;
-  PencilBuf<LB> b1{sm + ((0 * EPB + el) * PR_F) * LB + lane};
-  PencilBuf<LB> b2{sm + ((1 * EPB + el) * PR_F) * LB + lane};
+  float* f1b = sm + ((0 * EPB + el) * PR_F) * LB + lane;
+  float* f2b = sm + ((1 * EPB + el) * PR_F) * LB + lane;
+  PencilBuf<LB> b1{f1b, f1b + PR_U * LB};
+  PencilBuf<LB> b2{f2b, f2b + PR_U * LB};
   pencil_grad_eg<LB>(b1, t, xix);
   if (ADJ) pencil_grad_eg<LB>(b2, t, xix);
   __syncthreads();
@@ -611,6 +612,264 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// element kernel, pencil decomposition, persistent and software-pipelined
+// ---------------------------------------------------------------------------
+//
+// Persistent blocks walk element groups g, g + gridDim.x, ...  While group
+// k is computed, cp.async (LDGSTS) copies already bring the displacement
+// gather, kappa/mu and (adjoint) kernel accumulators of group k+1 and the
+// ibool of group k+2 into shared memory, so the gather latency that stalls
+// a one-shot element kernel overlaps the arithmetic of the previous group.
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// shared floats of the pipelined kernel per (field, element, lane)
+constexpr int PP_U = 625;  // U (3 comps) then B (5 sigma comps)
+constexpr int PP_A = 750;  // d_eta/d_gamma, then f_eta/f_gamma
+
+template <int LB, int EPB, int TPE, bool ADJ>
+struct PipeLayout {
+  static constexpr int NF = ADJ ? 2 : 1;
+  static constexpr int NE = EPB * NGLL3;                     // element points per group
+  static constexpr int OFF_IB = 0;                           // int [3][NE]
+  static constexpr int OFF_KM = OFF_IB + 3 * NE;             // float [2][2][NE] kappa, mu
+  static constexpr int OFF_U = OFF_KM + 4 * NE;              // float [2][NF][EPB][PP_U*LB]
+  static constexpr int OFF_A = OFF_U + 2 * NF * EPB * PP_U * LB;   // [NF][EPB][PP_A*LB]
+  static constexpr int OFF_K = OFF_A + NF * EPB * PP_A * LB; // [2][2][NE*LB] mu/kappa acc
+  static constexpr int TOTAL = OFF_K + (ADJ ? 4 * NE * LB : 0);
+  static constexpr size_t BYTES = (size_t)TOTAL * 4;
+};
+
+template <int LB, int EPB, int TPE, bool ADJ>
+__global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int ngroups) {
+  using LY = PipeLayout<LB, EPB, TPE, ADJ>;
+  constexpr int NT = EPB * TPE * LB;
+  constexpr int NE = LY::NE;
+  constexpr int NF = LY::NF;
+  extern __shared__ float sm[];
+  int* sIB = (int*)(sm + LY::OFF_IB);
+  float* sKM = sm + LY::OFF_KM;
+  float* sU = sm + LY::OFF_U;
+  float* sA = sm + LY::OFF_A;
+  float* sK = sm + LY::OFF_K;
+  __shared__ unsigned char s_act[2][LB];
+  __shared__ unsigned char s_scat2[LB];
+
+  const int tid = threadIdx.x;
+  const int lane = tid % LB;
+  const int t = (tid / LB) % TPE;
+  const int el = tid / (TPE * LB);
+  const bool pen = t < 25;
+  const int lg = blockIdx.y * LB + lane;
+  const int nev = A.nev;
+  const int nspec = A.m.nspec;
+
+  bool any = false;
+  if (tid < LB) {
+    bool a1 = false, a2 = false, sc = false;
+    const int l2 = blockIdx.y * LB + tid;
+    if (l2 < nev) {
+      const LaneDesc* L = A.lanes + l2;
+      const int it = L->it0 + A.s;
+      if (L->phase != PH_IDLE && it < L->nstep) {
+        a1 = true;
+        a2 = ADJ && L->phase == PH_ADJ;
+        sc = a2 && it > 0;
+      }
+    }
+    s_act[0][tid] = a1;
+    s_act[1][tid] = a2;
+    s_scat2[tid] = sc;
+    any = a1;
+  }
+  if (!__syncthreads_or(any)) return;
+  const bool act1 = s_act[0][lane], act2 = ADJ && s_act[1][lane];
+  const bool scat2 = ADJ && s_scat2[lane];
+
+  // ---- copy helpers --------------------------------------------------------
+  auto issue_ib = [&](int g, int slot) {
+    int* dst = sIB + slot * NE;
+    for (int i = tid; i < NE; i += NT) {
+      const int e = g * EPB + i / NGLL3;
+      if (g < ngroups && e < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)g * NE + i);
+      else
+        dst[i] = -1;
+    }
+  };
+  auto issue_data = [&](int g, int ibslot, int buf) {
+    if (g >= ngroups) return;
+    const int* ib = sIB + ibslot * NE;
+    float* km = sKM + buf * 2 * NE;
+    for (int i = tid; i < NE; i += NT) {
+      const int e = g * EPB + i / NGLL3;
+      if (e < nspec) {
+        cp_async4(km + i, A.m.kappa + (size_t)g * NE + i);
+        cp_async4(km + NE + i, A.m.mu + (size_t)g * NE + i);
+      }
+    }
+    if (pen) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const bool act = f == 0 ? act1 : act2;
+        const float* src = f == 0 ? A.f1.u : A.f2.u;
+        float* ub = sU + (((buf * NF + f) * EPB + el) * PP_U) * LB + lane;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+          const int p = t + 25 * r;
+          const int ig = ib[el * NGLL3 + p];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float* d = ub + (c * NGLL3 + p) * LB;
+            if (act && ig >= 0)
+              cp_async4(d, src + ((size_t)ig * 3 + c) * nev + lg);
+            else
+              *d = 0.f;
+          }
+        }
+      }
+      if (ADJ && act2) {
+        const int e = g * EPB + el;
+        float* kb = sK + buf * 2 * NE * LB;
+        if (e < nspec) {
+#pragma unroll
+          for (int r = 0; r < 5; ++r) {
+            const int p = t + 25 * r;
+            const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
+            cp_async4(kb + (el * NGLL3 + p) * LB + lane, A.k.mu + q);
+            cp_async4(kb + (NE + el * NGLL3 + p) * LB + lane, A.k.kappa + q);
+          }
+        }
+      }
+    }
+  };
+
+  // ---- prologue --------------------------------------------------------------
+  int g = blockIdx.x;
+  issue_ib(g, 0);
+  cp_commit();
+  cp_wait_all();
+  __syncthreads();
+  issue_data(g, 0, 0);
+  issue_ib(g + gridDim.x, 1);
+  cp_commit();
+
+  const float xix = A.m.xix, fac = A.m.jac * A.m.xix;
+  for (int k = 0; g < ngroups; ++k, g += gridDim.x) {
+    const int buf = k & 1;
+    const int ibs = k % 3;
+    cp_wait_all();
+    __syncthreads();
+    // prefetch the next group while this one is computed
+    issue_data(g + gridDim.x, (k + 1) % 3, buf ^ 1);
+    issue_ib(g + 2 * gridDim.x, (k + 2) % 3);
+    cp_commit();
+
+    const int e = g * EPB + el;
+    const float* kap = sKM + buf * 2 * NE + el * NGLL3;
+    const float* mu = kap + NE;
+    float* u1 = sU + (((buf * NF + 0) * EPB + el) * PP_U) * LB + lane;
+    float* u2 = sU + (((buf * NF + (NF - 1)) * EPB + el) * PP_U) * LB + lane;
+    float* a1 = sA + ((0 * EPB + el) * PP_A) * LB + lane;
+    float* a2 = sA + (((NF - 1) * EPB + el) * PP_A) * LB + lane;
+    PencilBuf<LB> b1{u1, a1};
+    PencilBuf<LB> b2{u2, a2};
+    if (pen) {
+      pencil_grad_eg<LB>(b1, t, xix);
+      if (ADJ) pencil_grad_eg<LB>(b2, t, xix);
+    }
+    __syncthreads();
+    float fx1[5][3], fx2[ADJ ? 5 : 1][3];
+    if (pen) {
+      if (ADJ) {
+        float g2[5][3][3];
+        pencil_grad_xi<LB>(b2, t, xix, g2);
+        float e2v[5][6];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const float tr = g2[i][0][0] + g2[i][1][1] + g2[i][2][2];
+          e2v[i][0] = g2[i][0][0] - tr * (1.0f / 3.0f);
+          e2v[i][1] = g2[i][1][1] - tr * (1.0f / 3.0f);
+          e2v[i][2] = 0.5f * (g2[i][0][1] + g2[i][1][0]);
+          e2v[i][3] = 0.5f * (g2[i][0][2] + g2[i][2][0]);
+          e2v[i][4] = 0.5f * (g2[i][1][2] + g2[i][2][1]);
+          e2v[i][5] = tr;
+        }
+        pencil_stress<LB>(b2, t, g2, kap, mu, fac, fx2);
+        float g1[5][3][3];
+        pencil_grad_xi<LB>(b1, t, xix, g1);
+        if (act2 && e < nspec) {
+          const float* kb = sK + buf * 2 * NE * LB;
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            const float tr1 = g1[i][0][0] + g1[i][1][1] + g1[i][2][2];
+            const float a_xx = g1[i][0][0] - tr1 * (1.0f / 3.0f);
+            const float a_yy = g1[i][1][1] - tr1 * (1.0f / 3.0f);
+            const float a_xy = 0.5f * (g1[i][0][1] + g1[i][1][0]);
+            const float a_xz = 0.5f * (g1[i][0][2] + g1[i][2][0]);
+            const float a_yz = 0.5f * (g1[i][1][2] + g1[i][2][1]);
+            const float* bv = e2v[i];
+            const float dd = a_xx * bv[0] + a_yy * bv[1] + (a_xx + a_yy) * (bv[0] + bv[1]) +
+                             2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
+            const int p = i + 5 * t;
+            const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
+            A.k.mu[q] = kb[(el * NGLL3 + p) * LB + lane] + A.dt * dd;
+            A.k.kappa[q] = kb[(NE + el * NGLL3 + p) * LB + lane] + A.dt * (tr1 * bv[5]);
+          }
+        }
+        pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
+      } else {
+        float g1[5][3][3];
+        pencil_grad_xi<LB>(b1, t, xix, g1);
+        pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
+      }
+    }
+    __syncthreads();
+    if (pen) {
+      pencil_div_eg<LB>(b1, t);
+      if (ADJ) pencil_div_eg<LB>(b2, t);
+    }
+    __syncthreads();
+    if (pen && e < nspec) {
+      const int* ib = sIB + ibs * NE + el * NGLL3;
+      if (act1) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, nev, lg);
+      if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, nev, lg);
+    }
+  }
+  cp_wait_all();
+}
+
+template <int LB, int EPB, int TPE, bool ADJ>
+static void forces_piped_cfg(const StepArgs& a, cudaStream_t st) {
+  using LY = PipeLayout<LB, EPB, TPE, ADJ>;
+  constexpr int NT = EPB * TPE * LB;
+  static int blocks_per_sm = 0, sms = 0;
+  if (!blocks_per_sm) {
+    cudaFuncSetAttribute(k_forces_piped<LB, EPB, TPE, ADJ>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
+                                                  k_forces_piped<LB, EPB, TPE, ADJ>, NT,
+                                                  LY::BYTES);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const int ngroups = (a.m.nspec + EPB - 1) / EPB;
+  const int nchunk = (a.nev + LB - 1) / LB;
+  int gx = (blocks_per_sm * sms + nchunk - 1) / nchunk;
+  if (gx > ngroups) gx = ngroups;
+  if (gx < 1) gx = 1;
+  dim3 grid(gx, nchunk);
+  k_forces_piped<LB, EPB, TPE, ADJ><<<grid, NT, LY::BYTES, st>>>(a, ngroups);
+}
+
 template <int LB, int EPB, bool ADJ>
 static void forces_pencil_cfg(const StepArgs& a, cudaStream_t st) {
   const size_t shm = (size_t)(ADJ ? 2 : 1) * EPB * PR_F * LB * sizeof(float);
@@ -638,6 +897,25 @@ static void forces_cfg(const StepArgs& a, cudaStream_t st) {
 }
 
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.variant == 2) {
+    if (a.nev == 1) {
+      if (adj)
+        forces_piped_cfg<1, 4, 32, true>(a, st);
+      else
+        forces_piped_cfg<1, 4, 32, false>(a, st);
+    } else if (a.nev <= 4) {
+      if (adj)
+        forces_piped_cfg<4, 1, 25, true>(a, st);
+      else
+        forces_piped_cfg<4, 1, 25, false>(a, st);
+    } else {
+      if (adj)
+        forces_piped_cfg<4, 1, 25, true>(a, st);
+      else
+        forces_piped_cfg<8, 1, 25, false>(a, st);
+    }
+    return 1;
+  }
   if (a.variant == 1) {
     if (a.nev == 1) {
       if (adj)
