@@ -185,6 +185,13 @@ int sem_sum_kernels_device(sem_run *run, double *dev_out);
  * the current state (sim_type 1 or 3 kernels).  Advances the wavefields. */
 int sem_time_kernels(sem_run *run, int sim_type, int nsteps, double *ms4);
 
+/* Element-kernel variants in use for the forward and adjoint phases
+ * (1 thread-per-point, 2 pencil, 3 pencil pipelined, 4 pencil pipelined
+ * with 2 events per block).  With kernel_variant = 0 the first
+ * sem_iterate_time times the candidates on this run and keeps the fastest
+ * per phase; -1 until then. */
+int sem_kernel_variants(sem_run *run, int *fwd, int *adj);
+
 /* Device-time of the last sem_iterate_time in milliseconds. */
 int sem_last_loop_ms(sem_run *run, double *ms);
 /* Number of kernel launches queued by the last sem_iterate_time. */

@@ -30,6 +30,7 @@ EXPORTS = (
     "sem_measure_l2", "sem_save_adjoint_kernels", "sem_sum_kernels",
     "sem_last_loop_ms", "sem_last_launch_count", "sem_set_observed",
     "sem_set_stream", "sem_sum_kernels_device", "sem_time_kernels",
+    "sem_kernel_variants",
 )
 
 
@@ -113,6 +114,7 @@ def load():
         "sem_set_stream": (C.c_int, [vp, vp]),
         "sem_sum_kernels_device": (C.c_int, [vp, vp]),
         "sem_time_kernels": (C.c_int, [vp, ip, ip, C.POINTER(C.c_double)]),
+        "sem_kernel_variants": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

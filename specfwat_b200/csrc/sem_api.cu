@@ -14,6 +14,7 @@
 // are advanced by a kernel at the end of each graph, so the graph needs no
 // parameter updates between replays.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -176,6 +177,7 @@ struct sem_mesh_s {
   int nspec = 0, nglob = 0, nf = 0;
   float xix = 0.f, jac = 0.f;
   DevArray<int> ibool;
+  DevArray<int> order;
   DevArray<float> kappa, mu, rho;
   DevArray<int> f_iglob;
   DevArray<float> f_rvp, f_rvs, f_jw, f_n;
@@ -196,6 +198,7 @@ struct sem_mesh_s {
     v.xix = xix;
     v.jac = jac;
     v.ibool = ibool.p;
+    v.order = order.p;
     v.kappa = kappa.p;
     v.mu = mu.p;
     v.f_iglob = f_iglob.p;
@@ -206,7 +209,7 @@ struct sem_mesh_s {
     return v;
   }
   size_t device_bytes() const {
-    return ibool.bytes() + kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
+    return ibool.bytes() + order.bytes() + kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
            f_rvp.bytes() + f_rvs.bytes() + f_jw.bytes() + f_n.bytes();
   }
 
@@ -265,6 +268,7 @@ struct sem_run_s {
   std::vector<char> have_src, have_rec, have_adj;
   bool fwd_saved = false, adj_done = false;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int variant[2] = {-1, -1};  // element-kernel variant per phase (fwd, adj)
   double last_ms = 0.0;
   long long last_launches = 0;
 
@@ -295,8 +299,13 @@ struct sem_run_s {
     a.dt = (float)dt;
     a.store_fp16 = cfg.store_kind == SEM_STORE_FP16;
     a.nrec_max = nrec_max;
-    // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined
-    a.variant = cfg.kernel_variant == 1 ? 0 : cfg.kernel_variant == 2 ? 1 : 2;
+    // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined;
+    // 0 = chosen by the autotuner per phase
+    const int v = variant[adjoint ? 1 : 0];
+    a.variant = cfg.kernel_variant == 1   ? 0
+                : cfg.kernel_variant == 2 ? 1
+                : cfg.kernel_variant == 3 ? 2
+                : (v >= 0 ? v : 2);
     return a;
   }
 
@@ -412,6 +421,34 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
         return fail(SEM_ERR_ARG, "element %d has non-positive extent along axis %d", e, k);
     }
   }
+  // Element traversal order: Morton (Z-curve) order of the element centres
+  // on a 1024^3 lattice over the mesh bounding box, so that the elements in
+  // flight at one time form a compact 3-D region whose shared GLL points
+  // stay in L2 across all event lanes.
+  std::vector<int> order(d->nspec);
+  {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int e = 0; e < d->nspec; ++e)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], m->centre[(size_t)e * 3 + k]);
+        hi[k] = std::max(hi[k], m->centre[(size_t)e * 3 + k]);
+      }
+    std::vector<std::pair<unsigned long long, int>> key(d->nspec);
+    for (int e = 0; e < d->nspec; ++e) {
+      unsigned q[3];
+      for (int k = 0; k < 3; ++k) {
+        const double span = hi[k] - lo[k];
+        const double v = span > 0 ? (m->centre[(size_t)e * 3 + k] - lo[k]) / span : 0.0;
+        q[k] = (unsigned)std::min(1023.0, std::max(0.0, std::floor(v * 1023.0 + 0.5)));
+      }
+      unsigned long long code = 0;
+      for (int b = 9; b >= 0; --b)
+        for (int k = 2; k >= 0; --k) code = (code << 1) | ((q[k] >> b) & 1u);
+      key[e] = {code, e};
+    }
+    std::sort(key.begin(), key.end());
+    for (int e = 0; e < d->nspec; ++e) order[e] = key[e].second;
+  }
   // absorbing faces: per face point global index and coefficients
   m->h_f_iglob.resize((size_t)nf * NGLL2);
   m->h_f_rvp.resize((size_t)nf * NGLL2);
@@ -438,6 +475,7 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
     }
   }
   CKM(m->ibool.alloc(ne), "ibool");
+  CKM(m->order.alloc(d->nspec), "element order");
   CKM(m->kappa.alloc(ne), "kappastore");
   CKM(m->mu.alloc(ne), "mustore");
   CKM(m->rho.alloc(ne), "rhostore");
@@ -447,6 +485,7 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
   CKM(m->f_jw.alloc((size_t)nf * NGLL2), "face jacobian2Dw");
   CKM(m->f_n.alloc((size_t)nf * NGLL2 * 3), "face normal");
   CK(cudaMemcpy(m->ibool.p, m->h_ibool.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m->order.p, order.data(), d->nspec * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m->kappa.p, d->kappastore, ne * sizeof(float), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m->mu.p, d->mustore, ne * sizeof(float), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m->rho.p, d->rhostore, ne * sizeof(float), cudaMemcpyHostToDevice));
@@ -696,6 +735,72 @@ static int ensure_store(sem_run* r) {
   return SEM_OK;
 }
 
+// Autotuner: time each element-kernel variant of a phase over a few steps
+// of the current run (its own event count, lanes per block and mesh) and
+// keep the fastest.  Runs on scratch state before the forward run: the
+// forward zeroes its wavefields and the adjoint run rebuilds its own.
+static int autotune_phase(sem_run* r, bool adj) {
+  const int cands_multi[] = {0, 2, 3};
+  const int cands_single[] = {0, 2};
+  const int* cands = r->nev > 1 ? cands_multi : cands_single;
+  const int ncand = r->nev > 1 ? 3 : 2;
+  const int nsteps = std::max(1, std::min(8, r->nstep - 2));
+  r->fill_lanes(adj ? PH_ADJ : PH_FWD, 0);
+  for (auto& L : r->h_lanes) L.it0 = 1;
+  CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
+                     r->stream));
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  double best = 1e300;
+  int bestv = 2;
+  for (int ci = 0; ci < ncand; ++ci) {
+    r->variant[adj ? 1 : 0] = cands[ci];
+    StepArgs a = r->args(adj);
+    a.s = 0;
+    launch_forces(a, adj, r->stream);  // warm-up (first-launch set-up)
+    CK(cudaEventRecord(t0, r->stream));
+    for (int s = 0; s < nsteps; ++s) {
+      a.s = s;
+      launch_forces(a, adj, r->stream);
+    }
+    CK(cudaEventRecord(t1, r->stream));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, t0, t1));
+    if (ms < best) {
+      best = ms;
+      bestv = cands[ci];
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  r->variant[adj ? 1 : 0] = bestv;
+  return SEM_OK;
+}
+
+static int ensure_tuned(sem_run* r) {
+  if (r->cfg.kernel_variant != 0 || (r->variant[0] >= 0 && r->variant[1] >= 0)) return SEM_OK;
+  if (r->nstep < 3) {
+    r->variant[0] = r->variant[1] = 2;
+    return SEM_OK;
+  }
+  int rc = ensure_adjoint_buffers(r);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(r->u2.p, 0, r->u2.bytes(), r->stream));
+  CK(cudaMemsetAsync(r->v2.p, 0, r->v2.bytes(), r->stream));
+  CK(cudaMemsetAsync(r->a2.p, 0, r->a2.bytes(), r->stream));
+  rc = autotune_phase(r, false);
+  if (rc) return rc;
+  rc = autotune_phase(r, true);
+  if (rc) return rc;
+  // discard the kernel products accumulated while timing
+  CK(cudaMemsetAsync(r->k_mu.p, 0, r->k_mu.bytes(), r->stream));
+  CK(cudaMemsetAsync(r->k_kappa.p, 0, r->k_kappa.bytes(), r->stream));
+  return SEM_OK;
+}
+
 // Queue the step loop of one phase (graphs or per-step launches).
 static int run_loop(sem_run* r, bool adjoint) {
   long long launches = 0;
@@ -750,6 +855,8 @@ int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
     for (int e = 0; e < r->nev; ++e)
       if (!r->have_src[e] || !r->have_rec[e])
         return fail(SEM_ERR_STATE, "event %d has no source or receivers", e);
+    int trc = ensure_tuned(r);
+    if (trc) return trc;
     if (save_forward) {
       int rc = ensure_store(r);
       if (rc) return rc;
@@ -1036,6 +1143,18 @@ int sem_time_kernels(sem_run* r, int sim_type, int nsteps, double* ms4) {
     }
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < 4; ++k) ms4[k] = acc[k] / nsteps;
+  return SEM_OK;
+}
+
+int sem_kernel_variants(sem_run* r, int* fwd, int* adj) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  // internal 0..3 -> public 1..4
+  auto pub = [&](int ph) {
+    if (r->cfg.kernel_variant != 0) return r->cfg.kernel_variant;
+    return r->variant[ph] < 0 ? -1 : r->variant[ph] + 1;
+  };
+  if (fwd) *fwd = pub(0);
+  if (adj) *adj = pub(1);
   return SEM_OK;
 }
 

@@ -43,6 +43,7 @@ struct MeshView {
   int nspec, nglob, nf;
   float xix, jac;
   const int* ibool;      // [nspec*125]
+  const int* order;      // [nspec] element traversal order (Morton curve)
   const float* kappa;    // [nspec*125]
   const float* mu;       // [nspec*125]
   const int* f_iglob;    // [nf*25]

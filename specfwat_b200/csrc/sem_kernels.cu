@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
   float* b1 = sm;
   float* b2 = sm + 6 * NGLL3 * LB;
 
-  const int e = blockIdx.x;
+  const int e = A.m.order[blockIdx.x];
   const int lane = threadIdx.x % LB;
   const int pg = threadIdx.x / LB;
   const int lg = blockIdx.y * LB + lane;
@@ -315,8 +315,10 @@ struct PencilBuf {
 };
 
 // eta / gamma derivative roles of thread t (pencils (i,k) and (i,j)).
+// Derivatives are left in reference coordinates; the regular-element
+// factor xix is folded into the stress and strain-product scalings.
 template <int LB>
-__device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t, float xix) {
+__device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t) {
   const int pi = t % 5, pq = t / 5;
   // eta-pencil (i = pi, k = pq): d/d eta at (pi, j, pq)
 #pragma unroll
@@ -329,7 +331,7 @@ __device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t, fl
       float s = 0.f;
 #pragma unroll
       for (int l = 0; l < 5; ++l) s = fmaf(gD(j, l), v[l], s);
-      b.Ar(c, pi + 5 * j + 25 * pq) = xix * s;
+      b.Ar(c, pi + 5 * j + 25 * pq) = s;
     }
   }
   // gamma-pencil (i = pi, j = pq): d/d gamma at (pi, pq, k)
@@ -343,16 +345,15 @@ __device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t, fl
       float s = 0.f;
 #pragma unroll
       for (int l = 0; l < 5; ++l) s = fmaf(gD(k, l), v[l], s);
-      b.Ar(3 + c, pi + 5 * pq + 25 * k) = xix * s;
+      b.Ar(3 + c, pi + 5 * pq + 25 * k) = s;
     }
   }
 }
 
 // xi role of thread t: full gradient on its xi-pencil (j,k) = (t%5, t/5).
-// g[i][c][d] = d u_c / d x_d at (i, j, k).
+// g[i][c][d] = d u_c / d xi_d at (i, j, k) (times xix: d u_c / d x_d).
 template <int LB>
-__device__ __forceinline__ void pencil_grad_xi(const PencilBuf<LB>& b, int t, float xix,
-                                               float g[5][3][3]) {
+__device__ __forceinline__ void pencil_grad_xi(const PencilBuf<LB>& b, int t, float g[5][3][3]) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     float v[5];
@@ -363,7 +364,7 @@ __device__ __forceinline__ void pencil_grad_xi(const PencilBuf<LB>& b, int t, fl
       float s = 0.f;
 #pragma unroll
       for (int l = 0; l < 5; ++l) s = fmaf(gD(i, l), v[l], s);
-      g[i][c][0] = xix * s;
+      g[i][c][0] = s;
       g[i][c][1] = b.Ar(c, i + 5 * t);
       g[i][c][2] = b.Ar(3 + c, i + 5 * t);
     }
@@ -486,7 +487,8 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   const int lane = tid % LB;
   const int t = (tid / LB) % 25;
   const int el = tid / (25 * LB);
-  const int e = blockIdx.x * EPB + el;
+  const int eslot = blockIdx.x * EPB + el;
+  const int e = eslot < A.m.nspec ? A.m.order[eslot] : A.m.nspec;
   const int lg = blockIdx.y * LB + lane;
   const int nev = A.nev;
 
@@ -516,9 +518,9 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   }
 
   for (int idx = tid; idx < EPB * NGLL3; idx += NT) {
-    const int e2 = blockIdx.x * EPB + idx / NGLL3;
-    if (e2 < A.m.nspec) {
-      const size_t ep = (size_t)blockIdx.x * EPB * NGLL3 + idx;
+    const int s2 = blockIdx.x * EPB + idx / NGLL3;
+    if (s2 < A.m.nspec) {
+      const size_t ep = (size_t)A.m.order[s2] * NGLL3 + idx % NGLL3;
       s_ib[idx] = A.m.ibool[ep];
       s_kap[idx] = A.m.kappa[ep];
       s_mu[idx] = A.m.mu[ep];
@@ -549,13 +551,16 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   }
   __syncthreads();
 
-  const float xix = A.m.xix, fac = A.m.jac * A.m.xix;
+  // gradients stay in reference coordinates: stress scale jac*xix*xix,
+  // strain products scale xix^2
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  const float dtk = A.dt * A.m.xix * A.m.xix;
   float* f1b = sm + ((0 * EPB + el) * PR_F) * LB + lane;
   float* f2b = sm + ((1 * EPB + el) * PR_F) * LB + lane;
   PencilBuf<LB> b1{f1b, f1b + PR_U * LB};
   PencilBuf<LB> b2{f2b, f2b + PR_U * LB};
-  pencil_grad_eg<LB>(b1, t, xix);
-  if (ADJ) pencil_grad_eg<LB>(b2, t, xix);
+  pencil_grad_eg<LB>(b1, t);
+  if (ADJ) pencil_grad_eg<LB>(b2, t);
   __syncthreads();
 
   const float* kap = s_kap + el * NGLL3;
@@ -563,7 +568,7 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   float fx1[5][3], fx2[ADJ ? 5 : 1][3];
   if (ADJ) {
     float g2[5][3][3];
-    pencil_grad_xi<LB>(b2, t, xix, g2);
+    pencil_grad_xi<LB>(b2, t, g2);
     float e2v[5][6];
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -577,7 +582,7 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
     }
     pencil_stress<LB>(b2, t, g2, kap, mu, fac, fx2);
     float g1[5][3][3];
-    pencil_grad_xi<LB>(b1, t, xix, g1);
+    pencil_grad_xi<LB>(b1, t, g1);
     if (s_act[1][lane] && e < A.m.nspec) {
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
@@ -591,14 +596,14 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
         const float dd = a_xx * bv[0] + a_yy * bv[1] + (a_xx + a_yy) * (bv[0] + bv[1]) +
                          2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
         const size_t q = ((size_t)e * NGLL3 + i + 5 * t) * nev + lg;
-        A.k.mu[q] += A.dt * dd;
-        A.k.kappa[q] += A.dt * (tr1 * bv[5]);
+        A.k.mu[q] += dtk * dd;
+        A.k.kappa[q] += dtk * (tr1 * bv[5]);
       }
     }
     pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
   } else {
     float g1[5][3][3];
-    pencil_grad_xi<LB>(b1, t, xix, g1);
+    pencil_grad_xi<LB>(b1, t, g1);
     pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
   }
   __syncthreads();
@@ -696,9 +701,9 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
   auto issue_ib = [&](int g, int slot) {
     int* dst = sIB + slot * NE;
     for (int i = tid; i < NE; i += NT) {
-      const int e = g * EPB + i / NGLL3;
-      if (g < ngroups && e < nspec)
-        cp_async4(dst + i, A.m.ibool + (size_t)g * NE + i);
+      const int es = g * EPB + i / NGLL3;
+      if (g < ngroups && es < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[es] * NGLL3 + i % NGLL3);
       else
         dst[i] = -1;
     }
@@ -708,10 +713,11 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
     const int* ib = sIB + ibslot * NE;
     float* km = sKM + buf * 2 * NE;
     for (int i = tid; i < NE; i += NT) {
-      const int e = g * EPB + i / NGLL3;
-      if (e < nspec) {
-        cp_async4(km + i, A.m.kappa + (size_t)g * NE + i);
-        cp_async4(km + NE + i, A.m.mu + (size_t)g * NE + i);
+      const int es = g * EPB + i / NGLL3;
+      if (es < nspec) {
+        const size_t ep = (size_t)A.m.order[es] * NGLL3 + i % NGLL3;
+        cp_async4(km + i, A.m.kappa + ep);
+        cp_async4(km + NE + i, A.m.mu + ep);
       }
     }
     if (pen) {
@@ -735,9 +741,10 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
         }
       }
       if (ADJ && act2) {
-        const int e = g * EPB + el;
+        const int es = g * EPB + el;
         float* kb = sK + buf * 2 * NE * LB;
-        if (e < nspec) {
+        if (es < nspec) {
+          const int e = A.m.order[es];
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
             const int p = t + 25 * r;
@@ -760,7 +767,10 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
   issue_ib(g + gridDim.x, 1);
   cp_commit();
 
-  const float xix = A.m.xix, fac = A.m.jac * A.m.xix;
+  // gradients stay in reference coordinates: stress scale jac*xix*xix,
+  // strain products scale xix^2
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  const float dtk = A.dt * A.m.xix * A.m.xix;
   for (int k = 0; g < ngroups; ++k, g += gridDim.x) {
     const int buf = k & 1;
     const int ibs = k % 3;
@@ -771,7 +781,8 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
     issue_ib(g + 2 * gridDim.x, (k + 2) % 3);
     cp_commit();
 
-    const int e = g * EPB + el;
+    const int es = g * EPB + el;
+    const int e = es < nspec ? A.m.order[es] : nspec;
     const float* kap = sKM + buf * 2 * NE + el * NGLL3;
     const float* mu = kap + NE;
     float* u1 = sU + (((buf * NF + 0) * EPB + el) * PP_U) * LB + lane;
@@ -781,15 +792,15 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
     PencilBuf<LB> b1{u1, a1};
     PencilBuf<LB> b2{u2, a2};
     if (pen) {
-      pencil_grad_eg<LB>(b1, t, xix);
-      if (ADJ) pencil_grad_eg<LB>(b2, t, xix);
+      pencil_grad_eg<LB>(b1, t);
+      if (ADJ) pencil_grad_eg<LB>(b2, t);
     }
     __syncthreads();
     float fx1[5][3], fx2[ADJ ? 5 : 1][3];
     if (pen) {
       if (ADJ) {
         float g2[5][3][3];
-        pencil_grad_xi<LB>(b2, t, xix, g2);
+        pencil_grad_xi<LB>(b2, t, g2);
         float e2v[5][6];
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
@@ -803,7 +814,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
         }
         pencil_stress<LB>(b2, t, g2, kap, mu, fac, fx2);
         float g1[5][3][3];
-        pencil_grad_xi<LB>(b1, t, xix, g1);
+        pencil_grad_xi<LB>(b1, t, g1);
         if (act2 && e < nspec) {
           const float* kb = sK + buf * 2 * NE * LB;
 #pragma unroll
@@ -819,14 +830,14 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
                              2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
             const int p = i + 5 * t;
             const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
-            A.k.mu[q] = kb[(el * NGLL3 + p) * LB + lane] + A.dt * dd;
-            A.k.kappa[q] = kb[(NE + el * NGLL3 + p) * LB + lane] + A.dt * (tr1 * bv[5]);
+            A.k.mu[q] = kb[(el * NGLL3 + p) * LB + lane] + dtk * dd;
+            A.k.kappa[q] = kb[(NE + el * NGLL3 + p) * LB + lane] + dtk * (tr1 * bv[5]);
           }
         }
         pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
       } else {
         float g1[5][3][3];
-        pencil_grad_xi<LB>(b1, t, xix, g1);
+        pencil_grad_xi<LB>(b1, t, g1);
         pencil_stress<LB>(b1, t, g1, kap, mu, fac, fx1);
       }
     }
@@ -896,8 +907,18 @@ static void forces_cfg(const StepArgs& a, cudaStream_t st) {
   k_forces<LB, NT, ADJ><<<grid, NT, shm, st>>>(a);
 }
 
+// Element-kernel variants (StepArgs::variant):
+//   0 thread-per-point, 1 pencil, 2 pencil pipelined (lanes per block by
+//   event count), 3 pencil pipelined with 2 lanes per block.
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
-  if (a.variant == 2) {
+  if (a.variant == 3 && a.nev > 1) {
+    if (adj)
+      forces_piped_cfg<2, 2, 25, true>(a, st);
+    else
+      forces_piped_cfg<2, 2, 25, false>(a, st);
+    return 1;
+  }
+  if (a.variant == 2 || a.variant == 3) {
     if (a.nev == 1) {
       if (adj)
         forces_piped_cfg<1, 4, 32, true>(a, st);

@@ -49,7 +49,8 @@ def main(argv=None):
     sim.iterate_time(3)
     adj_ms = sim.loop_ms()
     out = {"mesh": a.mesh, "nev": a.nev, "nstep": a.nstep,
-           "variant": a.variant, "fwd_ms_per_step": fwd_ms / a.nstep,
+           "variant": a.variant, "variants_used": sim.kernel_variants(),
+           "fwd_ms_per_step": fwd_ms / a.nstep,
            "adj_ms_per_step": adj_ms / a.nstep}
     if a.time_steps:
         names = ("forces", "stacey", "points", "update")

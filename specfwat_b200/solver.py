@@ -211,6 +211,12 @@ class Simulation:
         check(_lib.load().sem_sum_kernels(self._h, out.ctypes.data))
         return out
 
+    def kernel_variants(self):
+        """(forward, adjoint) element-kernel variants in use."""
+        f, a = C.c_int(), C.c_int()
+        check(_lib.load().sem_kernel_variants(self._h, C.byref(f), C.byref(a)))
+        return f.value, a.value
+
     def loop_ms(self) -> float:
         ms = C.c_double()
         check(_lib.load().sem_last_loop_ms(self._h, C.byref(ms)))

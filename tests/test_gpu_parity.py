@@ -29,7 +29,7 @@ def small():
     return db, rec, mt
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_forward_plain_matches_oracle(gpu, small, variant):
     db, rec, mt = small
     nstep, dt = 400, 0.02
@@ -83,7 +83,7 @@ def mini_adjoint():
     return db, rec, mt, src_xyz, nstep, dt, obs
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
@@ -113,7 +113,8 @@ def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
         assert e64 < KERN_TOL, (name, e64)
 
 
-@pytest.mark.parametrize("variant,nev", [(1, 5), (2, 3), (2, 11), (3, 3), (3, 11)])
+@pytest.mark.parametrize("variant,nev", [(1, 5), (2, 3), (2, 11), (3, 3), (3, 11),
+                                         (4, 3), (4, 6), (0, 7)])
 def test_batched_equals_plain(gpu, small, variant, nev):
     db, rec, _ = small
     nstep, dt = 300, 0.02
