@@ -101,9 +101,10 @@ typedef struct {
   int graph_steps;    /* steps per captured graph (0 = default 50)         */
   int max_receivers;  /* receivers per event upper bound (>= 1)            */
   int check_every;    /* steps between non-finite checks (0 = off)         */
-  int kernel_variant; /* element kernel: 0 default, 1 thread-per-point,
-                         2 pencil decomposition, 3 pencil, persistent and
-                         cp.async-pipelined                                */
+  int kernel_variant; /* element kernel: 0 autotuned per phase,
+                         1 thread-per-point, 2 pencil decomposition,
+                         3 pencil, persistent and cp.async-pipelined,
+                         4 as 3 with 2 events per block                    */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard

@@ -302,10 +302,7 @@ struct sem_run_s {
     // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined;
     // 0 = chosen by the autotuner per phase
     const int v = variant[adjoint ? 1 : 0];
-    a.variant = cfg.kernel_variant == 1   ? 0
-                : cfg.kernel_variant == 2 ? 1
-                : cfg.kernel_variant == 3 ? 2
-                : (v >= 0 ? v : 2);
+    a.variant = cfg.kernel_variant > 0 ? cfg.kernel_variant - 1 : (v >= 0 ? v : 2);
     return a;
   }
 
@@ -539,8 +536,8 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->max_receivers < 1 || c->max_receivers > 100000)
     return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
-  if (c->kernel_variant < 0 || c->kernel_variant > 3)
-    return fail(SEM_ERR_ARG, "kernel_variant must be 0..3");
+  if (c->kernel_variant < 0 || c->kernel_variant > 4)
+    return fail(SEM_ERR_ARG, "kernel_variant must be 0..4");
   return SEM_OK;
 }
 
