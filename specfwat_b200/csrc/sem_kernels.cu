@@ -651,8 +651,26 @@ struct PipeLayout {
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
 
+// Work items are (lane chunk, element group) pairs walked chunk-major, so
+// all resident blocks sweep the mesh for one group of event lanes at a
+// time and the working set of shared GLL points stays in L2; the sub-chunks
+// of one 32-byte sector of lanes (LB < 8) take adjacent items.
+struct PipeItems {
+  int ngroups, nchunk, spg;
+  __device__ __forceinline__ void decode(int w, int& chunk, int& g) const {
+    const int per = ngroups * spg;
+    const int sg = w / per;
+    const int rem = w - sg * per;
+    g = rem / spg;
+    chunk = sg * spg + (rem - g * spg);
+  }
+  __host__ __device__ __forceinline__ int count() const {
+    return ((nchunk + spg - 1) / spg) * spg * ngroups;
+  }
+};
+
 template <int LB, int EPB, int TPE, bool ADJ>
-__global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int ngroups) {
+__global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, PipeItems items) {
   using LY = PipeLayout<LB, EPB, TPE, ADJ>;
   constexpr int NT = EPB * TPE * LB;
   constexpr int NE = LY::NE;
@@ -663,53 +681,54 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
   float* sU = sm + LY::OFF_U;
   float* sA = sm + LY::OFF_A;
   float* sK = sm + LY::OFF_K;
-  __shared__ unsigned char s_act[2][LB];
-  __shared__ unsigned char s_scat2[LB];
 
   const int tid = threadIdx.x;
   const int lane = tid % LB;
   const int t = (tid / LB) % TPE;
   const int el = tid / (TPE * LB);
   const bool pen = t < 25;
-  const int lg = blockIdx.y * LB + lane;
   const int nev = A.nev;
   const int nspec = A.m.nspec;
+  const int nitems = items.count();
 
+  // whole launch idle (every lane finished or parked): nothing to do
   bool any = false;
-  if (tid < LB) {
-    bool a1 = false, a2 = false, sc = false;
-    const int l2 = blockIdx.y * LB + tid;
-    if (l2 < nev) {
-      const LaneDesc* L = A.lanes + l2;
-      const int it = L->it0 + A.s;
-      if (L->phase != PH_IDLE && it < L->nstep) {
-        a1 = true;
-        a2 = ADJ && L->phase == PH_ADJ;
-        sc = a2 && it > 0;
-      }
-    }
-    s_act[0][tid] = a1;
-    s_act[1][tid] = a2;
-    s_scat2[tid] = sc;
-    any = a1;
+  for (int l = tid; l < nev; l += NT) {
+    const LaneDesc* L = A.lanes + l;
+    any |= L->phase != PH_IDLE && L->it0 + A.s < L->nstep;
   }
   if (!__syncthreads_or(any)) return;
-  const bool act1 = s_act[0][lane], act2 = ADJ && s_act[1][lane];
-  const bool scat2 = ADJ && s_scat2[lane];
 
-  // ---- copy helpers --------------------------------------------------------
-  auto issue_ib = [&](int g, int slot) {
+  // lane state of this thread for item w: bit0 active, bit1 adjoint field,
+  // bit2 adjoint scatter
+  auto flags = [&](int w, int& lg, int& g) -> int {
+    int chunk;
+    items.decode(w, chunk, g);
+    lg = chunk * LB + lane;
+    if (chunk >= items.nchunk || lg >= nev) return 0;
+    const LaneDesc* L = A.lanes + lg;
+    const int it = L->it0 + A.s;
+    if (L->phase == PH_IDLE || it >= L->nstep) return 0;
+    int f = 1;
+    if (ADJ && L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
+    return f;
+  };
+  auto issue_ib = [&](int w, int slot) {
     int* dst = sIB + slot * NE;
+    int chunk = 0, g = 0;
+    if (w < nitems) items.decode(w, chunk, g);
     for (int i = tid; i < NE; i += NT) {
       const int es = g * EPB + i / NGLL3;
-      if (g < ngroups && es < nspec)
+      if (w < nitems && es < nspec)
         cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[es] * NGLL3 + i % NGLL3);
       else
         dst[i] = -1;
     }
   };
-  auto issue_data = [&](int g, int ibslot, int buf) {
-    if (g >= ngroups) return;
+  auto issue_data = [&](int w, int ibslot, int buf) {
+    if (w >= nitems) return;
+    int lg, g;
+    const int fl = flags(w, lg, g);
     const int* ib = sIB + ibslot * NE;
     float* km = sKM + buf * 2 * NE;
     for (int i = tid; i < NE; i += NT) {
@@ -723,7 +742,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
     if (pen) {
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
-        const bool act = f == 0 ? act1 : act2;
+        const bool act = f == 0 ? (fl & 1) : (fl & 2);
         const float* src = f == 0 ? A.f1.u : A.f2.u;
         float* ub = sU + (((buf * NF + f) * EPB + el) * PP_U) * LB + lane;
 #pragma unroll
@@ -740,7 +759,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
           }
         }
       }
-      if (ADJ && act2) {
+      if (ADJ && (fl & 2)) {
         const int es = g * EPB + el;
         float* kb = sK + buf * 2 * NE * LB;
         if (es < nspec) {
@@ -758,29 +777,32 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, int
   };
 
   // ---- prologue --------------------------------------------------------------
-  int g = blockIdx.x;
-  issue_ib(g, 0);
+  int w = blockIdx.x;
+  issue_ib(w, 0);
   cp_commit();
   cp_wait_all();
   __syncthreads();
-  issue_data(g, 0, 0);
-  issue_ib(g + gridDim.x, 1);
+  issue_data(w, 0, 0);
+  issue_ib(w + gridDim.x, 1);
   cp_commit();
 
   // gradients stay in reference coordinates: stress scale jac*xix*xix,
   // strain products scale xix^2
   const float fac = A.m.jac * A.m.xix * A.m.xix;
   const float dtk = A.dt * A.m.xix * A.m.xix;
-  for (int k = 0; g < ngroups; ++k, g += gridDim.x) {
+  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
     const int buf = k & 1;
     const int ibs = k % 3;
     cp_wait_all();
     __syncthreads();
-    // prefetch the next group while this one is computed
-    issue_data(g + gridDim.x, (k + 1) % 3, buf ^ 1);
-    issue_ib(g + 2 * gridDim.x, (k + 2) % 3);
+    // prefetch the next item while this one is computed
+    issue_data(w + gridDim.x, (k + 1) % 3, buf ^ 1);
+    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
     cp_commit();
 
+    int lg, g;
+    const int fl = flags(w, lg, g);
+    const bool act1 = fl & 1, act2 = ADJ && (fl & 2), scat2 = ADJ && (fl & 4);
     const int es = g * EPB + el;
     const int e = es < nspec ? A.m.order[es] : nspec;
     const float* kap = sKM + buf * 2 * NE + el * NGLL3;
@@ -872,13 +894,14 @@ static void forces_piped_cfg(const StepArgs& a, cudaStream_t st) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
-  const int ngroups = (a.m.nspec + EPB - 1) / EPB;
-  const int nchunk = (a.nev + LB - 1) / LB;
-  int gx = (blocks_per_sm * sms + nchunk - 1) / nchunk;
-  if (gx > ngroups) gx = ngroups;
+  PipeItems items;
+  items.ngroups = (a.m.nspec + EPB - 1) / EPB;
+  items.nchunk = (a.nev + LB - 1) / LB;
+  items.spg = (LB >= 8 || a.nev <= LB) ? 1 : 8 / LB;
+  int gx = blocks_per_sm * sms;
+  if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
-  dim3 grid(gx, nchunk);
-  k_forces_piped<LB, EPB, TPE, ADJ><<<grid, NT, LY::BYTES, st>>>(a, ngroups);
+  k_forces_piped<LB, EPB, TPE, ADJ><<<gx, NT, LY::BYTES, st>>>(a, items);
 }
 
 template <int LB, int EPB, bool ADJ>
