@@ -246,6 +246,8 @@ struct sem_run_s {
   sem_mesh_s* mesh = nullptr;
   sem_run_cfg cfg{};
   int nev = 1, nstep = 0, nrec_max = 1;
+  int nevp = 1;        // lanes allocated: nev rounded up to the lane-group width
+  LaneMap lm{0};       // lane-group layout of the per-event arrays
   double dt = 0.0;
   cudaStream_t stream = nullptr;      // stream work is queued on
   cudaStream_t own_stream = nullptr;  // the run's own stream
@@ -299,6 +301,7 @@ struct sem_run_s {
     a.dt = (float)dt;
     a.store_fp16 = cfg.store_kind == SEM_STORE_FP16;
     a.nrec_max = nrec_max;
+    a.lm = lm;
     // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined;
     // 0 = chosen by the autotuner per phase
     const int v = variant[adjoint ? 1 : 0];
@@ -543,7 +546,8 @@ static int validate_cfg(const sem_run_cfg* c) {
 
 long long sem_run_bytes(const sem_mesh* m, const sem_run_cfg* c) {
   if (!m || validate_cfg(c)) return -1;
-  const size_t ng = m->nglob, ne = (size_t)m->nspec * NGLL3, nev = c->nev, ns = c->nstep;
+  const size_t ng = m->nglob, ne = (size_t)m->nspec * NGLL3, ns = c->nstep;
+  const size_t nev = c->nev > 1 ? (size_t)((c->nev + 7) / 8) * 8 : 1;
   const size_t nr = c->max_receivers;
   size_t b = ng * 3 * 4;                         // minv
   b += 6 * ng * 3 * nev * 4;                     // two fields
@@ -570,6 +574,8 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   r->cfg = *c;
   if (r->cfg.graph_steps == 0) r->cfg.graph_steps = 50;
   r->nev = c->nev;
+  r->lm.lwlog = c->nev > 1 ? 3 : 0;
+  r->nevp = ((c->nev + (1 << r->lm.lwlog) - 1) >> r->lm.lwlog) << r->lm.lwlog;
   r->nstep = c->nstep;
   r->dt = c->dt;
   r->nrec_max = c->max_receivers;
@@ -600,7 +606,7 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   CK(cudaMemcpy(r->minv.p, mi.data(), r->minv.bytes(), cudaMemcpyHostToDevice));
 
   const size_t nev = r->nev, ns = r->nstep, nr = r->nrec_max, ne = (size_t)m->nspec * NGLL3;
-  const size_t nf3 = ng * 3 * nev;
+  const size_t nf3 = ng * 3 * (size_t)r->nevp;
   CKM(r->u1.alloc(nf3), "displ");
   CKM(r->v1.alloc(nf3), "veloc");
   CKM(r->a1.alloc(nf3), "accel");
@@ -710,7 +716,7 @@ int sem_set_receivers(sem_run* r, int ev, int nrec, const double* xyz) {
 }
 
 static int ensure_adjoint_buffers(sem_run* r) {
-  const size_t ng = r->mesh->nglob, nev = r->nev, ne = (size_t)r->mesh->nspec * NGLL3;
+  const size_t ng = r->mesh->nglob, nev = r->nevp, ne = (size_t)r->mesh->nspec * NGLL3;
   if (!r->u2.p) {
     CKM(r->u2.alloc(ng * 3 * nev), "backward displ");
     CKM(r->v2.alloc(ng * 3 * nev), "backward veloc");
@@ -847,7 +853,7 @@ static int run_loop(sem_run* r, bool adjoint) {
 
 int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
   if (!r) return fail(SEM_ERR_ARG, "null run");
-  const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nev;
+  const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nevp;
   if (sim_type == 1) {
     for (int e = 0; e < r->nev; ++e)
       if (!r->have_src[e] || !r->have_rec[e])
@@ -1052,7 +1058,7 @@ int sem_save_adjoint_kernels(sem_run* r, int ev, double* out) {
   const size_t ne = (size_t)r->mesh->nspec * NGLL3;
   if (!r->kout.p) CKM(r->kout.alloc(6 * ne), "kernel output");
   launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p, {r->k_rho.p, r->k_mu.p, r->k_kappa.p},
-                          r->nev, ev, r->kout.p, nullptr, r->stream);
+                          r->lm, ev, r->kout.p, nullptr, r->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, r->kout.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
   CK(cudaStreamSynchronize(r->stream));
@@ -1067,7 +1073,7 @@ int sem_sum_kernels(sem_run* r, double* out) {
   CK(cudaMemsetAsync(r->ksum.p, 0, r->ksum.bytes(), r->stream));
   for (int e = 0; e < r->nev; ++e)
     launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p,
-                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->nev, e, nullptr,
+                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->lm, e, nullptr,
                             r->ksum.p, r->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, r->ksum.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
@@ -1082,7 +1088,7 @@ int sem_sum_kernels_device(sem_run* r, double* dev_out) {
   CK(cudaMemsetAsync(dev_out, 0, 6 * ne * 8, r->stream));
   for (int e = 0; e < r->nev; ++e)
     launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p,
-                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->nev, e, nullptr, dev_out,
+                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->lm, e, nullptr, dev_out,
                             r->stream);
   CK(cudaGetLastError());
   return SEM_OK;

@@ -65,6 +65,23 @@ struct KernAcc {
   float* kappa;      // [nspec*125][nev]
 };
 
+// Per-event arrays use a lane-group layout: event lanes are grouped by
+// LW = 2^lwlog (1 for a single event, 8 otherwise) and an array of
+// per-point records is stored [group][point][record][LW], so one group's
+// data is contiguous and a warp of a group reads whole 32-byte sectors.
+struct LaneMap {
+  int lwlog;
+  // field value (point ig, component c) of lane lg; nglob points
+  __host__ __device__ __forceinline__ size_t f(size_t ig, int c, int lg, size_t nglob) const {
+    return ((((size_t)(lg >> lwlog)) * nglob + ig) * 3 + c) * ((size_t)1 << lwlog) +
+           (lg & ((1 << lwlog) - 1));
+  }
+  // one value per point (or element point) i of n
+  __host__ __device__ __forceinline__ size_t p(size_t i, int lg, size_t n) const {
+    return (((size_t)(lg >> lwlog)) * n + i) * ((size_t)1 << lwlog) + (lg & ((1 << lwlog) - 1));
+  }
+};
+
 struct StepArgs {
   MeshView m;
   Fields f1;             // forward field, or adjoint field in PH_ADJ
@@ -78,6 +95,16 @@ struct StepArgs {
   int store_fp16;
   int nrec_max;
   int variant;           // element kernel: 0 thread-per-point, 1 pencil
+  LaneMap lm;            // lane-group layout of the per-event arrays
+  __device__ __forceinline__ size_t fi(size_t ig, int c, int lg) const {
+    return lm.f(ig, c, lg, (size_t)m.nglob);
+  }
+  __device__ __forceinline__ size_t ei(size_t ep, int lg) const {
+    return lm.p(ep, lg, (size_t)m.nspec * NGLL3);
+  }
+  __device__ __forceinline__ size_t gi(size_t ig, int lg) const {
+    return lm.p(ig, lg, (size_t)m.nglob);
+  }
 };
 
 // Launch helpers (defined in sem_kernels.cu).  Each returns the number of
@@ -88,14 +115,14 @@ int launch_update(const StepArgs& a, bool adj, cudaStream_t st);
 int launch_points(const StepArgs& a, cudaStream_t st);
 int launch_advance(LaneDesc* lanes, int nev, int k, cudaStream_t st);
 int launch_finalize_kernels(const MeshView& m, const float* rho,
-                            const KernAcc& k, int nev, int lane,
+                            const KernAcc& k, LaneMap lm, int lane,
                             double* out6, double* sum6, cudaStream_t st);
 int launch_measure_l2(const float* seis, const double* obs, const double* taper,
                       const double* simpw, int nrec, int nstep, float* adj_out,
                       double* misfit_rc, cudaStream_t st);
-int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, int nev,
+int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, LaneMap lm,
                      int lane, cudaStream_t st);
-int launch_lane_zero(const Fields& f, int nglob, int nev, int lane,
+int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane,
                      cudaStream_t st);
 int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st);
 

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
       const size_t ig = (size_t)s_ib[p];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const size_t q = (ig * 3 + c) * nev + lg;
+        const size_t q = act1 || act2 ? A.fi(ig, c, lg) : 0;
         b1[(c * NGLL3 + p) * LB + lane] = act1 ? A.f1.u[q] : 0.f;
         if (ADJ) b2[(c * NGLL3 + p) * LB + lane] = act2 ? A.f2.u[q] : 0.f;
       }
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
           const float b_yz = 0.5f * (g2[1][2] + g2[2][1]);
           const float dd = a_xx * b_xx + a_yy * b_yy + (a_xx + a_yy) * (b_xx + b_yy) +
                            2.0f * (a_xy * b_xy + a_xz * b_xz + a_yz * b_yz);
-          const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
+          const size_t q = A.ei((size_t)e * NGLL3 + p, lg);
           A.k.mu[q] += A.dt * dd;
           A.k.kappa[q] += A.dt * (tr1 * tr2);
         }
@@ -233,13 +233,13 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
         float f[3];
         div_point<LB>(b1, i, j, k, lane, s_DWt, s_w, f);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[(ig * 3 + c) * nev + lg], f[c]);
+        for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[A.fi(ig, c, lg)], f[c]);
       }
       if (ADJ && scat2) {
         float f[3];
         div_point<LB>(b2, i, j, k, lane, s_DWt, s_w, f);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[(ig * 3 + c) * nev + lg], f[c]);
+        for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[A.fi(ig, c, lg)], f[c]);
       }
     }
   }
@@ -454,7 +454,8 @@ __device__ __forceinline__ void pencil_div_eg(const PencilBuf<LB>& b, int t) {
 // xi role: total force on the xi-pencil and scatter-add.
 template <int LB>
 __device__ __forceinline__ void pencil_scatter(const PencilBuf<LB>& b, int t, const float fx[5][3],
-                                               const int* s_ib, float* acc, int nev, int lg) {
+                                               const int* s_ib, float* acc, const StepArgs& A,
+                                               int lg) {
   const int pj = t % 5, pk = t / 5;
   float wj = 0.f, wk = 0.f;
 #pragma unroll
@@ -469,7 +470,7 @@ __device__ __forceinline__ void pencil_scatter(const PencilBuf<LB>& b, int t, co
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float f = -(wj * wk * fx[i][c] + gW(i) * wk * b.Ar(c, p) + gW(i) * wj * b.Ar(3 + c, p));
-      atomicAdd(&acc[(ig * 3 + c) * nev + lg], f);
+      atomicAdd(&acc[A.fi(ig, c, lg)], f);
     }
   }
 }
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
       const int ig = s_ib[e2 * NGLL3 + p];
       const int l2 = blockIdx.y * LB + ln;
       float v = 0.f;
-      if (ig >= 0 && s_act[f][ln]) v = src[((size_t)ig * 3 + c) * nev + l2];
+      if (ig >= 0 && s_act[f][ln]) v = src[A.fi((size_t)ig, c, l2)];
       sm[((f * EPB + e2) * PR_F + c * NGLL3 + p) * LB + ln] = v;
     }
   }
@@ -595,7 +596,7 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
         const float* bv = e2v[i];
         const float dd = a_xx * bv[0] + a_yy * bv[1] + (a_xx + a_yy) * (bv[0] + bv[1]) +
                          2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
-        const size_t q = ((size_t)e * NGLL3 + i + 5 * t) * nev + lg;
+        const size_t q = A.ei((size_t)e * NGLL3 + i + 5 * t, lg);
         A.k.mu[q] += dtk * dd;
         A.k.kappa[q] += dtk * (tr1 * bv[5]);
       }
@@ -612,8 +613,8 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   __syncthreads();
   if (e < A.m.nspec) {
     const int* ib = s_ib + el * NGLL3;
-    if (s_act[0][lane]) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, nev, lg);
-    if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, nev, lg);
+    if (s_act[0][lane]) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, A, lg);
+    if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, A, lg);
   }
 }
 
@@ -753,7 +754,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
           for (int c = 0; c < 3; ++c) {
             float* d = ub + (c * NGLL3 + p) * LB;
             if (act && ig >= 0)
-              cp_async4(d, src + ((size_t)ig * 3 + c) * nev + lg);
+              cp_async4(d, src + A.fi((size_t)ig, c, lg));
             else
               *d = 0.f;
           }
@@ -767,7 +768,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
             const int p = t + 25 * r;
-            const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
+            const size_t q = A.ei((size_t)e * NGLL3 + p, lg);
             cp_async4(kb + (el * NGLL3 + p) * LB + lane, A.k.mu + q);
             cp_async4(kb + (NE + el * NGLL3 + p) * LB + lane, A.k.kappa + q);
           }
@@ -851,7 +852,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
             const float dd = a_xx * bv[0] + a_yy * bv[1] + (a_xx + a_yy) * (bv[0] + bv[1]) +
                              2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
             const int p = i + 5 * t;
-            const size_t q = ((size_t)e * NGLL3 + p) * nev + lg;
+            const size_t q = A.ei((size_t)e * NGLL3 + p, lg);
             A.k.mu[q] = kb[(el * NGLL3 + p) * LB + lane] + dtk * dd;
             A.k.kappa[q] = kb[(NE + el * NGLL3 + p) * LB + lane] + dtk * (tr1 * bv[5]);
           }
@@ -871,8 +872,8 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
     __syncthreads();
     if (pen && e < nspec) {
       const int* ib = sIB + ibs * NE + el * NGLL3;
-      if (act1) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, nev, lg);
-      if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, nev, lg);
+      if (act1) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, A, lg);
+      if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, A, lg);
     }
   }
   cp_wait_all();
@@ -1035,9 +1036,9 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
     ig = (size_t)A.m.f_iglob[fp];
     if (absorb) {
       const float nx = A.m.f_n[fp * 3 + 0], ny = A.m.f_n[fp * 3 + 1], nz = A.m.f_n[fp * 3 + 2];
-      const float vx = A.f1.v[(ig * 3 + 0) * nev + lg];
-      const float vy = A.f1.v[(ig * 3 + 1) * nev + lg];
-      const float vz = A.f1.v[(ig * 3 + 2) * nev + lg];
+      const float vx = A.f1.v[A.fi(ig, 0, lg)];
+      const float vy = A.f1.v[A.fi(ig, 1, lg)];
+      const float vz = A.f1.v[A.fi(ig, 2, lg)];
       const float vn = vx * nx + vy * ny + vz * nz;
       const float rvp = A.m.f_rvp[fp], rvs = A.m.f_rvs[fp];
       const float jw = A.m.f_jw[fp];
@@ -1045,7 +1046,7 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
       sv[1] = (rvp * vn * ny + rvs * (vy - vn * ny)) * jw;
       sv[2] = (rvp * vn * nz + rvs * (vz - vn * nz)) * jw;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[(ig * 3 + c) * nev + lg], -sv[c]);
+      for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[A.fi(ig, c, lg)], -sv[c]);
       if (save && A.store_fp16) {
         const float m = fmaxf(fabsf(sv[0]), fmaxf(fabsf(sv[1]), fabsf(sv[2])));
         atomicMax(&s_max[fl * LBB + lane], __float_as_uint(m));
@@ -1083,7 +1084,7 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
       for (int c = 0; c < 3; ++c) val[c] = st[base + c];
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[(ig * 3 + c) * nev + lg], -val[c]);
+    for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[A.fi(ig, c, lg)], -val[c]);
   }
 }
 
@@ -1136,7 +1137,7 @@ __global__ void __launch_bounds__(128) k_points(StepArgs A) {
       const size_t ig = (size_t)A.m.ibool[(size_t)L->src_ispec * NGLL3 + p];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        atomicAdd(&acc[(ig * 3 + c) * nev + lg], L->srcarr[p * 3 + c] * s);
+        atomicAdd(&acc[A.fi(ig, c, lg)], L->srcarr[p * 3 + c] * s);
     }
     return;
   }
@@ -1154,9 +1155,9 @@ __global__ void __launch_bounds__(128) k_points(StepArgs A) {
     for (int p = ln; p < NGLL3; p += 32) {
       const size_t ig = (size_t)A.m.ibool[(size_t)e * NGLL3 + p];
       const float wp = w[p];
-      s0 = fmaf(wp, A.f1.u[(ig * 3 + 0) * nev + lg], s0);
-      s1 = fmaf(wp, A.f1.u[(ig * 3 + 1) * nev + lg], s1);
-      s2 = fmaf(wp, A.f1.u[(ig * 3 + 2) * nev + lg], s2);
+      s0 = fmaf(wp, A.f1.u[A.fi(ig, 0, lg)], s0);
+      s1 = fmaf(wp, A.f1.u[A.fi(ig, 1, lg)], s1);
+      s2 = fmaf(wp, A.f1.u[A.fi(ig, 2, lg)], s2);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -1179,9 +1180,9 @@ __global__ void __launch_bounds__(128) k_points(StepArgs A) {
     for (int p = ln; p < NGLL3; p += 32) {
       const size_t ig = (size_t)A.m.ibool[(size_t)e * NGLL3 + p];
       const float wp = w[p];
-      atomicAdd(&A.f1.a[(ig * 3 + 0) * nev + lg], wp * a0);
-      atomicAdd(&A.f1.a[(ig * 3 + 1) * nev + lg], wp * a1);
-      atomicAdd(&A.f1.a[(ig * 3 + 2) * nev + lg], wp * a2);
+      atomicAdd(&A.f1.a[A.fi(ig, 0, lg)], wp * a0);
+      atomicAdd(&A.f1.a[A.fi(ig, 1, lg)], wp * a1);
+      atomicAdd(&A.f1.a[A.fi(ig, 2, lg)], wp * a2);
     }
   }
 }
@@ -1190,13 +1191,20 @@ __global__ void __launch_bounds__(128) k_points(StepArgs A) {
 // Newmark corrector (this step) + predictor (next step)
 // ---------------------------------------------------------------------------
 
+// One thread per (point, lane), lanes of a group fastest.
 template <bool ADJ>
 __global__ void __launch_bounds__(256) k_update(StepArgs A) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nev = A.nev;
-  if (idx >= (size_t)A.m.nglob * nev) return;
-  const size_t ig = idx / nev;
-  const int lg = (int)(idx - ig * nev);
+  const int lwlog = A.lm.lwlog;
+  const size_t nglob = (size_t)A.m.nglob;
+  const size_t ngroups = ((size_t)nev + (1u << lwlog) - 1) >> lwlog;
+  if (idx >= (ngroups * nglob) << lwlog) return;
+  const size_t grp = idx / (nglob << lwlog);
+  const size_t rem = idx - grp * (nglob << lwlog);
+  const size_t ig = rem >> lwlog;
+  const int lg = (int)((grp << lwlog) + (rem & ((1u << lwlog) - 1)));
+  if (lg >= nev) return;
   const LaneDesc* L = A.lanes + lg;
   const int it = L->it0 + A.s;
   const int ph = L->phase;
@@ -1206,7 +1214,7 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
   float u[3], v[3], a[3], mi[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const size_t q = (ig * 3 + c) * nev + lg;
+    const size_t q = A.fi(ig, c, lg);
     mi[c] = A.minv[ig * 3 + c];
     a[c] = A.f1.a[q] * mi[c];
     v[c] = A.f1.v[q] + dt2 * a[c];
@@ -1216,7 +1224,7 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
     float bu[3], bv[3], ba[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const size_t q = (ig * 3 + c) * nev + lg;
+      const size_t q = A.fi(ig, c, lg);
       bu[c] = A.f2.u[q];
       bv[c] = A.f2.v[q];
       ba[c] = A.f2.a[q];
@@ -1225,7 +1233,7 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
         bv[c] = bv[c] - dt2 * ba[c];
       }
     }
-    A.k.rho_glob[ig * nev + lg] += dt * (a[0] * bu[0] + a[1] * bu[1] + a[2] * bu[2]);
+    A.k.rho_glob[A.gi(ig, lg)] += dt * (a[0] * bu[0] + a[1] * bu[1] + a[2] * bu[2]);
     if (pred) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -1236,7 +1244,7 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const size_t q = (ig * 3 + c) * nev + lg;
+      const size_t q = A.fi(ig, c, lg);
       A.f2.u[q] = bu[c];
       A.f2.v[q] = bv[c];
       A.f2.a[q] = ba[c];
@@ -1252,7 +1260,7 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const size_t q = (ig * 3 + c) * nev + lg;
+    const size_t q = A.fi(ig, c, lg);
     A.f1.u[q] = u[c];
     A.f1.v[q] = v[c];
     A.f1.a[q] = a[c];
@@ -1260,7 +1268,8 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
 }
 
 int launch_update(const StepArgs& a, bool adj, cudaStream_t st) {
-  const size_t n = (size_t)a.m.nglob * a.nev;
+  const int lw = 1 << a.lm.lwlog;
+  const size_t n = (size_t)a.m.nglob * (size_t)((a.nev + lw - 1) / lw) * lw;
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (adj)
     k_update<true><<<blocks, 256, 0, st>>>(a);
@@ -1289,15 +1298,15 @@ int launch_advance(LaneDesc* lanes, int nev, int k, cudaStream_t st) {
 // kernels: final scaling (FP64) and cross-event FP64 sum
 // ---------------------------------------------------------------------------
 
-__global__ void k_finalize(MeshView m, const float* __restrict__ rho, KernAcc k, int nev, int lane,
-                           double* __restrict__ out6, double* __restrict__ sum6) {
+__global__ void k_finalize(MeshView m, const float* __restrict__ rho, KernAcc k, LaneMap lm,
+                           int lane, double* __restrict__ out6, double* __restrict__ sum6) {
   const size_t ne = (size_t)m.nspec * NGLL3;
   const size_t ep = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ep >= ne) return;
   const double r = rho[ep], mu = m.mu[ep], kap = m.kappa[ep];
-  const double rk = -r * (double)k.rho_glob[(size_t)m.ibool[ep] * nev + lane];
-  const double mk = -2.0 * mu * (double)k.mu[ep * nev + lane];
-  const double kk = -kap * (double)k.kappa[ep * nev + lane];
+  const double rk = -r * (double)k.rho_glob[lm.p((size_t)m.ibool[ep], lane, (size_t)m.nglob)];
+  const double mk = -2.0 * mu * (double)k.mu[lm.p(ep, lane, ne)];
+  const double kk = -kap * (double)k.kappa[lm.p(ep, lane, ne)];
   const double v6[6] = {rk, mk, kk, rk + kk + mk, 2.0 * (mk - 4.0 / 3.0 * mu / kap * kk),
                         2.0 * (1.0 + 4.0 / 3.0 * mu / kap) * kk};
 #pragma unroll
@@ -1307,10 +1316,10 @@ __global__ void k_finalize(MeshView m, const float* __restrict__ rho, KernAcc k,
   }
 }
 
-int launch_finalize_kernels(const MeshView& m, const float* rho, const KernAcc& k, int nev,
+int launch_finalize_kernels(const MeshView& m, const float* rho, const KernAcc& k, LaneMap lm,
                             int lane, double* out6, double* sum6, cudaStream_t st) {
   const size_t ne = (size_t)m.nspec * NGLL3;
-  k_finalize<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, rho, k, nev, lane, out6, sum6);
+  k_finalize<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, rho, k, lm, lane, out6, sum6);
   return 1;
 }
 
@@ -1354,34 +1363,34 @@ int launch_measure_l2(const float* seis, const double* obs, const double* taper,
 // lane utilities (phase transitions) and health check
 // ---------------------------------------------------------------------------
 
-__global__ void k_lane_copy(Fields s, Fields d, int nglob, int nev, int lane) {
+__global__ void k_lane_copy(Fields s, Fields d, int nglob, LaneMap lm, int lane) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (size_t)nglob * 3) return;
-  const size_t q = i * nev + lane;
+  const size_t q = lm.f(i / 3, (int)(i % 3), lane, (size_t)nglob);
   d.u[q] = s.u[q];
   d.v[q] = s.v[q];
   d.a[q] = s.a[q];
 }
 
-__global__ void k_lane_zero(Fields f, int nglob, int nev, int lane) {
+__global__ void k_lane_zero(Fields f, int nglob, LaneMap lm, int lane) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (size_t)nglob * 3) return;
-  const size_t q = i * nev + lane;
+  const size_t q = lm.f(i / 3, (int)(i % 3), lane, (size_t)nglob);
   f.u[q] = 0.f;
   f.v[q] = 0.f;
   f.a[q] = 0.f;
 }
 
-int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, int nev, int lane,
+int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, LaneMap lm, int lane,
                      cudaStream_t st) {
   const size_t n = (size_t)nglob * 3;
-  k_lane_copy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, dst, nglob, nev, lane);
+  k_lane_copy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, dst, nglob, lm, lane);
   return 1;
 }
 
-int launch_lane_zero(const Fields& f, int nglob, int nev, int lane, cudaStream_t st) {
+int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane, cudaStream_t st) {
   const size_t n = (size_t)nglob * 3;
-  k_lane_zero<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f, nglob, nev, lane);
+  k_lane_zero<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f, nglob, lm, lane);
   return 1;
 }
 
