@@ -269,12 +269,14 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
             t1.record(stream)
             torch.cuda.synchronize()
         plain_ms = t0.elapsed_time(t1)
+        pvar = sp.kernel_variants()
         fms = sp.time_kernels(1, 20)
         ams = sp.time_kernels(3, 20)
         sp.close()
         result["plain"] = {
             "events_per_hour": 3600e3 / plain_ms, "ms_per_event": plain_ms,
             "store": "fp32", "graphs": False,
+            "kernel_variants": {"fwd": pvar[0], "adj": pvar[1]},
             "kernel_ms_fwd": dict(zip(("forces", "stacey", "points", "update"), fms)),
             "kernel_ms_adj": dict(zip(("forces", "stacey", "points", "update"), ams)),
         }
@@ -333,6 +335,7 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
     value = E * world * args.steps / (ms / 1e3) * 3600.0
 
     # kernel timing for the roofline (same run, further steps)
+    variants = sb.kernel_variants()
     fms = sb.time_kernels(1, 20)
     ams = sb.time_kernels(3, 20)
 
@@ -421,6 +424,7 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                    "parallelism": f"events sharded over {world} GPU(s), FP64 "
                                   "kernel-sum all-reduce per step"},
         "batched": {"events_per_hour": value, "ms_per_event": ms_per_step / E,
+                    "kernel_variants": {"fwd": variants[0], "adj": variants[1]},
                     "kernel_ms_fwd": dict(zip(("forces", "stacey", "points",
                                                "update"), fms)),
                     "kernel_ms_adj": dict(zip(("forces", "stacey", "points",
