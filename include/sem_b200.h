@@ -193,6 +193,27 @@ int sem_time_kernels(sem_run *run, int sim_type, int nsteps, double *ms4);
  * per phase; -1 until then. */
 int sem_kernel_variants(sem_run *run, int *fwd, int *adj);
 
+/* L2 waveform misfit and adjoint sources on caller-owned DEVICE buffers,
+ * allocating nothing.  No counterpart in the reference: it is for callers
+ * that cannot call cudaMalloc (code inside another framework's memory pool
+ * or a fixed device-memory budget, or a Fortran host that only passes
+ * buffers it already owns).  Same arithmetic as sem_measure_l2: seis_dev
+ * [nrec][3][nstep] float, obs_dev [nrec][3][nstep] double; writes adj_dev
+ * [nrec][3][nstep] float and the summed misfit to misfit_dev (one double).
+ * Working memory is one static device array per GPU (about 608 KiB, kept
+ * until exit) sized for SEM_L2_NOALLOC_MAX_RECEIVERS receivers and
+ * SEM_L2_NOALLOC_MAX_STEPS samples; larger requests return SEM_ERR_ARG.
+ * Work is queued on `stream` (a cudaStream_t, NULL = legacy default).  The
+ * first call on a device looks up that array's device address, so make it
+ * before capturing the stream into a CUDA graph.  All calls share the
+ * array: calls that overlap on the GPU race and must not be issued. */
+#define SEM_L2_NOALLOC_MAX_RECEIVERS 4096
+#define SEM_L2_NOALLOC_MAX_STEPS 32768
+int sem_measure_l2_noalloc(const float *seis_dev, const double *obs_dev,
+                           int nrec, int nstep, double dt, double taper_pct,
+                           int taper_type, float *adj_dev, double *misfit_dev,
+                           void *stream);
+
 /* Device-time of the last sem_iterate_time in milliseconds. */
 int sem_last_loop_ms(sem_run *run, double *ms);
 /* Number of kernel launches queued by the last sem_iterate_time. */

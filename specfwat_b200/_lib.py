@@ -30,8 +30,10 @@ EXPORTS = (
     "sem_measure_l2", "sem_save_adjoint_kernels", "sem_sum_kernels",
     "sem_last_loop_ms", "sem_last_launch_count", "sem_set_observed",
     "sem_set_stream", "sem_sum_kernels_device", "sem_time_kernels",
-    "sem_kernel_variants",
+    "sem_kernel_variants", "sem_measure_l2_noalloc",
 )
+L2_NOALLOC_MAX_RECEIVERS = 4096
+L2_NOALLOC_MAX_STEPS = 32768
 
 
 class SemError(RuntimeError):
@@ -115,6 +117,7 @@ def load():
         "sem_sum_kernels_device": (C.c_int, [vp, vp]),
         "sem_time_kernels": (C.c_int, [vp, ip, ip, C.POINTER(C.c_double)]),
         "sem_kernel_variants": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "sem_measure_l2_noalloc": (C.c_int, [vp, vp, ip, ip, dp, dp, ip, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

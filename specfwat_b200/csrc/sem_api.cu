@@ -169,6 +169,19 @@ int check_device() {
 
 }  // namespace
 
+namespace sem {
+// Records an error for sem_last_error from the other translation units.
+int report_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+}  // namespace sem
+
 // ----------------------------------------------------------------------------
 // mesh
 // ----------------------------------------------------------------------------

@@ -128,4 +128,7 @@ int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st);
 
 void set_gll_constants(const float* D, const float* DWt, const float* w);
 
+// Sets the per-thread error message returned by sem_last_error().
+int report_error(int code, const char* fmt, ...);
+
 }  // namespace sem
