@@ -230,6 +230,7 @@ def run_ours(args):
 
 
 def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
+    from specfwat_b200.shard import reduce_kernel_sum
     E, NS, dt = args.events, args.nstep, 0.02
 
     db, db_obs, rec, events = make_workload(args.mesh, E, 1000 + rank)
@@ -305,7 +306,7 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         sb.sum_kernels_device(ksum.data_ptr())
         n += E
         if dist is not None:
-            dist.all_reduce(ksum[:3])
+            reduce_kernel_sum(ksum)
         launches_per_step[0] = n
 
     for _ in range(args.warmup):
@@ -362,8 +363,8 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         kout = pin_k.numpy()
         sb.sum_kernels(out=kout)
         if dist is not None:
-            kt = torch.from_numpy(kout[:3]).to(dev)
-            dist.all_reduce(kt)
+            kt = torch.from_numpy(kout.reshape(6, -1)).to(dev)
+            reduce_kernel_sum(kt)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - w0) * 1e3)
     e2e = float(np.mean(e2e_ms))

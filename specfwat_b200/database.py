@@ -149,13 +149,14 @@ def _materials(db: Database, vp, vs, rho):
             (rho * vp).astype(f), (rho * vs).astype(f), rmass.astype(f))
 
 
-def make_box(box: BoxSpec) -> Database:
+def make_box(box: BoxSpec, absorb_top: bool = False) -> Database:
     """Structured mesh, global numbering and Stacey faces of a box.
 
     Global points form a ``(4 nex + 1) x (4 ney + 1) x (4 nez + 1)`` grid
     numbered x-fastest; elements are numbered x-fastest too, bottom layer
-    first.  The model arrays are left at zero: call :func:`homogeneous` or
-    :func:`with_model` next.
+    first.  ``absorb_top`` also makes the top face absorbing (a full-space
+    test box).  The model arrays are left at zero: call :func:`homogeneous`
+    or :func:`with_model` next.
     """
     nex, ney, nez, h = box.nex, box.ney, box.nez, box.h
     nxg, nyg, nzg = 4 * nex + 1, 4 * ney + 1, 4 * nez + 1
@@ -214,6 +215,8 @@ def make_box(box: BoxSpec) -> Database:
     add(ey == 0, np.stack([A, z0, B], 1), (0.0, -1.0, 0.0))
     add(ey == ney - 1, np.stack([A, z4, B], 1), (0.0, 1.0, 0.0))
     add(ez == 0, np.stack([A, B, z0], 1), (0.0, 0.0, -1.0))
+    if absorb_top:
+        add(ez == nez - 1, np.stack([A, B, z4], 1), (0.0, 0.0, 1.0))
     nf = len(faces_ispec)
     abs_ispec = np.asarray(faces_ispec, np.int32)
     abs_ijk = np.asarray(faces_ijk, np.int32).reshape(nf, 25, 3)

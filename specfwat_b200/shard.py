@@ -1,0 +1,45 @@
+"""Event sharding over ranks and the one exchange step of the path.
+
+Events are independent, so N GPUs run N disjoint event sets with no
+data-path collective.  The only exchange is the cross-event kernel sum
+(the reference's ``PostFlow%sum_kernel``, ``post_processing.f90:108-149``),
+done here as one FP64 all-reduce of the summed rho/mu/kappa kernels per
+batch; the derived rhop/beta/alpha kernels are linear in them and are
+formed after the reduction by whoever needs them.
+"""
+from __future__ import annotations
+
+from typing import Sequence
+
+
+def shard_events(n_events: int, rank: int, world: int) -> range:
+    """Contiguous block of global event indices owned by ``rank``."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank/world")
+    base, extra = divmod(n_events, world)
+    start = rank * base + min(rank, extra)
+    return range(start, start + base + (1 if rank < extra else 0))
+
+
+def reduce_kernel_sum(ksum, group=None):
+    """Sum the primary kernels (rho, mu, kappa: rows 0-2 of a [6, ...]
+    FP64 tensor) over all ranks in place, then rebuild rows 3-5
+    (rhop, beta, alpha) from them is left to the caller."""
+    import torch.distributed as dist
+    if ksum.dtype.itemsize != 8:
+        raise TypeError("kernel sums are reduced in FP64")
+    dist.all_reduce(ksum[:3], op=dist.ReduceOp.SUM, group=group)
+    return ksum
+
+
+def derived_kernels(k3, mu, kappa):
+    """rhop, beta, alpha from summed rho/mu/kappa kernels (Tromp, Tape &
+    Liu 2005), given the model's mu and kappa at the same points."""
+    rk, mk, kk = k3
+    return (rk + kk + mk, 2.0 * (mk - 4.0 / 3.0 * mu / kappa * kk),
+            2.0 * (1.0 + 4.0 / 3.0 * mu / kappa) * kk)
+
+
+def events_of(all_events: Sequence, rank: int, world: int):
+    r = shard_events(len(all_events), rank, world)
+    return [all_events[i] for i in r]
