@@ -104,7 +104,9 @@ typedef struct {
   int kernel_variant; /* element kernel: 0 autotuned per phase,
                          1 thread-per-point, 2 pencil decomposition,
                          3 pencil, persistent and cp.async-pipelined,
-                         4 as 3 with 2 events per block                    */
+                         4 as 3 with 2 events per block, 5 as 3 with 2
+                         events per thread, 6 as 5 with 4 events per
+                         thread (forward) / 8 per block (adjoint)          */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard
@@ -188,7 +190,8 @@ int sem_time_kernels(sem_run *run, int sim_type, int nsteps, double *ms4);
 
 /* Element-kernel variants in use for the forward and adjoint phases
  * (1 thread-per-point, 2 pencil, 3 pencil pipelined, 4 pencil pipelined
- * with 2 events per block).  With kernel_variant = 0 the first
+ * with 2 events per block, 5 and 6 pencil pipelined with 2 or 4 events
+ * per thread).  With kernel_variant = 0 the first
  * sem_iterate_time times the candidates on this run and keeps the fastest
  * per phase; -1 until then. */
 int sem_kernel_variants(sem_run *run, int *fwd, int *adj);

@@ -552,8 +552,8 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->max_receivers < 1 || c->max_receivers > 100000)
     return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
-  if (c->kernel_variant < 0 || c->kernel_variant > 4)
-    return fail(SEM_ERR_ARG, "kernel_variant must be 0..4");
+  if (c->kernel_variant < 0 || c->kernel_variant > 6)
+    return fail(SEM_ERR_ARG, "kernel_variant must be 0..6");
   return SEM_OK;
 }
 
@@ -756,10 +756,10 @@ static int ensure_store(sem_run* r) {
 // keep the fastest.  Runs on scratch state before the forward run: the
 // forward zeroes its wavefields and the adjoint run rebuilds its own.
 static int autotune_phase(sem_run* r, bool adj) {
-  const int cands_multi[] = {0, 2, 3};
+  const int cands_multi[] = {0, 2, 3, 4, 5};
   const int cands_single[] = {0, 2};
   const int* cands = r->nev > 1 ? cands_multi : cands_single;
-  const int ncand = r->nev > 1 ? 3 : 2;
+  const int ncand = r->nev > 1 ? 5 : 2;
   const int nsteps = std::max(1, std::min(8, r->nstep - 2));
   r->fill_lanes(adj ? PH_ADJ : PH_FWD, 0);
   for (auto& L : r->h_lanes) L.it0 = 1;

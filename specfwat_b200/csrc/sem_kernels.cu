@@ -639,15 +639,19 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_grou
 constexpr int PP_U = 625;  // U (3 comps) then B (5 sigma comps)
 constexpr int PP_A = 750;  // d_eta/d_gamma, then f_eta/f_gamma
 
+// Region offsets are rounded up to 4 floats so that every region starts on
+// a 16-byte boundary (float2 / float4 accesses and 16-byte cp.async).
+constexpr int al4(int x) { return (x + 3) & ~3; }
+
 template <int LB, int EPB, int TPE, bool ADJ>
 struct PipeLayout {
   static constexpr int NF = ADJ ? 2 : 1;
-  static constexpr int NE = EPB * NGLL3;                     // element points per group
-  static constexpr int OFF_IB = 0;                           // int [3][NE]
-  static constexpr int OFF_KM = OFF_IB + 3 * NE;             // float [2][2][NE] kappa, mu
-  static constexpr int OFF_U = OFF_KM + 4 * NE;              // float [2][NF][EPB][PP_U*LB]
-  static constexpr int OFF_A = OFF_U + 2 * NF * EPB * PP_U * LB;   // [NF][EPB][PP_A*LB]
-  static constexpr int OFF_K = OFF_A + NF * EPB * PP_A * LB; // [2][2][NE*LB] mu/kappa acc
+  static constexpr int NE = EPB * NGLL3;                          // element points per group
+  static constexpr int OFF_IB = 0;                                // int [3][NE]
+  static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);             // float [2][2][NE] kappa, mu
+  static constexpr int OFF_U = al4(OFF_KM + 4 * NE);              // [2][NF][EPB][PP_U*LB]
+  static constexpr int OFF_A = al4(OFF_U + 2 * NF * EPB * PP_U * LB);   // [NF][EPB][PP_A*LB]
+  static constexpr int OFF_K = al4(OFF_A + NF * EPB * PP_A * LB);  // [2][2][NE*LB] mu/kappa acc
   static constexpr int TOTAL = OFF_K + (ADJ ? 4 * NE * LB : 0);
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
@@ -931,10 +935,548 @@ static void forces_cfg(const StepArgs& a, cudaStream_t st) {
   k_forces<LB, NT, ADJ><<<grid, NT, shm, st>>>(a);
 }
 
+// ---------------------------------------------------------------------------
+// element kernel, pencil decomposition with NL event lanes per thread
+// ---------------------------------------------------------------------------
+//
+// As k_forces_piped, but each thread carries NL adjacent event lanes of its
+// pencil: shared-memory traffic moves as float2/float4 (one LDS/STS per NL
+// values), the gather as NL*4-byte cp.async, the scatter as vector atomics,
+// and every index computation is shared by the NL lanes.  The xi role also
+// fuses gradient and stress point by point so that only one point's nine
+// derivatives are live at a time.  In the adjoint phase the backward
+// field's strain is parked in its own A region (the xi role reads and
+// rewrites only its own pencil there) until the adjoint field's strain
+// at the same point is ready for the kernel products.
+
+template <int NL>
+struct LV {
+  float v[NL];
+};
+
+template <int NL>
+__device__ __forceinline__ LV<NL> lds_v(const float* p) {
+  LV<NL> r;
+  if constexpr (NL == 1) {
+    r.v[0] = *p;
+  } else if constexpr (NL == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    r.v[0] = t.x;
+    r.v[1] = t.y;
+  } else {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    r.v[0] = t.x;
+    r.v[1] = t.y;
+    r.v[2] = t.z;
+    r.v[3] = t.w;
+  }
+  return r;
+}
+
+template <int NL>
+__device__ __forceinline__ void sts_v(float* p, const LV<NL>& x) {
+  if constexpr (NL == 1) {
+    *p = x.v[0];
+  } else if constexpr (NL == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(x.v[0], x.v[1]);
+  } else {
+    *reinterpret_cast<float4*>(p) = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
+  }
+}
+
+template <int NL>
+__device__ __forceinline__ void cp_async_v(float* smem, const float* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (NL == 1)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+  else if constexpr (NL == 2)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <int NL>
+__device__ __forceinline__ void red_v(float* g, const LV<NL>& x) {
+  if constexpr (NL == 1) {
+    atomicAdd(g, x.v[0]);
+  } else if constexpr (NL == 2) {
+    atomicAdd(reinterpret_cast<float2*>(g), make_float2(x.v[0], x.v[1]));
+  } else {
+    atomicAdd(reinterpret_cast<float4*>(g), make_float4(x.v[0], x.v[1], x.v[2], x.v[3]));
+  }
+}
+
+// Shared block of one (field, element): U/B region then A region, each
+// value a run of LB lanes; `ub`/`ab` already include the thread's lane
+// offset.
+template <int LB>
+struct PBuf {
+  float* ub;
+  float* ab;
+  __device__ __forceinline__ float* U(int q, int p) const { return ub + (q * 125 + p) * LB; }
+  __device__ __forceinline__ float* Ar(int q, int p) const { return ab + (q * 125 + p) * LB; }
+};
+
+// eta / gamma derivative roles (pencils (i,k) and (i,j) of thread t).
+template <int LB, int NL>
+__device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    LV<NL> v[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) v[l] = lds_v<NL>(b.U(c, pi + 5 * l + 25 * pq));
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      LV<NL> s;
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = fmaf(gD(j, l), v[l].v[n], a);
+        s.v[n] = a;
+      }
+      sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    LV<NL> v[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) v[l] = lds_v<NL>(b.U(c, pi + 5 * pq + 25 * l));
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      LV<NL> s;
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = fmaf(gD(k, l), v[l].v[n], a);
+        s.v[n] = a;
+      }
+      sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
+    }
+  }
+}
+
+// eta / gamma divergence roles: B -> A.
+template <int LB, int NL>
+__device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
+  {
+    // eta pencil: sigma_{c,y} = (xy, yy, yz) = B0, B1, B2
+    LV<NL> v[3][5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      const int p = pi + 5 * l + 25 * pq;
+      v[0][l] = lds_v<NL>(b.U(0, p));
+      v[1][l] = lds_v<NL>(b.U(1, p));
+      v[2][l] = lds_v<NL>(b.U(2, p));
+    }
+#pragma unroll
+    for (int j = 0; j < 5; ++j)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        LV<NL> s;
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = fmaf(gDWt(j, l), v[c][l].v[n], a);
+          s.v[n] = a;
+        }
+        sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
+      }
+  }
+  {
+    // gamma pencil: sigma_{c,z} = (xz, yz, zz) = B3, B2, B4
+    LV<NL> v[3][5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      const int p = pi + 5 * pq + 25 * l;
+      v[0][l] = lds_v<NL>(b.U(3, p));
+      v[1][l] = lds_v<NL>(b.U(2, p));
+      v[2][l] = lds_v<NL>(b.U(4, p));
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        LV<NL> s;
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = fmaf(gDWt(k, l), v[c][l].v[n], a);
+          s.v[n] = a;
+        }
+        sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
+      }
+  }
+}
+
+// xi role on pencil t (points p = i + 5t): gradient and stress point by
+// point; sigma for the other roles into B; f_xi into fx.
+// MODE 0: plain.  MODE 1: backward field of the adjoint phase; its
+// deviatoric strain and trace are parked in its own A region at the
+// pencil's points.  MODE 2: adjoint field; the products with the parked
+// backward strain (read from `park`) are returned in kmu / kka.
+template <int LB, int NL, int MODE>
+__device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, int t,
+                                     const float* kap, const float* mu, float fac,
+                                     LV<NL> fx[5][3], LV<NL> kmu[5], LV<NL> kka[5]) {
+  LV<NL> u[3][5];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int l = 0; l < 5; ++l) u[c][l] = lds_v<NL>(b.U(c, l + 5 * t));
+  LV<NL> sx[3][5];  // sigma_xx, sigma_xy, sigma_xz along the pencil
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    LV<NL> de[3], dg[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      de[c] = lds_v<NL>(b.Ar(c, p));
+      dg[c] = lds_v<NL>(b.Ar(3 + c, p));
+    }
+    LV<NL> pk[6];
+    if (MODE == 2) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) pk[q] = lds_v<NL>(park.Ar(q, p));
+    }
+    LV<NL> o[5];
+    const float kp = kap[p], m = mu[p];
+#pragma unroll
+    for (int n = 0; n < NL; ++n) {
+      float g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = fmaf(gD(i, l), u[c][l].v[n], a);
+        g[c][0] = a;
+        g[c][1] = de[c].v[n];
+        g[c][2] = dg[c].v[n];
+      }
+      float sig[6];
+      stress_point(g, kp, m, fac, sig);
+      sx[0][i].v[n] = sig[0];
+      sx[1][i].v[n] = sig[3];
+      sx[2][i].v[n] = sig[4];
+      o[0].v[n] = sig[3];
+      o[1].v[n] = sig[1];
+      o[2].v[n] = sig[5];
+      o[3].v[n] = sig[4];
+      o[4].v[n] = sig[2];
+      if (MODE != 0) {
+        const float tr = g[0][0] + g[1][1] + g[2][2];
+        const float xx = g[0][0] - tr * (1.0f / 3.0f);
+        const float yy = g[1][1] - tr * (1.0f / 3.0f);
+        const float xy = 0.5f * (g[0][1] + g[1][0]);
+        const float xz = 0.5f * (g[0][2] + g[2][0]);
+        const float yz = 0.5f * (g[1][2] + g[2][1]);
+        if (MODE == 1) {
+          pk[0].v[n] = xx;
+          pk[1].v[n] = yy;
+          pk[2].v[n] = xy;
+          pk[3].v[n] = xz;
+          pk[4].v[n] = yz;
+          pk[5].v[n] = tr;
+        } else {
+          const float bxx = pk[0].v[n], byy = pk[1].v[n];
+          kmu[i].v[n] = xx * bxx + yy * byy + (xx + yy) * (bxx + byy) +
+                        2.0f * (xy * pk[2].v[n] + xz * pk[3].v[n] + yz * pk[4].v[n]);
+          kka[i].v[n] = tr * pk[5].v[n];
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) sts_v<NL>(b.U(q, p), o[q]);
+    if (MODE == 1) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) sts_v<NL>(b.Ar(q, p), pk[q]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = fmaf(gDWt(i, l), sx[c][l].v[n], a);
+        fx[i][c].v[n] = a;
+      }
+}
+
+// xi role: total force on the pencil and vector scatter-add.
+template <int LB, int NL>
+__device__ __forceinline__ void v_scatter(const PBuf<LB>& b, int t, const LV<NL> fx[5][3],
+                                          const int* ib, float* acc, const StepArgs& A, int lg,
+                                          const int* fl, int bit) {
+  const int pj = t % 5, pk = t / 5;
+  float wj = 0.f, wk = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q == pj) wj = gW(q);
+    if (q == pk) wk = gW(q);
+  }
+  const float wjk = wj * wk;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    const size_t ig = (size_t)ib[p];
+    const float wik = gW(i) * wk, wij = gW(i) * wj;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const LV<NL> e1 = lds_v<NL>(b.Ar(c, p));
+      const LV<NL> e2 = lds_v<NL>(b.Ar(3 + c, p));
+      LV<NL> f;
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        const float v = -(wjk * fx[i][c].v[n] + wik * e1.v[n] + wij * e2.v[n]);
+        f.v[n] = (fl[n] & bit) ? v : 0.f;  // lanes not in this phase add nothing
+      }
+      red_v<NL>(&acc[A.fi(ig, c, lg)], f);
+    }
+  }
+}
+
+// One block = one element x LB lanes, 25 * LB / NL threads (pencil t,
+// lane group of NL).  Persistent and cp.async-pipelined like
+// k_forces_piped, with the same chunk-major work items.
+template <int LB, int NL, bool ADJ>
+__global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeItems items) {
+  constexpr int NT = 25 * LB / NL;
+  constexpr int NF = ADJ ? 2 : 1;
+  using LY = PipeLayout<LB, 1, 25, ADJ>;
+  constexpr int NE = LY::NE;
+  extern __shared__ float sm[];
+  int* sIB = (int*)(sm + LY::OFF_IB);
+  float* sKM = sm + LY::OFF_KM;
+  float* sU = sm + LY::OFF_U;
+  float* sA = sm + LY::OFF_A;
+  float* sK = sm + LY::OFF_K;
+
+  const int tid = threadIdx.x;
+  const int lq = tid % (LB / NL);      // lane group within the block
+  const int t = tid / (LB / NL);       // pencil 0..24
+  const int lane = lq * NL;            // first lane of the group
+  const int pi = t % 5, pq = t / 5;
+  const int nev = A.nev;
+  const int nspec = A.m.nspec;
+  const int nitems = items.count();
+
+  bool any = false;
+  for (int l = tid; l < nev; l += NT) {
+    const LaneDesc* L = A.lanes + l;
+    any |= L->phase != PH_IDLE && L->it0 + A.s < L->nstep;
+  }
+  if (!__syncthreads_or(any)) return;
+
+  // Lane flags are per NL-group: lanes of a group share a phase in
+  // lock-step runs; in mixed batches a group is active if its first
+  // lane is, and per-lane activity masks the writes.
+  auto lane_flag = [&](int lg) -> int {
+    if (lg >= nev) return 0;
+    const LaneDesc* L = A.lanes + lg;
+    const int it = L->it0 + A.s;
+    if (L->phase == PH_IDLE || it >= L->nstep) return 0;
+    int f = 1;
+    if (ADJ && L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
+    return f;
+  };
+  auto group_flags = [&](int w, int& lg0, int& g, int fl[NL]) {
+    int chunk;
+    items.decode(w, chunk, g);
+    lg0 = chunk * LB + lane;
+    int any_f = 0;
+#pragma unroll
+    for (int n = 0; n < NL; ++n) {
+      fl[n] = (chunk < items.nchunk) ? lane_flag(lg0 + n) : 0;
+      any_f |= fl[n];
+    }
+    return any_f;
+  };
+  auto issue_ib = [&](int w, int slot) {
+    int* dst = sIB + slot * NE;
+    int chunk = 0, g = 0;
+    if (w < nitems) items.decode(w, chunk, g);
+    for (int i = tid; i < NE; i += NT) {
+      if (w < nitems && g < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      else
+        dst[i] = -1;
+    }
+  };
+  auto issue_data = [&](int w, int ibslot, int buf) {
+    if (w >= nitems) return;
+    int lg0, g, fl[NL];
+    const int anyf = group_flags(w, lg0, g, fl);
+    const int* ib = sIB + ibslot * NE;
+    float* km = sKM + buf * 2 * NE;
+    const int e = g < nspec ? A.m.order[g] : 0;
+    for (int i = tid; i < NE; i += NT) {
+      if (g < nspec) {
+        const size_t ep = (size_t)e * NGLL3 + i;
+        cp_async4(km + i, A.m.kappa + ep);
+        cp_async4(km + NE + i, A.m.mu + ep);
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const bool act = f == 0 ? (anyf & 1) : (anyf & 2);
+      const float* src = f == 0 ? A.f1.u : A.f2.u;
+      float* ub = sU + ((buf * NF + f) * PP_U) * LB + lane;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int p = t + 25 * r;
+        const int ig = ib[p];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float* d = ub + (c * NGLL3 + p) * LB;
+          if (act && ig >= 0) {
+            cp_async_v<NL>(d, src + A.fi((size_t)ig, c, lg0));
+          } else {
+            LV<NL> z;
+#pragma unroll
+            for (int n = 0; n < NL; ++n) z.v[n] = 0.f;
+            sts_v<NL>(d, z);
+          }
+        }
+      }
+    }
+    if (ADJ && (anyf & 2) && g < nspec) {
+      float* kb = sK + buf * 2 * NE * LB;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int p = t + 25 * r;
+        const size_t ep = (size_t)e * NGLL3 + p;
+        cp_async_v<NL>(kb + p * LB + lane, A.k.mu + A.ei(ep, lg0));
+        cp_async_v<NL>(kb + (NE + p) * LB + lane, A.k.kappa + A.ei(ep, lg0));
+      }
+    }
+  };
+
+  int w = blockIdx.x;
+  issue_ib(w, 0);
+  cp_commit();
+  cp_wait_all();
+  __syncthreads();
+  issue_data(w, 0, 0);
+  issue_ib(w + gridDim.x, 1);
+  cp_commit();
+
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  const float dtk = A.dt * A.m.xix * A.m.xix;
+  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+    const int buf = k & 1;
+    const int ibs = k % 3;
+    cp_wait_all();
+    __syncthreads();
+    issue_data(w + gridDim.x, (k + 1) % 3, buf ^ 1);
+    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    cp_commit();
+
+    int lg0, g, fl[NL];
+    const int anyf = group_flags(w, lg0, g, fl);
+    const int e = g < nspec ? A.m.order[g] : nspec;
+    const float* kap = sKM + buf * 2 * NE;
+    const float* mu = kap + NE;
+    float* u1 = sU + ((buf * NF + 0) * PP_U) * LB + lane;
+    float* u2 = sU + ((buf * NF + (NF - 1)) * PP_U) * LB + lane;
+    float* a1 = sA + (0 * PP_A) * LB + lane;
+    float* a2 = sA + ((NF - 1) * PP_A) * LB + lane;
+    PBuf<LB> b1{u1, a1};
+    PBuf<LB> b2{u2, a2};
+    v_grad_eg<LB, NL>(b1, pi, pq);
+    if (ADJ) v_grad_eg<LB, NL>(b2, pi, pq);
+    __syncthreads();
+    LV<NL> fx1[5][3], fx2[ADJ ? 5 : 1][3];
+    if (ADJ) {
+      LV<NL> km[5], kk[5];
+      v_xi<LB, NL, 1>(b2, b2, t, kap, mu, fac, fx2, km, kk);
+      v_xi<LB, NL, 2>(b1, b2, t, kap, mu, fac, fx1, km, kk);
+      if ((anyf & 2) && e < nspec) {
+        const float* kb = sK + buf * 2 * NE * LB;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const int p = i + 5 * t;
+          const LV<NL> m0 = lds_v<NL>(kb + p * LB + lane);
+          const LV<NL> k0 = lds_v<NL>(kb + (NE + p) * LB + lane);
+          LV<NL> mo, ko;
+#pragma unroll
+          for (int n = 0; n < NL; ++n) {
+            const bool on = fl[n] & 2;
+            mo.v[n] = on ? m0.v[n] + dtk * km[i].v[n] : m0.v[n];
+            ko.v[n] = on ? k0.v[n] + dtk * kk[i].v[n] : k0.v[n];
+          }
+          const size_t q = A.ei((size_t)e * NGLL3 + p, lg0);
+          sts_v<NL>(A.k.mu + q, mo);
+          sts_v<NL>(A.k.kappa + q, ko);
+        }
+      }
+    } else {
+      LV<NL> km[1], kk[1];
+      v_xi<LB, NL, 0>(b1, b1, t, kap, mu, fac, fx1, km, kk);
+    }
+    __syncthreads();
+    v_div_eg<LB, NL>(b1, pi, pq);
+    if (ADJ) v_div_eg<LB, NL>(b2, pi, pq);
+    __syncthreads();
+    if (e < nspec) {
+      const int* ib = sIB + ibs * NE;
+      if (anyf & 1) v_scatter<LB, NL>(b1, t, fx1, ib, A.f1.a, A, lg0, fl, 1);
+      if (ADJ && (anyf & 4)) v_scatter<LB, NL>(b2, t, fx2, ib, A.f2.a, A, lg0, fl, 4);
+    }
+  }
+  cp_wait_all();
+}
+
+template <int LB, int NL, bool ADJ>
+static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
+  using LY = PipeLayout<LB, 1, 25, ADJ>;
+  constexpr int NT = 25 * LB / NL;
+  static int blocks_per_sm = 0, sms = 0;
+  if (!blocks_per_sm) {
+    cudaFuncSetAttribute(k_forces_vec<LB, NL, ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)LY::BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_vec<LB, NL, ADJ>, NT,
+                                                  LY::BYTES);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  PipeItems items;
+  items.ngroups = a.m.nspec;
+  items.nchunk = (a.nev + LB - 1) / LB;
+  items.spg = (LB >= 8 || a.nev <= LB) ? 1 : 8 / LB;
+  int gx = blocks_per_sm * sms;
+  if (gx > items.count()) gx = items.count();
+  if (gx < 1) gx = 1;
+  k_forces_vec<LB, NL, ADJ><<<gx, NT, LY::BYTES, st>>>(a, items);
+}
+
 // Element-kernel variants (StepArgs::variant):
 //   0 thread-per-point, 1 pencil, 2 pencil pipelined (lanes per block by
-//   event count), 3 pencil pipelined with 2 lanes per block.
+//   event count), 3 pencil pipelined with 2 lanes per block, 4 pencil
+//   pipelined with 2 lanes per thread, 5 as 4 with more lanes per block.
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.variant == 4 && a.nev > 1) {
+    if (adj)
+      forces_vec_cfg<4, 2, true>(a, st);
+    else
+      forces_vec_cfg<8, 2, false>(a, st);
+    return 1;
+  }
+  if (a.variant == 5 && a.nev > 1) {
+    if (adj)
+      forces_vec_cfg<8, 2, true>(a, st);
+    else
+      forces_vec_cfg<8, 4, false>(a, st);
+    return 1;
+  }
   if (a.variant == 3 && a.nev > 1) {
     if (adj)
       forces_piped_cfg<2, 2, 25, true>(a, st);

@@ -114,7 +114,8 @@ def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
 
 
 @pytest.mark.parametrize("variant,nev", [(1, 5), (2, 3), (2, 11), (3, 3), (3, 11),
-                                         (4, 3), (4, 6), (0, 7)])
+                                         (4, 3), (4, 6), (5, 3), (5, 11), (6, 13),
+                                         (0, 7)])
 def test_batched_equals_plain(gpu, small, variant, nev):
     db, rec, _ = small
     nstep, dt = 300, 0.02
@@ -162,14 +163,14 @@ def test_graph_equals_stepwise(gpu, small):
     assert rel_l2(out[1], out[0]) < 1e-5
 
 
-@pytest.mark.parametrize("nev", [2, 9])
-def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev):
+@pytest.mark.parametrize("nev,variant", [(2, 0), (9, 0), (9, 5), (12, 6)])
+def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
     kern = {}
     for store in ("fp32", "fp16"):
         sim = S.Simulation(mesh, nstep, dt, nev=nev, store=store, use_graph=True,
-                           max_receivers=len(rec))
+                           max_receivers=len(rec), kernel_variant=variant)
         sim.set_sources([S.make_source(*sxyz, mt, 1.0)] * nev)
         sim.set_receivers(rec)
         sim.iterate_time(1, save_forward=True)
