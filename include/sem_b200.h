@@ -188,6 +188,36 @@ int sem_sum_kernels_device(sem_run *run, double *dev_out);
  * the current state (sim_type 1 or 3 kernels).  Advances the wavefields. */
 int sem_time_kernels(sem_run *run, int sim_type, int nsteps, double *ms4);
 
+/* Serving: each event lane of a run is driven on its own.  A lane takes a
+ * request (sem_lane_start_forward), advances with every other active lane
+ * in the same launches (sem_advance), switches to its adjoint run once its
+ * forward is complete (sem_lane_start_adjoint, FP64 L2 measurement on the
+ * device) and hands back its results (sem_lane_finish), after which it
+ * takes the next request while the others keep running.  Lanes have their
+ * own NSTEP (<= the run's nstep) and their own boundary store, allocated
+ * stream-ordered when the forward starts and freed when the lane
+ * finishes.  No counterpart in the reference, whose driver runs one event
+ * per process at a time (src/preproc/fwat_fwd_measure_adj.f90:43-51). */
+long long sem_lane_store_bytes(const sem_run *run, int nstep);
+int sem_lane_start_forward(sem_run *run, int lane, const sem_source *src,
+                           int nrec, const double *xyz, int nstep,
+                           int save_forward);
+int sem_lane_start_adjoint(sem_run *run, int lane, const double *obs,
+                           double taper_pct, int taper_type, double *misfit);
+/* Queue nsteps steps for every active lane (lanes that reach their NSTEP
+ * stop inside the launches).  Asynchronous. */
+int sem_advance(sem_run *run, int nsteps);
+/* phase: 0 idle, 1 forward, 3 adjoint; step: steps done in that phase. */
+int sem_lane_status(sem_run *run, int lane, int *phase, int *step,
+                    int *nstep);
+/* Results of a lane whose phase is complete: forward seismograms
+ * [nrec][3][nstep] (forward lanes), kernels [6][nspec][125] to the host
+ * and/or added in FP64 into the device array ksum_dev (adjoint lanes).  A
+ * forward lane that saved its store stays reserved for its adjoint run;
+ * any other lane becomes idle.  Blocks until the copies are done. */
+int sem_lane_finish(sem_run *run, int lane, float *seis, double *kernels6,
+                    double *ksum_dev);
+
 /* Element-kernel variants in use for the forward and adjoint phases
  * (1 thread-per-point, 2 pencil, 3 pencil pipelined, 4 pencil pipelined
  * with 2 events per block, 5 and 6 pencil pipelined with 2 or 4 events

@@ -31,6 +31,8 @@ EXPORTS = (
     "sem_last_loop_ms", "sem_last_launch_count", "sem_set_observed",
     "sem_set_stream", "sem_sum_kernels_device", "sem_time_kernels",
     "sem_kernel_variants", "sem_measure_l2_noalloc",
+    "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
+    "sem_advance", "sem_lane_status", "sem_lane_finish",
 )
 L2_NOALLOC_MAX_RECEIVERS = 4096
 L2_NOALLOC_MAX_STEPS = 32768
@@ -118,6 +120,13 @@ def load():
         "sem_time_kernels": (C.c_int, [vp, ip, ip, C.POINTER(C.c_double)]),
         "sem_kernel_variants": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "sem_measure_l2_noalloc": (C.c_int, [vp, vp, ip, ip, dp, dp, ip, vp, vp, vp]),
+        "sem_lane_store_bytes": (C.c_longlong, [vp, ip]),
+        "sem_lane_start_forward": (C.c_int, [vp, ip, C.POINTER(Source), ip, fp, ip, ip]),
+        "sem_lane_start_adjoint": (C.c_int, [vp, ip, fp, dp, ip, C.POINTER(C.c_double)]),
+        "sem_advance": (C.c_int, [vp, ip]),
+        "sem_lane_status": (C.c_int, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]),
+        "sem_lane_finish": (C.c_int, [vp, ip, fp, fp, fp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -278,6 +278,12 @@ struct sem_run_s {
   DevArray<double> obs, taper, simpw, misfit_rc, obs_ev;
   double taper_pct_cached = -1.0;
   int taper_type_cached = -1;
+  int taper_ns_cached = -1;
+  // serving: per-lane boundary stores (stream-ordered allocations)
+  std::vector<void*> lane_store;
+  std::vector<float*> lane_scale;
+  std::vector<char> lane_saved;   // lane finished a forward with saved store
+  bool lanes_mode = false;        // run driven through the sem_lane_* calls
   DevArray<int> flag;
   std::vector<int> src_ispec, nrec;
   std::vector<char> have_src, have_rec, have_adj;
@@ -288,6 +294,11 @@ struct sem_run_s {
   long long last_launches = 0;
 
   ~sem_run_s() {
+    for (size_t l = 0; l < lane_store.size(); ++l) {
+      if (lane_store[l]) cudaFreeAsync(lane_store[l], stream);
+      if (lane_scale[l]) cudaFreeAsync(lane_scale[l], stream);
+    }
+    if (stream) cudaStreamSynchronize(stream);
     for (auto& g : gexec)
       if (g) cudaGraphExecDestroy(g);
     if (e0) cudaEventDestroy(e0);
@@ -866,6 +877,8 @@ static int run_loop(sem_run* r, bool adjoint) {
 
 int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
   if (!r) return fail(SEM_ERR_ARG, "null run");
+  if (r->lanes_mode)
+    return fail(SEM_ERR_STATE, "run is driven lane by lane (sem_lane_*); use sem_advance");
   const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nevp;
   if (sim_type == 1) {
     for (int e = 0; e < r->nev; ++e)
@@ -959,14 +972,15 @@ int sem_set_adjoint_sources(sem_run* r, int ev, const double* adj) {
 
 // Taper (src/shared/signal.f90:419-491) and Simpson weights
 // (src/shared/utils.f90:1635-1663, as written there) for nstep samples.
-static int prepare_measure(sem_run* r, double taper_pct, int taper_type) {
-  const int ns = r->nstep;
+static int prepare_measure(sem_run* r, double taper_pct, int taper_type, int ns) {
   if (!r->taper.p) {
-    CKM(r->taper.alloc(ns), "taper");
-    CKM(r->simpw.alloc(ns), "simpson weights");
+    CKM(r->taper.alloc(r->nstep), "taper");
+    CKM(r->simpw.alloc(r->nstep), "simpson weights");
     CKM(r->misfit_rc.alloc((size_t)r->nrec_max * 3), "misfits");
   }
-  if (taper_pct == r->taper_pct_cached && taper_type == r->taper_type_cached) return SEM_OK;
+  if (taper_pct == r->taper_pct_cached && taper_type == r->taper_type_cached &&
+      ns == r->taper_ns_cached)
+    return SEM_OK;
   std::vector<double> w(ns, 1.0);
   const int frac = (taper_pct == 0.0 || taper_pct == 1.0) ? (int)(ns * taper_pct / 2.0)
                                                           : (int)(ns * taper_pct / 2.0 + 0.5);
@@ -1011,6 +1025,7 @@ static int prepare_measure(sem_run* r, double taper_pct, int taper_type) {
   CK(cudaStreamSynchronize(r->stream));
   r->taper_pct_cached = taper_pct;
   r->taper_type_cached = taper_type;
+  r->taper_ns_cached = ns;
   return SEM_OK;
 }
 
@@ -1035,7 +1050,7 @@ int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int 
   const int ns = r->nstep, nr = r->nrec[ev];
   if (nr == 0) return fail(SEM_ERR_STATE, "event %d has no receivers", ev);
   if (!obs && !r->obs_ev.p) return fail(SEM_ERR_STATE, "no observed data for event %d", ev);
-  int rc = prepare_measure(r, taper_pct, taper_type);
+  int rc = prepare_measure(r, taper_pct, taper_type, ns);
   if (rc) return rc;
   const size_t per = (size_t)r->nrec_max * 3 * ns;
   const double* dobs;
@@ -1159,6 +1174,286 @@ int sem_time_kernels(sem_run* r, int sim_type, int nsteps, double* ms4) {
     }
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < 4; ++k) ms4[k] = acc[k] / nsteps;
+  return SEM_OK;
+}
+
+// ----------------------------------------------------------------------------
+// serving primitives: one event per lane, lanes advance independently
+// ----------------------------------------------------------------------------
+
+static void lane_defaults(sem_run* r, int e) {
+  const size_t ns = (size_t)r->nstep;  // per-lane regions are sized for the run's nstep
+  LaneDesc& L = r->h_lanes[e];
+  L.stf = r->stf.p + (size_t)e * ns;
+  L.srcarr = r->srcarr.p + (size_t)e * 375;
+  L.rec_ispec = r->rec_ispec.p + (size_t)e * r->nrec_max;
+  L.rec_w = r->rec_w.p + (size_t)e * r->nrec_max * 125;
+  L.seis = r->seis.p + (size_t)e * r->nrec_max * 3 * ns;
+  L.adj = r->adj.p + (size_t)e * r->nrec_max * 3 * ns;
+}
+
+static int enter_lanes_mode(sem_run* r) {
+  if (r->lanes_mode) return SEM_OK;
+  int rc = ensure_tuned(r);
+  if (rc) return rc;
+  rc = ensure_adjoint_buffers(r);
+  if (rc) return rc;
+  const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nevp;
+  CK(cudaMemsetAsync(r->u1.p, 0, n3 * 4, r->stream));
+  CK(cudaMemsetAsync(r->v1.p, 0, n3 * 4, r->stream));
+  CK(cudaMemsetAsync(r->a1.p, 0, n3 * 4, r->stream));
+  CK(cudaMemsetAsync(r->u2.p, 0, n3 * 4, r->stream));
+  CK(cudaMemsetAsync(r->v2.p, 0, n3 * 4, r->stream));
+  CK(cudaMemsetAsync(r->a2.p, 0, n3 * 4, r->stream));
+  r->h_lanes.assign(r->nev, LaneDesc{});
+  for (int e = 0; e < r->nev; ++e) {
+    r->h_lanes[e].phase = PH_IDLE;
+    lane_defaults(r, e);
+  }
+  r->lane_store.assign(r->nev, nullptr);
+  r->lane_scale.assign(r->nev, nullptr);
+  r->lane_saved.assign(r->nev, 0);
+  if (r->variant[0] < 0) r->variant[0] = 2;
+  if (r->variant[1] < 0) r->variant[1] = 2;
+  r->lanes_mode = true;
+  return SEM_OK;
+}
+
+static size_t lane_store_bytes(const sem_run* r, int nstep) {
+  const size_t per = (size_t)nstep * r->mesh->nf * 75 * r->store_elem();
+  return per + (r->cfg.store_kind == SEM_STORE_FP16 ? (size_t)nstep * r->mesh->nf * 4 : 0);
+}
+
+long long sem_lane_store_bytes(const sem_run* r, int nstep) {
+  if (!r || nstep < 1) return -1;
+  return (long long)lane_store_bytes(r, nstep);
+}
+
+int sem_lane_start_forward(sem_run* r, int lane, const sem_source* src, int nrec,
+                           const double* xyz, int nstep, int save_forward) {
+  if (!r || !src) return fail(SEM_ERR_ARG, "null argument");
+  if (lane < 0 || lane >= r->nev) return fail(SEM_ERR_ARG, "lane %d out of range", lane);
+  if (nstep < 1 || nstep > r->nstep)
+    return fail(SEM_ERR_ARG, "nstep %d outside [1, run nstep %d]", nstep, r->nstep);
+  int rc = enter_lanes_mode(r);
+  if (rc) return rc;
+  if (r->h_lanes[lane].phase != PH_IDLE) return fail(SEM_ERR_STATE, "lane %d is busy", lane);
+  // source and receivers of this lane (same set-up as sem_set_sources for
+  // one event; the time function covers the lane's own nstep)
+  const sem_source& s = *src;
+  if (!(s.f0 > 0.0) || !std::isfinite(s.x + s.y + s.z))
+    return fail(SEM_ERR_ARG, "invalid source position or f0");
+  double xi3[3];
+  r->src_ispec[lane] = r->mesh->locate(s.x, s.y, s.z, xi3);
+  const double Mzz = s.Mrr, Myy = s.Mtt, Mxx = s.Mpp;
+  const double Myz = -s.Mrt, Mxz = s.Mrp, Mxy = -s.Mtp;
+  const double M[3][3] = {{Mxx, Mxy, Mxz}, {Mxy, Myy, Myz}, {Mxz, Myz, Mzz}};
+  double hx[5], hxd[5], hy[5], hyd[5], hz[5], hzd[5];
+  lagrange_all(xi3[0], hx, hxd);
+  lagrange_all(xi3[1], hy, hyd);
+  lagrange_all(xi3[2], hz, hzd);
+  const double xix = (double)r->mesh->xix;
+  std::vector<float> sa(375), stf(nstep);
+  for (int c = 0; c < 5; ++c)
+    for (int b = 0; b < 5; ++b)
+      for (int a = 0; a < 5; ++a) {
+        const double gr[3] = {xix * hxd[a] * hy[b] * hz[c], xix * hx[a] * hyd[b] * hz[c],
+                              xix * hx[a] * hy[b] * hzd[c]};
+        const int p = a + 5 * b + 25 * c;
+        for (int k = 0; k < 3; ++k)
+          sa[p * 3 + k] = (float)(M[k][0] * gr[0] + M[k][1] * gr[1] + M[k][2] * gr[2]);
+      }
+  const double t0 = 1.2 / s.f0 + s.tshift;
+  for (int it = 0; it < nstep; ++it) stf[it] = (float)ricker((double)it * r->dt - t0, s.f0);
+  CK(cudaMemcpyAsync(r->srcarr.p + (size_t)lane * 375, sa.data(), 375 * 4,
+                     cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->stf.p + (size_t)lane * r->nstep, stf.data(), (size_t)nstep * 4,
+                     cudaMemcpyHostToDevice, r->stream));
+  r->have_src[lane] = 1;
+  rc = sem_set_receivers(r, lane, nrec, xyz);
+  if (rc) return rc;
+  // boundary store for the later adjoint run
+  if (r->lane_store[lane]) {
+    CK(cudaFreeAsync(r->lane_store[lane], r->stream));
+    r->lane_store[lane] = nullptr;
+  }
+  if (r->lane_scale[lane]) {
+    CK(cudaFreeAsync(r->lane_scale[lane], r->stream));
+    r->lane_scale[lane] = nullptr;
+  }
+  if (save_forward && r->mesh->nf > 0) {
+    cudaError_t e = cudaMallocAsync(&r->lane_store[lane],
+                                    (size_t)nstep * r->mesh->nf * 75 * r->store_elem(), r->stream);
+    if (e == cudaSuccess && r->cfg.store_kind == SEM_STORE_FP16)
+      e = cudaMallocAsync((void**)&r->lane_scale[lane], (size_t)nstep * r->mesh->nf * 4,
+                          r->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(SEM_ERR_NOMEM, "boundary store of lane %d (%d steps): %s", lane, nstep,
+                  cudaGetErrorString(e));
+    }
+  }
+  launch_lane_zero({r->u1.p, r->v1.p, r->a1.p}, r->mesh->nglob, r->lm, lane, r->stream);
+  CK(cudaGetLastError());
+  LaneDesc& L = r->h_lanes[lane];
+  lane_defaults(r, lane);
+  L.phase = PH_FWD;
+  L.it0 = 0;
+  L.nstep = nstep;
+  L.save = save_forward ? 1 : 0;
+  L.src_ispec = r->src_ispec[lane];
+  L.nrec = nrec;
+  L.store = r->lane_store[lane];
+  L.scale = r->lane_scale[lane];
+  r->lane_saved[lane] = 0;
+  return SEM_OK;
+}
+
+int sem_lane_start_adjoint(sem_run* r, int lane, const double* obs, double taper_pct,
+                           int taper_type, double* misfit) {
+  if (!r || !obs) return fail(SEM_ERR_ARG, "null argument");
+  if (!r->lanes_mode || lane < 0 || lane >= r->nev)
+    return fail(SEM_ERR_ARG, "lane %d is not a serving lane", lane);
+  LaneDesc& L = r->h_lanes[lane];
+  if (L.phase != PH_FWD || L.it0 < L.nstep || !L.save)
+    return fail(SEM_ERR_STATE, "lane %d has no completed forward run with a saved store", lane);
+  if (!(taper_pct >= 0.0 && taper_pct <= 1.0) || taper_type < 1 || taper_type > 4)
+    return fail(SEM_ERR_ARG, "invalid taper");
+  const int ns = L.nstep, nr = L.nrec;
+  int rc = prepare_measure(r, taper_pct, taper_type, ns);
+  if (rc) return rc;
+  if (!r->obs.p) CKM(r->obs.alloc((size_t)r->nrec_max * 3 * r->nstep), "observed data");
+  CK(cudaMemcpyAsync(r->obs.p, obs, (size_t)nr * 3 * ns * 8, cudaMemcpyHostToDevice,
+                     r->stream));
+  launch_measure_l2(L.seis, r->obs.p, r->taper.p, r->simpw.p, nr, ns, (float*)L.adj,
+                    r->misfit_rc.p, r->stream);
+  // backward field starts from this lane's final forward state
+  const Fields f1{r->u1.p, r->v1.p, r->a1.p}, f2{r->u2.p, r->v2.p, r->a2.p};
+  launch_lane_copy(f1, f2, r->mesh->nglob, r->lm, lane, r->stream);
+  launch_lane_zero(f1, r->mesh->nglob, r->lm, lane, r->stream);
+  launch_lane_zero_acc({r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->mesh->nglob,
+                       (size_t)r->mesh->nspec * NGLL3, r->lm, lane, r->stream);
+  CK(cudaGetLastError());
+  if (misfit) {
+    std::vector<double> m((size_t)nr * 3);
+    CK(cudaMemcpyAsync(m.data(), r->misfit_rc.p, m.size() * 8, cudaMemcpyDeviceToHost,
+                       r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    double t = 0.0;
+    for (double v : m) t += v;
+    *misfit = t;
+  }
+  L.phase = PH_ADJ;
+  L.it0 = 0;
+  L.save = 0;
+  return SEM_OK;
+}
+
+int sem_advance(sem_run* r, int nsteps) {
+  if (!r || nsteps < 1) return fail(SEM_ERR_ARG, "bad argument");
+  if (!r->lanes_mode) return fail(SEM_ERR_STATE, "no lane has been started");
+  bool any = false, adj = false;
+  for (auto& L : r->h_lanes)
+    if (L.phase != PH_IDLE && L.it0 < L.nstep) {
+      any = true;
+      adj |= L.phase == PH_ADJ;
+    }
+  if (!any) return SEM_OK;
+  CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
+                     r->stream));
+  StepArgs a = r->args(adj);
+  long long launches = 0;
+  int done = 0;
+  const int K = r->cfg.graph_steps;
+  if (r->cfg.use_graph && nsteps >= K) {
+    cudaGraphExec_t& gx = r->gexec[adj ? 1 : 0];
+    if (!gx) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
+      for (int s = 0; s < K; ++s) {
+        a.s = s;
+        launch_forces(a, adj, r->stream);
+        launch_boundary(a, adj, r->stream);
+        launch_points(a, r->stream);
+        launch_update(a, adj, r->stream);
+      }
+      launch_advance(r->lanes.p, r->nev, K, r->stream);
+      cudaError_t ce = cudaStreamEndCapture(r->stream, &g);
+      if (ce != cudaSuccess) return fail(SEM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&gx, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess)
+        return fail(SEM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+    }
+    for (; done + K <= nsteps; done += K) {
+      CK(cudaGraphLaunch(gx, r->stream));
+      launches += 4LL * K + 1;
+    }
+  }
+  if (done < nsteps) {
+    // remaining steps: lanes' device step counters have advanced by `done`
+    for (auto& L : r->h_lanes) L.it0 += done;
+    CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
+                       r->stream));
+    for (auto& L : r->h_lanes) L.it0 -= done;
+    for (int s = 0; s < nsteps - done; ++s) {
+      a.s = s;
+      launches += launch_forces(a, adj, r->stream);
+      launches += launch_boundary(a, adj, r->stream);
+      launches += launch_points(a, r->stream);
+      launches += launch_update(a, adj, r->stream);
+    }
+  }
+  CK(cudaGetLastError());
+  for (auto& L : r->h_lanes)
+    if (L.phase != PH_IDLE) L.it0 = std::min(L.nstep, L.it0 + nsteps);
+  r->last_launches = launches;
+  return SEM_OK;
+}
+
+int sem_lane_status(sem_run* r, int lane, int* phase, int* step, int* nstep) {
+  if (!r || lane < 0 || lane >= r->nev) return fail(SEM_ERR_ARG, "bad lane");
+  if (!r->lanes_mode) {
+    if (phase) *phase = PH_IDLE;
+    if (step) *step = 0;
+    if (nstep) *nstep = 0;
+    return SEM_OK;
+  }
+  const LaneDesc& L = r->h_lanes[lane];
+  if (phase) *phase = L.phase;
+  if (step) *step = L.it0;
+  if (nstep) *nstep = L.nstep;
+  return SEM_OK;
+}
+
+int sem_lane_finish(sem_run* r, int lane, float* seis, double* kernels6, double* ksum_dev) {
+  if (!r || !r->lanes_mode || lane < 0 || lane >= r->nev)
+    return fail(SEM_ERR_ARG, "lane %d is not a serving lane", lane);
+  LaneDesc& L = r->h_lanes[lane];
+  if (L.phase == PH_IDLE || L.it0 < L.nstep)
+    return fail(SEM_ERR_STATE, "lane %d has not completed a run", lane);
+  if (seis && L.phase == PH_FWD)
+    CK(cudaMemcpyAsync(seis, L.seis, (size_t)L.nrec * 3 * L.nstep * 4, cudaMemcpyDeviceToHost,
+                       r->stream));
+  if (L.phase == PH_ADJ && (kernels6 || ksum_dev)) {
+    const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+    if (kernels6 && !r->kout.p) CKM(r->kout.alloc(6 * ne), "kernel output");
+    launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p,
+                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->lm, lane,
+                            kernels6 ? r->kout.p : nullptr, ksum_dev, r->stream);
+    CK(cudaGetLastError());
+    if (kernels6)
+      CK(cudaMemcpyAsync(kernels6, r->kout.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  }
+  const bool keep_store = L.phase == PH_FWD && L.save;
+  if (!keep_store) {
+    if (r->lane_store[lane]) CK(cudaFreeAsync(r->lane_store[lane], r->stream));
+    if (r->lane_scale[lane]) CK(cudaFreeAsync(r->lane_scale[lane], r->stream));
+    r->lane_store[lane] = nullptr;
+    r->lane_scale[lane] = nullptr;
+    L.phase = PH_IDLE;
+  }
+  CK(cudaStreamSynchronize(r->stream));
   return SEM_OK;
 }
 

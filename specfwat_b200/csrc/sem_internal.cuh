@@ -125,6 +125,8 @@ int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, LaneMap lm
 int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane,
                      cudaStream_t st);
 int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st);
+int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int lane,
+                         cudaStream_t st);
 
 void set_gll_constants(const float* D, const float* DWt, const float* w);
 

@@ -13,6 +13,7 @@
 // k_update (Newmark corrector of this step fused with the predictor of the
 // next, plus the density-kernel product).
 
+#include <algorithm>
 #include <cstdio>
 
 #include "sem_internal.cuh"
@@ -1933,6 +1934,22 @@ int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, LaneMap lm
 int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane, cudaStream_t st) {
   const size_t n = (size_t)nglob * 3;
   k_lane_zero<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f, nglob, lm, lane);
+  return 1;
+}
+
+__global__ void k_lane_zero_acc(KernAcc k, int nglob, size_t ne, LaneMap lm, int lane) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < (size_t)nglob) k.rho_glob[lm.p(i, lane, (size_t)nglob)] = 0.f;
+  if (i < ne) {
+    k.mu[lm.p(i, lane, ne)] = 0.f;
+    k.kappa[lm.p(i, lane, ne)] = 0.f;
+  }
+}
+
+int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int lane,
+                         cudaStream_t st) {
+  const size_t n = std::max((size_t)nglob, ne);
+  k_lane_zero_acc<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(k, nglob, ne, lm, lane);
   return 1;
 }
 

@@ -1,0 +1,210 @@
+"""Serving loop: continuous batching of simulation requests on resident meshes.
+
+Requests (forward-only or forward+adjoint, each with its own source,
+receivers and record length) arrive over time.  Every resident mesh keeps
+one lane-batched run (``slots`` event lanes); a request is admitted into a
+free lane as soon as one exists and its boundary store fits the HBM budget,
+then advances together with whatever else is on that mesh in the same
+kernels.  A forward+adjoint request switches its lane to the adjoint run
+when its forward is done (FP64 L2 measurement on the device) and frees the
+lane when its kernels are summed; the next queued request takes the lane
+while the other lanes keep running.  Runs of different meshes sit on their
+own CUDA streams, so their work overlaps on the GPU.
+
+The reference has no serving layer: ``xfwat_fwd_measure_adj`` runs events
+one after another in one process (``fwat_fwd_measure_adj.f90:43-51``).
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from collections import deque
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import solver as S
+
+PH_IDLE, PH_FWD, PH_ADJ = 0, 1, 3
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    mesh: str
+    kind: str                  # "fwd" or "fwdadj"
+    nstep: int
+    source: object             # solver.make_source(...)
+    receivers: np.ndarray      # [nrec, 3]
+    obs: Optional[np.ndarray] = None   # [nrec, 3, nstep] for "fwdadj"
+    arrival: float = 0.0       # seconds after the start of the stream
+    want_kernels: bool = False
+    # results
+    admitted: float = float("nan")
+    done: float = float("nan")
+    misfit: float = float("nan")
+    seismograms: Optional[np.ndarray] = None
+    kernels: Optional[np.ndarray] = None
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+class MeshServer:
+    """One resident mesh and its lane-batched run."""
+
+    def __init__(self, name, db, slots, nstep_max, dt, store="fp16",
+                 graph_steps=50, max_receivers=128, store_budget=None,
+                 ksum_dev_ptr=0, taper_pct=0.05, taper_type=1):
+        self.name = name
+        self.mesh = S.Mesh(db)
+        self.sim = S.Simulation(self.mesh, nstep_max, dt, nev=slots,
+                                store=store, use_graph=True,
+                                graph_steps=graph_steps,
+                                max_receivers=max_receivers)
+        self.slots = slots
+        self.nstep_max = nstep_max
+        self.lanes: List[Optional[Request]] = [None] * slots
+        self.queue: deque = deque()
+        self.store_budget = store_budget
+        self.store_in_use = 0
+        self.lane_store = [0] * slots
+        self.ksum_dev_ptr = ksum_dev_ptr
+        self.taper = (taper_pct, taper_type)
+        self.nspec = db.nspec
+
+    # -- admission ----------------------------------------------------------
+    def try_admit(self, now):
+        started = 0
+        while self.queue:
+            req = self.queue[0]
+            free = [i for i, r in enumerate(self.lanes) if r is None]
+            if not free:
+                break
+            need = self.sim.lane_store_bytes(req.nstep) if req.kind == "fwdadj" else 0
+            if self.store_budget is not None and need and \
+                    self.store_in_use + need > self.store_budget:
+                break
+            self.queue.popleft()
+            lane = free[0]
+            self.sim.lane_start_forward(lane, req.source, req.receivers, req.nstep,
+                                        save_forward=req.kind == "fwdadj")
+            self.lanes[lane] = req
+            self.lane_store[lane] = need
+            self.store_in_use += need
+            req.admitted = now
+            started += 1
+        return started
+
+    def busy(self):
+        return any(r is not None for r in self.lanes)
+
+    def advance(self, nsteps):
+        if self.busy():
+            self.sim.advance(nsteps)
+
+    def remaining(self):
+        """Fewest steps until some active lane completes its phase."""
+        best = None
+        for lane, req in enumerate(self.lanes):
+            if req is None:
+                continue
+            ph, st, ns = self.sim.lane_status(lane)
+            if ph != PH_IDLE and st < ns:
+                best = ns - st if best is None else min(best, ns - st)
+        return best
+
+    # -- phase transitions ----------------------------------------------------
+    def poll(self, clock):
+        finished = []
+        for lane, req in enumerate(self.lanes):
+            if req is None:
+                continue
+            ph, st, ns = self.sim.lane_status(lane)
+            if ph == PH_IDLE or st < ns:
+                continue
+            if ph == PH_FWD and req.kind == "fwd":
+                req.seismograms = np.zeros((len(req.receivers), 3, req.nstep), np.float32)
+                self.sim.lane_finish(lane, seis_out=req.seismograms)
+                self._free(lane)
+                req.done = clock()
+                finished.append(req)
+            elif ph == PH_FWD:
+                req.seismograms = np.zeros((len(req.receivers), 3, req.nstep), np.float32)
+                self.sim.lane_finish(lane, seis_out=req.seismograms)
+                req.misfit = self.sim.lane_start_adjoint(lane, req.obs, *self.taper)
+            elif ph == PH_ADJ:
+                if req.want_kernels:
+                    req.kernels = np.zeros((6, self.nspec, 5, 5, 5), np.float64)
+                self.sim.lane_finish(lane, kernels_out=req.kernels,
+                                     ksum_dev_ptr=self.ksum_dev_ptr)
+                self._free(lane)
+                req.done = clock()
+                finished.append(req)
+        return finished
+
+    def _free(self, lane):
+        self.store_in_use -= self.lane_store[lane]
+        self.lane_store[lane] = 0
+        self.lanes[lane] = None
+
+    def close(self):
+        self.sim.close()
+        self.mesh.close()
+
+
+class Server:
+    """Request loop over several mesh servers.
+
+    ``run(requests)`` replays a stream: a request becomes visible at its
+    ``arrival`` time (wall clock from the start of the call), is queued on
+    its mesh, admitted when a lane and budget are free, and completes when
+    its results are on the host (and its kernels summed).  ``quantum`` is
+    the number of steps every busy mesh advances between scheduling
+    decisions (shortened when a lane completes sooner)."""
+
+    def __init__(self, servers: Dict[str, MeshServer], quantum=100):
+        self.servers = servers
+        self.quantum = quantum
+
+    def run(self, requests: List[Request], timeout=3600.0):
+        pending = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        clock = lambda: time.perf_counter() - t0  # noqa: E731
+        done: List[Request] = []
+        i = 0
+        while len(done) < len(requests):
+            now = clock()
+            if now > timeout:
+                raise TimeoutError("serving stream did not finish")
+            while i < len(pending) and pending[i].arrival <= now:
+                self.servers[pending[i].mesh].queue.append(pending[i])
+                i += 1
+            for srv in self.servers.values():
+                srv.try_admit(now)
+            busy = [s for s in self.servers.values() if s.busy()]
+            if not busy:
+                if i < len(pending):
+                    time.sleep(max(0.0, min(0.01, pending[i].arrival - clock())))
+                continue
+            for srv in busy:
+                rem = srv.remaining()
+                n = self.quantum if rem is None else max(1, min(self.quantum, rem))
+                srv.advance(n)
+            # one quantum in flight per mesh: new arrivals wait at most one
+            # quantum before they can take a lane
+            for srv in busy:
+                srv.sim.synchronize()
+            for srv in busy:
+                done += srv.poll(clock)
+        return done
+
+
+def latency_stats(reqs: List[Request]):
+    lat = np.array([r.latency for r in reqs])
+    span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
+    return {"n": len(reqs), "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "span_s": float(span),
+            "events_per_hour": len(reqs) / span * 3600.0}

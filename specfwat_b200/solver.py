@@ -211,6 +211,44 @@ class Simulation:
         check(_lib.load().sem_sum_kernels(self._h, out.ctypes.data))
         return out
 
+    # -- serving primitives (one event per lane, lanes advance together) --
+    def lane_store_bytes(self, nstep: int) -> int:
+        return int(_lib.load().sem_lane_store_bytes(self._h, nstep))
+
+    def lane_start_forward(self, lane: int, source, receivers, nstep: int,
+                           save_forward: bool):
+        xyz = np.ascontiguousarray(receivers, np.float64).reshape(-1, 3)
+        check(_lib.load().sem_lane_start_forward(
+            self._h, lane, C.byref(source), xyz.shape[0], xyz.ctypes.data,
+            int(nstep), int(save_forward)))
+        self.nrec[lane] = xyz.shape[0]
+
+    def lane_start_adjoint(self, lane: int, obs, taper_pct=0.05, taper_type=1,
+                           want_misfit=True):
+        obs = np.ascontiguousarray(obs, np.float64)
+        m = C.c_double()
+        check(_lib.load().sem_lane_start_adjoint(
+            self._h, lane, obs.ctypes.data, float(taper_pct), int(taper_type),
+            C.byref(m) if want_misfit else None))
+        return m.value if want_misfit else None
+
+    def advance(self, nsteps: int):
+        check(_lib.load().sem_advance(self._h, int(nsteps)))
+
+    def lane_status(self, lane: int):
+        ph, st, ns = C.c_int(), C.c_int(), C.c_int()
+        check(_lib.load().sem_lane_status(self._h, lane, C.byref(ph), C.byref(st),
+                                          C.byref(ns)))
+        return ph.value, st.value, ns.value
+
+    def lane_finish(self, lane: int, seis_out=None, kernels_out=None,
+                    ksum_dev_ptr: int = 0):
+        check(_lib.load().sem_lane_finish(
+            self._h, lane,
+            None if seis_out is None else seis_out.ctypes.data,
+            None if kernels_out is None else kernels_out.ctypes.data,
+            C.c_void_p(ksum_dev_ptr) if ksum_dev_ptr else None))
+
     def kernel_variants(self):
         """(forward, adjoint) element-kernel variants in use."""
         f, a = C.c_int(), C.c_int()

@@ -1,0 +1,102 @@
+"""Serving: continuous batching gives each request the result it gets alone.
+
+Requests of different kinds (forward-only, forward+adjoint), record lengths
+and meshes arrive at different times into fewer lanes than requests, so
+lanes are reused while others run; every result is compared with the same
+request run alone on the plain one-event path.
+"""
+import numpy as np
+import pytest
+
+from specfwat_b200 import database as D
+from specfwat_b200 import solver as S
+from specfwat_b200.serving import MeshServer, Request, Server, latency_stats
+
+pytestmark = pytest.mark.gpu
+
+SEIS_TOL = 1e-4
+KERN_TOL = 1e-3
+
+
+def rel(a, b, floor=0.0):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b)
+                 / max(np.linalg.norm(b), floor))
+
+
+def _requests(rng, name, db, n, kinds, nsteps, t0):
+    box = db.box
+    rec = D.surface_receivers(box, 3)
+    out = []
+    for k in range(n):
+        src = S.make_source(rng.uniform(0.3, 0.7) * box.lx, rng.uniform(0.3, 0.7) * box.ly,
+                            -rng.uniform(0.2, 0.5) * box.lz,
+                            D.random_moment_tensor(rng), rng.uniform(0.8, 1.2))
+        kind = kinds[k % len(kinds)]
+        ns = nsteps[k % len(nsteps)]
+        obs = None
+        if kind == "fwdadj":
+            obs = 0.01 * rng.standard_normal((len(rec), 3, ns)) * 1e-4
+        out.append(Request(rid=len(out), mesh=name, kind=kind, nstep=ns, source=src,
+                           receivers=rec, obs=obs, arrival=t0 + 0.03 * k,
+                           want_kernels=kind == "fwdadj"))
+    return out
+
+
+def _alone(db, req, dt):
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, req.nstep, dt, max_receivers=len(req.receivers))
+    sim.set_sources([req.source])
+    sim.set_receivers(req.receivers)
+    sim.iterate_time(1, save_forward=req.kind == "fwdadj")
+    seis = sim.seismograms(0)
+    out = dict(seis=seis)
+    if req.kind == "fwdadj":
+        out["misfit"] = sim.measure_l2(0, req.obs)
+        sim.iterate_time(3)
+        out["kernels"] = sim.save_adjoint_kernels(0)
+    sim.close()
+    mesh.close()
+    return out
+
+
+def test_results_same_alone_and_in_the_mix(gpu):
+    rng = np.random.default_rng(77)
+    dbs = {"small": D.build("small"), "mini": D.build("mini")}
+    dt = 0.02
+    reqs = (_requests(rng, "small", dbs["small"], 6, ["fwdadj", "fwd"], [300, 420, 240], 0.0)
+            + _requests(rng, "mini", dbs["mini"], 5, ["fwd", "fwdadj"], [260, 380], 0.01))
+    servers = {name: MeshServer(name, db, slots=3, nstep_max=450, dt=dt, store="fp32",
+                                graph_steps=20, max_receivers=16)
+               for name, db in dbs.items()}
+    done = Server(servers, quantum=40).run(reqs, timeout=600)
+    assert len(done) == len(reqs)
+    st = latency_stats(done)
+    assert st["p99_s"] >= st["p50_s"] > 0
+    for r in reqs:
+        a = _alone(dbs[r.mesh], r, dt)
+        floor = 0.01 * np.linalg.norm(a["seis"]) + 1e-30
+        assert rel(r.seismograms, a["seis"], floor) < SEIS_TOL, r.rid
+        if r.kind == "fwdadj":
+            assert abs(r.misfit - a["misfit"]) <= 1e-4 * abs(a["misfit"]), r.rid
+            for q in range(3):
+                assert rel(r.kernels[q], a["kernels"][q]) < KERN_TOL, (r.rid, q)
+    for srv in servers.values():
+        assert srv.store_in_use == 0
+        srv.close()
+
+
+def test_store_budget_limits_admission(gpu):
+    rng = np.random.default_rng(5)
+    db = D.build("mini")
+    srv = MeshServer("mini", db, slots=4, nstep_max=300, dt=0.02, store="fp16",
+                     graph_steps=20, max_receivers=16)
+    one = srv.sim.lane_store_bytes(300)
+    srv.store_budget = int(1.5 * one)      # room for one forward+adjoint store
+    reqs = _requests(rng, "mini", db, 3, ["fwdadj"], [300], 0.0)
+    for r in reqs:
+        srv.queue.append(r)
+    assert srv.try_admit(0.0) == 1
+    assert srv.store_in_use == one
+    done = Server({"mini": srv}, quantum=50).run([], timeout=60)
+    assert done == []
+    srv.close()
