@@ -48,7 +48,7 @@ WORKLOAD = ("medium box 40x40x20 el over 160x160x80 km (2,099,601 GLL pts), "
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=2)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--events", type=int, default=32)
@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=1)
     p.add_argument("--store", default="fp16", choices=["fp16", "fp32"])
+    p.add_argument("--served-requests", type=int, default=48)
+    p.add_argument("--served-load", type=float, default=0.8,
+                   help="Poisson arrival rate as a fraction of batched capacity")
     return p.parse_args()
 
 
@@ -238,15 +241,22 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
 
     # observed data (synthetic, before timing): batched forward on the
     # anomaly model
-    mesh_obs = S.Mesh(db_obs)
-    so = S.Simulation(mesh_obs, NS, dt, nev=E, use_graph=True,
-                      max_receivers=len(rec))
-    so.set_sources(srcs)
-    so.set_receivers(rec)
-    so.iterate_time(1)
-    obs = [so.seismograms(e).astype(np.float64) for e in range(E)]
-    so.close()
-    mesh_obs.close()
+    def observed(sources):
+        mesh_obs = S.Mesh(db_obs)
+        out = []
+        for c0 in range(0, len(sources), 32):
+            chunk = sources[c0:c0 + 32]
+            so = S.Simulation(mesh_obs, NS, dt, nev=len(chunk), use_graph=True,
+                              max_receivers=len(rec))
+            so.set_sources(chunk)
+            so.set_receivers(rec)
+            so.iterate_time(1)
+            out += [so.seismograms(e).astype(np.float64) for e in range(len(chunk))]
+            so.close()
+        mesh_obs.close()
+        return out
+
+    obs = observed(srcs)
 
     mesh = S.Mesh(db)
     result = {}
@@ -374,6 +384,46 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         e2e = float(tt.item())
     sb.close()
 
+    # ---- served: continuous batching of a Poisson request stream ----------
+    served = None
+    if args.served_requests > 0:
+        from specfwat_b200.serving import MeshServer, Request, Server, latency_stats
+        NR = args.served_requests
+        _, _, _, sev = make_workload(args.mesh, NR, 5000 + rank)
+        ssrc = [S.make_source(x, y, z, mt, f0) for (x, y, z, mt, f0) in sev]
+        sobs = observed(ssrc)
+        cap = E / (ms_per_step / 1e3)            # batched capacity, events/s
+        lam = args.served_load * cap
+        arr = np.cumsum(np.random.default_rng(99 + rank).exponential(1.0 / lam, NR))
+        arr -= arr[0]
+        reqs = [Request(rid=i, mesh=args.mesh, kind="fwdadj", nstep=NS, source=ssrc[i],
+                        receivers=rec, obs=sobs[i], arrival=float(arr[i]))
+                for i in range(NR)]
+        ksum_srv = torch.zeros((6, ne), dtype=torch.float64, device=dev)
+        srv = MeshServer(args.mesh, db, slots=E, nstep_max=NS, dt=dt, store=args.store,
+                         graph_steps=50, max_receivers=len(rec),
+                         ksum_dev_ptr=ksum_srv.data_ptr())
+        if dist is not None:
+            dist.barrier()
+        done = Server({args.mesh: srv}, quantum=100).run(reqs, timeout=3000)
+        srv.close()
+        st = latency_stats(done)
+        served = {"requests": NR, "kind": "fwd+adj", "arrivals": "Poisson",
+                  "arrival_rate_per_hour": lam * 3600.0, "slots": E, **st}
+        if "plain" in result:
+            # the plain path serves one request at a time (FIFO) with its
+            # measured per-event time, on the same arrival sequence
+            svc = result["plain"]["ms_per_event"] / 1e3
+            t_free, lat = 0.0, []
+            for a in arr:
+                start = max(a, t_free)
+                t_free = start + svc
+                lat.append(t_free - a)
+            served["plain_fifo"] = {
+                "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)),
+                "events_per_hour": NR / (t_free - arr[0]) * 3600.0}
+
     nglob = db.nglob
     adj_bytes = algorithmic_bytes(db.nspec, nglob, E, True)
     fwd_bytes = algorithmic_bytes(db.nspec, nglob, E, False)
@@ -445,6 +495,8 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
     }
     if "plain" in result:
         line["plain"] = result["plain"]
+    if served:
+        line["served"] = served
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
