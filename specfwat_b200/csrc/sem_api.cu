@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -603,6 +604,18 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   r->nstep = c->nstep;
   r->dt = c->dt;
   r->nrec_max = c->max_receivers;
+  // SEM_FORCE_VARIANTS="f,a" pins the autotuned element-kernel variants
+  // (public numbering 1..6) for the forward and adjoint phases, so that a
+  // profiler run replays the choice made by an unprofiled run.
+  if (c->kernel_variant == 0) {
+    const char* fv = std::getenv("SEM_FORCE_VARIANTS");
+    int vf = 0, va = 0;
+    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 6 && va >= 1 &&
+        va <= 6) {
+      r->variant[0] = vf - 1;
+      r->variant[1] = va - 1;
+    }
+  }
   CK(cudaStreamCreateWithFlags(&r->own_stream, cudaStreamNonBlocking));
   r->stream = r->own_stream;
   CK(cudaEventCreate(&r->e0));
