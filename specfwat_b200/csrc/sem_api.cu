@@ -286,6 +286,7 @@ struct sem_run_s {
   std::vector<char> lane_saved;   // lane finished a forward with saved store
   bool lanes_mode = false;        // run driven through the sem_lane_* calls
   DevArray<int> flag;
+  DevArray<int> gmap;             // serving: active 8-lane groups
   std::vector<int> src_ispec, nrec;
   std::vector<char> have_src, have_rec, have_adj;
   bool fwd_saved = false, adj_done = false;
@@ -1366,56 +1367,38 @@ int sem_advance(sem_run* r, int nsteps) {
   if (!r || nsteps < 1) return fail(SEM_ERR_ARG, "bad argument");
   if (!r->lanes_mode) return fail(SEM_ERR_STATE, "no lane has been started");
   bool any = false, adj = false;
-  for (auto& L : r->h_lanes)
+  const int lw = 1 << r->lm.lwlog;
+  std::vector<int> groups;
+  for (int e = 0; e < r->nev; ++e) {
+    const LaneDesc& L = r->h_lanes[e];
     if (L.phase != PH_IDLE && L.it0 < L.nstep) {
       any = true;
       adj |= L.phase == PH_ADJ;
+      const int g = e / lw;
+      if (groups.empty() || groups.back() != g) groups.push_back(g);
     }
+  }
   if (!any) return SEM_OK;
   CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
                      r->stream));
   StepArgs a = r->args(adj);
-  long long launches = 0;
-  int done = 0;
-  const int K = r->cfg.graph_steps;
-  if (r->cfg.use_graph && nsteps >= K) {
-    cudaGraphExec_t& gx = r->gexec[adj ? 1 : 0];
-    if (!gx) {
-      cudaGraph_t g;
-      CK(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
-      for (int s = 0; s < K; ++s) {
-        a.s = s;
-        launch_forces(a, adj, r->stream);
-        launch_boundary(a, adj, r->stream);
-        launch_points(a, r->stream);
-        launch_update(a, adj, r->stream);
-      }
-      launch_advance(r->lanes.p, r->nev, K, r->stream);
-      cudaError_t ce = cudaStreamEndCapture(r->stream, &g);
-      if (ce != cudaSuccess) return fail(SEM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-      ce = cudaGraphInstantiate(&gx, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess)
-        return fail(SEM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-    }
-    for (; done + K <= nsteps; done += K) {
-      CK(cudaGraphLaunch(gx, r->stream));
-      launches += 4LL * K + 1;
-    }
+  if (lw > 1) {
+    // only the 8-lane groups that hold running events are worked
+    if (!r->gmap.p) CKM(r->gmap.alloc((size_t)(r->nevp / lw)), "group map");
+    CK(cudaMemcpyAsync(r->gmap.p, groups.data(), groups.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, r->stream));
+    a.gmap = r->gmap.p;
+    a.ngmap = (int)groups.size();
+    // the persistent element kernels are the ones that walk a group map
+    if (a.variant < 2) a.variant = 2;
   }
-  if (done < nsteps) {
-    // remaining steps: lanes' device step counters have advanced by `done`
-    for (auto& L : r->h_lanes) L.it0 += done;
-    CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
-                       r->stream));
-    for (auto& L : r->h_lanes) L.it0 -= done;
-    for (int s = 0; s < nsteps - done; ++s) {
-      a.s = s;
-      launches += launch_forces(a, adj, r->stream);
-      launches += launch_boundary(a, adj, r->stream);
-      launches += launch_points(a, r->stream);
-      launches += launch_update(a, adj, r->stream);
-    }
+  long long launches = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    a.s = s;
+    launches += launch_forces(a, adj, r->stream);
+    launches += launch_boundary(a, adj, r->stream);
+    launches += launch_points(a, r->stream);
+    launches += launch_update(a, adj, r->stream);
   }
   CK(cudaGetLastError());
   for (auto& L : r->h_lanes)

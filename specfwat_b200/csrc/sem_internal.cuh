@@ -96,6 +96,8 @@ struct StepArgs {
   int nrec_max;
   int variant;           // element kernel: 0 thread-per-point, 1 pencil
   LaneMap lm;            // lane-group layout of the per-event arrays
+  const int* gmap;       // serving: active 8-lane groups (device), or null
+  int ngmap;
   __device__ __forceinline__ size_t fi(size_t ig, int c, int lg) const {
     return lm.f(ig, c, lg, (size_t)m.nglob);
   }

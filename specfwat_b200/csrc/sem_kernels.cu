@@ -661,19 +661,37 @@ struct PipeLayout {
 // all resident blocks sweep the mesh for one group of event lanes at a
 // time and the working set of shared GLL points stays in L2; the sub-chunks
 // of one 32-byte sector of lanes (LB < 8) take adjacent items.
+// With `gmap` (serving: only some 8-lane groups hold running events) the
+// sector groups walked are gmap[0..nsg-1]; otherwise 0..nsg-1.
 struct PipeItems {
   int ngroups, nchunk, spg;
+  int nsg;              // sector groups walked
+  const int* gmap;      // device list of active sector groups, or null
   __device__ __forceinline__ void decode(int w, int& chunk, int& g) const {
     const int per = ngroups * spg;
-    const int sg = w / per;
-    const int rem = w - sg * per;
+    const int k = w / per;
+    const int rem = w - k * per;
     g = rem / spg;
+    const int sg = gmap ? gmap[k] : k;
     chunk = sg * spg + (rem - g * spg);
   }
-  __host__ __device__ __forceinline__ int count() const {
-    return ((nchunk + spg - 1) / spg) * spg * ngroups;
-  }
+  __host__ __device__ __forceinline__ int count() const { return nsg * spg * ngroups; }
 };
+
+// Work items of a launch: lane chunks of LB lanes, grouped by the 8-lane
+// (32-byte) sector groups of the lane-group layout.
+template <int LB>
+static PipeItems make_items(const StepArgs& a, int ngroups) {
+  PipeItems it;
+  it.ngroups = ngroups;
+  it.nchunk = (a.nev + LB - 1) / LB;
+  const int lw = 1 << a.lm.lwlog;
+  it.spg = (lw > LB && a.nev > LB) ? lw / LB : 1;
+  const int nsg_all = (it.nchunk + it.spg - 1) / it.spg;
+  it.gmap = a.gmap;
+  it.nsg = a.gmap ? a.ngmap : nsg_all;
+  return it;
+}
 
 template <int LB, int EPB, int TPE, bool ADJ>
 __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, PipeItems items) {
@@ -900,10 +918,8 @@ static void forces_piped_cfg(const StepArgs& a, cudaStream_t st) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
-  PipeItems items;
-  items.ngroups = (a.m.nspec + EPB - 1) / EPB;
-  items.nchunk = (a.nev + LB - 1) / LB;
-  items.spg = (LB >= 8 || a.nev <= LB) ? 1 : 8 / LB;
+  PipeItems items = make_items<LB>(a, (a.m.nspec + EPB - 1) / EPB);
+  if (items.count() == 0) return;
   int gx = blocks_per_sm * sms;
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
@@ -1449,10 +1465,8 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
-  PipeItems items;
-  items.ngroups = a.m.nspec;
-  items.nchunk = (a.nev + LB - 1) / LB;
-  items.spg = (LB >= 8 || a.nev <= LB) ? 1 : 8 / LB;
+  PipeItems items = make_items<LB>(a, a.m.nspec);
+  if (items.count() == 0) return;
   int gx = blocks_per_sm * sms;
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
@@ -1741,10 +1755,11 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
   const int nev = A.nev;
   const int lwlog = A.lm.lwlog;
   const size_t nglob = (size_t)A.m.nglob;
-  const size_t ngroups = ((size_t)nev + (1u << lwlog) - 1) >> lwlog;
+  const size_t ngroups = A.gmap ? (size_t)A.ngmap : ((size_t)nev + (1u << lwlog) - 1) >> lwlog;
   if (idx >= (ngroups * nglob) << lwlog) return;
-  const size_t grp = idx / (nglob << lwlog);
-  const size_t rem = idx - grp * (nglob << lwlog);
+  const size_t kg = idx / (nglob << lwlog);
+  const size_t rem = idx - kg * (nglob << lwlog);
+  const size_t grp = A.gmap ? (size_t)A.gmap[kg] : kg;
   const size_t ig = rem >> lwlog;
   const int lg = (int)((grp << lwlog) + (rem & ((1u << lwlog) - 1)));
   if (lg >= nev) return;
@@ -1812,7 +1827,9 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
 
 int launch_update(const StepArgs& a, bool adj, cudaStream_t st) {
   const int lw = 1 << a.lm.lwlog;
-  const size_t n = (size_t)a.m.nglob * (size_t)((a.nev + lw - 1) / lw) * lw;
+  const size_t ng = a.gmap ? (size_t)a.ngmap : (size_t)((a.nev + lw - 1) / lw);
+  const size_t n = (size_t)a.m.nglob * ng * lw;
+  if (n == 0) return 0;
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (adj)
     k_update<true><<<blocks, 256, 0, st>>>(a);
