@@ -58,9 +58,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=1)
     p.add_argument("--store", default="fp16", choices=["fp16", "fp32"])
-    p.add_argument("--served-requests", type=int, default=48)
-    p.add_argument("--served-load", type=float, default=0.8,
-                   help="Poisson arrival rate as a fraction of batched capacity")
+    p.add_argument("--served-requests", type=int, default=64)
+    p.add_argument("--served-load", type=float, default=1.25,
+                   help="Poisson arrival rate as a fraction of batched capacity "
+                        "(above 1: a saturated server, throughput-limited)")
     return p.parse_args()
 
 

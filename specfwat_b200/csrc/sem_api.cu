@@ -1366,39 +1366,60 @@ int sem_lane_start_adjoint(sem_run* r, int lane, const double* obs, double taper
 int sem_advance(sem_run* r, int nsteps) {
   if (!r || nsteps < 1) return fail(SEM_ERR_ARG, "bad argument");
   if (!r->lanes_mode) return fail(SEM_ERR_STATE, "no lane has been started");
-  bool any = false, adj = false;
+  // 8-lane groups with running events, split by phase: a group with any
+  // adjoint lane goes to the two-field kernels, an all-forward group to the
+  // one-field kernels
   const int lw = 1 << r->lm.lwlog;
-  std::vector<int> groups;
+  const int ngr = r->nevp / lw;
+  std::vector<int> has(ngr, 0);
+  bool any = false;
   for (int e = 0; e < r->nev; ++e) {
     const LaneDesc& L = r->h_lanes[e];
     if (L.phase != PH_IDLE && L.it0 < L.nstep) {
       any = true;
-      adj |= L.phase == PH_ADJ;
-      const int g = e / lw;
-      if (groups.empty() || groups.back() != g) groups.push_back(g);
+      has[e / lw] |= (L.phase == PH_ADJ) ? 2 : 1;
     }
   }
   if (!any) return SEM_OK;
+  std::vector<int> gmap;  // [fwd groups..., adj groups...]
+  for (int g = 0; g < ngr; ++g)
+    if (has[g] == 1) gmap.push_back(g);
+  const int nf = (int)gmap.size();
+  for (int g = 0; g < ngr; ++g)
+    if (has[g] & 2) gmap.push_back(g);
+  const int na = (int)gmap.size() - nf;
   CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
                      r->stream));
-  StepArgs a = r->args(adj);
+  if (!r->gmap.p) CKM(r->gmap.alloc((size_t)std::max(1, ngr)), "group map");
+  CK(cudaMemcpyAsync(r->gmap.p, gmap.data(), gmap.size() * sizeof(int), cudaMemcpyHostToDevice,
+                     r->stream));
+  StepArgs af = r->args(false), aa = r->args(true), ab = r->args(na > 0);
   if (lw > 1) {
-    // only the 8-lane groups that hold running events are worked
-    if (!r->gmap.p) CKM(r->gmap.alloc((size_t)(r->nevp / lw)), "group map");
-    CK(cudaMemcpyAsync(r->gmap.p, groups.data(), groups.size() * sizeof(int),
-                       cudaMemcpyHostToDevice, r->stream));
-    a.gmap = r->gmap.p;
-    a.ngmap = (int)groups.size();
+    af.gmap = r->gmap.p;
+    af.ngmap = nf;
+    aa.gmap = r->gmap.p + nf;
+    aa.ngmap = na;
     // the persistent element kernels are the ones that walk a group map
-    if (a.variant < 2) a.variant = 2;
+    if (af.variant < 2) af.variant = 2;
+    if (aa.variant < 2) aa.variant = 2;
   }
   long long launches = 0;
   for (int s = 0; s < nsteps; ++s) {
-    a.s = s;
-    launches += launch_forces(a, adj, r->stream);
-    launches += launch_boundary(a, adj, r->stream);
-    launches += launch_points(a, r->stream);
-    launches += launch_update(a, adj, r->stream);
+    af.s = aa.s = ab.s = s;
+    if (lw == 1) {
+      launches += launch_forces(ab, na > 0, r->stream);
+    } else {
+      if (nf) launches += launch_forces(af, false, r->stream);
+      if (na) launches += launch_forces(aa, true, r->stream);
+    }
+    launches += launch_boundary(ab, na > 0, r->stream);
+    launches += launch_points(ab, r->stream);
+    if (lw == 1) {
+      launches += launch_update(ab, na > 0, r->stream);
+    } else {
+      if (nf) launches += launch_update(af, false, r->stream);
+      if (na) launches += launch_update(aa, true, r->stream);
+    }
   }
   CK(cudaGetLastError());
   for (auto& L : r->h_lanes)

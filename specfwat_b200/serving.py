@@ -73,6 +73,7 @@ class MeshServer:
         self.ksum_dev_ptr = ksum_dev_ptr
         self.taper = (taper_pct, taper_type)
         self.nspec = db.nspec
+        self.phase = [PH_IDLE] * slots
 
     # -- admission ----------------------------------------------------------
     def try_admit(self, now):
@@ -87,15 +88,23 @@ class MeshServer:
                     self.store_in_use + need > self.store_budget:
                 break
             self.queue.popleft()
-            lane = free[0]
+            # prefer a lane whose 8-lane group runs no adjoint field, so
+            # forward lanes share the cheaper one-field launches
+            lane = min(free, key=lambda l: (self._adj_in_group(l), l))
             self.sim.lane_start_forward(lane, req.source, req.receivers, req.nstep,
                                         save_forward=req.kind == "fwdadj")
             self.lanes[lane] = req
+            self.phase[lane] = PH_FWD
             self.lane_store[lane] = need
             self.store_in_use += need
             req.admitted = now
             started += 1
         return started
+
+    def _adj_in_group(self, lane):
+        g = lane // 8
+        return sum(1 for l in range(8 * g, min(8 * g + 8, self.slots))
+                   if self.phase[l] == PH_ADJ)
 
     def busy(self):
         return any(r is not None for r in self.lanes)
@@ -134,6 +143,7 @@ class MeshServer:
                 req.seismograms = np.zeros((len(req.receivers), 3, req.nstep), np.float32)
                 self.sim.lane_finish(lane, seis_out=req.seismograms)
                 req.misfit = self.sim.lane_start_adjoint(lane, req.obs, *self.taper)
+                self.phase[lane] = PH_ADJ
             elif ph == PH_ADJ:
                 if req.want_kernels:
                     req.kernels = np.zeros((6, self.nspec, 5, 5, 5), np.float64)
@@ -145,6 +155,7 @@ class MeshServer:
         return finished
 
     def _free(self, lane):
+        self.phase[lane] = PH_IDLE
         self.store_in_use -= self.lane_store[lane]
         self.lane_store[lane] = 0
         self.lanes[lane] = None
