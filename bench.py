@@ -403,14 +403,16 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         ksum_srv = torch.zeros((6, ne), dtype=torch.float64, device=dev)
         srv = MeshServer(args.mesh, db, slots=E, nstep_max=NS, dt=dt, store=args.store,
                          graph_steps=50, max_receivers=len(rec),
-                         ksum_dev_ptr=ksum_srv.data_ptr())
+                         ksum_dev_ptr=ksum_srv.data_ptr(), policy="group",
+                         max_wait=2.0)
         if dist is not None:
             dist.barrier()
         done = Server({args.mesh: srv}, quantum=100).run(reqs, timeout=3000)
         srv.close()
         st = latency_stats(done)
         served = {"requests": NR, "kind": "fwd+adj", "arrivals": "Poisson",
-                  "arrival_rate_per_hour": lam * 3600.0, "slots": E, **st}
+                  "arrival_rate_per_hour": lam * 3600.0, "slots": E,
+                  "policy": "8-lane groups, admitted when full or after 2 s", **st}
         if "plain" in result:
             # the plain path serves one request at a time (FIFO) with its
             # measured per-event time, on the same arrival sequence

@@ -56,7 +56,8 @@ class MeshServer:
 
     def __init__(self, name, db, slots, nstep_max, dt, store="fp16",
                  graph_steps=50, max_receivers=128, store_budget=None,
-                 ksum_dev_ptr=0, taper_pct=0.05, taper_type=1):
+                 ksum_dev_ptr=0, taper_pct=0.05, taper_type=1, policy="lane",
+                 group=8, max_wait=1.5):
         self.name = name
         self.mesh = S.Mesh(db)
         self.sim = S.Simulation(self.mesh, nstep_max, dt, nev=slots,
@@ -74,9 +75,34 @@ class MeshServer:
         self.taper = (taper_pct, taper_type)
         self.nspec = db.nspec
         self.phase = [PH_IDLE] * slots
+        # "lane": a request takes any free lane at once.  "group": requests
+        # enter an 8-lane group together once the group is free and either a
+        # full group is queued or the oldest request has waited `max_wait`
+        # seconds, so a group's lanes stay in the same phase and share the
+        # cheaper one-field launches while forward.
+        self.policy = policy
+        self.group = group
+        self.max_wait = max_wait
 
     # -- admission ----------------------------------------------------------
+    def _admit_one(self, req, lane, now):
+        need = self.sim.lane_store_bytes(req.nstep) if req.kind == "fwdadj" else 0
+        self.sim.lane_start_forward(lane, req.source, req.receivers, req.nstep,
+                                    save_forward=req.kind == "fwdadj")
+        self.lanes[lane] = req
+        self.phase[lane] = PH_FWD
+        self.lane_store[lane] = need
+        self.store_in_use += need
+        req.admitted = now
+
+    def _fits(self, req):
+        need = self.sim.lane_store_bytes(req.nstep) if req.kind == "fwdadj" else 0
+        return self.store_budget is None or not need or \
+            self.store_in_use + need <= self.store_budget
+
     def try_admit(self, now):
+        if self.policy == "group":
+            return self._admit_groups(now)
         started = 0
         while self.queue:
             req = self.queue[0]
@@ -99,6 +125,28 @@ class MeshServer:
             self.store_in_use += need
             req.admitted = now
             started += 1
+        return started
+
+    def _admit_groups(self, now):
+        started = 0
+        g = self.group
+        while self.queue:
+            full = len(self.queue) >= g
+            waited = now - self.queue[0].arrival >= self.max_wait
+            if not (full or waited):
+                break
+            free = [k for k in range(self.slots // g)
+                    if all(self.lanes[l] is None for l in range(k * g, (k + 1) * g))]
+            if not free:
+                break
+            base = free[0] * g
+            n = 0
+            while self.queue and n < g and self._fits(self.queue[0]):
+                self._admit_one(self.queue.popleft(), base + n, now)
+                n += 1
+            if n == 0:
+                break
+            started += n
         return started
 
     def _adj_in_group(self, lane):

@@ -85,6 +85,24 @@ def test_results_same_alone_and_in_the_mix(gpu):
         srv.close()
 
 
+def test_group_policy_same_results(gpu):
+    rng = np.random.default_rng(31)
+    db = D.build("small")
+    dt = 0.02
+    reqs = _requests(rng, "small", db, 10, ["fwdadj"], [260], 0.0)
+    srv = MeshServer("small", db, slots=16, nstep_max=260, dt=dt, store="fp16",
+                     graph_steps=20, max_receivers=16, policy="group", max_wait=0.05)
+    done = Server({"small": srv}, quantum=60).run(reqs, timeout=600)
+    assert len(done) == len(reqs)
+    for r in reqs[:3]:
+        a = _alone(db, r, dt)
+        floor = 0.01 * np.linalg.norm(a["seis"]) + 1e-30
+        assert rel(r.seismograms, a["seis"], floor) < SEIS_TOL
+        for q in range(3):
+            assert rel(r.kernels[q], a["kernels"][q]) < 5e-3   # FP16 store
+    srv.close()
+
+
 def test_store_budget_limits_admission(gpu):
     rng = np.random.default_rng(5)
     db = D.build("mini")
