@@ -1,0 +1,144 @@
+"""The standard workloads at their real sizes (B200).
+
+* small box (10x10x10 el, 41^3 points), full NSTEP 2000 forward against the
+  FP32 and FP64 oracle;
+* medium box (40x40x20 el, 2.1M points) forward + adjoint with kernels
+  against the FP32 oracle over a shortened record;
+* large box (96x96x48 el, 28.6M points, layered model): 4 events batched
+  vs each event alone, FP16 store, and the HBM sizing of 8 events;
+* failure detection: a time step far above the stability limit is
+  reported as SEM_ERR_NUMERIC by the device non-finite check, the context
+  stays usable.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from specfwat_b200 import database as D
+from specfwat_b200 import solver as S
+from oracle.oracle import Oracle, l2_adjoint_source
+
+pytestmark = pytest.mark.gpu
+NTH = os.cpu_count() or 1
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+def test_small_full_record_matches_oracle(gpu):
+    db = D.build("small")
+    rec = D.surface_receivers(db.box, 5)
+    mt = D.random_moment_tensor(np.random.default_rng(1234))
+    nstep, dt = 2000, 0.02
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec), use_graph=True)
+    sim.set_sources([S.make_source(20000., 20000., -10000., mt, 1.0)])
+    sim.set_receivers(rec)
+    sim.iterate_time(1)
+    g = sim.seismograms(0)
+    src = Oracle.source(20000., 20000., -10000., mt, 1.0)
+    o32 = Oracle(db, precision=4, nthreads=NTH).forward(dt, nstep, src, rec)
+    o64 = Oracle(db, precision=8, nthreads=NTH).forward(dt, nstep, src, rec)
+    assert rel(g, o32) < 1e-4
+    assert rel(g, o64) < 1e-4
+
+
+def test_medium_fwd_adj_kernels_match_oracle(gpu):
+    db = D.build("medium")
+    vp, vs, rho = D.background_model(db, seed=1234)
+    db_obs = db.with_model(vp, D.gaussian_vs_anomaly(db, vs), rho)
+    rec = D.surface_receivers(db.box, 10)
+    mt = D.random_moment_tensor(np.random.default_rng(7))
+    xyz = (80000.0, 80000.0, -20000.0)
+    nstep, dt = 150, 0.02
+    src = Oracle.source(*xyz, mt, 1.0)
+    # observed data from the anomaly model on the GPU (validated path)
+    mesh_obs = S.Mesh(db_obs)
+    so = S.Simulation(mesh_obs, nstep, dt, max_receivers=len(rec))
+    so.set_sources([S.make_source(*xyz, mt, 1.0)])
+    so.set_receivers(rec)
+    so.iterate_time(1)
+    obs = so.seismograms(0).astype(np.float64) + 1e-9
+    so.close()
+    mesh_obs.close()
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec))
+    sim.set_sources([S.make_source(*xyz, mt, 1.0)])
+    sim.set_receivers(rec)
+    sim.iterate_time(1, save_forward=True)
+    syn = sim.seismograms(0)
+    sim.measure_l2(0, obs)
+    sim.iterate_time(3)
+    kg = sim.save_adjoint_kernels(0)
+    o = Oracle(db, precision=4, nthreads=NTH)
+    osyn = o.forward(dt, nstep, src, rec, save_forward=True)
+    _, adj = l2_adjoint_source(osyn, obs, dt)
+    ok = o.adjoint(rec, adj)
+    assert rel(syn, osyn) < 1e-4
+    for q in range(3):
+        assert rel(kg[q], ok[q]) < 1e-3, q
+
+
+def test_large_mesh_batched_equals_alone_and_fits(gpu):
+    db = D.build("large")
+    assert db.nglob == 385 * 385 * 193
+    rec = D.surface_receivers(db.box, 10)
+    rng = np.random.default_rng(3)
+    box = db.box
+    srcs = [S.make_source(rng.uniform(0.3, 0.7) * box.lx, rng.uniform(0.3, 0.7) * box.ly,
+                          -rng.uniform(5e3, 40e3), D.random_moment_tensor(rng),
+                          rng.uniform(0.5, 1.5)) for _ in range(4)]
+    nstep, dt = 120, 0.015
+    mesh = S.Mesh(db)
+    # 8 events with NSTEP 6000 and an FP16 store: the run's device bytes
+    big = S._lib.RunCfg(8, 6000, dt, S._lib.SEM_STORE_FP16, 1, 50, len(rec), 0, 0)
+    need = S._lib.load().sem_run_bytes(mesh.handle, big)
+    assert need > 150e9
+    b = S.Simulation(mesh, nstep, dt, nev=4, store="fp16", use_graph=True,
+                     max_receivers=len(rec))
+    b.set_sources(srcs)
+    b.set_receivers(rec)
+    b.iterate_time(1, save_forward=True)
+    for e in range(4):
+        b.measure_l2(e, np.zeros((len(rec), 3, nstep)))
+    b.iterate_time(3)
+    kb = b.save_adjoint_kernels(2)
+    sb = b.seismograms(2)
+    b.close()
+    p = S.Simulation(mesh, nstep, dt, nev=1, store="fp16", max_receivers=len(rec))
+    p.set_sources([srcs[2]])
+    p.set_receivers(rec)
+    p.iterate_time(1, save_forward=True)
+    p.measure_l2(0, np.zeros((len(rec), 3, nstep)))
+    p.iterate_time(3)
+    assert rel(sb, p.seismograms(0)) < 1e-4
+    kp = p.save_adjoint_kernels(0)
+    for q in range(3):
+        assert rel(kb[q], kp[q]) < 1e-3
+    p.close()
+    mesh.close()
+
+
+def test_unstable_time_step_is_reported_not_faulted(gpu):
+    db = D.build("tiny")
+    rec = D.surface_receivers(db.box, 2)
+    mt = D.random_moment_tensor(np.random.default_rng(1))
+    mesh = S.Mesh(db)
+    # dt 40x above the CFL limit: the explicit scheme blows up
+    sim = S.Simulation(mesh, 400, 0.8, max_receivers=len(rec), check_every=1)
+    sim.set_sources([S.make_source(6000., 6000., -6000., mt, 0.2)])
+    sim.set_receivers(rec)
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.iterate_time(1)
+    assert ei.value.code == -6
+    sim.close()
+    # the context is still usable afterwards
+    ok = S.Simulation(mesh, 50, 0.02, max_receivers=len(rec), check_every=1)
+    ok.set_sources([S.make_source(6000., 6000., -6000., mt, 1.0)])
+    ok.set_receivers(rec)
+    ok.iterate_time(1)
+    assert np.isfinite(ok.seismograms(0)).all()
+    ok.close()
+    mesh.close()
