@@ -202,3 +202,40 @@ def test_state_errors(gpu, small):
     with pytest.raises(S._lib.SemError) as ei:
         sim.set_receivers(np.zeros((len(rec) + 1, 3)))
     assert ei.value.code == -1
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
+def test_batched_adjoint_distinct_events_equal_alone(gpu, variant):
+    """Each lane has its own source and observed data: the batched adjoint
+    must give every event the kernels it gets alone."""
+    db = D.build("mini")
+    rec = D.surface_receivers(db.box, 3)
+    rng = np.random.default_rng(40 + variant)
+    nev, nstep, dt = 5, 260, 0.02
+    box = db.box
+    srcs = [S.make_source(rng.uniform(0.3, 0.7) * box.lx, rng.uniform(0.3, 0.7) * box.ly,
+                          -rng.uniform(0.2, 0.6) * box.lz, D.random_moment_tensor(rng),
+                          rng.uniform(0.8, 1.3)) for _ in range(nev)]
+    obs = [1e-5 * rng.standard_normal((len(rec), 3, nstep)) for _ in range(nev)]
+    mesh = S.Mesh(db)
+    b = S.Simulation(mesh, nstep, dt, nev=nev, max_receivers=len(rec),
+                     kernel_variant=variant)
+    b.set_sources(srcs)
+    b.set_receivers(rec)
+    b.iterate_time(1, save_forward=True)
+    for e in range(nev):
+        b.measure_l2(e, obs[e])
+    b.iterate_time(3)
+    kb = [b.save_adjoint_kernels(e) for e in range(nev)]
+    b.close()
+    for e in range(nev):
+        p = S.Simulation(mesh, nstep, dt, nev=1, max_receivers=len(rec), kernel_variant=2)
+        p.set_sources([srcs[e]])
+        p.set_receivers(rec)
+        p.iterate_time(1, save_forward=True)
+        p.measure_l2(0, obs[e])
+        p.iterate_time(3)
+        kp = p.save_adjoint_kernels(0)
+        p.close()
+        for q in range(3):
+            assert rel_l2(kb[e][q], kp[q]) < 1e-3, (e, q, rel_l2(kb[e][q], kp[q]))
