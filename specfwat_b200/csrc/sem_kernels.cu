@@ -301,6 +301,23 @@ __device__ __forceinline__ float gW(int i) {
   return t[i];
 }
 
+// Per-lane base offsets of the lane-group layout with the group width known
+// at compile time (LWLOG 0: one event, 3: groups of 8): a field value is
+// base(lg) + (ig*3 + c) << LWLOG, a per-point value base(lg) + i << LWLOG.
+template <int LWLOG>
+__device__ __forceinline__ size_t fbase(const StepArgs& A, int lg) {
+  return (((size_t)(lg >> LWLOG) * (size_t)A.m.nglob * 3) << LWLOG) + (lg & ((1 << LWLOG) - 1));
+}
+template <int LWLOG>
+__device__ __forceinline__ size_t ebase(const StepArgs& A, int lg) {
+  return (((size_t)(lg >> LWLOG) * (size_t)A.m.nspec * NGLL3) << LWLOG) +
+         (lg & ((1 << LWLOG) - 1));
+}
+template <int LWLOG>
+__device__ __forceinline__ size_t foff(int ig, int c) {
+  return ((size_t)ig * 3 + c) << LWLOG;
+}
+
 // shared floats per (field, element, lane): U/B region then A region
 constexpr int PR_U = 640;  // >= 625 (B: 5 sigma components)
 constexpr int PR_A = 768;  // >= 750 (6 derivative / divergence components)
@@ -455,8 +472,8 @@ __device__ __forceinline__ void pencil_div_eg(const PencilBuf<LB>& b, int t) {
 // xi role: total force on the xi-pencil and scatter-add.
 template <int LB>
 __device__ __forceinline__ void pencil_scatter(const PencilBuf<LB>& b, int t, const float fx[5][3],
-                                               const int* s_ib, float* acc, const StepArgs& A,
-                                               int lg) {
+                                               const int* s_ib, float* accb) {
+  constexpr int LWLOG = LB == 1 ? 0 : 3;
   const int pj = t % 5, pk = t / 5;
   float wj = 0.f, wk = 0.f;
 #pragma unroll
@@ -471,7 +488,7 @@ __device__ __forceinline__ void pencil_scatter(const PencilBuf<LB>& b, int t, co
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float f = -(wj * wk * fx[i][c] + gW(i) * wk * b.Ar(c, p) + gW(i) * wj * b.Ar(3 + c, p));
-      atomicAdd(&acc[A.fi(ig, c, lg)], f);
+      atomicAdd(&accb[foff<LWLOG>((int)ig, c)], f);
     }
   }
 }
@@ -614,8 +631,9 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
   __syncthreads();
   if (e < A.m.nspec) {
     const int* ib = s_ib + el * NGLL3;
-    if (s_act[0][lane]) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, A, lg);
-    if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, A, lg);
+    constexpr int LWL = LB == 1 ? 0 : 3;
+    if (s_act[0][lane]) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a + fbase<LWL>(A, lg));
+    if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a + fbase<LWL>(A, lg));
   }
 }
 
@@ -667,13 +685,24 @@ struct PipeItems {
   int ngroups, nchunk, spg;
   int nsg;              // sector groups walked
   const int* gmap;      // device list of active sector groups, or null
+  int spg_log;          // spg = 1 << spg_log
+  float inv_per;        // 1 / (ngroups * spg)
   __device__ __forceinline__ void decode(int w, int& chunk, int& g) const {
-    const int per = ngroups * spg;
-    const int k = w / per;
-    const int rem = w - k * per;
-    g = rem / spg;
+    // w / per by a float reciprocal, corrected to the exact quotient
+    const int per = ngroups << spg_log;
+    int k = __float2int_rz((float)w * inv_per);
+    int rem = w - k * per;
+    while (rem < 0) {
+      --k;
+      rem += per;
+    }
+    while (rem >= per) {
+      ++k;
+      rem -= per;
+    }
+    g = rem >> spg_log;
     const int sg = gmap ? gmap[k] : k;
-    chunk = sg * spg + (rem - g * spg);
+    chunk = (sg << spg_log) + (rem & (spg - 1));
   }
   __host__ __device__ __forceinline__ int count() const { return nsg * spg * ngroups; }
 };
@@ -690,6 +719,8 @@ static PipeItems make_items(const StepArgs& a, int ngroups) {
   const int nsg_all = (it.nchunk + it.spg - 1) / it.spg;
   it.gmap = a.gmap;
   it.nsg = a.gmap ? a.ngmap : nsg_all;
+  it.spg_log = it.spg == 1 ? 0 : it.spg == 2 ? 1 : it.spg == 4 ? 2 : 3;
+  it.inv_per = 1.0f / (float)(it.ngroups * it.spg);
   return it;
 }
 
@@ -723,18 +754,28 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
   }
   if (!__syncthreads_or(any)) return;
 
+  constexpr int LWLOG = LB == 1 ? 0 : 3;
+  if (A.lm.lwlog != LWLOG) return;  // launched only with the matching layout
+
   // lane state of this thread for item w: bit0 active, bit1 adjoint field,
-  // bit2 adjoint scatter
+  // bit2 adjoint scatter; cached per lane chunk (fixed within a launch)
+  int c_chunk = -1, c_flag = 0;
   auto flags = [&](int w, int& lg, int& g) -> int {
     int chunk;
     items.decode(w, chunk, g);
     lg = chunk * LB + lane;
-    if (chunk >= items.nchunk || lg >= nev) return 0;
-    const LaneDesc* L = A.lanes + lg;
-    const int it = L->it0 + A.s;
-    if (L->phase == PH_IDLE || it >= L->nstep) return 0;
-    int f = 1;
-    if (ADJ && L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
+    if (chunk == c_chunk) return c_flag;
+    int f = 0;
+    if (chunk < items.nchunk && lg < nev) {
+      const LaneDesc* L = A.lanes + lg;
+      const int it = L->it0 + A.s;
+      if (L->phase != PH_IDLE && it < L->nstep) {
+        f = 1;
+        if (ADJ && L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
+      }
+    }
+    c_chunk = chunk;
+    c_flag = f;
     return f;
   };
   auto issue_ib = [&](int w, int slot) {
@@ -764,10 +805,11 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
       }
     }
     if (pen) {
+      const size_t fb = fbase<LWLOG>(A, lg);
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
         const bool act = f == 0 ? (fl & 1) : (fl & 2);
-        const float* src = f == 0 ? A.f1.u : A.f2.u;
+        const float* src = (f == 0 ? A.f1.u : A.f2.u) + fb;
         float* ub = sU + (((buf * NF + f) * EPB + el) * PP_U) * LB + lane;
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
@@ -777,7 +819,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
           for (int c = 0; c < 3; ++c) {
             float* d = ub + (c * NGLL3 + p) * LB;
             if (act && ig >= 0)
-              cp_async4(d, src + A.fi((size_t)ig, c, lg));
+              cp_async4(d, src + foff<LWLOG>(ig, c));
             else
               *d = 0.f;
           }
@@ -787,11 +829,11 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
         const int es = g * EPB + el;
         float* kb = sK + buf * 2 * NE * LB;
         if (es < nspec) {
-          const int e = A.m.order[es];
+          const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)A.m.order[es] * NGLL3) << LWLOG);
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
             const int p = t + 25 * r;
-            const size_t q = A.ei((size_t)e * NGLL3 + p, lg);
+            const size_t q = eb + ((size_t)p << LWLOG);
             cp_async4(kb + (el * NGLL3 + p) * LB + lane, A.k.mu + q);
             cp_async4(kb + (NE + el * NGLL3 + p) * LB + lane, A.k.kappa + q);
           }
@@ -875,7 +917,7 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
             const float dd = a_xx * bv[0] + a_yy * bv[1] + (a_xx + a_yy) * (bv[0] + bv[1]) +
                              2.0f * (a_xy * bv[2] + a_xz * bv[3] + a_yz * bv[4]);
             const int p = i + 5 * t;
-            const size_t q = A.ei((size_t)e * NGLL3 + p, lg);
+            const size_t q = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3 + p) << LWLOG);
             A.k.mu[q] = kb[(el * NGLL3 + p) * LB + lane] + dtk * dd;
             A.k.kappa[q] = kb[(NE + el * NGLL3 + p) * LB + lane] + dtk * (tr1 * bv[5]);
           }
@@ -895,8 +937,8 @@ __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, Pip
     __syncthreads();
     if (pen && e < nspec) {
       const int* ib = sIB + ibs * NE + el * NGLL3;
-      if (act1) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a, A, lg);
-      if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a, A, lg);
+      if (act1) pencil_scatter<LB>(b1, t, fx1, ib, A.f1.a + fbase<LWLOG>(A, lg));
+      if (ADJ && scat2) pencil_scatter<LB>(b2, t, fx2, ib, A.f2.a + fbase<LWLOG>(A, lg));
     }
   }
   cp_wait_all();
@@ -1229,8 +1271,7 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
 // xi role: total force on the pencil and vector scatter-add.
 template <int LB, int NL>
 __device__ __forceinline__ void v_scatter(const PBuf<LB>& b, int t, const LV<NL> fx[5][3],
-                                          const int* ib, float* acc, const StepArgs& A, int lg,
-                                          const int* fl, int bit) {
+                                          const int* ib, float* accb, const int* fl, int bit) {
   const int pj = t % 5, pk = t / 5;
   float wj = 0.f, wk = 0.f;
 #pragma unroll
@@ -1254,7 +1295,7 @@ __device__ __forceinline__ void v_scatter(const PBuf<LB>& b, int t, const LV<NL>
         const float v = -(wjk * fx[i][c].v[n] + wik * e1.v[n] + wij * e2.v[n]);
         f.v[n] = (fl[n] & bit) ? v : 0.f;  // lanes not in this phase add nothing
       }
-      red_v<NL>(&acc[A.fi(ig, c, lg)], f);
+      red_v<NL>(&accb[foff<3>((int)ig, c)], f);
     }
   }
 }
@@ -1303,17 +1344,28 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
     if (ADJ && L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
     return f;
   };
+  constexpr int LWLOG = 3;
+  if (A.lm.lwlog != LWLOG) return;  // batched layout only
+  int c_chunk = -1, c_any = 0, c_fl[NL];
+#pragma unroll
+  for (int n = 0; n < NL; ++n) c_fl[n] = 0;
+  // flags of the NL lanes of item w, cached per lane chunk
   auto group_flags = [&](int w, int& lg0, int& g, int fl[NL]) {
     int chunk;
     items.decode(w, chunk, g);
     lg0 = chunk * LB + lane;
-    int any_f = 0;
+    if (chunk != c_chunk) {
+      c_any = 0;
 #pragma unroll
-    for (int n = 0; n < NL; ++n) {
-      fl[n] = (chunk < items.nchunk) ? lane_flag(lg0 + n) : 0;
-      any_f |= fl[n];
+      for (int n = 0; n < NL; ++n) {
+        c_fl[n] = (chunk < items.nchunk) ? lane_flag(lg0 + n) : 0;
+        c_any |= c_fl[n];
+      }
+      c_chunk = chunk;
     }
-    return any_f;
+#pragma unroll
+    for (int n = 0; n < NL; ++n) fl[n] = c_fl[n];
+    return c_any;
   };
   auto issue_ib = [&](int w, int slot) {
     int* dst = sIB + slot * NE;
@@ -1340,10 +1392,11 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
         cp_async4(km + NE + i, A.m.mu + ep);
       }
     }
+    const size_t fb = fbase<LWLOG>(A, lg0);
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
       const bool act = f == 0 ? (anyf & 1) : (anyf & 2);
-      const float* src = f == 0 ? A.f1.u : A.f2.u;
+      const float* src = (f == 0 ? A.f1.u : A.f2.u) + fb;
       float* ub = sU + ((buf * NF + f) * PP_U) * LB + lane;
 #pragma unroll
       for (int r = 0; r < 5; ++r) {
@@ -1353,7 +1406,7 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
         for (int c = 0; c < 3; ++c) {
           float* d = ub + (c * NGLL3 + p) * LB;
           if (act && ig >= 0) {
-            cp_async_v<NL>(d, src + A.fi((size_t)ig, c, lg0));
+            cp_async_v<NL>(d, src + foff<LWLOG>(ig, c));
           } else {
             LV<NL> z;
 #pragma unroll
@@ -1365,12 +1418,13 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
     }
     if (ADJ && (anyf & 2) && g < nspec) {
       float* kb = sK + buf * 2 * NE * LB;
+      const size_t eb = ebase<LWLOG>(A, lg0) + (((size_t)e * NGLL3) << LWLOG);
 #pragma unroll
       for (int r = 0; r < 5; ++r) {
         const int p = t + 25 * r;
-        const size_t ep = (size_t)e * NGLL3 + p;
-        cp_async_v<NL>(kb + p * LB + lane, A.k.mu + A.ei(ep, lg0));
-        cp_async_v<NL>(kb + (NE + p) * LB + lane, A.k.kappa + A.ei(ep, lg0));
+        const size_t q = eb + ((size_t)p << LWLOG);
+        cp_async_v<NL>(kb + p * LB + lane, A.k.mu + q);
+        cp_async_v<NL>(kb + (NE + p) * LB + lane, A.k.kappa + q);
       }
     }
   };
@@ -1428,7 +1482,7 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
             mo.v[n] = on ? m0.v[n] + dtk * km[i].v[n] : m0.v[n];
             ko.v[n] = on ? k0.v[n] + dtk * kk[i].v[n] : k0.v[n];
           }
-          const size_t q = A.ei((size_t)e * NGLL3 + p, lg0);
+          const size_t q = ebase<LWLOG>(A, lg0) + (((size_t)e * NGLL3 + p) << LWLOG);
           sts_v<NL>(A.k.mu + q, mo);
           sts_v<NL>(A.k.kappa + q, ko);
         }
@@ -1443,8 +1497,9 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
     __syncthreads();
     if (e < nspec) {
       const int* ib = sIB + ibs * NE;
-      if (anyf & 1) v_scatter<LB, NL>(b1, t, fx1, ib, A.f1.a, A, lg0, fl, 1);
-      if (ADJ && (anyf & 4)) v_scatter<LB, NL>(b2, t, fx2, ib, A.f2.a, A, lg0, fl, 4);
+      const size_t fb = fbase<LWLOG>(A, lg0);
+      if (anyf & 1) v_scatter<LB, NL>(b1, t, fx1, ib, A.f1.a + fb, fl, 1);
+      if (ADJ && (anyf & 4)) v_scatter<LB, NL>(b2, t, fx2, ib, A.f2.a + fb, fl, 4);
     }
   }
   cp_wait_all();
