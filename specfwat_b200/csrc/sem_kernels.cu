@@ -1505,6 +1505,306 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
   cp_wait_all();
 }
 
+// ---------------------------------------------------------------------------
+// adjoint-phase element kernel: (adjoint, backward) field pair as a float2
+// ---------------------------------------------------------------------------
+//
+// In the adjoint phase every event carries two fields on the same element
+// with the same kappa and mu.  Here they are the two values of one float2:
+// shared memory holds "virtual lanes" (event, field), a thread works one
+// event's pencil for both fields with float2 shared traffic, and the
+// strain products for the mu/kappa kernels are formed in registers at each
+// point, with no parking in shared memory.
+
+template <int VL>
+__device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* kap, const float* mu,
+                                        float fac, LV<2> fx[5][3], float kmu[5], float kka[5]) {
+  LV<2> u[3][5];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int l = 0; l < 5; ++l) u[c][l] = lds_v<2>(b.U(c, l + 5 * t));
+  LV<2> sx[3][5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    LV<2> de[3], dg[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      de[c] = lds_v<2>(b.Ar(c, p));
+      dg[c] = lds_v<2>(b.Ar(3 + c, p));
+    }
+    LV<2> o[5];
+    float ev[2][6];
+    const float kp = kap[p], m = mu[p];
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+      float g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = fmaf(gD(i, l), u[c][l].v[n], a);
+        g[c][0] = a;
+        g[c][1] = de[c].v[n];
+        g[c][2] = dg[c].v[n];
+      }
+      float sig[6];
+      stress_point(g, kp, m, fac, sig);
+      sx[0][i].v[n] = sig[0];
+      sx[1][i].v[n] = sig[3];
+      sx[2][i].v[n] = sig[4];
+      o[0].v[n] = sig[3];
+      o[1].v[n] = sig[1];
+      o[2].v[n] = sig[5];
+      o[3].v[n] = sig[4];
+      o[4].v[n] = sig[2];
+      const float tr = g[0][0] + g[1][1] + g[2][2];
+      ev[n][0] = g[0][0] - tr * (1.0f / 3.0f);
+      ev[n][1] = g[1][1] - tr * (1.0f / 3.0f);
+      ev[n][2] = 0.5f * (g[0][1] + g[1][0]);
+      ev[n][3] = 0.5f * (g[0][2] + g[2][0]);
+      ev[n][4] = 0.5f * (g[1][2] + g[2][1]);
+      ev[n][5] = tr;
+    }
+    // adjoint (n = 0) x backward (n = 1) deviatoric products and traces
+    kmu[i] = ev[0][0] * ev[1][0] + ev[0][1] * ev[1][1] +
+             (ev[0][0] + ev[0][1]) * (ev[1][0] + ev[1][1]) +
+             2.0f * (ev[0][2] * ev[1][2] + ev[0][3] * ev[1][3] + ev[0][4] * ev[1][4]);
+    kka[i] = ev[0][5] * ev[1][5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) sts_v<2>(b.U(q, p), o[q]);
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = fmaf(gDWt(i, l), sx[c][l].v[n], a);
+        fx[i][c].v[n] = a;
+      }
+}
+
+template <int VL>
+__device__ __forceinline__ void pair_scatter(const PBuf<VL>& b, int t, const LV<2> fx[5][3],
+                                             const int* ib, float* accb1, float* accb2, bool on1,
+                                             bool on2) {
+  const int pj = t % 5, pk = t / 5;
+  float wj = 0.f, wk = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q == pj) wj = gW(q);
+    if (q == pk) wk = gW(q);
+  }
+  const float wjk = wj * wk;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    const int ig = ib[p];
+    const float wik = gW(i) * wk, wij = gW(i) * wj;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const LV<2> e1 = lds_v<2>(b.Ar(c, p));
+      const LV<2> e2 = lds_v<2>(b.Ar(3 + c, p));
+      const size_t q = foff<3>(ig, c);
+      if (on1) atomicAdd(&accb1[q], -(wjk * fx[i][c].v[0] + wik * e1.v[0] + wij * e2.v[0]));
+      if (on2) atomicAdd(&accb2[q], -(wjk * fx[i][c].v[1] + wik * e1.v[1] + wij * e2.v[1]));
+    }
+  }
+}
+
+template <int LB>
+struct PairLayout {
+  using LY = PipeLayout<2 * LB, 1, 25, false>;
+  static constexpr int OFF_K = al4(LY::TOTAL);                     // [2][2][125][LB]
+  static constexpr int TOTAL = OFF_K + 4 * NGLL3 * LB;
+  static constexpr size_t BYTES = (size_t)TOTAL * 4;
+};
+
+template <int LB>
+__global__ void __launch_bounds__(25 * LB) k_forces_adjpair(StepArgs A, PipeItems items) {
+  constexpr int VL = 2 * LB;
+  constexpr int NT = 25 * LB;
+  using LY = typename PairLayout<LB>::LY;
+  constexpr int NE = LY::NE;
+  constexpr int LWLOG = 3;
+  extern __shared__ float sm[];
+  int* sIB = (int*)(sm + LY::OFF_IB);
+  float* sKM = sm + LY::OFF_KM;
+  float* sU = sm + LY::OFF_U;
+  float* sA = sm + LY::OFF_A;
+  float* sK = sm + PairLayout<LB>::OFF_K;
+
+  const int tid = threadIdx.x;
+  const int lq = tid % LB;
+  const int t = tid / LB;
+  const int pi = t % 5, pq = t / 5;
+  const int nev = A.nev;
+  const int nspec = A.m.nspec;
+  const int nitems = items.count();
+
+  bool any = false;
+  for (int l = tid; l < nev; l += NT) {
+    const LaneDesc* L = A.lanes + l;
+    any |= L->phase != PH_IDLE && L->it0 + A.s < L->nstep;
+  }
+  if (!__syncthreads_or(any)) return;
+  if (A.lm.lwlog != LWLOG) return;  // batched layout only
+
+  int c_chunk = -1, c_flag = 0;
+  auto flags = [&](int w, int& lg, int& g) -> int {
+    int chunk;
+    items.decode(w, chunk, g);
+    lg = chunk * LB + lq;
+    if (chunk == c_chunk) return c_flag;
+    int f = 0;
+    if (chunk < items.nchunk && lg < nev) {
+      const LaneDesc* L = A.lanes + lg;
+      const int it = L->it0 + A.s;
+      if (L->phase != PH_IDLE && it < L->nstep) {
+        f = 1;
+        if (L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
+      }
+    }
+    c_chunk = chunk;
+    c_flag = f;
+    return f;
+  };
+  auto issue_ib = [&](int w, int slot) {
+    int* dst = sIB + slot * NE;
+    int chunk = 0, g = 0;
+    if (w < nitems) items.decode(w, chunk, g);
+    for (int i = tid; i < NE; i += NT) {
+      if (w < nitems && g < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      else
+        dst[i] = -1;
+    }
+  };
+  auto issue_data = [&](int w, int ibslot, int buf) {
+    if (w >= nitems) return;
+    int lg, g;
+    const int fl = flags(w, lg, g);
+    const int* ib = sIB + ibslot * NE;
+    float* km = sKM + buf * 2 * NE;
+    const int e = g < nspec ? A.m.order[g] : 0;
+    for (int i = tid; i < NE; i += NT) {
+      if (g < nspec) {
+        const size_t ep = (size_t)e * NGLL3 + i;
+        cp_async4(km + i, A.m.kappa + ep);
+        cp_async4(km + NE + i, A.m.mu + ep);
+      }
+    }
+    const size_t fb = fbase<LWLOG>(A, lg);
+    float* ub = sU + (buf * PP_U) * VL + 2 * lq;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int p = t + 25 * r;
+      const int ig = ib[p];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float* d = ub + (c * NGLL3 + p) * VL;
+        if ((fl & 1) && ig >= 0)
+          cp_async4(d, A.f1.u + fb + foff<LWLOG>(ig, c));
+        else
+          d[0] = 0.f;
+        if ((fl & 2) && ig >= 0)
+          cp_async4(d + 1, A.f2.u + fb + foff<LWLOG>(ig, c));
+        else
+          d[1] = 0.f;
+      }
+    }
+    if ((fl & 2) && g < nspec) {
+      float* kb = sK + buf * 2 * NGLL3 * LB;
+      const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3) << LWLOG);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int p = t + 25 * r;
+        const size_t q = eb + ((size_t)p << LWLOG);
+        cp_async4(kb + p * LB + lq, A.k.mu + q);
+        cp_async4(kb + (NGLL3 + p) * LB + lq, A.k.kappa + q);
+      }
+    }
+  };
+
+  int w = blockIdx.x;
+  issue_ib(w, 0);
+  cp_commit();
+  cp_wait_all();
+  __syncthreads();
+  issue_data(w, 0, 0);
+  issue_ib(w + gridDim.x, 1);
+  cp_commit();
+
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  const float dtk = A.dt * A.m.xix * A.m.xix;
+  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+    const int buf = k & 1;
+    const int ibs = k % 3;
+    cp_wait_all();
+    __syncthreads();
+    issue_data(w + gridDim.x, (k + 1) % 3, buf ^ 1);
+    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    cp_commit();
+
+    int lg, g;
+    const int fl = flags(w, lg, g);
+    const int e = g < nspec ? A.m.order[g] : nspec;
+    const float* kap = sKM + buf * 2 * NE;
+    const float* mu = kap + NE;
+    PBuf<VL> b{sU + (buf * PP_U) * VL + 2 * lq, sA + 2 * lq};
+    v_grad_eg<VL, 2>(b, pi, pq);
+    __syncthreads();
+    LV<2> fx[5][3];
+    float kmu[5], kka[5];
+    pair_xi<VL>(b, t, kap, mu, fac, fx, kmu, kka);
+    if ((fl & 2) && e < nspec) {
+      const float* kb = sK + buf * 2 * NGLL3 * LB;
+      const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3) << LWLOG);
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const int p = i + 5 * t;
+        const size_t q = eb + ((size_t)p << LWLOG);
+        A.k.mu[q] = kb[p * LB + lq] + dtk * kmu[i];
+        A.k.kappa[q] = kb[(NGLL3 + p) * LB + lq] + dtk * kka[i];
+      }
+    }
+    __syncthreads();
+    v_div_eg<VL, 2>(b, pi, pq);
+    __syncthreads();
+    if (e < nspec && (fl & 1)) {
+      const size_t fb = fbase<LWLOG>(A, lg);
+      pair_scatter<VL>(b, t, fx, sIB + ibs * NE, A.f1.a + fb, A.f2.a + fb, true, (fl & 4) != 0);
+    }
+  }
+  cp_wait_all();
+}
+
+template <int LB>
+static void forces_adjpair_cfg(const StepArgs& a, cudaStream_t st) {
+  constexpr int NT = 25 * LB;
+  constexpr size_t BYTES = PairLayout<LB>::BYTES;
+  static int blocks_per_sm = 0, sms = 0;
+  if (!blocks_per_sm) {
+    cudaFuncSetAttribute(k_forces_adjpair<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_adjpair<LB>, NT, BYTES);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  PipeItems items = make_items<LB>(a, a.m.nspec);
+  if (items.count() == 0) return;
+  int gx = blocks_per_sm * sms;
+  if (gx > items.count()) gx = items.count();
+  if (gx < 1) gx = 1;
+  k_forces_adjpair<LB><<<gx, NT, BYTES, st>>>(a, items);
+}
+
 template <int LB, int NL, bool ADJ>
 static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
   using LY = PipeLayout<LB, 1, 25, ADJ>;
@@ -1531,8 +1831,19 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
 // Element-kernel variants (StepArgs::variant):
 //   0 thread-per-point, 1 pencil, 2 pencil pipelined (lanes per block by
 //   event count), 3 pencil pipelined with 2 lanes per block, 4 pencil
-//   pipelined with 2 lanes per thread, 5 as 4 with more lanes per block.
+//   pipelined with 2 lanes per thread, 5 as 4 with more lanes per block,
+//   6 / 7 adjoint phase with the (adjoint, backward) field pair of an
+//   event as a float2, 4 / 8 events per block.
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if ((a.variant == 6 || a.variant == 7) && a.nev > 1) {
+    if (!adj)
+      forces_vec_cfg<8, 2, false>(a, st);
+    else if (a.variant == 6)
+      forces_adjpair_cfg<4>(a, st);
+    else
+      forces_adjpair_cfg<8>(a, st);
+    return 1;
+  }
   if (a.variant == 4 && a.nev > 1) {
     if (adj)
       forces_vec_cfg<4, 2, true>(a, st);
