@@ -163,7 +163,8 @@ def test_graph_equals_stepwise(gpu, small):
     assert rel_l2(out[1], out[0]) < 1e-5
 
 
-@pytest.mark.parametrize("nev,variant", [(2, 0), (9, 0), (9, 5), (12, 6), (9, 7), (12, 8)])
+@pytest.mark.parametrize("nev,variant", [(2, 0), (9, 0), (9, 5), (12, 6), (9, 7), (12, 8),
+                                         (9, 9), (12, 10)])
 def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
@@ -204,7 +205,7 @@ def test_state_errors(gpu, small):
     assert ei.value.code == -1
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 def test_batched_adjoint_distinct_events_equal_alone(gpu, variant):
     """Each lane has its own source and observed data: the batched adjoint
     must give every event the kernels it gets alone."""
