@@ -565,8 +565,8 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->max_receivers < 1 || c->max_receivers > 100000)
     return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
-  if (c->kernel_variant < 0 || c->kernel_variant > 10)
-    return fail(SEM_ERR_ARG, "kernel_variant must be 0..10");
+  if (c->kernel_variant < 0 || c->kernel_variant > 11)
+    return fail(SEM_ERR_ARG, "kernel_variant must be 0..11");
   return SEM_OK;
 }
 
@@ -611,8 +611,8 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   if (c->kernel_variant == 0) {
     const char* fv = std::getenv("SEM_FORCE_VARIANTS");
     int vf = 0, va = 0;
-    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 10 && va >= 1 &&
-        va <= 10) {
+    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 11 && va >= 1 &&
+        va <= 11) {
       r->variant[0] = vf - 1;
       r->variant[1] = va - 1;
     }
@@ -781,10 +781,10 @@ static int ensure_store(sem_run* r) {
 // keep the fastest.  Runs on scratch state before the forward run: the
 // forward zeroes its wavefields and the adjoint run rebuilds its own.
 static int autotune_phase(sem_run* r, bool adj) {
-  const int cands_multi[] = {0, 2, 3, 4, 5, 6, 7, 8, 9};
+  const int cands_multi[] = {0, 2, 3, 4, 5, 6, 7, 8, 9, 10};
   const int cands_single[] = {0, 2};
   const int* cands = r->nev > 1 ? cands_multi : cands_single;
-  const int ncand = r->nev > 1 ? 9 : 2;
+  const int ncand = r->nev > 1 ? 10 : 2;
   const int nsteps = std::max(1, std::min(8, r->nstep - 2));
   r->fill_lanes(adj ? PH_ADJ : PH_FWD, 0);
   for (auto& L : r->h_lanes) L.it0 = 1;

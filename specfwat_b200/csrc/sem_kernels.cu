@@ -1998,6 +1998,189 @@ static void forces_adjpair_r_cfg(const StepArgs& a, cudaStream_t st) {
   k_forces_adjpair_r<LB><<<gx, NT, BYTES, st>>>(a, items);
 }
 
+// Forward-phase element kernel with 2 events per thread and the next
+// element's gather prefetched into registers (single-buffered shared
+// displacement), LB events per block.  LB is at most the 8-lane sector
+// group, so a work item never spans two groups of a group map.
+template <int LB>
+struct FwdRLayout {
+  static constexpr int NE = NGLL3;
+  static constexpr int OFF_IB = 0;                      // int [3][NE]
+  static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);   // [2][2][NE]
+  static constexpr int OFF_U = al4(OFF_KM + 4 * NE);    // [PP_U][LB]
+  static constexpr int OFF_A = al4(OFF_U + PP_U * LB);  // [PP_A][LB]
+  static constexpr int TOTAL = OFF_A + PP_A * LB;
+  static constexpr size_t BYTES = (size_t)TOTAL * 4;
+};
+
+template <int LB>
+__global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeItems items) {
+  constexpr int NL = 2;
+  constexpr int NT = 25 * LB / NL;
+  using LY = FwdRLayout<LB>;
+  constexpr int NE = NGLL3;
+  constexpr int LWLOG = 3;
+  extern __shared__ float sm[];
+  int* sIB = (int*)(sm + LY::OFF_IB);
+  float* sKM = sm + LY::OFF_KM;
+  float* sU = sm + LY::OFF_U;
+  float* sA = sm + LY::OFF_A;
+
+  const int tid = threadIdx.x;
+  const int lq = tid % (LB / NL);
+  const int t = tid / (LB / NL);
+  const int lane = lq * NL;
+  const int pi = t % 5, pq = t / 5;
+  const int nev = A.nev;
+  const int nspec = A.m.nspec;
+  const int nitems = items.count();
+
+  bool any = false;
+  for (int l = tid; l < nev; l += NT) {
+    const LaneDesc* L = A.lanes + l;
+    any |= L->phase != PH_IDLE && L->it0 + A.s < L->nstep;
+  }
+  if (!__syncthreads_or(any)) return;
+  if (A.lm.lwlog != LWLOG) return;  // batched layout only
+
+  int c_chunk = -1, c_fl[NL] = {0, 0};
+  auto flags = [&](int w, int& lg0, int& g, int fl[NL]) -> int {
+    int chunk;
+    items.decode(w, chunk, g);
+    lg0 = chunk * LB + lane;
+    if (chunk != c_chunk) {
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        int f = 0;
+        const int lg = lg0 + n;
+        if (chunk < items.nchunk && lg < nev) {
+          const LaneDesc* L = A.lanes + lg;
+          const int it = L->it0 + A.s;
+          if (L->phase != PH_IDLE && it < L->nstep) f = 1;
+        }
+        c_fl[n] = f;
+      }
+      c_chunk = chunk;
+    }
+    fl[0] = c_fl[0];
+    fl[1] = c_fl[1];
+    return fl[0] | fl[1];
+  };
+  auto issue_ib = [&](int w, int slot) {
+    int* dst = sIB + slot * NE;
+    int chunk = 0, g = 0;
+    if (w < nitems) items.decode(w, chunk, g);
+    for (int i = tid; i < NE; i += NT) {
+      if (w < nitems && g < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      else
+        dst[i] = -1;
+    }
+  };
+  auto issue_km = [&](int w, int buf) {
+    if (w >= nitems) return;
+    int chunk, g;
+    items.decode(w, chunk, g);
+    float* km = sKM + buf * 2 * NE;
+    const int e = g < nspec ? A.m.order[g] : 0;
+    for (int i = tid; i < NE; i += NT) {
+      if (g < nspec) {
+        const size_t ep = (size_t)e * NGLL3 + i;
+        cp_async4(km + i, A.m.kappa + ep);
+        cp_async4(km + NE + i, A.m.mu + ep);
+      }
+    }
+  };
+  float2 pre[5][3];
+  auto load_u = [&](int w, int ibslot) {
+    int lg0 = 0, g = 0, fl[NL] = {0, 0}, anyf = 0;
+    if (w < nitems) anyf = flags(w, lg0, g, fl);
+    const int* ib = sIB + ibslot * NE;
+    const float* src = A.f1.u + fbase<LWLOG>(A, lg0);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        pre[r][c] = (anyf && ig >= 0)
+                        ? __ldg(reinterpret_cast<const float2*>(src + foff<LWLOG>(ig, c)))
+                        : make_float2(0.f, 0.f);
+    }
+  };
+
+  int w = blockIdx.x;
+  issue_ib(w, 0);
+  cp_commit();
+  cp_wait_all();
+  __syncthreads();
+  issue_km(w, 0);
+  issue_ib(w + gridDim.x, 1);
+  cp_commit();
+  load_u(w, 0);
+
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+    const int buf = k & 1;
+    const int ibs = k % 3;
+    cp_wait_all();
+    __syncthreads();
+    {
+      float* ub = sU + lane;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int p = t + 25 * r;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          *reinterpret_cast<float2*>(ub + (c * NGLL3 + p) * LB) = pre[r][c];
+      }
+    }
+    issue_km(w + gridDim.x, buf ^ 1);
+    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    cp_commit();
+    __syncthreads();
+    load_u(w + gridDim.x, (k + 1) % 3);
+
+    int lg0, g, fl[NL];
+    const int anyf = flags(w, lg0, g, fl);
+    const int e = g < nspec ? A.m.order[g] : nspec;
+    const float* kap = sKM + buf * 2 * NE;
+    const float* mu = kap + NE;
+    PBuf<LB> b{sU + lane, sA + lane};
+    v_grad_eg<LB, NL>(b, pi, pq);
+    __syncthreads();
+    LV<NL> fx[5][3], km[1], kk[1];
+    v_xi<LB, NL, 0>(b, b, t, kap, mu, fac, fx, km, kk);
+    __syncthreads();
+    v_div_eg<LB, NL>(b, pi, pq);
+    __syncthreads();
+    if (e < nspec && anyf)
+      v_scatter<LB, NL>(b, t, fx, sIB + ibs * NE, A.f1.a + fbase<LWLOG>(A, lg0), fl, 1);
+  }
+  cp_wait_all();
+}
+
+template <int LB>
+static void forces_fwd_r_cfg(const StepArgs& a, cudaStream_t st) {
+  constexpr int NT = 25 * LB / 2;
+  constexpr size_t BYTES = FwdRLayout<LB>::BYTES;
+  static int blocks_per_sm = 0, sms = 0;
+  if (!blocks_per_sm) {
+    cudaFuncSetAttribute(k_forces_fwd_r<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_fwd_r<LB>, NT, BYTES);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  PipeItems items = make_items<LB>(a, a.m.nspec);
+  if (items.count() == 0) return;
+  int gx = blocks_per_sm * sms;
+  if (gx > items.count()) gx = items.count();
+  if (gx < 1) gx = 1;
+  k_forces_fwd_r<LB><<<gx, NT, BYTES, st>>>(a, items);
+}
+
 template <int LB>
 static void forces_adjpair_cfg(const StepArgs& a, cudaStream_t st) {
   constexpr int NT = 25 * LB;
@@ -2049,8 +2232,16 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
 //   pipelined with 2 lanes per thread, 5 as 4 with more lanes per block,
 //   6 / 7 adjoint phase with the (adjoint, backward) field pair of an
 //   event as a float2, 4 / 8 events per block, 8 / 9 the same with the
-//   displacement prefetched into registers.
+//   displacement prefetched into registers, 10 forward phase with 2 events
+//   per thread and register prefetch (8 events per block).
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.variant == 10 && a.nev > 1) {
+    if (!adj)
+      forces_fwd_r_cfg<8>(a, st);
+    else
+      forces_adjpair_r_cfg<8>(a, st);
+    return 1;
+  }
   if ((a.variant >= 6 && a.variant <= 9) && a.nev > 1) {
     if (!adj)
       forces_vec_cfg<8, 2, false>(a, st);

@@ -115,7 +115,7 @@ def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
 
 @pytest.mark.parametrize("variant,nev", [(1, 5), (2, 3), (2, 11), (3, 3), (3, 11),
                                          (4, 3), (4, 6), (5, 3), (5, 11), (6, 13),
-                                         (0, 7)])
+                                         (11, 5), (11, 19), (11, 7), (0, 7)])
 def test_batched_equals_plain(gpu, small, variant, nev):
     db, rec, _ = small
     nstep, dt = 300, 0.02
@@ -205,7 +205,7 @@ def test_state_errors(gpu, small):
     assert ei.value.code == -1
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11])
 def test_batched_adjoint_distinct_events_equal_alone(gpu, variant):
     """Each lane has its own source and observed data: the batched adjoint
     must give every event the kernels it gets alone."""
