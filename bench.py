@@ -464,6 +464,17 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                          f"(FP32 CPU restatement, OpenMP), extrapolated to NSTEP {NS}"}
 
     flops_evt_step = 29750 * db.nspec
+    fp32_peak = None
+    try:
+        import ctypes as C
+        from specfwat_b200 import _lib
+        pk, pm = C.c_double(0.0), C.c_double(0.0)
+        if _lib.load().sem_fp32_fma_peak(C.byref(pk), C.byref(pm)) == 0:
+            fp32_peak = pk.value
+    except Exception:
+        fp32_peak = None
+    fp32_adj = (2 * flops_evt_step + 2500 * db.nspec) * E / (ams[0] * 1e-3) / 1e12
+    fp32_fwd = flops_evt_step * E / (fms[0] * 1e-3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": "events/hour",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -489,7 +500,13 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                      "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes_per_launch": adj_bytes,
                      "fwd_achieved": fwd_bytes / (fms[0] * 1e-3) / 1e9,
-                     "fp32_tflops_adj": 2 * flops_evt_step * E / (ams[0] * 1e-3) / 1e12},
+                     "fp32": {"achieved_tflops_adj": fp32_adj,
+                              "achieved_tflops_fwd": fp32_fwd,
+                              "peak_tflops": fp32_peak,
+                              "peak_source": "measured by sem_fp32_fma_peak "
+                                             "(fmaf chains on every SM, best of 5)",
+                              "frac_adj": fp32_adj / fp32_peak if fp32_peak else None,
+                              "frac_fwd": fp32_fwd / fp32_peak if fp32_peak else None}},
         "e2e": {"value": E * world / (e2e / 1e3) * 3600.0, "unit": "events/hour",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e},

@@ -254,6 +254,13 @@ int sem_measure_l2_noalloc(const float *seis_dev, const double *obs_dev,
                            int taper_type, float *adj_dev, double *misfit_dev,
                            void *stream);
 
+/* FP32 FMA throughput of the current device in TFLOP/s (an FMA counts
+ * as 2 flops), the best of 5 timed launches of independent fmaf chains on
+ * every SM; *ms (may be null) is that launch's time.  No reference
+ * counterpart: it is the denominator of the element kernels' FP32
+ * roofline fraction. */
+int sem_fp32_fma_peak(double *tflops, double *ms);
+
 /* Device-time of the last sem_iterate_time in milliseconds. */
 int sem_last_loop_ms(sem_run *run, double *ms);
 /* Number of kernel launches queued by the last sem_iterate_time. */

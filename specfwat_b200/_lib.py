@@ -32,7 +32,7 @@ EXPORTS = (
     "sem_set_stream", "sem_sum_kernels_device", "sem_time_kernels",
     "sem_kernel_variants", "sem_measure_l2_noalloc",
     "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
-    "sem_advance", "sem_lane_status", "sem_lane_finish",
+    "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
 )
 L2_NOALLOC_MAX_RECEIVERS = 4096
 L2_NOALLOC_MAX_STEPS = 32768
@@ -127,6 +127,7 @@ def load():
         "sem_lane_status": (C.c_int, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
         "sem_lane_finish": (C.c_int, [vp, ip, fp, fp, fp]),
+        "sem_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -144,3 +144,15 @@ def test_unstable_time_step_is_reported_not_faulted(gpu):
     assert np.isfinite(ok.seismograms(0)).all()
     ok.close()
     mesh.close()
+
+
+def test_fp32_fma_peak_probe(gpu):
+    """The FP32 roofline denominator: B200 has 148 SMs x 128 FP32 lanes, so
+    the probe must land below 2 x 148 x 128 x 2.1 GHz (80 TFLOP/s) and well
+    above a tenth of it."""
+    import ctypes as C
+    from specfwat_b200 import _lib
+    t, ms = C.c_double(0.0), C.c_double(0.0)
+    _lib.check(_lib.load().sem_fp32_fma_peak(C.byref(t), C.byref(ms)))
+    assert 8.0 < t.value < 80.0, t.value
+    assert ms.value > 0.0
