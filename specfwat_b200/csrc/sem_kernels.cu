@@ -269,15 +269,22 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
 // (-1, -sqrt(3/7), 0, sqrt(3/7), 1): double-precision values rounded to
 // float, identical to the host-built tables.  Only ever indexed with
 // compile-time constants (fully unrolled loops), so they fold to immediates.
+// Contraction term with a compile-time GLL coefficient: a zero coefficient
+// (the interior diagonal D[i][i] = 0 of the GLL derivative matrix, and the
+// matching entries of the weighted transpose) costs no instruction.
+__device__ __forceinline__ float cfma(float c, float v, float a) {
+  return c == 0.0f ? a : fmaf(c, v, a);
+}
+
 __device__ __forceinline__ float gD(int i, int l) {
   constexpr float t[25] = {
       -5.0f, 6.7565024887242409f, -2.6666666666666674f, 1.410164177942427f, -0.5f,
-      -1.2409902530309822f, -4.4408920985006262e-16f, 1.7457431218879393f,
+      -1.2409902530309822f, 0.0f, 1.7457431218879393f,
       -0.76376261582597327f, 0.25900974696901707f,
       0.37499999999999989f, -1.3365845776954535f, 0.0f, 1.3365845776954532f,
       -0.37499999999999989f,
       -0.25900974696901713f, 0.76376261582597349f, -1.7457431218879396f,
-      4.4408920985006262e-16f, 1.2409902530309824f,
+      0.0f, 1.2409902530309824f,
       0.5f, -1.4101641779424272f, 2.6666666666666674f, -6.75650248872424f, 5.0f};
   return t[i * 5 + l];
 }
@@ -285,12 +292,12 @@ __device__ __forceinline__ float gDWt(int i, int l) {
   constexpr float t[25] = {
       -0.5f, -0.67565024887242353f, 0.26666666666666661f, -0.14101641779424265f,
       0.050000000000000003f,
-      0.67565024887242409f, -2.4178190314058963e-16f, -0.95046014413898916f,
+      0.67565024887242409f, 0.0f, -0.95046014413898916f,
       0.41582631306080775f, -0.14101641779424273f,
       -0.26666666666666677f, 0.95046014413898916f, 0.0f, -0.95046014413898927f,
       0.26666666666666677f,
       0.1410164177942427f, -0.41582631306080764f, 0.95046014413898905f,
-      2.4178190314058963e-16f, -0.67565024887242409f,
+      0.0f, -0.67565024887242409f,
       -0.050000000000000003f, 0.14101641779424262f, -0.26666666666666661f,
       0.67565024887242375f, 0.5f};
   return t[i * 5 + l];
@@ -348,7 +355,7 @@ __device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t) {
     for (int j = 0; j < 5; ++j) {
       float s = 0.f;
 #pragma unroll
-      for (int l = 0; l < 5; ++l) s = fmaf(gD(j, l), v[l], s);
+      for (int l = 0; l < 5; ++l) s = cfma(gD(j, l), v[l], s);
       b.Ar(c, pi + 5 * j + 25 * pq) = s;
     }
   }
@@ -362,7 +369,7 @@ __device__ __forceinline__ void pencil_grad_eg(const PencilBuf<LB>& b, int t) {
     for (int k = 0; k < 5; ++k) {
       float s = 0.f;
 #pragma unroll
-      for (int l = 0; l < 5; ++l) s = fmaf(gD(k, l), v[l], s);
+      for (int l = 0; l < 5; ++l) s = cfma(gD(k, l), v[l], s);
       b.Ar(3 + c, pi + 5 * pq + 25 * k) = s;
     }
   }
@@ -381,7 +388,7 @@ __device__ __forceinline__ void pencil_grad_xi(const PencilBuf<LB>& b, int t, fl
     for (int i = 0; i < 5; ++i) {
       float s = 0.f;
 #pragma unroll
-      for (int l = 0; l < 5; ++l) s = fmaf(gD(i, l), v[l], s);
+      for (int l = 0; l < 5; ++l) s = cfma(gD(i, l), v[l], s);
       g[i][c][0] = s;
       g[i][c][1] = b.Ar(c, i + 5 * t);
       g[i][c][2] = b.Ar(3 + c, i + 5 * t);
@@ -415,9 +422,9 @@ __device__ __forceinline__ void pencil_stress(const PencilBuf<LB>& b, int t, con
     float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
-      ax = fmaf(gDWt(i, l), sxx[l], ax);
-      ay = fmaf(gDWt(i, l), sxy[l], ay);
-      az = fmaf(gDWt(i, l), sxz[l], az);
+      ax = cfma(gDWt(i, l), sxx[l], ax);
+      ay = cfma(gDWt(i, l), sxy[l], ay);
+      az = cfma(gDWt(i, l), sxz[l], az);
     }
     fx[i][0] = ax;
     fx[i][1] = ay;
@@ -444,7 +451,7 @@ __device__ __forceinline__ void pencil_div_eg(const PencilBuf<LB>& b, int t) {
       for (int c = 0; c < 3; ++c) {
         float s = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) s = fmaf(gDWt(j, l), v[c][l], s);
+        for (int l = 0; l < 5; ++l) s = cfma(gDWt(j, l), v[c][l], s);
         b.Ar(c, pi + 5 * j + 25 * pq) = s;
       }
   }
@@ -463,7 +470,7 @@ __device__ __forceinline__ void pencil_div_eg(const PencilBuf<LB>& b, int t) {
       for (int c = 0; c < 3; ++c) {
         float s = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) s = fmaf(gDWt(k, l), v[c][l], s);
+        for (int l = 0; l < 5; ++l) s = cfma(gDWt(k, l), v[c][l], s);
         b.Ar(3 + c, pi + 5 * pq + 25 * k) = s;
       }
   }
@@ -650,6 +657,24 @@ __global__ void __launch_bounds__(EPB * 25 * LB) k_forces_pencil(StepArgs A) {
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+// Read-only global load into registers that were zeroed first, issued as
+// a predicated load: nothing depends on the loaded value until it is used,
+// so a prefetch made one work item ahead does not stall at the load.
+__device__ __forceinline__ void ldg_pred(float& x, const float* g, bool ok) {
+  x = 0.f;
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %1, 0;\n\t@q ld.global.nc.f32 %0, [%2];\n\t}\n"
+      : "+f"(x)
+      : "r"((int)ok), "l"(g));
+}
+__device__ __forceinline__ void ldg_pred(float2& x, const float* g, bool ok) {
+  x = make_float2(0.f, 0.f);
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q ld.global.nc.v2.f32 {%0, %1}, "
+      "[%3];\n\t}\n"
+      : "+f"(x.x), "+f"(x.y)
+      : "r"((int)ok), "l"(g));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
@@ -1091,7 +1116,7 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
       for (int n = 0; n < NL; ++n) {
         float a = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = fmaf(gD(j, l), v[l].v[n], a);
+        for (int l = 0; l < 5; ++l) a = cfma(gD(j, l), v[l].v[n], a);
         s.v[n] = a;
       }
       sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
@@ -1109,7 +1134,7 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
       for (int n = 0; n < NL; ++n) {
         float a = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = fmaf(gD(k, l), v[l].v[n], a);
+        for (int l = 0; l < 5; ++l) a = cfma(gD(k, l), v[l].v[n], a);
         s.v[n] = a;
       }
       sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
@@ -1139,7 +1164,7 @@ __device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
         for (int n = 0; n < NL; ++n) {
           float a = 0.f;
 #pragma unroll
-          for (int l = 0; l < 5; ++l) a = fmaf(gDWt(j, l), v[c][l].v[n], a);
+          for (int l = 0; l < 5; ++l) a = cfma(gDWt(j, l), v[c][l].v[n], a);
           s.v[n] = a;
         }
         sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
@@ -1164,7 +1189,7 @@ __device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
         for (int n = 0; n < NL; ++n) {
           float a = 0.f;
 #pragma unroll
-          for (int l = 0; l < 5; ++l) a = fmaf(gDWt(k, l), v[c][l].v[n], a);
+          for (int l = 0; l < 5; ++l) a = cfma(gDWt(k, l), v[c][l].v[n], a);
           s.v[n] = a;
         }
         sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
@@ -1211,7 +1236,7 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
       for (int c = 0; c < 3; ++c) {
         float a = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = fmaf(gD(i, l), u[c][l].v[n], a);
+        for (int l = 0; l < 5; ++l) a = cfma(gD(i, l), u[c][l].v[n], a);
         g[c][0] = a;
         g[c][1] = de[c].v[n];
         g[c][2] = dg[c].v[n];
@@ -1263,7 +1288,7 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
       for (int n = 0; n < NL; ++n) {
         float a = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = fmaf(gDWt(i, l), sx[c][l].v[n], a);
+        for (int l = 0; l < 5; ++l) a = cfma(gDWt(i, l), sx[c][l].v[n], a);
         fx[i][c].v[n] = a;
       }
 }
@@ -1544,7 +1569,7 @@ __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* k
       for (int c = 0; c < 3; ++c) {
         float a = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = fmaf(gD(i, l), u[c][l].v[n], a);
+        for (int l = 0; l < 5; ++l) a = cfma(gD(i, l), u[c][l].v[n], a);
         g[c][0] = a;
         g[c][1] = de[c].v[n];
         g[c][2] = dg[c].v[n];
@@ -1583,7 +1608,7 @@ __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* k
       for (int n = 0; n < 2; ++n) {
         float a = 0.f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = fmaf(gDWt(i, l), sx[c][l].v[n], a);
+        for (int l = 0; l < 5; ++l) a = cfma(gDWt(i, l), sx[c][l].v[n], a);
         fx[i][c].v[n] = a;
       }
 }
@@ -1899,8 +1924,8 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeIt
       const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        pre[0][r][c] = ((fl & 1) && ig >= 0) ? __ldg(A.f1.u + fb + foff<LWLOG>(ig, c)) : 0.f;
-        pre[1][r][c] = ((fl & 2) && ig >= 0) ? __ldg(A.f2.u + fb + foff<LWLOG>(ig, c)) : 0.f;
+        ldg_pred(pre[0][r][c], A.f1.u + fb + foff<LWLOG>(ig, c), (fl & 1) && ig >= 0);
+        ldg_pred(pre[1][r][c], A.f2.u + fb + foff<LWLOG>(ig, c), (fl & 2) && ig >= 0);
       }
     }
   };
@@ -2102,9 +2127,7 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
       const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        pre[r][c] = (anyf && ig >= 0)
-                        ? __ldg(reinterpret_cast<const float2*>(src + foff<LWLOG>(ig, c)))
-                        : make_float2(0.f, 0.f);
+        ldg_pred(pre[r][c], src + foff<LWLOG>(ig, c), anyf && ig >= 0);
     }
   };
 
