@@ -254,6 +254,53 @@ int sem_measure_l2_noalloc(const float *seis_dev, const double *obs_dev,
                            int taper_type, float *adj_dev, double *misfit_dev,
                            void *stream);
 
+/* ------------------------------------------------------------------------
+ * Kernel post-processing: PDE smoothing of element fields.
+ *
+ * Replaces smooth_sem_pde (src/postproc/smooth.f90:7-437), called from
+ * PostFlow%pde_smooth and %sum_precond (src/postproc/post_processing.f90:
+ * 222,270), and its GPU form smooth_pde_cuda_ (src/postproc/
+ * smooth_sem_pde.cu:298-478).  Each field (a kernel or Hessian,
+ * dat(NGLLX,NGLLY,NGLLZ,NSPEC)) is projected onto the global points, then
+ * diffused for nstep explicit steps with horizontal/vertical coefficients
+ * ch/cv, and gathered back.  cmax = distance_min^2/9; the larger of
+ * sigma_h, sigma_v gets cmax and the other cmax*(sigma_small/sigma_large)^2;
+ * nstep = ceiling(max(sigma)^2 / (2 cmax)) (smooth.f90:99-109).  Points of
+ * CPML elements are held at 0 (ZERO_PML).
+ *
+ * mapping: SEM_SMOOTH_MAP_CUBE uses the regular element's diagonal mapping
+ * (xix = etay = gammaz = xix_regular).  SEM_SMOOTH_MAP_REFERENCE reproduces
+ * the reference's regular-element branch as written, which sets all nine
+ * mapping terms to xix_regular (smooth.f90:269-279): a diffusion along
+ * (1,1,1) that exceeds the step-size bound and grows without limit within
+ * tens of steps.  It exists for parity checks.
+ * ------------------------------------------------------------------------ */
+#define SEM_SMOOTH_MAP_CUBE 0
+#define SEM_SMOOTH_MAP_REFERENCE 1
+
+typedef struct {
+  double sigma_h, sigma_v; /* smoothing lengths (mesh units)                 */
+  double distance_min;     /* minimum GLL point distance (distance_min_glob);
+                              <= 0: (xi_1 - xi_0)/xix_regular of the mesh  */
+  int is_sph;              /* 1: vertical = radial r = x/|x| (spherical)     */
+  int mapping;             /* SEM_SMOOTH_MAP_CUBE or SEM_SMOOTH_MAP_REFERENCE */
+  int nstep;               /* > 0 replaces the computed step count           */
+} sem_smooth_cfg;
+
+typedef struct {
+  int nstep;               /* steps taken                                    */
+  int fields_per_pass;     /* fields smoothed together on the device (1/2/4) */
+  double cv, ch;           /* diffusion coefficients (FP32 values)           */
+  double distance_min;     /* the distance used                              */
+  double step_ms;          /* device time of the diffusion steps (all passes)*/
+} sem_smooth_stats;
+
+/* dat_in, dat_out: host [nfield][nspec][125] FP32 (Fortran dat order);
+ * is_cpml: [nspec] or NULL; stats may be NULL.  Blocking. */
+int sem_smooth_pde(sem_mesh *mesh, const sem_smooth_cfg *cfg, int nfield,
+                   const float *dat_in, const int *is_cpml, float *dat_out,
+                   sem_smooth_stats *stats);
+
 /* FP32 FMA throughput of the current device in TFLOP/s (an FMA counts
  * as 2 flops), the best of 5 timed launches of independent fmaf chains on
  * every SM; *ms (may be null) is that launch's time.  No reference

@@ -69,6 +69,10 @@ def lib():
             C.c_void_p]
         L.oracle_source_element.argtypes = [C.c_void_p, C.c_double,
                                             C.c_double, C.c_double, C.c_void_p]
+        L.oracle_smooth_pde.argtypes = [
+            C.POINTER(OracleMesh), C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+            C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+            C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -189,6 +193,31 @@ class Oracle:
         xi = np.zeros(3, np.float64)
         e = lib().oracle_source_element(self._h, x, y, z, xi.ctypes.data)
         return e, xi
+
+    def smooth_pde(self, dat, sigma_h, sigma_v, distance_min, is_sph=False,
+                   mapping=0, nstep=0, is_cpml=None):
+        """PDE smoothing of element fields ``dat`` [nfield, nspec, 5, 5, 5]
+        (or one field [nspec, 5, 5, 5]) in this oracle's precision, as the
+        CPU branch of ``smooth_sem_pde`` (src/postproc/smooth.f90:7-437).
+        ``mapping`` 0: the cube's diagonal mapping; 1: the reference's
+        regular branch as written (all nine mapping terms xix_regular).
+        Returns (smoothed fields, step count, (cv, ch))."""
+        d = np.ascontiguousarray(dat, np.float32)
+        one = d.ndim == 4
+        d = d.reshape(-1, self.db.nspec * 125)
+        out = np.zeros(d.shape, np.float64)
+        cpml = (None if is_cpml is None
+                else np.ascontiguousarray(is_cpml, np.int32))
+        cvch = np.zeros(2, np.float64)
+        n = lib().oracle_smooth_pde(
+            C.byref(self._mesh), self.precision, d.shape[0], d.ctypes.data,
+            None if cpml is None else cpml.ctypes.data, float(sigma_h),
+            float(sigma_v), float(distance_min), int(bool(is_sph)), int(mapping),
+            int(nstep), out.ctypes.data, cvch.ctypes.data)
+        if n < 0:
+            raise RuntimeError("oracle_smooth_pde: bad arguments")
+        out = out.reshape((-1, self.db.nspec, 5, 5, 5))
+        return (out[0] if one else out), n, (cvch[0], cvch[1])
 
 
 # -- FP64 measurement restatement (L2 waveform misfit) ----------------------

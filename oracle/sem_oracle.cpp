@@ -635,6 +635,163 @@ struct Solver {
   }
 };
 
+// ---------------------------------------------------------------------------
+// PDE smoothing of element fields: the CPU branch of smooth_sem_pde
+// (src/postproc/smooth.f90:7-437) restated in precision T.
+//
+// Steps, in the reference's order:
+//   * rotate_r = x/|x| at every element point                (smooth.f90:81-94)
+//   * cmax = dmin^2/9, cv/ch from sigma_v/sigma_h, ntstep     (smooth.f90:99-109)
+//     (always in FP32, CUSTOM_REAL, so both precisions take the same steps)
+//   * rvol_local = real(dble(jac) * w_i w_j w_k); rvol = 1 / sum (smooth.f90:142-164)
+//   * project: dat_glob = sum(dat * rvol_local) * rvol        (smooth.f90:193-214)
+//   * per step: ddat = 0; per element the gradient with hprime_xxT, the
+//     fluxes stemp1..3, the divergence with hprimewgll and wgllwgll
+//     weights, ddat -= ...; then ddat *= rvol, dat_glob += ddat, and
+//     points of CPML elements reset to dat_bak = 0 (ZERO_PML)   (smooth.f90:244-370)
+//   * output dat(e) = dat_glob(ibool(e))
+// Regular elements only.  mapping 1 reproduces the reference's regular
+// branch, where all nine derivative terms (xix .. gammaz) are xix_regular
+// (smooth.f90:269-279, get_gradient_element_regular :648-689); mapping 0
+// uses the cube's diagonal mapping (xix = etay = gammaz = xix_regular,
+// zero off the diagonal).
+// ---------------------------------------------------------------------------
+
+struct SmoothParams {
+  float cv, ch, cmax;
+  int nstep;
+};
+
+SmoothParams smooth_params(double sigma_h, double sigma_v, double dmin, int nstep_override) {
+  SmoothParams q{};
+  const float sh = (float)sigma_h, sv = (float)sigma_v, d = (float)dmin;
+  q.cmax = d * d / 9.0f;
+  if (sv >= sh) {
+    q.cv = q.cmax;
+    q.ch = q.cv * (sh * sh) / (sv * sv);
+  } else {
+    q.ch = q.cmax;
+    q.cv = q.ch * (sv * sv) / (sh * sh);
+  }
+  const float mx = sh > sv ? sh : sv;
+  q.nstep = (int)std::ceil(mx * mx / (2.0f * q.cmax));
+  if (nstep_override > 0) q.nstep = nstep_override;
+  return q;
+}
+
+template <typename T>
+void smooth_run(const oracle_mesh& m, int nfield, const float* dat_in, const int* is_cpml,
+                const SmoothParams& q, int is_sph, int mapping, double* out) {
+  const Gll g = make_gll();
+  T D[NG][NG], DWt[NG][NG];
+  for (int i = 0; i < NG; ++i) {
+    for (int l = 0; l < NG; ++l) {
+      D[i][l] = (T)g.D[i][l];              // hprime_xxT(l,i) = hprime_xx(i,l)
+      DWt[i][l] = (T)(g.w[l] * g.D[l][i]); // hprimewgll_xx(l,i)
+    }
+  }
+  const T xix = (T)(float)m.xix, jac = (T)(float)m.jac;
+  const T cv = (T)q.cv, ch = (T)q.ch;
+  // mapping rows: derivative terms of xi, eta, gamma along x, y, z
+  T M[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) M[a][b] = (mapping == 1 || a == b) ? xix : (T)0;
+  const size_t ne = (size_t)m.nspec * NG3;
+  std::vector<T> rvol_local(NG3), rvol(m.nglob, (T)0);
+  for (int k = 0; k < NG; ++k)
+    for (int j = 0; j < NG; ++j)
+      for (int i = 0; i < NG; ++i) {
+        const double weight = g.w[i] * g.w[j] * g.w[k];
+        rvol_local[i + NG * j + NG2 * k] = (T)((double)(float)m.jac * weight);
+      }
+  for (int e = 0; e < m.nspec; ++e)
+    for (int p = 0; p < NG3; ++p) rvol[m.ibool[e * NG3 + p]] += rvol_local[p];
+  for (int ig = 0; ig < m.nglob; ++ig) rvol[ig] = (T)1 / rvol[ig];
+  std::vector<char> cpml_pt(m.nglob, 0);
+  if (is_cpml)
+    for (int e = 0; e < m.nspec; ++e)
+      if (is_cpml[e])
+        for (int p = 0; p < NG3; ++p) cpml_pt[m.ibool[e * NG3 + p]] = 1;
+  std::vector<T> rx, ry, rz;
+  if (is_sph) {
+    rx.resize(m.nglob);
+    ry.resize(m.nglob);
+    rz.resize(m.nglob);
+    for (int ig = 0; ig < m.nglob; ++ig) {
+      const T xl = (T)m.x[ig], yl = (T)m.y[ig], zl = (T)m.z[ig];
+      const T rl = std::sqrt(xl * xl + yl * yl + zl * zl);
+      rx[ig] = xl / rl;
+      ry[ig] = yl / rl;
+      rz[ig] = zl / rl;
+    }
+  }
+  std::vector<T> dat_glob(m.nglob), ddat(m.nglob);
+  for (int f = 0; f < nfield; ++f) {
+    const float* din = dat_in + (size_t)f * ne;
+    std::fill(dat_glob.begin(), dat_glob.end(), (T)0);
+    for (int e = 0; e < m.nspec; ++e)
+      for (int p = 0; p < NG3; ++p)
+        dat_glob[m.ibool[e * NG3 + p]] += (T)din[(size_t)e * NG3 + p] * rvol_local[p];
+    for (int ig = 0; ig < m.nglob; ++ig) dat_glob[ig] = dat_glob[ig] * rvol[ig];
+    for (int it = 0; it < q.nstep; ++it) {
+      std::fill(ddat.begin(), ddat.end(), (T)0);
+      for (int e = 0; e < m.nspec; ++e) {
+        const int* ib = &m.ibool[(size_t)e * NG3];
+        T s[NG3], st1[NG3], st2[NG3], st3[NG3];
+        for (int p = 0; p < NG3; ++p) s[p] = dat_glob[ib[p]];
+        for (int k = 0; k < NG; ++k)
+          for (int j = 0; j < NG; ++j)
+            for (int i = 0; i < NG; ++i) {
+              T t1 = 0, t2 = 0, t3 = 0;
+              for (int l = 0; l < NG; ++l) t1 += s[l + NG * j + NG2 * k] * D[i][l];
+              for (int l = 0; l < NG; ++l) t2 += s[i + NG * l + NG2 * k] * D[j][l];
+              for (int l = 0; l < NG; ++l) t3 += s[i + NG * j + NG2 * l] * D[k][l];
+              const T dx = t1 * M[0][0] + t2 * M[1][0] + t3 * M[2][0];
+              const T dy = t1 * M[0][1] + t2 * M[1][1] + t3 * M[2][1];
+              const T dz = t1 * M[0][2] + t2 * M[1][2] + t3 * M[2][2];
+              const int p = i + NG * j + NG2 * k;
+              T* st[3] = {st1, st2, st3};
+              for (int a = 0; a < 3; ++a) {
+                T v;
+                if (is_sph) {
+                  const T r0 = rx[ib[p]], r1 = ry[ib[p]], r2 = rz[ib[p]];
+                  v = ((cv - ch) * (r0 * M[a][0] + r1 * M[a][1] + r2 * M[a][2]) *
+                           (r0 * dx + r1 * dy + r2 * dz) +
+                       ch * (M[a][0] * dx + M[a][1] * dy + M[a][2] * dz)) *
+                      jac;
+                } else {
+                  v = ((cv - ch) * M[a][2] * dz + ch * (M[a][0] * dx + M[a][1] * dy + M[a][2] * dz)) *
+                      jac;
+                }
+                st[a][p] = v;
+              }
+            }
+        for (int k = 0; k < NG; ++k)
+          for (int j = 0; j < NG; ++j)
+            for (int i = 0; i < NG; ++i) {
+              T n1 = 0, n2 = 0, n3 = 0;
+              for (int l = 0; l < NG; ++l) {
+                n1 += st1[l + NG * j + NG2 * k] * DWt[i][l];
+                n2 += st2[i + NG * l + NG2 * k] * DWt[j][l];
+                n3 += st3[i + NG * j + NG2 * l] * DWt[k][l];
+              }
+              // wgllwgll_yz(j,k), wgllwgll_xz(i,k), wgllwgll_xy(i,j)
+              const T fac1 = (T)(g.w[j] * g.w[k]), fac2 = (T)(g.w[i] * g.w[k]),
+                      fac3 = (T)(g.w[i] * g.w[j]);
+              const int p = i + NG * j + NG2 * k;
+              ddat[ib[p]] -= fac1 * n1 + fac2 * n2 + fac3 * n3;
+            }
+      }
+      for (int ig = 0; ig < m.nglob; ++ig) {
+        dat_glob[ig] += ddat[ig] * rvol[ig];
+        if (cpml_pt[ig]) dat_glob[ig] = (T)0;
+      }
+    }
+    double* o = out + (size_t)f * ne;
+    for (size_t i = 0; i < ne; ++i) o[i] = (double)dat_glob[m.ibool[i]];
+  }
+}
+
 struct Handle {
   int prec;
   std::unique_ptr<Solver<float>> s32;
@@ -728,6 +885,24 @@ int oracle_source_element(void* p, double x, double y, double z, double* xi3) {
   xi3[1] = L.eta;
   xi3[2] = L.gam;
   return L.ispec;
+}
+
+// PDE smoothing (see smooth_run): dat_in/out are [nfield][nspec][125];
+// is_cpml may be null.  Returns the step count, or -1 on bad arguments.
+int oracle_smooth_pde(const oracle_mesh* m, int precision, int nfield, const float* dat_in,
+                      const int* is_cpml, double sigma_h, double sigma_v, double dmin,
+                      int is_sph, int mapping, int nstep_override, double* out, double* cvch) {
+  if (!m || !dat_in || !out || nfield < 1 || !(dmin > 0.0)) return -1;
+  const SmoothParams q = smooth_params(sigma_h, sigma_v, dmin, nstep_override);
+  if (cvch) {
+    cvch[0] = q.cv;
+    cvch[1] = q.ch;
+  }
+  if (precision == 4)
+    smooth_run<float>(*m, nfield, dat_in, is_cpml, q, is_sph, mapping, out);
+  else
+    smooth_run<double>(*m, nfield, dat_in, is_cpml, q, is_sph, mapping, out);
+  return q.nstep;
 }
 
 }  // extern "C"

@@ -33,7 +33,10 @@ EXPORTS = (
     "sem_kernel_variants", "sem_measure_l2_noalloc",
     "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
     "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
+    "sem_smooth_pde",
 )
+SMOOTH_MAP_CUBE = 0
+SMOOTH_MAP_REFERENCE = 1
 L2_NOALLOC_MAX_RECEIVERS = 4096
 L2_NOALLOC_MAX_STEPS = 32768
 
@@ -75,6 +78,18 @@ class Source(C.Structure):
                 ("Mrr", C.c_double), ("Mtt", C.c_double), ("Mpp", C.c_double),
                 ("Mrt", C.c_double), ("Mrp", C.c_double), ("Mtp", C.c_double),
                 ("f0", C.c_double), ("tshift", C.c_double)]
+
+
+class SmoothCfg(C.Structure):
+    _fields_ = [("sigma_h", C.c_double), ("sigma_v", C.c_double),
+                ("distance_min", C.c_double), ("is_sph", C.c_int),
+                ("mapping", C.c_int), ("nstep", C.c_int)]
+
+
+class SmoothStats(C.Structure):
+    _fields_ = [("nstep", C.c_int), ("fields_per_pass", C.c_int),
+                ("cv", C.c_double), ("ch", C.c_double),
+                ("distance_min", C.c_double), ("step_ms", C.c_double)]
 
 
 _lib = None
@@ -128,6 +143,8 @@ def load():
                                       C.POINTER(C.c_int)]),
         "sem_lane_finish": (C.c_int, [vp, ip, fp, fp, fp]),
         "sem_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "sem_smooth_pde": (C.c_int, [vp, C.POINTER(SmoothCfg), ip, fp, fp, fp,
+                                     C.POINTER(SmoothStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

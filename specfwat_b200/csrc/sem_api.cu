@@ -200,6 +200,7 @@ struct sem_mesh_s {
   std::vector<float> h_rmass;
   std::vector<int> h_f_iglob;
   std::vector<float> h_f_rvp, h_f_rvs, h_f_jw, h_f_n;
+  std::vector<float> h_x, h_y, h_z;  // point coordinates (kernel smoother)
   std::vector<double> centre;  // [nspec][3]
   std::vector<double> half;    // [nspec][3]
   int live_runs = 0;
@@ -358,6 +359,23 @@ struct sem_run_s {
   }
 };
 
+namespace sem {
+int mesh_smooth_view(const sem_mesh_s* m, SmoothMeshView* out) {
+  if (!m || !out) return fail(SEM_ERR_ARG, "null mesh");
+  out->nspec = m->nspec;
+  out->nglob = m->nglob;
+  out->xix = m->xix;
+  out->jac = m->jac;
+  out->ibool = m->ibool.p;
+  out->order = m->order.p;
+  out->h_ibool = m->h_ibool.data();
+  out->x = m->h_x.data();
+  out->y = m->h_y.data();
+  out->z = m->h_z.data();
+  return SEM_OK;
+}
+}  // namespace sem
+
 // ----------------------------------------------------------------------------
 // C ABI
 // ----------------------------------------------------------------------------
@@ -430,6 +448,9 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
       return fail(SEM_ERR_ARG, "invalid material at element point %zu", i);
   }
   m->h_rmass.assign(d->rmass, d->rmass + d->nglob);
+  m->h_x.assign(d->xstore, d->xstore + d->nglob);
+  m->h_y.assign(d->ystore, d->ystore + d->nglob);
+  m->h_z.assign(d->zstore, d->zstore + d->nglob);
   for (int g = 0; g < d->nglob; ++g)
     if (!(m->h_rmass[g] > 0.f) || !std::isfinite(m->h_rmass[g]))
       return fail(SEM_ERR_ARG, "mass matrix is not positive at point %d", g);

@@ -7,6 +7,8 @@
 #include <cstddef>
 #include <cstdint>
 
+struct sem_mesh_s;
+
 namespace sem {
 
 constexpr int NGLL = 5;
@@ -131,6 +133,18 @@ int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int
                          cudaStream_t st);
 
 void set_gll_constants(const float* D, const float* DWt, const float* w);
+
+// What the kernel smoother reads from a prepared mesh (defined in
+// sem_api.cu, where the mesh type lives).
+struct SmoothMeshView {
+  int nspec, nglob;
+  float xix, jac;
+  const int* ibool;       // device [nspec*125], 0-based
+  const int* order;       // device [nspec] element traversal order
+  const int* h_ibool;     // host copy of ibool
+  const float *x, *y, *z; // host [nglob] coordinates
+};
+int mesh_smooth_view(const ::sem_mesh_s* m, SmoothMeshView* out);
 
 // Sets the per-thread error message returned by sem_last_error().
 int report_error(int code, const char* fmt, ...);

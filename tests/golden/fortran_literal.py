@@ -78,3 +78,186 @@ def l2_adjoint_source(syn, dat, dt, taper_percentage, itaper_type):
     adj_tw = window_taper(adj_tw, taper_percentage, itaper_type)
     misfit = 0.5 * simpson([(a - b) ** 2 for a, b in zip(s, d)], dt)
     return misfit, adj_tw
+
+
+def smooth_sem_pde_cpu(dat_in, ibool, xstore, ystore, zstore, xix_regular,
+                       jacobian_regular, sigma_h, sigma_v, distance_min_glob,
+                       is_sph, is_cpml=None, nstep=None):
+    """CPU branch of ``smooth_sem_pde`` (src/postproc/smooth.f90:7-437) for
+    regular elements, one field, CUSTOM_REAL = float32.
+
+    ``dat_in`` is dat(NGLLX,NGLLY,NGLLZ,NSPEC) flattened in Fortran order,
+    ``ibool`` the same shape with 1-based global numbers, the stores 1-D.
+    Returns the smoothed dat in the same layout and ntstep.  ``nstep``
+    replaces ntstep (the regular branch diverges within a few tens of
+    steps, so comparisons use a few).
+    """
+    import numpy as np
+    f32 = np.float32
+    N = 5
+    nspec = len(dat_in) // 125
+
+    def idx(i, j, k, ispec):               # dat(i,j,k,ispec), all 1-based
+        return (i - 1) + N * (j - 1) + 25 * (k - 1) + 125 * (ispec - 1)
+
+    # GLL points, weights, derivative matrices (define_derivation_matrices)
+    xigll, wxgll = _gll5()
+    hprime_xx = [[f32(0)] * (N + 1) for _ in range(N + 1)]
+    hprimewgll_xx = [[f32(0)] * (N + 1) for _ in range(N + 1)]
+    for i1 in range(1, N + 1):
+        for i2 in range(1, N + 1):
+            d = _lagrange_deriv(i1 - 1, i2 - 1, xigll)
+            hprime_xx[i2][i1] = f32(d)
+            hprimewgll_xx[i2][i1] = f32(wxgll[i2 - 1] * d)
+    hprime_xxT = [[f32(0)] * (N + 1) for _ in range(N + 1)]
+    for j in range(1, N + 1):
+        for i in range(1, N + 1):
+            hprime_xxT[j][i] = hprime_xx[i][j]
+    wgllwgll = [[f32(wxgll[a - 1] * wxgll[b - 1]) if a and b else f32(0)
+                 for b in range(N + 1)] for a in range(N + 1)]
+
+    # rotate_r  (smooth.f90:81-94)
+    rot = {}
+    if is_sph:
+        for ispec in range(1, nspec + 1):
+            for k in range(1, N + 1):
+                for j in range(1, N + 1):
+                    for i in range(1, N + 1):
+                        iglob = ibool[idx(i, j, k, ispec)]
+                        xl = f32(xstore[iglob - 1])
+                        yl = f32(ystore[iglob - 1])
+                        zl = f32(zstore[iglob - 1])
+                        rl = f32(np.sqrt(f32(f32(xl * xl + yl * yl) + zl * zl)))
+                        rot[idx(i, j, k, ispec)] = (f32(xl / rl), f32(yl / rl), f32(zl / rl))
+
+    # cmax, cv, ch, ntstep  (smooth.f90:99-109)
+    sh, sv = f32(sigma_h), f32(sigma_v)
+    cmax = f32(f32(distance_min_glob) ** 2 / f32(9.0))
+    if sv >= sh:
+        cv = cmax
+        ch = f32(f32(cv * f32(sh ** 2)) / f32(sv ** 2))
+    else:
+        ch = cmax
+        cv = f32(f32(ch * f32(sv ** 2)) / f32(sh ** 2))
+    ntstep = int(math.ceil(float(f32(max(sh, sv) ** 2) / f32(2.0 * cmax))))
+    if nstep:
+        ntstep = nstep
+
+    # rvol  (smooth.f90:142-164)
+    nglob = max(ibool)
+    rvol = [f32(0)] * (nglob + 1)
+    rvol_local = [f32(0)] * (125 * nspec)
+    for ispec in range(1, nspec + 1):
+        for k in range(1, N + 1):
+            for j in range(1, N + 1):
+                for i in range(1, N + 1):
+                    weight = wxgll[i - 1] * wxgll[j - 1] * wxgll[k - 1]
+                    jacobianl = f32(jacobian_regular)
+                    rvol_local[idx(i, j, k, ispec)] = f32(float(jacobianl) * weight)
+                    iglob = ibool[idx(i, j, k, ispec)]
+                    rvol[iglob] = f32(rvol[iglob] + rvol_local[idx(i, j, k, ispec)])
+    for g in range(1, nglob + 1):
+        rvol[g] = f32(f32(1.0) / rvol[g])
+
+    dat = [f32(v) for v in dat_in]
+    # project  (smooth.f90:193-214)
+    dat_glob = [f32(0)] * (nglob + 1)
+    for ispec in range(1, nspec + 1):
+        for k in range(1, N + 1):
+            for j in range(1, N + 1):
+                for i in range(1, N + 1):
+                    q = idx(i, j, k, ispec)
+                    iglob = ibool[q]
+                    dat_glob[iglob] = f32(dat_glob[iglob] + f32(dat[q] * rvol_local[q]))
+    for g in range(1, nglob + 1):
+        dat_glob[g] = f32(dat_glob[g] * rvol[g])
+    for q in range(125 * nspec):
+        dat[q] = dat_glob[ibool[q]]
+
+    xix = f32(xix_regular)
+    for _istep in range(ntstep):                      # smooth.f90:244-370
+        ddat_glob = [f32(0)] * (nglob + 1)
+        for ispec in range(1, nspec + 1):
+            dx, dy, dz = {}, {}, {}
+            for k in range(1, N + 1):                 # get_gradient_element_regular
+                for j in range(1, N + 1):
+                    for i in range(1, N + 1):
+                        t1 = t2 = t3 = f32(0)
+                        for l in range(1, N + 1):
+                            t1 = f32(t1 + f32(dat[idx(l, j, k, ispec)] * hprime_xxT[l][i]))
+                        for l in range(1, N + 1):
+                            t2 = f32(t2 + f32(dat[idx(i, l, k, ispec)] * hprime_xxT[l][j]))
+                        for l in range(1, N + 1):
+                            t3 = f32(t3 + f32(dat[idx(i, j, l, ispec)] * hprime_xxT[l][k]))
+                        v = f32(f32(f32(t1 * xix) + f32(t2 * xix)) + f32(t3 * xix))
+                        dx[(i, j, k)] = dy[(i, j, k)] = dz[(i, j, k)] = v
+            st1, st2, st3 = {}, {}, {}
+            jacobianl = f32(jacobian_regular)
+            for k in range(1, N + 1):
+                for j in range(1, N + 1):
+                    for i in range(1, N + 1):
+                        a, b, c = dx[(i, j, k)], dy[(i, j, k)], dz[(i, j, k)]
+                        if is_sph:
+                            rxl, ryl, rzl = rot[idx(i, j, k, ispec)]
+                            rdot = f32(f32(f32(rxl * a) + f32(ryl * b)) + f32(rzl * c))
+                            mr = f32(f32(f32(rxl * xix) + f32(ryl * xix)) + f32(rzl * xix))
+                            g = f32(f32(f32(xix * a) + f32(xix * b)) + f32(xix * c))
+                            v = f32(f32(f32(f32(cv - ch) * mr) * rdot) + f32(ch * g))
+                            v = f32(v * jacobianl)
+                        else:
+                            g = f32(f32(f32(xix * a) + f32(xix * b)) + f32(xix * c))
+                            v = f32(f32(f32(f32(cv - ch) * xix) * c) + f32(ch * g))
+                            v = f32(v * jacobianl)
+                        st1[(i, j, k)] = st2[(i, j, k)] = st3[(i, j, k)] = v
+            for k in range(1, N + 1):
+                for j in range(1, N + 1):
+                    for i in range(1, N + 1):
+                        n1 = n2 = n3 = f32(0)
+                        for l in range(1, N + 1):
+                            n1 = f32(n1 + f32(st1[(l, j, k)] * hprimewgll_xx[l][i]))
+                            n2 = f32(n2 + f32(st2[(i, l, k)] * hprimewgll_xx[l][j]))
+                            n3 = f32(n3 + f32(st3[(i, j, l)] * hprimewgll_xx[l][k]))
+                        fac1 = wgllwgll[j][k]
+                        fac2 = wgllwgll[i][k]
+                        fac3 = wgllwgll[i][j]
+                        iglob = ibool[idx(i, j, k, ispec)]
+                        ddat_glob[iglob] = f32(ddat_glob[iglob] - f32(
+                            f32(f32(fac1 * n1) + f32(fac2 * n2)) + f32(fac3 * n3)))
+        for g in range(1, nglob + 1):
+            ddat_glob[g] = f32(ddat_glob[g] * rvol[g])
+            dat_glob[g] = f32(dat_glob[g] + ddat_glob[g])
+        if is_cpml is not None:
+            for ispec in range(1, nspec + 1):
+                if is_cpml[ispec - 1]:
+                    for q in range(125 * (ispec - 1), 125 * ispec):
+                        dat_glob[ibool[q]] = f32(0)   # dat_bak = 0 (ZERO_PML)
+        for q in range(125 * nspec):
+            dat[q] = dat_glob[ibool[q]]
+    return dat, ntstep
+
+
+def _gll5():
+    """GLL points and weights for 5 points in FP64 (zwgljd)."""
+    import numpy as np
+    from numpy.polynomial import legendre as L
+    c = [0, 0, 0, 0, 1]                            # P_4
+    inner = np.sort(np.real(L.legroots(L.legder(c))))
+    x = np.concatenate(([-1.0], inner, [1.0]))
+    w = 2.0 / (4 * 5 * L.legval(x, c) ** 2)
+    return list(x), list(w)
+
+
+def _lagrange_deriv(i, j, x):
+    """Derivative of the i-th Lagrange interpolant at x[j] (0-based)."""
+    s = 0.0
+    n = len(x)
+    for m in range(n):
+        if m == i:
+            continue
+        prod = 1.0 / (x[i] - x[m])
+        for q in range(n):
+            if q in (i, m):
+                continue
+            prod *= (x[j] - x[q]) / (x[i] - x[q])
+        s += prod
+    return s
