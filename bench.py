@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--mesh", default="medium")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-smooth", action="store_true",
+                   help="skip the kernel-smoothing leg")
     p.add_argument("--e2e-steps", type=int, default=1)
     p.add_argument("--store", default="fp16", choices=["fp16", "fp32"])
     p.add_argument("--served-requests", type=int, default=64)
@@ -385,6 +387,28 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         e2e = float(tt.item())
     sb.close()
 
+    # ---- kernel post-processing: PDE smoothing of the six summed kernels ---
+    smooth = None
+    if rank == 0 and not args.no_smooth:
+        from specfwat_b200.postproc import smooth_sem_pde
+        kf = pin_k.numpy().astype(np.float32)
+        _, sst = smooth_sem_pde(mesh, kf, 10000.0, 5000.0)
+        nfield = kf.shape[0]
+        fpp = sst["fields_per_pass"]
+        passes = -(-nfield // fpp)
+        # per step and pass, each datum once: gather 4 B, scatter
+        # read-modify-write 8 B, update reads dat and ddat and writes both
+        # (16 B) per point and field; the volume (4 B/point) and ibool
+        # (500 B/element) per pass
+        sbytes = (28 * fpp + 4) * db.nglob + 500 * db.nspec
+        smooth = {"fields": nfield, "sigma_h": 10000.0, "sigma_v": 5000.0,
+                  "nstep": sst["nstep"], "fields_per_pass": fpp,
+                  "device_ms": sst["step_ms"],
+                  "us_per_field_step": sst["step_ms"] * 1e3 / (sst["nstep"] * nfield),
+                  "achieved_gbs": sbytes * sst["nstep"] * passes
+                                  / (sst["step_ms"] * 1e-3) / 1e9,
+                  "algorithmic_bytes_per_step_pass": sbytes}
+
     # ---- served: continuous batching of a Poisson request stream ----------
     served = None
     if args.served_requests > 0:
@@ -462,6 +486,20 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                "kind": "port",
                "sample": f"20 forward + 20 adjoint/backward steps of one event "
                          f"(FP32 CPU restatement, OpenMP), extrapolated to NSTEP {NS}"}
+        if smooth is not None:
+            from oracle.oracle import Oracle
+            o = Oracle(db, precision=4, nthreads=1)
+            one = np.random.default_rng(3).standard_normal(
+                (db.nspec, 5, 5, 5)).astype(np.float32)
+            c0 = time.perf_counter()
+            o.smooth_pde(one, 10000.0, 5000.0, 690.0, nstep=2)
+            c1 = time.perf_counter()
+            o.smooth_pde(one, 10000.0, 5000.0, 690.0, nstep=4)
+            c2 = time.perf_counter()
+            per = ((c2 - c1) - (c1 - c0)) / 2.0
+            smooth["cpu_us_per_field_step"] = per * 1e6
+            smooth["cpu_sample"] = ("FP32 CPU restatement of smooth.f90's loops, "
+                                    "1 thread, steps 3-4 of one field")
 
     flops_evt_step = 29750 * db.nspec
     fp32_peak = None
@@ -517,6 +555,8 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         line["plain"] = result["plain"]
     if served:
         line["served"] = served
+    if smooth:
+        line["smooth"] = smooth
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
