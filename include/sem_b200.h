@@ -255,6 +255,66 @@ int sem_measure_l2_noalloc(const float *seis_dev, const double *obs_dev,
                            void *stream);
 
 /* ------------------------------------------------------------------------
+ * Waveform measurement with the reference's pre-processing, on the device.
+ *
+ * Replaces LEQData%measure_adj for the waveform (L2) misfit
+ * (src/preproc/leq_data.f90:48-188) with one window per trace and band,
+ * the window types whose windows are given by formula (group velocity,
+ * arrival time; leq_data.f90:132-146): observed traces are interpolated
+ * onto the synthetic axis, detrended, demeaned, Hann-tapered (pre_taper)
+ * and band-passed; synthetics are rotated to Z,R,T (rotate = 1), tapered
+ * and band-passed; the window's L2 misfit and adjoint source follow
+ * waveform_misfit.f90:15-64 and filter_adj (adjoint_source.f90:92-114);
+ * bands are summed (or normalised, ADJ_SRC_NORM) and rotated back to
+ * E,N,Z (noise_data.f90:213-252).  The Butterworth band-pass is xapiir's
+ * design (order, passes as IORD, PASSES) computed and applied in FP64; the
+ * reference runs it in FP32.
+ *
+ * Arrays: obs [nrec][3][obs_npts] FP64 (components Z,R,T when rotate,
+ * else x=E,y=N,z=Z); windows [max(nband,1)][nrec][3][2] start/end in
+ * origin time (s); baz [nrec] back-azimuth in degrees (rotate only).
+ * ------------------------------------------------------------------------ */
+#define SEM_MEAS_MAX_BANDS 4
+
+typedef struct {
+  double t0;               /* the synthetic record starts at -t0 (s)           */
+  double obs_tbeg;         /* time of the first observed sample (s)            */
+  double obs_dt;           /* observed sampling interval (s)                   */
+  int obs_npts;            /* observed samples per trace                       */
+  int nband;               /* band-pass filters, 0 (none) .. SEM_MEAS_MAX_BANDS */
+  double short_p[SEM_MEAS_MAX_BANDS]; /* SHORT_P per band (s)                  */
+  double long_p[SEM_MEAS_MAX_BANDS];  /* LONG_P per band (s)                   */
+  int order;               /* Butterworth order IORD (reference: 2)            */
+  int passes;              /* 1 or 2 (reference PASSES: 2, zero phase)         */
+  double pre_taper;        /* taper_per of whole traces (reference: 0.1)       */
+  double win_taper;        /* taper_percentage of the windows                  */
+  int win_taper_type;      /* itaper_type, 1..4                                */
+  double weight;           /* src_weight of the event                          */
+  int rotate;              /* 1: obs and windows are Z,R,T; needs baz          */
+  int adj_norm;            /* ADJ_SRC_NORM across bands                        */
+} sem_meas_cfg;
+
+/* Run form: measures event ev's resident seismograms (after
+ * sem_iterate_time(run, 1, 1)) and leaves the adjoint source on the device
+ * for sem_iterate_time(run, 3, 0).  misfit_band [max(nband,1)] and
+ * misfit_trace [max(nband,1)][nrec][3] (host, either may be NULL).
+ * No reference counterpart for the exact signature: it bundles
+ * measure_adj's per-trace loop for one event. */
+int sem_measure_waveform(sem_run *run, int ev, const sem_meas_cfg *cfg,
+                         const double *obs, const double *windows,
+                         const double *baz, double *misfit_band,
+                         double *misfit_trace);
+
+/* Device-buffer form on caller-owned device memory: seis [nrec][3][nstep]
+ * FP32 (x,y,z), adj out [nrec][3][nstep] FP32, misfit_trace out
+ * [max(nband,1)][nrec][3] FP64 (NaN for a window outside the record).
+ * Asynchronous on `stream`; allocates its scratch stream-ordered. */
+int sem_measure_waveform_dev(const float *seis_dev, int nrec, int nstep, double dt,
+                             const sem_meas_cfg *cfg, const double *obs_dev,
+                             const double *windows_dev, const double *baz_dev,
+                             float *adj_dev, double *misfit_trace_dev, void *stream);
+
+/* ------------------------------------------------------------------------
  * Kernel post-processing: PDE smoothing of element fields.
  *
  * Replaces smooth_sem_pde (src/postproc/smooth.f90:7-437), called from

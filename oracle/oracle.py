@@ -283,3 +283,177 @@ def l2_adjoint_source(syn, obs, dt, taper_pct=0.05, itype=1):
     r = s - d
     misfit = 0.5 * simpson(r * r, dt)
     return misfit, r * w
+
+
+# -- FP64 measurement pipeline: LEQData%measure_adj for IMEAS_WAVEFORM -------
+#
+# src/preproc/leq_data.f90:48-188 per receiver, component and band:
+#   obs: interpolate_func_dp onto the synthetic axis (signal.f90:85-125),
+#        detrend (signal.f90:382-406), demean (:408-417), Hann taper
+#        taper_per (config.f90:69), bandpass_dp (signal.f90:7-36)
+#   syn: rotated to Z,R,T (syn_data.f90:64-66, common.f90:136-152), Hann
+#        taper, bandpass_dp
+#   WaveformMisfit over the window (waveform_misfit.f90:15-64), filter_adj
+#   (adjoint_source.f90:92-114), times src_weight
+# then rotate_adj_src (noise_data.f90:213-252): sum (or normalised sum) over
+# bands and rotation Z,R,T -> Z,N,E (common.f90:272-291).
+# bandpass_dp runs SAC's xapiir (xapiir_sub.f90) in FP32; this restatement
+# designs and applies the same Butterworth band-pass in FP64.
+
+def butterworth_bandpass_sos(order, flo, fhi, dt):
+    """Second-order sections [nsect, 5] = (b0, b1, b2, a1, a2), a0 = 1, of
+    the Butterworth band-pass that xapiir designs (DESIGN, BUROOTS, WARP,
+    LPTBP, BILIN2: xapiir_sub.f90:237-304,334-368,712-726,855-961,
+    1270-1305): analog prototype poles on the unit circle, tangent-warped
+    band edges, low-pass to band-pass transform, gain 1 at the geometric
+    centre of the band, bilinear transform."""
+    poles, kinds = [], []
+    half = order // 2
+    if 2 * half < order:
+        poles.append(complex(-1.0, 0.0))
+        kinds.append("SP")
+    for k in range(1, half + 1):
+        ang = np.pi * (0.5 + (2 * k - 1) / (2.0 * order))
+        poles.append(complex(np.cos(ang), np.sin(ang)))
+        kinds.append("CP")
+    flw = np.tan(np.pi * flo * dt) / (2.0 * np.pi)
+    fhw = np.tan(np.pi * fhi * dt) / (2.0 * np.pi)
+    A = (2.0 * np.pi) ** 2 * flw * fhw
+    B = 2.0 * np.pi * (fhw - flw)
+    sn, sd = [], []
+    for p, kind in zip(poles, kinds):
+        if kind == "CP":
+            c = np.sqrt(complex((B * p) ** 2 - 4.0 * A))
+            for q in (0.5 * (B * p + c), 0.5 * (B * p - c)):
+                sn.append([0.0, B, 0.0])
+                sd.append([abs(q) ** 2, -2.0 * q.real, 1.0])
+        else:
+            sn.append([0.0, B, 0.0])
+            sd.append([A, -B * p.real, 1.0])
+    s = complex(0.0, np.sqrt(A))
+    h = complex(1.0, 0.0)
+    for n_, d_ in zip(sn, sd):
+        h *= ((n_[2] * s + n_[1]) * s + n_[0]) / ((d_[2] * s + d_[1]) * s + d_[0])
+    scale = 1.0 / abs(h)
+    sn[0] = [v * scale for v in sn[0]]
+    out = []
+    for n_, d_ in zip(sn, sd):
+        a0, a1, a2 = d_
+        sc = a2 + a1 + a0
+        b0, b1, b2 = n_
+        out.append([(b2 + b1 + b0) / sc, 2.0 * (b0 - b2) / sc, (b2 - b1 + b0) / sc,
+                    2.0 * (a0 - a2) / sc, (a2 - a1 + a0) / sc])
+    return np.array(out, np.float64)
+
+
+def iir_apply(x, sos, passes=2):
+    """xapiir's APPLY (xapiir_sub.f90:118-200): the sections in turn over
+    the whole trace, then (passes = 2) again over the reversed trace."""
+    from scipy.signal import sosfilt
+    sc = np.concatenate([sos[:, :3], np.ones((len(sos), 1)), sos[:, 3:]], axis=1)
+    y = sosfilt(sc, np.asarray(x, np.float64), axis=-1)
+    if passes == 2:
+        y = sosfilt(sc, y[..., ::-1], axis=-1)[..., ::-1]
+    return np.ascontiguousarray(y)
+
+
+def interpolate_onto(data, t1, dt1, t2, dt2, npt2):
+    """interpolate_func_dp (signal.f90:85-125): linear interpolation of a
+    trace starting at t1 with step dt1 onto npt2 samples from t2 with step
+    dt2; samples not strictly inside the data span are 0."""
+    data = np.asarray(data, np.float64)
+    npt1 = data.shape[-1]
+    time = t2 + np.arange(npt2) * dt2
+    inside = (time > t1) & (time < t1 + (npt1 - 1) * dt1)
+    ii = np.floor((time - t1) / dt1).astype(np.int64)
+    ii = np.clip(ii, 0, npt1 - 2)
+    tt = time - (ii * dt1 + t1)
+    out = (data[..., ii + 1] - data[..., ii]) * tt / dt1 + data[..., ii]
+    return np.where(inside, out, 0.0)
+
+
+def detrend(x):
+    """signal.f90:382-406 as written: least-squares slope, removed about the
+    1-based mean index (n+1)/2 from the 0-based index i-1."""
+    x = np.asarray(x, np.float64)
+    n = x.shape[-1]
+    ds1 = x.sum(-1)
+    ds2 = np.cumsum(x, axis=-1).sum(-1)
+    davei = 0.5 * (n + 1.0)
+    davex = ds1 / n
+    dslope = -12.0 * (ds2 - davei * ds1) / (n * (n * n - 1.0))
+    i = np.arange(n, dtype=np.float64)
+    return x - davex[..., None] - dslope[..., None] * (i - davei)
+
+
+def demean(x):
+    x = np.asarray(x, np.float64)
+    return x - x.sum(-1, keepdims=True) / x.shape[-1]
+
+
+def measure_waveform(syn, obs, dt, t0, obs_tbeg, obs_dt, bands, windows,
+                     order=2, passes=2, pre_taper=0.1, win_taper=0.05,
+                     win_type=1, weight=1.0, baz=None, adj_norm=False):
+    """FP64 restatement of LEQData%measure_adj (IMEAS_WAVEFORM), one
+    window per trace and band.
+
+    syn [nrec, 3, nstep] in x=E, y=N, z=Z; obs [nrec, 3, obs_npts] in Z,R,T
+    when ``baz`` (degrees, per receiver) is given, else in x, y, z;
+    ``bands`` [(short_p, long_p), ...] or [] for no band-pass; windows
+    [nband, nrec, 3, 2] start/end in origin time (s).  Returns
+    (misfit per band, adjoint source [nrec, 3, nstep] in x, y, z, per-trace
+    misfits [nband, nrec, 3])."""
+    syn = np.asarray(syn, np.float64)
+    nrec, _, nstep = syn.shape
+    if baz is not None:
+        b = np.deg2rad(np.asarray(baz, np.float64))[:, None]
+        e, nn, z = syn[:, 0], syn[:, 1], syn[:, 2]
+        syn = np.stack([z, -e * np.sin(b) - nn * np.cos(b),
+                        -e * np.cos(b) + nn * np.sin(b)], axis=1)
+    d0 = interpolate_onto(obs, obs_tbeg, obs_dt, -t0, dt, nstep)
+    d0 = demean(detrend(d0))
+    wpre = taper_window(nstep, pre_taper, 1)
+    d0 = d0 * wpre
+    s0 = syn * wpre
+    nb_ = max(1, len(bands))
+    adjs = np.zeros((nb_, nrec, 3, nstep))
+    mis = np.zeros((nb_, nrec, 3))
+    for ib in range(nb_):
+        if bands:
+            sos = butterworth_bandpass_sos(order, 1.0 / bands[ib][1], 1.0 / bands[ib][0], dt)
+            d = iir_apply(d0, sos, passes)
+            s = iir_apply(s0, sos, passes)
+        else:
+            sos, d, s = None, d0, s0
+        for r in range(nrec):
+            for c in range(3):
+                w0, w1 = windows[ib][r][c]
+                nb = int((w0 + t0) / dt) + 1
+                ne = int((w1 + t0) / dt)
+                if ne - nb + 1 <= 0:
+                    raise ValueError("empty window")
+                tw = taper_window(ne - nb + 1, win_taper, win_type)
+                sw = s[r, c, nb - 1:ne] * tw
+                dw = d[r, c, nb - 1:ne] * tw
+                res = sw - dw
+                mis[ib, r, c] = 0.5 * simpson(res * res, dt) * weight
+                a = np.zeros(nstep)
+                a[nb - 1:ne] = res * tw
+                if sos is not None:
+                    a = iir_apply(a, sos, passes)
+                out = np.zeros(nstep)
+                out[nb - 1:ne] = a[nb - 1:ne] * tw
+                adjs[ib, r, c] = out * weight
+    if adj_norm and nb_ > 1:
+        amax = np.abs(adjs).max(-1)                       # [band, rec, comp]
+        mx = amax.max(0)                                  # [rec, comp]
+        safe = np.where(amax > 0, amax, 1.0)
+        comb = np.where((amax > 0)[..., None], adjs / safe[..., None] * mx[None, ..., None], 0.0).sum(0)
+    else:
+        comb = adjs.sum(0)
+    if baz is not None:
+        b = np.deg2rad(np.asarray(baz, np.float64))[:, None]
+        z, rr, tt = comb[:, 0], comb[:, 1], comb[:, 2]
+        comb = np.stack([-rr * np.sin(b) - tt * np.cos(b),
+                         -rr * np.cos(b) + tt * np.sin(b), z], axis=1)
+    return mis.sum((1, 2)), comb, mis

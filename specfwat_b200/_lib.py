@@ -33,8 +33,9 @@ EXPORTS = (
     "sem_kernel_variants", "sem_measure_l2_noalloc",
     "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
     "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
-    "sem_smooth_pde",
+    "sem_smooth_pde", "sem_measure_waveform", "sem_measure_waveform_dev",
 )
+MEAS_MAX_BANDS = 4
 SMOOTH_MAP_CUBE = 0
 SMOOTH_MAP_REFERENCE = 1
 L2_NOALLOC_MAX_RECEIVERS = 4096
@@ -78,6 +79,17 @@ class Source(C.Structure):
                 ("Mrr", C.c_double), ("Mtt", C.c_double), ("Mpp", C.c_double),
                 ("Mrt", C.c_double), ("Mrp", C.c_double), ("Mtp", C.c_double),
                 ("f0", C.c_double), ("tshift", C.c_double)]
+
+
+class MeasCfg(C.Structure):
+    _fields_ = [("t0", C.c_double), ("obs_tbeg", C.c_double),
+                ("obs_dt", C.c_double), ("obs_npts", C.c_int),
+                ("nband", C.c_int), ("short_p", C.c_double * 4),
+                ("long_p", C.c_double * 4), ("order", C.c_int),
+                ("passes", C.c_int), ("pre_taper", C.c_double),
+                ("win_taper", C.c_double), ("win_taper_type", C.c_int),
+                ("weight", C.c_double), ("rotate", C.c_int),
+                ("adj_norm", C.c_int)]
 
 
 class SmoothCfg(C.Structure):
@@ -145,6 +157,10 @@ def load():
         "sem_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "sem_smooth_pde": (C.c_int, [vp, C.POINTER(SmoothCfg), ip, fp, fp, fp,
                                      C.POINTER(SmoothStats)]),
+        "sem_measure_waveform": (C.c_int, [vp, ip, C.POINTER(MeasCfg), fp, fp, fp,
+                                           fp, fp]),
+        "sem_measure_waveform_dev": (C.c_int, [vp, ip, ip, dp, C.POINTER(MeasCfg), vp,
+                                               vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

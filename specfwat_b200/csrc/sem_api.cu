@@ -1114,6 +1114,67 @@ int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int 
   return SEM_OK;
 }
 
+int sem_measure_waveform(sem_run* r, int ev, const sem_meas_cfg* cfg, const double* obs,
+                         const double* windows, const double* baz, double* misfit_band,
+                         double* misfit_trace) {
+  if (!r || !cfg || !obs || !windows) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  if (cfg->rotate && !baz) return fail(SEM_ERR_ARG, "rotate needs the back-azimuths");
+  const int ns = r->nstep, nr = r->nrec[ev];
+  if (nr == 0) return fail(SEM_ERR_STATE, "event %d has no receivers", ev);
+  MeasParams p;
+  int rc = check_measure_params(cfg, nr, ns, r->dt, windows, &p);
+  if (rc) return rc;
+  const int nb = p.nband > 0 ? p.nband : 1;
+  const size_t n_obs = (size_t)nr * 3 * p.obs_npts, n_win = (size_t)nb * nr * 3 * 2;
+  const size_t n_mis = (size_t)nb * nr * 3, n_scr = measure_scratch_doubles(p);
+  double* buf = nullptr;
+  const size_t total = n_obs + n_win + nr + n_mis + n_scr;
+  cudaError_t e = cudaMallocAsync((void**)&buf, total * sizeof(double), r->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SEM_ERR_NOMEM, "measurement buffers (%zu MB): %s", total * 8 >> 20,
+                cudaGetErrorString(e));
+  }
+  double* d_obs = buf;
+  double* d_win = d_obs + n_obs;
+  double* d_baz = d_win + n_win;
+  double* d_mis = d_baz + nr;
+  double* d_scr = d_mis + n_mis;
+  std::vector<double> mis(n_mis);
+  auto run = [&]() -> cudaError_t {
+    cudaError_t err = cudaMemcpyAsync(d_obs, obs, n_obs * 8, cudaMemcpyHostToDevice, r->stream);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(d_win, windows, n_win * 8, cudaMemcpyHostToDevice, r->stream);
+    if (err == cudaSuccess && baz)
+      err = cudaMemcpyAsync(d_baz, baz, (size_t)nr * 8, cudaMemcpyHostToDevice, r->stream);
+    if (err != cudaSuccess) return err;
+    const size_t per = (size_t)r->nrec_max * 3 * ns;
+    launch_measure_waveform(p, r->seis.p + per * ev, d_obs, d_win, d_baz, d_scr,
+                            r->adj.p + per * ev, d_mis, r->stream);
+    err = cudaGetLastError();
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(mis.data(), d_mis, n_mis * 8, cudaMemcpyDeviceToHost, r->stream);
+    return err;
+  };
+  e = run();
+  cudaFreeAsync(buf, r->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SEM_ERR_CUDA, "waveform measurement: %s", cudaGetErrorString(e));
+  }
+  r->have_adj[ev] = 1;
+  if (misfit_band)
+    for (int b = 0; b < nb; ++b) {
+      double t = 0.0;
+      for (int q = 0; q < nr * 3; ++q) t += mis[(size_t)b * nr * 3 + q];
+      misfit_band[b] = t;
+    }
+  if (misfit_trace) std::copy(mis.begin(), mis.end(), misfit_trace);
+  return SEM_OK;
+}
+
 int sem_save_adjoint_kernels(sem_run* r, int ev, double* out) {
   if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
   if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);

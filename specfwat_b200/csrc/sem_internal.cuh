@@ -7,7 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 
-struct sem_mesh_s;
+#include "sem_b200.h"
 
 namespace sem {
 
@@ -133,6 +133,29 @@ int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int
                          cudaStream_t st);
 
 void set_gll_constants(const float* D, const float* DWt, const float* w);
+
+// Waveform measurement (sem_measure.cu): Butterworth band-pass sections
+// (b0, b1, b2, a1, a2 with a0 = 1) per band and the launch parameters.
+constexpr int kMeasMaxBands = 4;
+constexpr int kMeasMaxSections = 10;
+struct MeasBand {
+  int nsect;
+  double b0[kMeasMaxSections], b1[kMeasMaxSections], b2[kMeasMaxSections];
+  double a1[kMeasMaxSections], a2[kMeasMaxSections];
+};
+struct MeasParams {
+  int nrec, nstep, obs_npts, nband, passes, win_taper_type, rotate, adj_norm;
+  double dt, t0, obs_tbeg, obs_dt, pre_taper, win_taper, weight;
+  MeasBand band[kMeasMaxBands];
+};
+int design_bandpass(int order, double flo, double fhi, double dt, MeasBand* out);
+// Checks a configuration (and host windows, when given) and fills p.
+int check_measure_params(const sem_meas_cfg* c, int nrec, int nstep, double dt,
+                         const double* windows_host, MeasParams* p);
+size_t measure_scratch_doubles(const MeasParams& p);
+int launch_measure_waveform(const MeasParams& p, const float* seis, const double* obs,
+                            const double* win, const double* baz, double* scratch, float* adj,
+                            double* mis, cudaStream_t st);
 
 // What the kernel smoother reads from a prepared mesh (defined in
 // sem_api.cu, where the mesh type lives).

@@ -164,6 +164,26 @@ class Simulation:
                                          C.byref(m)))
         return m.value
 
+    def measure_waveform(self, ev: int, obs, windows, cfg, baz=None):
+        """Waveform measurement of event ``ev`` with the reference's
+        pre-processing (see :mod:`specfwat_b200.measure`); the adjoint
+        source stays on the device.  ``obs`` [nrec, 3, obs_npts], windows
+        [nband, nrec, 3, 2] (origin time).  Returns (misfit per band,
+        per-trace misfits [nband, nrec, 3])."""
+        obs = np.ascontiguousarray(obs, np.float64)
+        nr = self.nrec[ev]
+        assert obs.ndim == 3 and obs.shape[:2] == (nr, 3)
+        win = np.ascontiguousarray(windows, np.float64)
+        assert win.shape == (cfg.nband_out, nr, 3, 2)
+        b = None if baz is None else np.ascontiguousarray(baz, np.float64)
+        mb = np.zeros(cfg.nband_out)
+        mt = np.zeros((cfg.nband_out, nr, 3))
+        c = cfg.to_c(self.dt, obs.shape[-1])
+        check(_lib.load().sem_measure_waveform(
+            self._h, ev, C.byref(c), obs.ctypes.data, win.ctypes.data,
+            None if b is None else b.ctypes.data, mb.ctypes.data, mt.ctypes.data))
+        return mb, mt
+
     def set_observed(self, ev: int, obs):
         """Keep observed data of ``ev`` in device memory for measure_l2."""
         obs = np.ascontiguousarray(obs, np.float64)

@@ -261,3 +261,126 @@ def _lagrange_deriv(i, j, x):
             prod *= (x[j] - x[q]) / (x[i] - x[q])
         s += prod
     return s
+
+
+def xapiir_bu_bp(data, iord, flo, fhi, ts, passes):
+    """SAC's XAPIIR for APROTO='BU', TYPE='BP' (src/shared/xapiir_sub.f90:
+    58-86 XAPIIR, 118-200 APPLY, 237-304 DESIGN, 334-368 BUROOTS, 712-726
+    WARP, 855-961 LPTBP, 1270-1305 BILIN2), REAL/COMPLEX as float32 /
+    complex64 like the Fortran.  Returns the filtered trace (float32)."""
+    import numpy as np
+    f32, c64 = np.float32, np.complex64
+
+    def warp(f, t):
+        twopi = f32(6.2831853)
+        angle = f32(f32(twopi * f) * t) / f32(2.0)
+        w = f32(f32(2.0) * f32(np.tan(angle))) / t
+        return f32(w / twopi)
+
+    # BUROOTS
+    pi = f32(3.14159265)
+    half = iord // 2
+    p, rtype = [], []
+    if 2 * half < iord:
+        p.append(c64(complex(-1.0, 0.0)))
+        rtype.append("SP")
+    for k in range(1, half + 1):
+        angle = f32(pi * f32(f32(0.5) + f32(2 * k - 1) / f32(2 * iord)))
+        p.append(c64(complex(np.cos(angle), np.sin(angle))))
+        rtype.append("CP")
+    dcvalue = f32(1.0)
+    # DESIGN: BP mapping
+    flw = warp(f32(f32(flo) * f32(ts)) / f32(2.0), f32(2.0))
+    fhw = warp(f32(f32(fhi) * f32(ts)) / f32(2.0), f32(2.0))
+    # LPTBP
+    twopi = f32(f32(2.0) * pi)
+    A = f32(f32(f32(twopi * twopi) * flw) * fhw)
+    B = f32(twopi * f32(fhw - flw))
+    sn, sd = [], []
+    for i in range(len(p)):
+        if rtype[i] == "CP":
+            bp = c64(B * p[i])
+            ctemp = c64(np.sqrt(c64(c64(bp * bp) - c64(f32(4.0) * A))))
+            p1 = c64(f32(0.5) * c64(bp + ctemp))
+            p2 = c64(f32(0.5) * c64(bp - ctemp))
+            for q in (p1, p2):
+                sn += [f32(0.0), B, f32(0.0)]
+                sd += [f32((q * np.conj(q)).real), f32(f32(-2.0) * f32(q.real)), f32(1.0)]
+        else:
+            sn += [f32(0.0), B, f32(0.0)]
+            sd += [A, f32(-B * f32(p[i].real)), f32(1.0)]
+    nsects = len(sn) // 3
+    s = c64(complex(0.0, float(np.sqrt(A))))
+    h = c64(complex(1.0, 0.0))
+    for j in range(nsects):
+        k = 3 * j
+        num = c64(c64(c64(sn[k + 2] * s) + sn[k + 1]) * s) + sn[k]
+        den = c64(c64(c64(sd[k + 2] * s) + sd[k + 1]) * s) + sd[k]
+        h = c64(h * c64(num / den))
+    scale = f32(dcvalue / f32(np.sqrt(f32((h * np.conj(h)).real))))
+    sn[0] = f32(sn[0] * scale)
+    sn[1] = f32(sn[1] * scale)
+    sn[2] = f32(sn[2] * scale)
+    # BILIN2
+    for j in range(nsects):
+        k = 3 * j
+        a0, a1, a2 = sd[k], sd[k + 1], sd[k + 2]
+        sc = f32(f32(a2 + a1) + a0)
+        sd[k] = f32(1.0)
+        sd[k + 1] = f32(f32(f32(2.0) * f32(a0 - a2)) / sc)
+        sd[k + 2] = f32(f32(f32(a2 - a1) + a0) / sc)
+        a0, a1, a2 = sn[k], sn[k + 1], sn[k + 2]
+        sn[k] = f32(f32(f32(a2 + a1) + a0) / sc)
+        sn[k + 1] = f32(f32(f32(2.0) * f32(a0 - a2)) / sc)
+        sn[k + 2] = f32(f32(f32(a2 - a1) + a0) / sc)
+    # APPLY
+    x = [f32(v) for v in data]
+    n = len(x)
+
+    def run(order):
+        for j in range(nsects):
+            k = 3 * j
+            x1 = x2 = y1 = y2 = f32(0.0)
+            b0, b1, b2, a1, a2 = sn[k], sn[k + 1], sn[k + 2], sd[k + 1], sd[k + 2]
+            for i in order:
+                out = f32(f32(f32(b0 * x[i]) + f32(b1 * x1)) + f32(b2 * x2))
+                out = f32(out - f32(f32(a1 * y1) + f32(a2 * y2)))
+                y2, y1 = y1, out
+                x2, x1 = x1, x[i]
+                x[i] = out
+
+    run(range(n))
+    if passes != 1:
+        run(range(n - 1, -1, -1))
+    return np.array(x, np.float32)
+
+
+def detrend(x):
+    """src/shared/signal.f90:382-406 line by line (FP64)."""
+    n = len(x)
+    dan = float(n)
+    ds1 = 0.0
+    ds2 = 0.0
+    for i in range(1, n + 1):
+        ds1 = ds1 + x[i - 1]
+        ds2 = ds2 + ds1
+    davei = 0.5 * (dan + 1.0)
+    davex = ds1 / dan
+    dslope = -12.0 * (ds2 - davei * ds1) / (dan * (dan * dan - 1.0))
+    out = list(x)
+    for i in range(1, n + 1):
+        dai = float(i - 1)
+        out[i - 1] = x[i - 1] - davex - dslope * (dai - davei)
+    return out
+
+
+def interpolate_func_dp(syn, t1, dt1, npt1, t2, dt2, npt2):
+    """src/shared/signal.f90:85-125 line by line (FP64)."""
+    syn1 = [0.0] * npt2
+    for i in range(1, npt2 + 1):
+        time = t2 + (i - 1) * dt2
+        if time > t1 and time < t1 + (npt1 - 1) * dt1:
+            ii = math.floor((time - t1) / dt1) + 1
+            tt = time - ((ii - 1) * dt1 + t1)
+            syn1[i - 1] = (syn[ii + 1 - 1] - syn[ii - 1]) * tt / dt1 + syn[ii - 1]
+    return syn1
