@@ -112,7 +112,11 @@ typedef struct {
                          one float2 (4 / 8 events per block), 9 / 10 as
                          7 / 8 with the gather prefetched in registers,
                          11 forward with 2 events per thread and the
-                         gather in registers, adjoint as 10                */
+                         gather in registers, adjoint as 10, 12 as 11
+                         with the forward scatter as plain read-modify-
+                         writes in one launch per element colour, 13
+                         thread per point with xi contractions by warp
+                         shuffles (one event per block)                    */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard
@@ -228,7 +232,9 @@ int sem_lane_finish(sem_run *run, int lane, float *seis, double *kernels6,
  * (1 thread-per-point, 2 pencil, 3 pencil pipelined, 4 pencil pipelined
  * with 2 events per block, 5 and 6 pencil pipelined with 2 or 4 events
  * per thread, 7 to 10 with the adjoint-phase field pair as a float2,
- * 11 forward with register prefetch).  With kernel_variant = 0 the first
+ * 11 forward with register prefetch, 12 as 11 with colour-ordered
+ * non-atomic forward assembly, 13 thread per point with warp-shuffle
+ * contractions).  With kernel_variant = 0 the first
  * sem_iterate_time times the candidates on this run and keeps the fastest
  * per phase; -1 until then. */
 int sem_kernel_variants(sem_run *run, int *fwd, int *adj);

@@ -192,6 +192,9 @@ struct sem_mesh_s {
   float xix = 0.f, jac = 0.f;
   DevArray<int> ibool;
   DevArray<int> order;
+  DevArray<int> corder;          // elements grouped by colour
+  int ncolour = 0;
+  std::vector<int> cstart;       // [ncolour + 1]
   DevArray<float> kappa, mu, rho;
   DevArray<int> f_iglob;
   DevArray<float> f_rvp, f_rvs, f_jw, f_n;
@@ -214,6 +217,10 @@ struct sem_mesh_s {
     v.jac = jac;
     v.ibool = ibool.p;
     v.order = order.p;
+    v.corder = corder.p;
+    v.ncolour = ncolour;
+    for (int c = 0; c <= MeshView::kMaxColours; ++c)
+      v.cstart[c] = c <= ncolour && ncolour > 0 ? cstart[c] : 0;
     v.kappa = kappa.p;
     v.mu = mu.p;
     v.f_iglob = f_iglob.p;
@@ -224,7 +231,7 @@ struct sem_mesh_s {
     return v;
   }
   size_t device_bytes() const {
-    return ibool.bytes() + order.bytes() + kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
+    return ibool.bytes() + order.bytes() + corder.bytes() + kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
            f_rvp.bytes() + f_rvs.bytes() + f_jw.bytes() + f_n.bytes();
   }
 
@@ -533,6 +540,41 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
   CKM(m->f_n.alloc((size_t)nf * NGLL2 * 3), "face normal");
   CK(cudaMemcpy(m->ibool.p, m->h_ibool.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m->order.p, order.data(), d->nspec * sizeof(int), cudaMemcpyHostToDevice));
+  {
+    // Greedy colouring in traversal order: an element takes the first
+    // colour none of whose elements shares a point with it.  Within a colour
+    // the elements keep the Morton order.  A structured hexahedral mesh
+    // needs 8 colours.
+    std::vector<int> col(d->nspec, -1);
+    std::vector<std::vector<char>> used;
+    int ncol = 0;
+    for (int q = 0; q < d->nspec && ncol <= MeshView::kMaxColours; ++q) {
+      const int e = order[q];
+      const int* ib = &m->h_ibool[(size_t)e * NGLL3];
+      int c = 0;
+      for (;; ++c) {
+        if (c == ncol) {
+          used.emplace_back(d->nglob, 0);
+          ++ncol;
+        }
+        bool ok = true;
+        for (int p = 0; p < NGLL3 && ok; ++p) ok = !used[c][ib[p]];
+        if (ok) break;
+      }
+      col[e] = c;
+      for (int p = 0; p < NGLL3; ++p) used[c][ib[p]] = 1;
+    }
+    if (ncol <= MeshView::kMaxColours) {
+      m->ncolour = ncol;
+      m->cstart.assign(ncol + 1, 0);
+      for (int e = 0; e < d->nspec; ++e) m->cstart[col[e] + 1]++;
+      for (int c = 0; c < ncol; ++c) m->cstart[c + 1] += m->cstart[c];
+      std::vector<int> pos(m->cstart.begin(), m->cstart.end() - 1), corder(d->nspec);
+      for (int q = 0; q < d->nspec; ++q) corder[pos[col[order[q]]]++] = order[q];
+      CKM(m->corder.alloc(d->nspec), "colour order");
+      CK(cudaMemcpy(m->corder.p, corder.data(), d->nspec * sizeof(int), cudaMemcpyHostToDevice));
+    }
+  }
   CK(cudaMemcpy(m->kappa.p, d->kappastore, ne * sizeof(float), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m->mu.p, d->mustore, ne * sizeof(float), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m->rho.p, d->rhostore, ne * sizeof(float), cudaMemcpyHostToDevice));
@@ -586,8 +628,8 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->max_receivers < 1 || c->max_receivers > 100000)
     return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
-  if (c->kernel_variant < 0 || c->kernel_variant > 11)
-    return fail(SEM_ERR_ARG, "kernel_variant must be 0..11");
+  if (c->kernel_variant < 0 || c->kernel_variant > 13)
+    return fail(SEM_ERR_ARG, "kernel_variant must be 0..13");
   return SEM_OK;
 }
 
@@ -632,8 +674,8 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   if (c->kernel_variant == 0) {
     const char* fv = std::getenv("SEM_FORCE_VARIANTS");
     int vf = 0, va = 0;
-    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 11 && va >= 1 &&
-        va <= 11) {
+    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 13 && va >= 1 &&
+        va <= 13) {
       r->variant[0] = vf - 1;
       r->variant[1] = va - 1;
     }
@@ -802,10 +844,10 @@ static int ensure_store(sem_run* r) {
 // keep the fastest.  Runs on scratch state before the forward run: the
 // forward zeroes its wavefields and the adjoint run rebuilds its own.
 static int autotune_phase(sem_run* r, bool adj) {
-  const int cands_multi[] = {0, 2, 3, 4, 5, 6, 7, 8, 9, 10};
-  const int cands_single[] = {0, 2};
+  const int cands_multi[] = {0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11};
+  const int cands_single[] = {0, 2, 12};
   const int* cands = r->nev > 1 ? cands_multi : cands_single;
-  const int ncand = r->nev > 1 ? 10 : 2;
+  const int ncand = r->nev > 1 ? 11 : 3;
   const int nsteps = std::max(1, std::min(8, r->nstep - 2));
   r->fill_lanes(adj ? PH_ADJ : PH_FWD, 0);
   for (auto& L : r->h_lanes) L.it0 = 1;

@@ -53,6 +53,12 @@ struct MeshView {
   const float* f_rvs;    // [nf*25] rho*vs
   const float* f_jw;     // [nf*25] jacobian2D * weights
   const float* f_n;      // [nf*25*3]
+  // element colouring for assembly without atomics: colour c's elements
+  // are corder[cstart[c] .. cstart[c+1]), no two of them share a point
+  static constexpr int kMaxColours = 32;
+  int ncolour;           // 0: not coloured (more than kMaxColours needed)
+  const int* corder;     // [nspec]
+  int cstart[kMaxColours + 1];
 };
 
 struct Fields {

@@ -248,6 +248,158 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// element kernel, thread per GLL point, xi contractions by warp shuffles
+// ---------------------------------------------------------------------------
+//
+// Warp w holds GLL rows r = 6w .. 6w+5 (row r is (j,k) = (r%5, r/5)); lane l
+// is point i = l%5 of row 6w + l/5, and lanes 30, 31 idle, so the five
+// points of a row sit in five consecutive lanes of one warp.  The
+// xi-derivatives and the xi part of the divergence read the row through
+// __shfl_sync; the eta and gamma directions go through shared memory as in
+// the thread-per-point kernel.  One lane per block (grid.y = lane).
+
+template <bool ADJ>
+__global__ void __launch_bounds__(160) k_forces_shfl(StepArgs A) {
+  constexpr int NF = ADJ ? 2 : 1;
+  __shared__ float sU[NF][3][NGLL3];
+  __shared__ float sS[NF][6][NGLL3];
+  __shared__ float sD[25], sDWt[25], sW[5];
+  const int e = A.m.order[blockIdx.x];
+  const int lg = blockIdx.y;
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  const int r = 6 * w + ln / 5;
+  const bool act = ln < 30 && r < 25;
+  const int rr = act ? r : 0;
+  const int i = act ? ln % 5 : 0, j = rr % 5, k = rr / 5;
+  const int p = i + 5 * rr;
+  const int base = (ln / 5) * 5;
+  bool act1 = false, act2 = false, scat2 = false;
+  {
+    const LaneDesc* L = A.lanes + lg;
+    const int it = L->it0 + A.s;
+    if (L->phase != PH_IDLE && it < L->nstep) {
+      act1 = true;
+      if (ADJ && L->phase == PH_ADJ) {
+        act2 = true;
+        scat2 = it > 0;
+      }
+    }
+  }
+  if (threadIdx.x < 25) {
+    sD[threadIdx.x] = c_D[threadIdx.x];
+    sDWt[threadIdx.x] = c_DWt[threadIdx.x];
+  }
+  if (threadIdx.x < 5) sW[threadIdx.x] = c_w[threadIdx.x];
+  if (!__syncthreads_or(act1)) return;
+
+  const size_t ep = (size_t)e * NGLL3 + p;
+  const int ig = A.m.ibool[ep];
+  const float kp = A.m.kappa[ep], mu = A.m.mu[ep];
+  float u[NF][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const size_t q = A.fi((size_t)ig, c, lg);
+    u[0][c] = act1 ? A.f1.u[q] : 0.f;
+    if (ADJ) u[NF - 1][c] = act2 ? A.f2.u[q] : 0.f;
+  }
+  if (act)
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sU[f][c][p] = u[f][c];
+  __syncthreads();
+
+  const float xix = A.m.xix;
+  const float fac = A.m.jac * A.m.xix;
+  float di[5], dj[5], dk[5];
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    di[l] = sD[i * 5 + l];
+    dj[l] = sD[j * 5 + l];
+    dk[l] = sD[k * 5 + l];
+  }
+  float sig[NF][6];
+  float g[NF][3][3];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float a = 0.f, b = 0.f, cc = 0.f;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        a = fmaf(di[l], __shfl_sync(0xffffffffu, u[f][c], base + l), a);
+        b = fmaf(dj[l], sU[f][c][i + 5 * l + 25 * k], b);
+        cc = fmaf(dk[l], sU[f][c][i + 5 * j + 25 * l], cc);
+      }
+      g[f][c][0] = a * xix;
+      g[f][c][1] = b * xix;
+      g[f][c][2] = cc * xix;
+    }
+    stress_point(g[f], kp, mu, fac, sig[f]);
+  }
+  if (ADJ && act2 && act) {
+    const float tr1 = g[0][0][0] + g[0][1][1] + g[0][2][2];
+    const float tr2 = g[1][0][0] + g[1][1][1] + g[1][2][2];
+    const float a_xx = g[0][0][0] - tr1 * (1.0f / 3.0f), a_yy = g[0][1][1] - tr1 * (1.0f / 3.0f);
+    const float b_xx = g[1][0][0] - tr2 * (1.0f / 3.0f), b_yy = g[1][1][1] - tr2 * (1.0f / 3.0f);
+    const float a_xy = 0.5f * (g[0][0][1] + g[0][1][0]), a_xz = 0.5f * (g[0][0][2] + g[0][2][0]);
+    const float a_yz = 0.5f * (g[0][1][2] + g[0][2][1]);
+    const float b_xy = 0.5f * (g[1][0][1] + g[1][1][0]), b_xz = 0.5f * (g[1][0][2] + g[1][2][0]);
+    const float b_yz = 0.5f * (g[1][1][2] + g[1][2][1]);
+    const float dd = a_xx * b_xx + a_yy * b_yy + (a_xx + a_yy) * (b_xx + b_yy) +
+                     2.0f * (a_xy * b_xy + a_xz * b_xz + a_yz * b_yz);
+    const size_t q = A.ei(ep, lg);
+    A.k.mu[q] += A.dt * dd;
+    A.k.kappa[q] += A.dt * (tr1 * tr2);
+  }
+  __syncthreads();  // every eta/gamma read of sU is done
+  if (act)
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) sS[f][q][p] = sig[f][q];
+  __syncthreads();
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    di[l] = sDWt[i * 5 + l];
+    dj[l] = sDWt[j * 5 + l];
+    dk[l] = sDWt[k * 5 + l];
+  }
+  const float wjk = sW[j] * sW[k], wik = sW[i] * sW[k], wij = sW[i] * sW[j];
+  // flux components: xi direction sigma_{c,x} = (xx, xy, xz), eta
+  // sigma_{c,y} = (xy, yy, yz), gamma sigma_{c,z} = (xz, yz, zz)
+  constexpr int QX[3] = {0, 3, 4}, QY[3] = {3, 1, 5}, QZ[3] = {4, 5, 2};
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    float fo[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float a = 0.f, b = 0.f, cc = 0.f;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        a = fmaf(di[l], __shfl_sync(0xffffffffu, sig[f][QX[c]], base + l), a);
+        b = fmaf(dj[l], sS[f][QY[c]][i + 5 * l + 25 * k], b);
+        cc = fmaf(dk[l], sS[f][QZ[c]][i + 5 * j + 25 * l], cc);
+      }
+      fo[c] = -(wjk * a + wik * b + wij * cc);
+    }
+    const bool on = f == 0 ? act1 : scat2;
+    if (act && on) {
+      float* acc = f == 0 ? A.f1.a : A.f2.a;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) atomicAdd(&acc[A.fi((size_t)ig, c, lg)], fo[c]);
+    }
+  }
+}
+
+template <bool ADJ>
+static int forces_shfl_cfg(const StepArgs& a, cudaStream_t st) {
+  dim3 grid(a.m.nspec, a.nev);
+  k_forces_shfl<ADJ><<<grid, 160, 0, st>>>(a);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
 // element kernel, pencil decomposition
 // ---------------------------------------------------------------------------
 //
@@ -1252,7 +1404,30 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
 }
 
 // xi role: total force on the pencil and vector scatter-add.
-template <int LB, int NL>
+// Plain read-modify-write of NL consecutive floats, for colour-ordered
+// launches in which no other thread touches the same point.
+template <int NL>
+__device__ __forceinline__ void rmw_v(float* g, const LV<NL>& x) {
+  if constexpr (NL == 1) {
+    *g += x.v[0];
+  } else if constexpr (NL == 2) {
+    float2* q = reinterpret_cast<float2*>(g);
+    float2 o = *q;
+    o.x += x.v[0];
+    o.y += x.v[1];
+    *q = o;
+  } else {
+    float4* q = reinterpret_cast<float4*>(g);
+    float4 o = *q;
+    o.x += x.v[0];
+    o.y += x.v[1];
+    o.z += x.v[2];
+    o.w += x.v[3];
+    *q = o;
+  }
+}
+
+template <int LB, int NL, bool ATOMIC = true>
 __device__ __forceinline__ void v_scatter(const PBuf<LB>& b, int t, const LV<NL> fx[5][3],
                                           const int* ib, float* accb, const int* fl, int bit) {
   const int pj = t % 5, pk = t / 5;
@@ -1278,7 +1453,10 @@ __device__ __forceinline__ void v_scatter(const PBuf<LB>& b, int t, const LV<NL>
         const float v = -(wjk * fx[i][c].v[n] + wik * e1.v[n] + wij * e2.v[n]);
         f.v[n] = (fl[n] & bit) ? v : 0.f;  // lanes not in this phase add nothing
       }
-      red_v<NL>(&accb[foff<3>((int)ig, c)], f);
+      if constexpr (ATOMIC)
+        red_v<NL>(&accb[foff<3>((int)ig, c)], f);
+      else
+        rmw_v<NL>(&accb[foff<3>((int)ig, c)], f);
     }
   }
 }
@@ -1996,7 +2174,7 @@ struct FwdRLayout {
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
 
-template <int LB>
+template <int LB, bool COLOURED>
 __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeItems items) {
   constexpr int NL = 2;
   constexpr int NT = 25 * LB / NL;
@@ -2015,7 +2193,7 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
   const int lane = lq * NL;
   const int pi = t % 5, pq = t / 5;
   const int nev = A.nev;
-  const int nspec = A.m.nspec;
+  const int ngr = items.ngroups;  // elements of this launch (one colour, or all)
   const int nitems = items.count();
 
   bool any = false;
@@ -2054,7 +2232,7 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     int chunk = 0, g = 0;
     if (w < nitems) items.decode(w, chunk, g);
     for (int i = tid; i < NE; i += NT) {
-      if (w < nitems && g < nspec)
+      if (w < nitems && g < ngr)
         cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
       else
         dst[i] = -1;
@@ -2065,9 +2243,9 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     int chunk, g;
     items.decode(w, chunk, g);
     float* km = sKM + buf * 2 * NE;
-    const int e = g < nspec ? A.m.order[g] : 0;
+    const int e = g < ngr ? A.m.order[g] : 0;
     for (int i = tid; i < NE; i += NT) {
-      if (g < nspec) {
+      if (g < ngr) {
         const size_t ep = (size_t)e * NGLL3 + i;
         cp_async4(km + i, A.m.kappa + ep);
         cp_async4(km + NE + i, A.m.mu + ep);
@@ -2123,7 +2301,7 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
 
     int lg0, g, fl[NL];
     const int anyf = flags(w, lg0, g, fl);
-    const int e = g < nspec ? A.m.order[g] : nspec;
+    const bool valid = g < ngr;
     const float* kap = sKM + buf * 2 * NE;
     const float* mu = kap + NE;
     PBuf<LB> b{sU + lane, sA + lane};
@@ -2134,32 +2312,46 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     __syncthreads();
     v_div_eg<LB, NL>(b, pi, pq);
     __syncthreads();
-    if (e < nspec && anyf)
-      v_scatter<LB, NL>(b, t, fx, sIB + ibs * NE, A.f1.a + fbase<LWLOG>(A, lg0), fl, 1);
+    if (valid && anyf)
+      v_scatter<LB, NL, !COLOURED>(b, t, fx, sIB + ibs * NE, A.f1.a + fbase<LWLOG>(A, lg0), fl, 1);
   }
   cp_wait_all();
 }
 
-template <int LB>
-static void forces_fwd_r_cfg(const StepArgs& a, cudaStream_t st) {
+template <int LB, bool COLOURED>
+static int forces_fwd_r_cfg(const StepArgs& a, cudaStream_t st) {
   constexpr int NT = 25 * LB / 2;
   constexpr size_t BYTES = FwdRLayout<LB>::BYTES;
   static int blocks_per_sm = 0, sms = 0;
   if (!blocks_per_sm) {
-    cudaFuncSetAttribute(k_forces_fwd_r<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_forces_fwd_r<LB, COLOURED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_fwd_r<LB>, NT, BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_fwd_r<LB, COLOURED>, NT,
+                                                  BYTES);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
-  PipeItems items = make_items<LB>(a, a.m.nspec);
-  if (items.count() == 0) return;
-  int gx = blocks_per_sm * sms;
-  if (gx > items.count()) gx = items.count();
-  if (gx < 1) gx = 1;
-  k_forces_fwd_r<LB><<<gx, NT, BYTES, st>>>(a, items);
+  auto launch = [&](const StepArgs& ac, int nel) {
+    PipeItems items = make_items<LB>(ac, nel);
+    if (items.count() == 0) return 0;
+    int gx = blocks_per_sm * sms;
+    if (gx > items.count()) gx = items.count();
+    if (gx < 1) gx = 1;
+    k_forces_fwd_r<LB, COLOURED><<<gx, NT, BYTES, st>>>(ac, items);
+    return 1;
+  };
+  if (!COLOURED) return launch(a, a.m.nspec);
+  // one launch per colour: within a colour no two elements share a point,
+  // so the scatter is a plain read-modify-write
+  int n = 0;
+  for (int c = 0; c < a.m.ncolour; ++c) {
+    StepArgs ac = a;
+    ac.m.order = a.m.corder + a.m.cstart[c];
+    n += launch(ac, a.m.cstart[c + 1] - a.m.cstart[c]);
+  }
+  return n;
 }
 
 template <int LB>
@@ -2216,11 +2408,16 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
 //   displacement prefetched into registers, 10 forward phase with 2 events
 //   per thread and register prefetch (8 events per block).
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.variant == 12 && !a.gmap) return adj ? forces_shfl_cfg<true>(a, st) : forces_shfl_cfg<false>(a, st);
   if (a.variant == 10 && a.nev > 1) {
-    if (!adj)
-      forces_fwd_r_cfg<8>(a, st);
-    else
-      forces_adjpair_r_cfg<8>(a, st);
+    if (!adj) return forces_fwd_r_cfg<8, false>(a, st);
+    forces_adjpair_r_cfg<8>(a, st);
+    return 1;
+  }
+  if (a.variant == 11 && a.nev > 1) {
+    if (!adj) return a.m.ncolour > 0 ? forces_fwd_r_cfg<8, true>(a, st)
+                                     : forces_fwd_r_cfg<8, false>(a, st);
+    forces_adjpair_r_cfg<8>(a, st);
     return 1;
   }
   if ((a.variant >= 6 && a.variant <= 9) && a.nev > 1) {

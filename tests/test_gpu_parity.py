@@ -29,7 +29,7 @@ def small():
     return db, rec, mt
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 13])
 def test_forward_plain_matches_oracle(gpu, small, variant):
     db, rec, mt = small
     nstep, dt = 400, 0.02
@@ -83,7 +83,7 @@ def mini_adjoint():
     return db, rec, mt, src_xyz, nstep, dt, obs
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 13])
 def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
@@ -115,7 +115,8 @@ def test_adjoint_kernels_match_oracle(gpu, mini_adjoint, variant):
 
 @pytest.mark.parametrize("variant,nev", [(1, 5), (2, 3), (2, 11), (3, 3), (3, 11),
                                          (4, 3), (4, 6), (5, 3), (5, 11), (6, 13),
-                                         (11, 5), (11, 19), (11, 7), (0, 7)])
+                                         (11, 5), (11, 19), (11, 7), (12, 5), (12, 19), (13, 3),
+                                         (0, 7)])
 def test_batched_equals_plain(gpu, small, variant, nev):
     db, rec, _ = small
     nstep, dt = 300, 0.02
@@ -205,7 +206,7 @@ def test_state_errors(gpu, small):
     assert ei.value.code == -1
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13])
 def test_batched_adjoint_distinct_events_equal_alone(gpu, variant):
     """Each lane has its own source and observed data: the batched adjoint
     must give every event the kernels it gets alone."""
