@@ -32,6 +32,7 @@ class OracleMesh(C.Structure):
         ("nf", C.c_int),
         ("f_ispec", C.POINTER(C.c_int)), ("f_ijk", C.POINTER(C.c_int)),
         ("f_jw", C.POINTER(C.c_float)), ("f_n", C.POINTER(C.c_float)),
+        ("irreg", C.POINTER(C.c_int)), ("geo", C.POINTER(C.c_float)),
     ]
 
 
@@ -105,6 +106,10 @@ class Oracle:
             f_jw=np.ascontiguousarray(db.abs_jw.reshape(-1), np.float32),
             f_n=np.ascontiguousarray(db.abs_normal.reshape(-1), np.float32),
         )
+        irr = getattr(db, "irregular", None)
+        if irr is not None and (irr >= 0).any():
+            self._keep["irreg"] = np.ascontiguousarray(irr, np.int32)
+            self._keep["geo"] = np.ascontiguousarray(db.geo.reshape(-1), np.float32)
         k = self._keep
         f, i = C.c_float, C.c_int
         self._mesh = OracleMesh(
@@ -114,7 +119,9 @@ class Oracle:
             _ptr(k["rho"], f), _ptr(k["rmass"], f), _ptr(k["rho_vp"], f),
             _ptr(k["rho_vs"], f), db.nfaces if stacey else 0,
             _ptr(k["f_ispec"], i), _ptr(k["f_ijk"], i), _ptr(k["f_jw"], f),
-            _ptr(k["f_n"], f))
+            _ptr(k["f_n"], f),
+            _ptr(k["irreg"], i) if "irreg" in k else None,
+            _ptr(k["geo"], f) if "geo" in k else None)
         self._h = lib().oracle_create(C.byref(self._mesh), precision, nthreads)
         if not self._h:
             raise RuntimeError("oracle_create failed")

@@ -32,6 +32,7 @@
 //   adjoint step j (adjoint source sample N-1-j) is paired with the
 //   backward state N-1-j for kernel accumulation.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -152,6 +153,11 @@ struct oracle_mesh {
   const int* f_ijk;     // [nf][25][3]
   const float* f_jw;    // [nf][25]
   const float* f_n;     // [nf][25][3]
+  // irregular elements (may be null): irreg[e] = -1 for a regular element,
+  // else its row in geo [nirreg][125][10] = xix, xiy, xiz, etax, etay,
+  // etaz, gammax, gammay, gammaz, jacobian at each GLL point
+  const int* irreg;
+  const float* geo;
 };
 
 struct oracle_source {
@@ -169,9 +175,116 @@ struct Located {
   double xi, eta, gam;
 };
 
+// Coordinates of the element's GLL interpolant at (xi, eta, gamma) and
+// their derivatives dX[a][d] = dx_a / dxi_d.
+void element_map(const oracle_mesh& m, const Gll& g, int e, const double xi[3], double X[3],
+                 double dX[3][3]) {
+  double l[3][NG], dl[3][NG];
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < NG; ++a) {
+      l[d][a] = lagrange(g, a, xi[d]);
+      dl[d][a] = lagrange_d(g, a, xi[d]);
+    }
+  for (int a = 0; a < 3; ++a) {
+    X[a] = 0.0;
+    for (int d = 0; d < 3; ++d) dX[a][d] = 0.0;
+  }
+  const float* cs[3] = {m.x, m.y, m.z};
+  for (int k = 0; k < NG; ++k)
+    for (int j = 0; j < NG; ++j)
+      for (int i = 0; i < NG; ++i) {
+        const int ig = m.ibool[(size_t)e * NG3 + i + NG * j + NG2 * k];
+        const double w0 = l[0][i] * l[1][j] * l[2][k];
+        const double wd[3] = {dl[0][i] * l[1][j] * l[2][k], l[0][i] * dl[1][j] * l[2][k],
+                              l[0][i] * l[1][j] * dl[2][k]};
+        for (int a = 0; a < 3; ++a) {
+          const double c = (double)cs[a][ig];
+          X[a] += w0 * c;
+          for (int d = 0; d < 3; ++d) dX[a][d] += wd[d] * c;
+        }
+      }
+}
+
+bool invert3(const double A[3][3], double B[3][3]) {
+  const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  if (!(std::fabs(det) > 0.0)) return false;
+  B[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+  B[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+  B[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+  B[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+  B[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+  B[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) / det;
+  B[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+  B[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+  B[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) / det;
+  return true;
+}
+
+// Newton iteration for the reference coordinates of point p in element e;
+// returns the distance of the mapped (clamped) point from p.
+double newton_xi(const oracle_mesh& m, const Gll& g, int e, const double p[3], double xi[3]) {
+  xi[0] = xi[1] = xi[2] = 0.0;
+  double X[3], dX[3][3], inv[3][3];
+  for (int it = 0; it < 30; ++it) {
+    element_map(m, g, e, xi, X, dX);
+    if (!invert3(dX, inv)) break;
+    double step = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      double dd = 0.0;
+      for (int a = 0; a < 3; ++a) dd += inv[d][a] * (p[a] - X[a]);
+      xi[d] += dd;
+      if (xi[d] > 1.5) xi[d] = 1.5;
+      if (xi[d] < -1.5) xi[d] = -1.5;
+      step = std::max(step, std::fabs(dd));
+    }
+    if (step < 1e-13) break;
+  }
+  for (int d = 0; d < 3; ++d) xi[d] = xi[d] < -1.0 ? -1.0 : (xi[d] > 1.0 ? 1.0 : xi[d]);
+  element_map(m, g, e, xi, X, dX);
+  return std::sqrt((X[0] - p[0]) * (X[0] - p[0]) + (X[1] - p[1]) * (X[1] - p[1]) +
+                   (X[2] - p[2]) * (X[2] - p[2]));
+}
+
+Located locate_regular(const oracle_mesh& m, double px, double py, double pz);
+
+// On a mesh with irregular elements: of the 8 elements with the nearest
+// centres, the one whose Newton-located point lies closest (inside: 0).
+Located locate(const oracle_mesh& m, double px, double py, double pz) {
+  if (!m.irreg) return locate_regular(m, px, py, pz);
+  static const Gll g = make_gll();
+  std::vector<std::pair<double, int>> cand;
+  cand.reserve(m.nspec);
+  for (int e = 0; e < m.nspec; ++e) {
+    double c[3] = {0, 0, 0};
+    const int corner[8] = {0, 4, 20, 24, 100, 104, 120, 124};
+    const float* cs[3] = {m.x, m.y, m.z};
+    for (int q = 0; q < 8; ++q) {
+      const int ig = m.ibool[(size_t)e * NG3 + corner[q]];
+      for (int a = 0; a < 3; ++a) c[a] += 0.125 * (double)cs[a][ig];
+    }
+    const double d = (px - c[0]) * (px - c[0]) + (py - c[1]) * (py - c[1]) + (pz - c[2]) * (pz - c[2]);
+    cand.push_back({d, e});
+  }
+  std::partial_sort(cand.begin(), cand.begin() + std::min<size_t>(8, cand.size()), cand.end());
+  Located best{-1, 0, 0, 0};
+  double bd = 1e300;
+  const double p[3] = {px, py, pz};
+  for (size_t q = 0; q < std::min<size_t>(8, cand.size()); ++q) {
+    double xi[3];
+    const double d = newton_xi(m, g, cand[q].second, p, xi);
+    if (d < bd - 1e-9 * (1.0 + bd)) {
+      bd = d;
+      best = {cand[q].second, xi[0], xi[1], xi[2]};
+    }
+  }
+  return best;
+}
+
 // Element whose centre is nearest (ties: lowest index), reference
 // coordinates from the element's axis-aligned extent.
-Located locate(const oracle_mesh& m, double px, double py, double pz) {
+Located locate_regular(const oracle_mesh& m, double px, double py, double pz) {
   Located best{-1, 0, 0, 0};
   double bd = 1e300;
   for (int e = 0; e < m.nspec; ++e) {
@@ -312,6 +425,8 @@ struct Solver {
   }
 
   void element(int e, const std::vector<T>& uu, std::vector<T>& acc, std::vector<T>* eps) {
+    const float* gen =
+        (m.irreg && m.irreg[e] >= 0) ? m.geo + (size_t)m.irreg[e] * NG3 * 10 : nullptr;
     T ul[3][NG3];
     const int* ib = &m.ibool[(size_t)e * NG3];
     for (int p = 0; p < NG3; ++p)
@@ -334,9 +449,23 @@ struct Solver {
             det[c] = s2;
             dga[c] = s3;
           }
-          T duxdx = xix * dxi[0], duxdy = xix * det[0], duxdz = xix * dga[0];
-          T duydx = xix * dxi[1], duydy = xix * det[1], duydz = xix * dga[1];
-          T duzdx = xix * dxi[2], duzdy = xix * det[2], duzdz = xix * dga[2];
+          T duxdx, duxdy, duxdz, duydx, duydy, duydz, duzdx, duzdy, duzdz;
+          const float* G = gen ? gen + (size_t)p * 10 : nullptr;
+          if (!G) {
+            duxdx = xix * dxi[0], duxdy = xix * det[0], duxdz = xix * dga[0];
+            duydx = xix * dxi[1], duydy = xix * det[1], duydz = xix * dga[1];
+            duzdx = xix * dxi[2], duzdy = xix * det[2], duzdz = xix * dga[2];
+          } else {
+            // du_c/dx = xix dxi + etax deta + gammax dgamma, and likewise
+            // for y (xiy, etay, gammay) and z (xiz, etaz, gammaz)
+            T du[3][3];
+            for (int c = 0; c < 3; ++c)
+              for (int d = 0; d < 3; ++d)
+                du[c][d] = (T)G[d] * dxi[c] + (T)G[3 + d] * det[c] + (T)G[6 + d] * dga[c];
+            duxdx = du[0][0], duxdy = du[0][1], duxdz = du[0][2];
+            duydx = du[1][0], duydy = du[1][1], duydz = du[1][2];
+            duzdx = du[2][0], duzdy = du[2][1], duzdz = du[2][2];
+          }
           size_t ep = (size_t)e * NG3 + p;
           T kap = kappa[ep], mul = mu[ep];
           T l2m = kap + four3 * mul;
@@ -347,10 +476,22 @@ struct Solver {
           T sxy = mul * (duxdy + duydx);
           T sxz = mul * (duxdz + duzdx);
           T syz = mul * (duydz + duzdy);
-          T fac = jac * xix;
-          t1[0][p] = fac * sxx; t2[0][p] = fac * sxy; t3[0][p] = fac * sxz;
-          t1[1][p] = fac * sxy; t2[1][p] = fac * syy; t3[1][p] = fac * syz;
-          t1[2][p] = fac * sxz; t2[2][p] = fac * syz; t3[2][p] = fac * szz;
+          if (!G) {
+            T fac = jac * xix;
+            t1[0][p] = fac * sxx; t2[0][p] = fac * sxy; t3[0][p] = fac * sxz;
+            t1[1][p] = fac * sxy; t2[1][p] = fac * syy; t3[1][p] = fac * syz;
+            t1[2][p] = fac * sxz; t2[2][p] = fac * syz; t3[2][p] = fac * szz;
+          } else {
+            // flux of component c through the xi, eta, gamma directions:
+            // jacobian * sigma_c . (xix, xiy, xiz) etc.
+            const T jl = (T)G[9];
+            const T sc[3][3] = {{sxx, sxy, sxz}, {sxy, syy, syz}, {sxz, syz, szz}};
+            for (int c = 0; c < 3; ++c) {
+              t1[c][p] = jl * (sc[c][0] * (T)G[0] + sc[c][1] * (T)G[1] + sc[c][2] * (T)G[2]);
+              t2[c][p] = jl * (sc[c][0] * (T)G[3] + sc[c][1] * (T)G[4] + sc[c][2] * (T)G[5]);
+              t3[c][p] = jl * (sc[c][0] * (T)G[6] + sc[c][1] * (T)G[7] + sc[c][2] * (T)G[8]);
+            }
+          }
           if (eps) {
             T tr = duxdx + duydy + duzdz;
             T tr3 = tr / (T)3;
@@ -425,14 +566,26 @@ struct Solver {
     double Myz = -s.mt[3], Mxz = s.mt[4], Mxy = -s.mt[5];
     double M[3][3] = {{Mxx, Mxy, Mxz}, {Mxy, Myy, Myz}, {Mxz, Myz, Mzz}};
     srcarr.assign(NG3 * 3, (T)0);
+    // d(xi_d)/dx_a at the source: the regular element's xix on the
+    // diagonal, or the inverse of the interpolated mapping's Jacobian
+    double dxi[3][3] = {{m.xix, 0, 0}, {0, m.xix, 0}, {0, 0, m.xix}};
+    if (m.irreg && m.irreg[L.ispec] >= 0) {
+      const double xi3[3] = {L.xi, L.eta, L.gam};
+      double X[3], dX[3][3];
+      element_map(m, g, L.ispec, xi3, X, dX);
+      invert3(dX, dxi);
+    }
     for (int c3 = 0; c3 < NG; ++c3)
       for (int b = 0; b < NG; ++b)
         for (int a3 = 0; a3 < NG; ++a3) {
           double la = lagrange(g, a3, L.xi), lb = lagrange(g, b, L.eta),
                  lc = lagrange(g, c3, L.gam);
-          double grad[3] = {m.xix * lagrange_d(g, a3, L.xi) * lb * lc,
-                            m.xix * la * lagrange_d(g, b, L.eta) * lc,
-                            m.xix * la * lb * lagrange_d(g, c3, L.gam)};
+          const double dr[3] = {lagrange_d(g, a3, L.xi) * lb * lc,
+                                la * lagrange_d(g, b, L.eta) * lc,
+                                la * lb * lagrange_d(g, c3, L.gam)};
+          double grad[3];
+          for (int a = 0; a < 3; ++a)
+            grad[a] = dxi[0][a] * dr[0] + dxi[1][a] * dr[1] + dxi[2][a] * dr[2];
           int p = a3 + NG * b + NG2 * c3;
           for (int r = 0; r < 3; ++r)
             srcarr[p * 3 + r] =

@@ -117,6 +117,16 @@ class Database:
     abs_normal: np.ndarray     # float32 [nf,25,3]
     vp: Optional[np.ndarray] = None   # float32 [nspec,5,5,5] (diagnostics)
     vs: Optional[np.ndarray] = None
+    # irregular elements (deformed meshes): irregular[e] = -1 for a regular
+    # element, else its row in geo; geo [nirreg,5,5,5,10] holds xix, xiy,
+    # xiz, etax, etay, etaz, gammax, gammay, gammaz, jacobian per point
+    # (Fortran xixstore(i,j,k,ispec_irreg) ... jacobianstore)
+    irregular: Optional[np.ndarray] = None
+    geo: Optional[np.ndarray] = None
+
+    @property
+    def nspec_irregular(self):
+        return 0 if self.geo is None else int(self.geo.shape[0])
 
     @property
     def nfaces(self):
@@ -141,7 +151,11 @@ def _materials(db: Database, vp, vs, rho):
     _, w = gll_points_weights()
     www = (w[None, :, None, None] * w[None, None, :, None]
            * w[None, None, None, :])  # [1,k,j,i]
-    mass_el = rho * www * db.jacobian_regular
+    jac = np.full(rho.shape, db.jacobian_regular, np.float64)
+    if db.irregular is not None:
+        sel = db.irregular >= 0
+        jac[sel] = db.geo[db.irregular[sel], ..., 9]
+    mass_el = rho * www * jac
     rmass = np.zeros(db.nglob, np.float64)
     np.add.at(rmass, db.ibool.reshape(-1), mass_el.reshape(-1))
     f = np.float32
@@ -149,14 +163,71 @@ def _materials(db: Database, vp, vs, rho):
             (rho * vp).astype(f), (rho * vs).astype(f), rmass.astype(f))
 
 
-def make_box(box: BoxSpec, absorb_top: bool = False) -> Database:
+def hill_topography(box: BoxSpec, height: float, width: float):
+    """A Gaussian hill of ``height`` metres and 1/e half-width ``width``
+    centred on the box, as a function z_surface(x, y)."""
+    cx, cy = box.x0 + 0.5 * box.lx, box.y0 + 0.5 * box.ly
+
+    def f(x, y):
+        return height * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / width ** 2)
+    return f
+
+
+def gll_derivative_matrix():
+    """D[i][l] = l_l'(xi_i) for the GLL nodes (FP64)."""
+    x, _ = gll_points_weights()
+    n = len(x)
+    D = np.zeros((n, n))
+    for i in range(n):
+        for l in range(n):
+            s = 0.0
+            for m in range(n):
+                if m == l:
+                    continue
+                prod = 1.0 / (x[l] - x[m])
+                for q in range(n):
+                    if q not in (l, m):
+                        prod *= (x[i] - x[q]) / (x[l] - x[q])
+                s += prod
+            D[i, l] = s
+    return D
+
+
+def _geometry(ibool, xs, ys, zs):
+    """Mapping derivatives of every element from its GLL coordinates:
+    returns dX [nspec,5,5,5,3(a),3(d)] = dx_a/dxi_d (k, j, i order)."""
+    D = gll_derivative_matrix()
+    X = np.stack([xs[ibool], ys[ibool], zs[ibool]], axis=-1)   # [e,k,j,i,a]
+    dxi = np.einsum("il,ekjla->ekjia", D, X)
+    deta = np.einsum("jl,eklia->ekjia", D, X)
+    dgam = np.einsum("kl,eljia->ekjia", D, X)
+    return np.stack([dxi, deta, dgam], axis=-1)
+
+
+def interior_warp(box: BoxSpec, amp: float):
+    """Smooth displacement of the mesh interior that vanishes on the box
+    faces: (dx, dy, dz) = amp * s(x) s(y) s(z) * (1, -1, 1) with
+    s(q) = sin(pi (q - q0) / L)."""
+    def f(x, y, z):
+        s = (np.sin(np.pi * (x - box.x0) / box.lx) * np.sin(np.pi * (y - box.y0) / box.ly)
+             * np.sin(np.pi * (z + box.lz) / box.lz))
+        return amp * s, -amp * s, amp * s
+    return f
+
+
+def make_box(box: BoxSpec, absorb_top: bool = False, topo=None, warp=None) -> Database:
     """Structured mesh, global numbering and Stacey faces of a box.
 
     Global points form a ``(4 nex + 1) x (4 ney + 1) x (4 nez + 1)`` grid
     numbered x-fastest; elements are numbered x-fastest too, bottom layer
     first.  ``absorb_top`` also makes the top face absorbing (a full-space
-    test box).  The model arrays are left at zero: call :func:`homogeneous`
-    or :func:`with_model` next.
+    test box).  ``topo(x, y)`` stretches the columns so the free surface
+    follows it (bottom fixed); ``warp(x, y, z)`` displaces every point.
+    Either makes elements irregular: their mapping derivatives and Jacobian
+    are computed from the GLL coordinates and stored per point in ``geo``,
+    and the Stacey faces get per-point normals and jacobian2Dw.  The model
+    arrays are left at zero: call :func:`homogeneous` or :func:`with_model`
+    next.
     """
     nex, ney, nez, h = box.nex, box.ney, box.nez, box.h
     nxg, nyg, nzg = 4 * nex + 1, 4 * ney + 1, 4 * nez + 1
@@ -189,9 +260,31 @@ def make_box(box: BoxSpec, absorb_top: bool = False) -> Database:
     gx = np.arange(nglob) % nxg
     gy = (np.arange(nglob) // nxg) % nyg
     gz = np.arange(nglob) // (nxg * nyg)
-    xstore = xl[gx].astype(np.float32)
-    ystore = yl[gy].astype(np.float32)
-    zstore = zl[gz].astype(np.float32)
+    xg64, yg64, zg64 = xl[gx], yl[gy], zl[gz]
+    if topo is not None:
+        # columns stretched so the top follows topo(x, y), bottom fixed
+        zg64 = zg64 + topo(xg64, yg64) * (zg64 + box.lz) / box.lz
+    if warp is not None:
+        dxw, dyw, dzw = warp(xg64, yg64, zg64)
+        xg64, yg64, zg64 = xg64 + dxw, yg64 + dyw, zg64 + dzw
+    xstore = xg64.astype(np.float32)
+    ystore = yg64.astype(np.float32)
+    zstore = zg64.astype(np.float32)
+    irregular = geo = None
+    dX = None
+    if topo is not None or warp is not None:
+        dX = _geometry(ibool, xg64, yg64, zg64)                  # [e,k,j,i,3,3]
+        jac = np.linalg.det(dX)
+        inv = np.linalg.inv(dX)                                   # [.., d, a] = dxi_d/dx_a
+        reg = np.zeros_like(dX)
+        for a in range(3):
+            reg[..., a, a] = 0.5 * h
+        dev = np.abs(dX - reg).reshape(nspec, -1).max(axis=1)
+        irr = dev > 1e-9 * h
+        irregular = np.full(nspec, -1, np.int32)
+        irregular[irr] = np.arange(int(irr.sum()), dtype=np.int32)
+        g = np.concatenate([inv.reshape(inv.shape[:4] + (9,)), jac[..., None]], axis=-1)
+        geo = g[irr].astype(np.float32)
 
     # Stacey faces: xmin, xmax, ymin, ymax, zmin (top is a free surface)
     a = np.arange(NGLL)
@@ -201,12 +294,28 @@ def make_box(box: BoxSpec, absorb_top: bool = False) -> Database:
     jw2 = (w[A] * w[B] * (0.5 * h) ** 2).astype(np.float32)
     faces_ispec, faces_ijk, faces_n = [], [], []
 
+    faces_jw = []
+
     def add(sel, ijk, normal):
         els = np.nonzero(sel)[0]
         for e in els:
             faces_ispec.append(e)
             faces_ijk.append(ijk)
-            faces_n.append(normal)
+            if dX is None:
+                faces_n.append(np.broadcast_to(np.asarray(normal, np.float64), (25, 3)))
+                faces_jw.append(jw2.astype(np.float64))
+                continue
+            # deformed face: n = t1 x t2 of the two in-face mapping
+            # derivatives, oriented outward; jacobian2D = |n|
+            ii_, jj_, kk_ = ijk[:, 0], ijk[:, 1], ijk[:, 2]
+            J = dX[e, kk_, jj_, ii_]                      # [25, a, d]
+            fixed = [d for d in range(3) if np.all(ijk[:, d] == ijk[0, d])][0]
+            d1, d2 = [d for d in range(3) if d != fixed]
+            nv = np.cross(J[:, :, d1], J[:, :, d2])
+            nv *= np.sign((nv * np.asarray(normal)).sum(axis=1))[:, None]
+            nn = np.linalg.norm(nv, axis=1)
+            faces_n.append(nv / nn[:, None])
+            faces_jw.append(nn * w[ijk[:, d1]] * w[ijk[:, d2]])
 
     z4 = np.full(25, 4)
     z0 = np.zeros(25, np.int64)
@@ -220,9 +329,8 @@ def make_box(box: BoxSpec, absorb_top: bool = False) -> Database:
     nf = len(faces_ispec)
     abs_ispec = np.asarray(faces_ispec, np.int32)
     abs_ijk = np.asarray(faces_ijk, np.int32).reshape(nf, 25, 3)
-    abs_normal = np.broadcast_to(
-        np.asarray(faces_n, np.float32)[:, None, :], (nf, 25, 3)).copy()
-    abs_jw = np.broadcast_to(jw2[None, :], (nf, 25)).copy()
+    abs_normal = np.asarray(faces_n, np.float32).reshape(nf, 25, 3)
+    abs_jw = np.asarray(faces_jw, np.float32).reshape(nf, 25)
 
     z = np.zeros((nspec, NGLL, NGLL, NGLL), np.float32)
     return Database(
@@ -232,7 +340,7 @@ def make_box(box: BoxSpec, absorb_top: bool = False) -> Database:
         xix_regular=float(2.0 / h), jacobian_regular=float((0.5 * h) ** 3),
         kappa=z, mu=z, rho=z, rmass=np.zeros(nglob, np.float32),
         rho_vp=z, rho_vs=z, abs_ispec=abs_ispec, abs_ijk=abs_ijk,
-        abs_jw=abs_jw, abs_normal=abs_normal)
+        abs_jw=abs_jw, abs_normal=abs_normal, irregular=irregular, geo=geo)
 
 
 def gll_xyz(db: Database):
@@ -347,6 +455,17 @@ def gaussian_vs_anomaly(db: Database, vs, amp=0.10, radius=15000.0,
     cy = db.box.y0 + 0.5 * db.box.ly
     r2 = (x - cx) ** 2 + (y - cy) ** 2 + (z + depth) ** 2
     return vs * (1.0 + amp * np.exp(-r2 / (radius * radius)))
+
+
+def as_irregular(db: Database) -> Database:
+    """The same regular mesh with every element flagged irregular and its
+    constant mapping stored per point: runs the general-element path on a
+    mesh whose answer the regular path gives."""
+    geo = np.zeros((db.nspec, NGLL, NGLL, NGLL, 10), np.float32)
+    for d in range(3):
+        geo[..., 4 * d] = db.xix_regular
+    geo[..., 9] = db.jacobian_regular
+    return dataclasses.replace(db, irregular=np.arange(db.nspec, dtype=np.int32), geo=geo)
 
 
 def surface_receivers(box: BoxSpec, n: int, frac=(0.2, 0.8)):
