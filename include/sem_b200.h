@@ -53,7 +53,7 @@
 extern "C" {
 #endif
 
-#define SEM_ABI_VERSION 1
+#define SEM_ABI_VERSION 2
 
 typedef enum {
   SEM_OK = 0,
@@ -67,9 +67,12 @@ typedef enum {
 } sem_status;
 
 /* Mesh database of one slice (read_mesh_databases.f90:158-193,455-486,
- * 766-804).  All elements must be regular (cubes: one xix_regular and one
- * jacobian_regular); irregular_element_number, when given, must be all <= 0
- * (SEM_ERR_UNSUPPORTED otherwise). */
+ * 766-804).  Regular elements (cubes) share xix_regular and
+ * jacobian_regular.  irregular_element_number[e] (read_mesh_databases.f90:
+ * 168) is 0 for a regular element and k >= 1 for an irregular one, whose
+ * mapping derivatives and Jacobian are row k-1 of xixstore .. jacobianstore
+ * (read_mesh_databases.f90:172-181), each [nspec_irregular][5][5][5].  A
+ * mesh with irregular elements runs the thread-per-point element kernel. */
 typedef struct {
   int nspec;
   int nglob;
@@ -87,6 +90,11 @@ typedef struct {
   const int *abs_boundary_ijk;      /* [nf][25][3]                         */
   const float *abs_boundary_jacobian2Dw;   /* [nf][25]                     */
   const float *abs_boundary_normal; /* [nf][25][3]                         */
+  int nspec_irregular;              /* rows of the irregular arrays (>= 0) */
+  const float *xixstore, *xiystore, *xizstore;         /* [nirr][125]      */
+  const float *etaxstore, *etaystore, *etazstore;      /* [nirr][125]      */
+  const float *gammaxstore, *gammaystore, *gammazstore;/* [nirr][125]      */
+  const float *jacobianstore;                          /* [nirr][125]      */
 } sem_mesh_desc;
 
 /* Run options (prepare_timerun_fwat.f90:29-168 + Par_file switches). */

@@ -249,8 +249,9 @@ double newton_xi(const oracle_mesh& m, const Gll& g, int e, const double p[3], d
 
 Located locate_regular(const oracle_mesh& m, double px, double py, double pz);
 
-// On a mesh with irregular elements: of the 8 elements with the nearest
-// centres, the one whose Newton-located point lies closest (inside: 0).
+// On a mesh with irregular elements: of the 12 elements with the nearest
+// centres, the lowest-numbered one containing the point (Newton iteration),
+// else the one whose located point lies closest.
 Located locate(const oracle_mesh& m, double px, double py, double pz) {
   if (!m.irreg) return locate_regular(m, px, py, pz);
   static const Gll g = make_gll();
@@ -267,16 +268,27 @@ Located locate(const oracle_mesh& m, double px, double py, double pz) {
     const double d = (px - c[0]) * (px - c[0]) + (py - c[1]) * (py - c[1]) + (pz - c[2]) * (pz - c[2]);
     cand.push_back({d, e});
   }
-  std::partial_sort(cand.begin(), cand.begin() + std::min<size_t>(8, cand.size()), cand.end());
+  const size_t nc = std::min<size_t>(12, cand.size());
+  std::partial_sort(cand.begin(), cand.begin() + nc, cand.end());
+  // a point on a face, edge or corner lies in several elements, whose
+  // source arrays differ: take the lowest-numbered element containing it
+  // (distance below 1e-6 of the element size), else the closest
   Located best{-1, 0, 0, 0};
   double bd = 1e300;
+  bool inside = false;
   const double p[3] = {px, py, pz};
-  for (size_t q = 0; q < std::min<size_t>(8, cand.size()); ++q) {
+  for (size_t q = 0; q < nc; ++q) {
+    const int e = cand[q].second;
     double xi[3];
-    const double d = newton_xi(m, g, cand[q].second, p, xi);
-    if (d < bd - 1e-9 * (1.0 + bd)) {
+    const double d = newton_xi(m, g, e, p, xi);
+    const int g0 = m.ibool[(size_t)e * NG3], g7 = m.ibool[(size_t)e * NG3 + 124];
+    const double size = std::fabs((double)m.x[g7] - (double)m.x[g0]);
+    const bool in = d <= 1e-6 * size;
+    const bool better = in ? (!inside || e < best.ispec) : (!inside && d < bd);
+    if (better) {
+      inside = inside || in;
       bd = d;
-      best = {cand[q].second, xi[0], xi[1], xi[2]};
+      best = {e, xi[0], xi[1], xi[2]};
     }
   }
   return best;

@@ -64,6 +64,12 @@ class MeshDesc(C.Structure):
         ("abs_boundary_ijk", C.POINTER(C.c_int)),
         ("abs_boundary_jacobian2Dw", C.POINTER(C.c_float)),
         ("abs_boundary_normal", C.POINTER(C.c_float)),
+        ("nspec_irregular", C.c_int),
+        ("xixstore", C.POINTER(C.c_float)), ("xiystore", C.POINTER(C.c_float)),
+        ("xizstore", C.POINTER(C.c_float)), ("etaxstore", C.POINTER(C.c_float)),
+        ("etaystore", C.POINTER(C.c_float)), ("etazstore", C.POINTER(C.c_float)),
+        ("gammaxstore", C.POINTER(C.c_float)), ("gammaystore", C.POINTER(C.c_float)),
+        ("gammazstore", C.POINTER(C.c_float)), ("jacobianstore", C.POINTER(C.c_float)),
     ]
 
 

@@ -124,6 +124,23 @@ void lagrange_all(double x, double h[5], double hd[5]) {
   }
 }
 
+bool invert3(const double A[3][3], double B[3][3]) {
+  const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  if (!(std::fabs(det) > 0.0)) return false;
+  B[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+  B[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+  B[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+  B[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+  B[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+  B[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) / det;
+  B[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+  B[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+  B[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) / det;
+  return true;
+}
+
 double ricker(double t, double f0) {
   const double a = M_PI * M_PI * f0 * f0;
   return (1.0 - 2.0 * a * t * t) * std::exp(-a * t * t);
@@ -203,7 +220,10 @@ struct sem_mesh_s {
   std::vector<float> h_rmass;
   std::vector<int> h_f_iglob;
   std::vector<float> h_f_rvp, h_f_rvs, h_f_jw, h_f_n;
-  std::vector<float> h_x, h_y, h_z;  // point coordinates (kernel smoother)
+  std::vector<float> h_x, h_y, h_z;  // point coordinates
+  std::vector<int> h_irreg;          // [nspec] -1 or row of geo; empty: all regular
+  DevArray<int> irreg;
+  DevArray<float> geo;               // [nirreg][125][10] xix..gammaz, jacobian
   std::vector<double> centre;  // [nspec][3]
   std::vector<double> half;    // [nspec][3]
   int live_runs = 0;
@@ -218,6 +238,8 @@ struct sem_mesh_s {
     v.ibool = ibool.p;
     v.order = order.p;
     v.corder = corder.p;
+    v.irreg = irreg.p;
+    v.geo = geo.p;
     v.ncolour = ncolour;
     for (int c = 0; c <= MeshView::kMaxColours; ++c)
       v.cstart[c] = c <= ncolour && ncolour > 0 ? cstart[c] : 0;
@@ -231,13 +253,107 @@ struct sem_mesh_s {
     return v;
   }
   size_t device_bytes() const {
-    return ibool.bytes() + order.bytes() + corder.bytes() + kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
+    return ibool.bytes() + order.bytes() + corder.bytes() + irreg.bytes() + geo.bytes() +
+           kappa.bytes() + mu.bytes() + rho.bytes() + f_iglob.bytes() +
            f_rvp.bytes() + f_rvs.bytes() + f_jw.bytes() + f_n.bytes();
   }
 
-  // Element whose centre is nearest to the point (ties: lowest index), and
-  // the reference coordinates inside it, clamped to [-1, 1].
+  // GLL interpolant of element e's coordinates at xi and its derivatives
+  // dX[a][d] = dx_a / dxi_d.
+  void element_map(int e, const double xi[3], double X[3], double dX[3][3]) const {
+    double l[3][5], dl[3][5];
+    for (int d = 0; d < 3; ++d) lagrange_all(xi[d], l[d], dl[d]);
+    for (int a = 0; a < 3; ++a) {
+      X[a] = 0.0;
+      for (int d = 0; d < 3; ++d) dX[a][d] = 0.0;
+    }
+    const float* cs[3] = {h_x.data(), h_y.data(), h_z.data()};
+    for (int k = 0; k < 5; ++k)
+      for (int j = 0; j < 5; ++j)
+        for (int i = 0; i < 5; ++i) {
+          const int ig = h_ibool[(size_t)e * NGLL3 + i + 5 * j + 25 * k];
+          const double w0 = l[0][i] * l[1][j] * l[2][k];
+          const double wd[3] = {dl[0][i] * l[1][j] * l[2][k], l[0][i] * dl[1][j] * l[2][k],
+                                l[0][i] * l[1][j] * dl[2][k]};
+          for (int a = 0; a < 3; ++a) {
+            const double c = (double)cs[a][ig];
+            X[a] += w0 * c;
+            for (int d = 0; d < 3; ++d) dX[a][d] += wd[d] * c;
+          }
+        }
+  }
+
+  // d xi_d / d x_a at xi in element e: xix_regular on the diagonal for a
+  // regular element, else the inverse of the interpolated mapping Jacobian.
+  void dxi_dx(int e, const double xi[3], double B[3][3]) const {
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < 3; ++a) B[d][a] = d == a ? (double)xix : 0.0;
+    if (h_irreg.empty() || h_irreg[e] < 0) return;
+    double X[3], A[3][3];
+    element_map(e, xi, X, A);
+    invert3(A, B);
+  }
+
+  // Newton iteration for point p in element e, xi clamped to [-1, 1];
+  // returns the distance of the mapped point from p.
+  double newton(int e, const double p[3], double xi[3]) const {
+    xi[0] = xi[1] = xi[2] = 0.0;
+    double X[3], A[3][3], B[3][3];
+    for (int it = 0; it < 30; ++it) {
+      element_map(e, xi, X, A);
+      if (!invert3(A, B)) break;
+      double step = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        double dd = 0.0;
+        for (int a = 0; a < 3; ++a) dd += B[d][a] * (p[a] - X[a]);
+        xi[d] = std::min(1.5, std::max(-1.5, xi[d] + dd));
+        step = std::max(step, std::fabs(dd));
+      }
+      if (step < 1e-13) break;
+    }
+    for (int d = 0; d < 3; ++d) xi[d] = std::min(1.0, std::max(-1.0, xi[d]));
+    element_map(e, xi, X, A);
+    return std::sqrt((X[0] - p[0]) * (X[0] - p[0]) + (X[1] - p[1]) * (X[1] - p[1]) +
+                     (X[2] - p[2]) * (X[2] - p[2]));
+  }
+
+  // Element holding the point and the reference coordinates in it.  All
+  // regular: the element whose centre is nearest (ties: lowest index),
+  // coordinates from its axis-aligned extent, clamped to [-1, 1].  With
+  // irregular elements: of the 12 nearest centres, the lowest-numbered
+  // element containing the point (Newton iteration; a point on a shared
+  // face, edge or corner lies in several, whose source arrays differ), else
+  // the element whose located point lies closest.
   int locate(double px, double py, double pz, double xi3[3]) const {
+    if (!h_irreg.empty()) {
+      std::vector<std::pair<double, int>> cand((size_t)nspec);
+      for (int e = 0; e < nspec; ++e) {
+        const double* c = &centre[(size_t)e * 3];
+        cand[e] = {(px - c[0]) * (px - c[0]) + (py - c[1]) * (py - c[1]) +
+                       (pz - c[2]) * (pz - c[2]),
+                   e};
+      }
+      const size_t nc = std::min<size_t>(12, cand.size());
+      std::partial_sort(cand.begin(), cand.begin() + nc, cand.end());
+      const double p[3] = {px, py, pz};
+      int best = -1;
+      double bd = 1e300;
+      bool inside = false;
+      for (size_t q = 0; q < nc; ++q) {
+        const int e = cand[q].second;
+        double xi[3];
+        const double d = newton(e, p, xi);
+        const bool in = d <= 1e-6 * 2.0 * half[(size_t)e * 3];
+        const bool better = in ? (!inside || e < best) : (!inside && d < bd);
+        if (better) {
+          inside = inside || in;
+          bd = d;
+          best = e;
+          for (int k = 0; k < 3; ++k) xi3[k] = xi[k];
+        }
+      }
+      return best;
+    }
     int best = -1;
     double bd = 1e300;
     for (int e = 0; e < nspec; ++e) {
@@ -425,11 +541,21 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
     return fail(SEM_ERR_ARG, "missing absorbing-boundary array");
   if (!(d->xix_regular > 0.f) || !(d->jacobian_regular > 0.f))
     return fail(SEM_ERR_ARG, "xix_regular and jacobian_regular must be > 0");
+  bool any_irregular = false;
   if (d->irregular_element_number)
-    for (int e = 0; e < d->nspec; ++e)
-      if (d->irregular_element_number[e] > 0)
-        return fail(SEM_ERR_UNSUPPORTED,
-                    "element %d is irregular; this build implements regular elements only", e);
+    for (int e = 0; e < d->nspec; ++e) {
+      const int k = d->irregular_element_number[e];
+      if (k < 0 || k > d->nspec_irregular)
+        return fail(SEM_ERR_ARG, "irregular_element_number[%d] = %d outside [0, %d]", e, k,
+                    d->nspec_irregular);
+      any_irregular |= k > 0;
+    }
+  const float* const geo_in[10] = {d->xixstore,    d->xiystore,    d->xizstore,   d->etaxstore,
+                                   d->etaystore,   d->etazstore,   d->gammaxstore, d->gammaystore,
+                                   d->gammazstore, d->jacobianstore};
+  if (any_irregular)
+    for (int q = 0; q < 10; ++q)
+      if (!geo_in[q]) return fail(SEM_ERR_ARG, "irregular elements need all ten mapping arrays");
   int rc = check_device();
   if (rc) return rc;
 
@@ -455,6 +581,25 @@ int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
       return fail(SEM_ERR_ARG, "invalid material at element point %zu", i);
   }
   m->h_rmass.assign(d->rmass, d->rmass + d->nglob);
+  if (any_irregular) {
+    const size_t nirr = (size_t)d->nspec_irregular;
+    m->h_irreg.assign(d->nspec, -1);
+    for (int e = 0; e < d->nspec; ++e)
+      if (d->irregular_element_number[e] > 0) m->h_irreg[e] = d->irregular_element_number[e] - 1;
+    std::vector<float> hg(nirr * NGLL3 * 10);
+    for (size_t r = 0; r < nirr; ++r)
+      for (int p = 0; p < NGLL3; ++p)
+        for (int q = 0; q < 10; ++q) {
+          const float v = geo_in[q][r * NGLL3 + p];
+          if (!std::isfinite(v) || (q == 9 && !(v > 0.f)))
+            return fail(SEM_ERR_ARG, "irregular element row %zu point %d: invalid mapping", r, p);
+          hg[(r * NGLL3 + p) * 10 + q] = v;
+        }
+    CKM(m->irreg.alloc(d->nspec), "irregular element map");
+    CKM(m->geo.alloc(hg.size()), "irregular element mapping");
+    CK(cudaMemcpy(m->irreg.p, m->h_irreg.data(), d->nspec * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->geo.p, hg.data(), hg.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
   m->h_x.assign(d->xstore, d->xstore + d->nglob);
   m->h_y.assign(d->ystore, d->ystore + d->nglob);
   m->h_z.assign(d->zstore, d->zstore + d->nglob);
@@ -630,6 +775,7 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
   if (c->kernel_variant < 0 || c->kernel_variant > 13)
     return fail(SEM_ERR_ARG, "kernel_variant must be 0..13");
+
   return SEM_OK;
 }
 
@@ -656,6 +802,11 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   *out = nullptr;
   int rc = validate_cfg(c);
   if (rc) return rc;
+  if (!m->h_irreg.empty() && c->kernel_variant > 1)
+    return fail(SEM_ERR_UNSUPPORTED,
+                "kernel_variant %d needs regular elements; this mesh has irregular ones "
+                "(use 0 or 1)",
+                c->kernel_variant);
   auto r = new sem_run_s();
   std::unique_ptr<sem_run_s> guard(r);
   r->mesh = m;
@@ -759,12 +910,16 @@ int sem_set_sources(sem_run* r, int nev, const sem_source* src) {
     lagrange_all(xi3[0], hx, hxd);
     lagrange_all(xi3[1], hy, hyd);
     lagrange_all(xi3[2], hz, hzd);
-    const double xix = (double)r->mesh->xix;
+    double B[3][3];
+    r->mesh->dxi_dx(ispec, xi3, B);
     for (int c = 0; c < 5; ++c)
       for (int b = 0; b < 5; ++b)
         for (int a = 0; a < 5; ++a) {
-          const double gr[3] = {xix * hxd[a] * hy[b] * hz[c], xix * hx[a] * hyd[b] * hz[c],
-                                xix * hx[a] * hy[b] * hzd[c]};
+          // gradient of the interpolant phi_abc at the source
+          const double dr[3] = {hxd[a] * hy[b] * hz[c], hx[a] * hyd[b] * hz[c],
+                                hx[a] * hy[b] * hzd[c]};
+          double gr[3];
+          for (int k = 0; k < 3; ++k) gr[k] = B[0][k] * dr[0] + B[1][k] * dr[1] + B[2][k] * dr[2];
           const int p = a + 5 * b + 25 * c;
           for (int k = 0; k < 3; ++k)
             sa[(size_t)e * 375 + p * 3 + k] =
@@ -886,6 +1041,11 @@ static int autotune_phase(sem_run* r, bool adj) {
 
 static int ensure_tuned(sem_run* r) {
   if (r->cfg.kernel_variant != 0 || (r->variant[0] >= 0 && r->variant[1] >= 0)) return SEM_OK;
+  if (!r->mesh->h_irreg.empty()) {
+    // irregular elements run the thread-per-point kernel only
+    r->variant[0] = r->variant[1] = 0;
+    return SEM_OK;
+  }
   if (r->nstep < 3) {
     r->variant[0] = r->variant[1] = 2;
     return SEM_OK;
@@ -1390,13 +1550,16 @@ int sem_lane_start_forward(sem_run* r, int lane, const sem_source* src, int nrec
   lagrange_all(xi3[0], hx, hxd);
   lagrange_all(xi3[1], hy, hyd);
   lagrange_all(xi3[2], hz, hzd);
-  const double xix = (double)r->mesh->xix;
+  double B[3][3];
+  r->mesh->dxi_dx(r->src_ispec[lane], xi3, B);
   std::vector<float> sa(375), stf(nstep);
   for (int c = 0; c < 5; ++c)
     for (int b = 0; b < 5; ++b)
       for (int a = 0; a < 5; ++a) {
-        const double gr[3] = {xix * hxd[a] * hy[b] * hz[c], xix * hx[a] * hyd[b] * hz[c],
-                              xix * hx[a] * hy[b] * hzd[c]};
+        const double dr[3] = {hxd[a] * hy[b] * hz[c], hx[a] * hyd[b] * hz[c],
+                              hx[a] * hy[b] * hzd[c]};
+        double gr[3];
+        for (int k = 0; k < 3; ++k) gr[k] = B[0][k] * dr[0] + B[1][k] * dr[1] + B[2][k] * dr[2];
         const int p = a + 5 * b + 25 * c;
         for (int k = 0; k < 3; ++k)
           sa[p * 3 + k] = (float)(M[k][0] * gr[0] + M[k][1] * gr[1] + M[k][2] * gr[2]);

@@ -59,6 +59,11 @@ struct MeshView {
   int ncolour;           // 0: not coloured (more than kMaxColours needed)
   const int* corder;     // [nspec]
   int cstart[kMaxColours + 1];
+  // irregular elements: irreg[e] = -1 or the row of geo [nirr][125][10]
+  // (xix, xiy, xiz, etax, etay, etaz, gammax, gammay, gammaz, jacobian);
+  // both null when every element is regular
+  const int* irreg;
+  const float* geo;
 };
 
 struct Fields {

@@ -77,6 +77,51 @@ __device__ __forceinline__ void stress_point(const float g[3][3], float kap, flo
   sig[5] = fac * (mu * (g[1][2] + g[2][1]));
 }
 
+// General element (per-point mapping G = xix, xiy, xiz, etax, etay, etaz,
+// gammax, gammay, gammaz, jacobian): physical gradient from the reference
+// derivatives r[c][d] (d = xi, eta, gamma), and the fluxes of each
+// component through the three reference directions,
+// F[c*3+d] = jacobian * sum_a sigma_{c,a} d(xi_d)/d(x_a).
+__device__ __forceinline__ void map_gradient(const float r[3][3], const float* G, float g[3][3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[c][a] = r[c][0] * G[a] + r[c][1] * G[3 + a] + r[c][2] * G[6 + a];
+}
+__device__ __forceinline__ void map_flux(const float sig[6], const float* G, float F[9]) {
+  const float sc[3][3] = {{sig[0], sig[3], sig[4]}, {sig[3], sig[1], sig[5]},
+                          {sig[4], sig[5], sig[2]}};
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      F[c * 3 + d] = G[9] * (sc[c][0] * G[3 * d] + sc[c][1] * G[3 * d + 1] + sc[c][2] * G[3 * d + 2]);
+}
+
+// Divergence from the nine fluxes F[c*3+d] staged per point.
+template <int LB>
+__device__ __forceinline__ void div_point_gen(const float* __restrict__ b, int i, int j, int k,
+                                              int lane, const float* __restrict__ sDWt,
+                                              const float* __restrict__ sw, float f[3]) {
+  float a[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f}, cc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    const float wi = sDWt[i * 5 + l], wj = sDWt[j * 5 + l], wk = sDWt[k * 5 + l];
+    const int qi = (l + 5 * j + 25 * k) * LB + lane;
+    const int qj = (i + 5 * l + 25 * k) * LB + lane;
+    const int qk = (i + 5 * j + 25 * l) * LB + lane;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      a[c] = fmaf(wi, b[(c * 3 + 0) * NGLL3 * LB + qi], a[c]);
+      bb[c] = fmaf(wj, b[(c * 3 + 1) * NGLL3 * LB + qj], bb[c]);
+      cc[c] = fmaf(wk, b[(c * 3 + 2) * NGLL3 * LB + qk], cc[c]);
+    }
+  }
+  const float wjk = sw[j] * sw[k], wik = sw[i] * sw[k], wij = sw[i] * sw[j];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[c] = -(wjk * a[c] + wik * bb[c] + wij * cc[c]);
+}
+
 // Weak-form divergence at (i,j,k): f_c = -sum_d w w sum_l DW * sig_{c,d}.
 template <int LB>
 __device__ __forceinline__ void div_point(const float* __restrict__ b, int i, int j, int k,
@@ -114,16 +159,17 @@ __device__ __forceinline__ void div_point(const float* __restrict__ b, int i, in
 
 // One block = one element x LB lanes.  ADJ: lanes in the adjoint phase also
 // carry the backward field (f2) and accumulate the mu/kappa kernels.
-template <int LB, int NT, bool ADJ>
+template <int LB, int NT, bool ADJ, bool GEN = false>
 __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
   constexpr int G = NT / LB;
   constexpr int P = (NGLL3 + G - 1) / G;
+  constexpr int NQ = GEN ? 9 : 6;   // staged values per point: fluxes or stresses
   extern __shared__ float sm[];
   __shared__ int s_ib[NGLL3];
   __shared__ float s_kap[NGLL3], s_mu[NGLL3];
   __shared__ float s_D[25], s_DWt[25], s_w[5];
   float* b1 = sm;
-  float* b2 = sm + 6 * NGLL3 * LB;
+  float* b2 = sm + NQ * NGLL3 * LB;
 
   const int e = A.m.order[blockIdx.x];
   const int lane = threadIdx.x % LB;
@@ -175,20 +221,65 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
 
   const float xix = A.m.xix;
   const float fac = A.m.jac * A.m.xix;
-  float sg1[P][6];
-  float sg2[ADJ ? P : 1][6];
+  // general elements: this element's mapping, or the regular one
+  const float* geo = nullptr;
+  if (GEN) {
+    const int ir = A.m.irreg[e];
+    if (ir >= 0) geo = A.m.geo + (size_t)ir * NGLL3 * 10;
+  }
+  float sg1[P][NQ];
+  float sg2[ADJ ? P : 1][NQ];
 #pragma unroll
   for (int t = 0; t < P; ++t) {
     const int p = pg + t * G;
     if (p < NGLL3) {
       const int i = p % 5, j = (p / 5) % 5, k = p / 25;
+      float Gp[10];
+      if (GEN && geo) {
+#pragma unroll
+        for (int q = 0; q < 10; ++q) Gp[q] = geo[p * 10 + q];
+      }
       float g1[3][3];
-      grad_point<LB>(b1, i, j, k, lane, s_D, xix, g1);
-      stress_point(g1, s_kap[p], s_mu[p], fac, sg1[t]);
+      if (GEN && geo) {
+        float r1[3][3];
+        grad_point<LB>(b1, i, j, k, lane, s_D, 1.0f, r1);
+        map_gradient(r1, Gp, g1);
+        float sg[6];
+        stress_point(g1, s_kap[p], s_mu[p], 1.0f, sg);
+        map_flux(sg, Gp, sg1[t]);
+      } else {
+        grad_point<LB>(b1, i, j, k, lane, s_D, xix, g1);
+        if (GEN) {
+          float sg[6];
+          stress_point(g1, s_kap[p], s_mu[p], fac, sg);
+          const float F[9] = {sg[0], sg[3], sg[4], sg[3], sg[1], sg[5], sg[4], sg[5], sg[2]};
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) sg1[t][q] = F[q];
+        } else {
+          stress_point(g1, s_kap[p], s_mu[p], fac, sg1[t]);
+        }
+      }
       if (ADJ) {
         float g2[3][3];
-        grad_point<LB>(b2, i, j, k, lane, s_D, xix, g2);
-        stress_point(g2, s_kap[p], s_mu[p], fac, sg2[t]);
+        if (GEN && geo) {
+          float r2[3][3];
+          grad_point<LB>(b2, i, j, k, lane, s_D, 1.0f, r2);
+          map_gradient(r2, Gp, g2);
+          float sg[6];
+          stress_point(g2, s_kap[p], s_mu[p], 1.0f, sg);
+          map_flux(sg, Gp, sg2[t]);
+        } else {
+          grad_point<LB>(b2, i, j, k, lane, s_D, xix, g2);
+          if (GEN) {
+            float sg[6];
+            stress_point(g2, s_kap[p], s_mu[p], fac, sg);
+            const float F[9] = {sg[0], sg[3], sg[4], sg[3], sg[1], sg[5], sg[4], sg[5], sg[2]};
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) sg2[t][q] = F[q];
+          } else {
+            stress_point(g2, s_kap[p], s_mu[p], fac, sg2[t]);
+          }
+        }
         if (act2) {
           // deviatoric strain products (adjoint x backward) and traces
           const float tr1 = g1[0][0] + g1[1][1] + g1[2][2];
@@ -218,7 +309,7 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
     const int p = pg + t * G;
     if (p < NGLL3) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
+      for (int q = 0; q < NQ; ++q) {
         b1[(q * NGLL3 + p) * LB + lane] = sg1[t][q];
         if (ADJ) b2[(q * NGLL3 + p) * LB + lane] = sg2[t][q];
       }
@@ -233,13 +324,19 @@ __global__ void __launch_bounds__(NT) k_forces(StepArgs A) {
       const size_t ig = (size_t)s_ib[p];
       if (act1) {
         float f[3];
-        div_point<LB>(b1, i, j, k, lane, s_DWt, s_w, f);
+        if (GEN)
+          div_point_gen<LB>(b1, i, j, k, lane, s_DWt, s_w, f);
+        else
+          div_point<LB>(b1, i, j, k, lane, s_DWt, s_w, f);
 #pragma unroll
         for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[A.fi(ig, c, lg)], f[c]);
       }
       if (ADJ && scat2) {
         float f[3];
-        div_point<LB>(b2, i, j, k, lane, s_DWt, s_w, f);
+        if (GEN)
+          div_point_gen<LB>(b2, i, j, k, lane, s_DWt, s_w, f);
+        else
+          div_point<LB>(b2, i, j, k, lane, s_DWt, s_w, f);
 #pragma unroll
         for (int c = 0; c < 3; ++c) atomicAdd(&A.f2.a[A.fi(ig, c, lg)], f[c]);
       }
@@ -1116,17 +1213,17 @@ static void forces_pencil_cfg(const StepArgs& a, cudaStream_t st) {
   k_forces_pencil<LB, EPB, ADJ><<<grid, EPB * 25 * LB, shm, st>>>(a);
 }
 
-template <int LB, int NT, bool ADJ>
+template <int LB, int NT, bool ADJ, bool GEN = false>
 static void forces_cfg(const StepArgs& a, cudaStream_t st) {
-  const size_t shm = (size_t)(ADJ ? 2 : 1) * 6 * NGLL3 * LB * sizeof(float);
+  const size_t shm = (size_t)(ADJ ? 2 : 1) * (GEN ? 9 : 6) * NGLL3 * LB * sizeof(float);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_forces<LB, NT, ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_forces<LB, NT, ADJ, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)shm);
     attr = true;
   }
   dim3 grid(a.m.nspec, (a.nev + LB - 1) / LB);
-  k_forces<LB, NT, ADJ><<<grid, NT, shm, st>>>(a);
+  k_forces<LB, NT, ADJ, GEN><<<grid, NT, shm, st>>>(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -2408,6 +2505,22 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
 //   displacement prefetched into registers, 10 forward phase with 2 events
 //   per thread and register prefetch (8 events per block).
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  if (a.m.geo) {
+    // a mesh with irregular elements: the thread-per-point kernel with the
+    // general mapping, for every variant
+    if (a.nev == 1) {
+      if (adj)
+        forces_cfg<1, 128, true, true>(a, st);
+      else
+        forces_cfg<1, 128, false, true>(a, st);
+    } else {
+      if (adj)
+        forces_cfg<8, 256, true, true>(a, st);
+      else
+        forces_cfg<8, 256, false, true>(a, st);
+    }
+    return 1;
+  }
   if (a.variant == 12 && !a.gmap) return adj ? forces_shfl_cfg<true>(a, st) : forces_shfl_cfg<false>(a, st);
   if (a.variant == 10 && a.nev > 1) {
     if (!adj) return forces_fwd_r_cfg<8, false>(a, st);

@@ -57,13 +57,26 @@ class Mesh:
             f_n=np.ascontiguousarray(db.abs_normal.reshape(-1), np.float32),
         )
         f, i = C.c_float, C.c_int
+        irr = getattr(db, "irregular", None)
+        nirr = 0
+        geo_p = [None] * 10
+        irr_p = None
+        if irr is not None and (irr >= 0).any():
+            # irregular_element_number: 0 regular, k >= 1 row k-1 of the
+            # xixstore .. jacobianstore arrays (each [nirr][125])
+            k["irr"] = np.ascontiguousarray(np.where(irr >= 0, irr + 1, 0), np.int32)
+            nirr = int(db.geo.shape[0])
+            for q in range(10):
+                k[f"geo{q}"] = np.ascontiguousarray(db.geo[..., q].reshape(nirr, -1), np.float32)
+            geo_p = [_p(k[f"geo{q}"], f) for q in range(10)]
+            irr_p = _p(k["irr"], i)
         desc = _lib.MeshDesc(
             db.nspec, db.nglob, index_base, _p(k["ibool"], i), _p(k["x"], f),
             _p(k["y"], f), _p(k["z"], f), db.xix_regular, db.jacobian_regular,
-            None, _p(k["kappa"], f), _p(k["mu"], f), _p(k["rho"], f),
+            irr_p, _p(k["kappa"], f), _p(k["mu"], f), _p(k["rho"], f),
             _p(k["rmass"], f), _p(k["rho_vp"], f), _p(k["rho_vs"], f),
             db.nfaces, _p(k["f_ispec"], i), _p(k["f_ijk"], i), _p(k["f_jw"], f),
-            _p(k["f_n"], f))
+            _p(k["f_n"], f), nirr, *geo_p)
         h = C.c_void_p()
         check(L.sem_prepare_mesh(C.byref(desc), C.byref(h)))
         self._h = h

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _lib.load().sem_abi_version() == 1
+    assert _lib.load().sem_abi_version() == 2
 
 
 def test_no_device_is_reported_not_crashed():
