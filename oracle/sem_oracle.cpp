@@ -20,7 +20,10 @@
 //   * kernel names/derivation  src/postproc/post_processing.f90:417-422
 // It is pinned by physics instead: energy conservation, exact time
 // reversibility of the backward reconstruction, the analytic full-space
-// moment-tensor Green's function and a finite-difference gradient test.
+// moment-tensor Green's function and a finite-difference gradient test,
+// on regular meshes and on meshes of irregular (deformed) elements, whose
+// per-point mapping (xixstore .. jacobianstore, read_mesh_databases.f90:
+// 172-181) enters the gradient and the fluxes of the weak form.
 //
 // Time stepping convention (shared with the CUDA solver):
 //   step it (0-based) = predictor, forces on the predicted displacement,
