@@ -61,6 +61,9 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=1)
     p.add_argument("--store", default="fp16", choices=["fp16", "fp32"])
     p.add_argument("--served-requests", type=int, default=64)
+    p.add_argument("--served-mixed", type=int, default=48,
+                   help="requests of the mixed served stream (two meshes, forward "
+                        "and forward+adjoint, record lengths NSTEP/4 .. NSTEP); 0 skips it")
     p.add_argument("--served-load", type=float, default=1.25,
                    help="Poisson arrival rate as a fraction of batched capacity "
                         "(above 1: a saturated server, throughput-limited)")
@@ -451,6 +454,89 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                 "p99_s": float(np.percentile(lat, 99)),
                 "events_per_hour": NR / (t_free - arr[0]) * 3600.0}
 
+    # ---- served, mixed stream: two resident meshes, both request kinds and
+    # four record lengths arriving as a Poisson stream --------------------
+    served_mixed = None
+    if args.served_mixed > 0 and world == 1:
+        from specfwat_b200.serving import MeshServer, Request, Server, latency_stats
+        NR = args.served_mixed
+        rng = np.random.default_rng(4242)
+        lengths = tuple(NS * q // 4 for q in (1, 2, 3, 4))   # 1000 .. 4000 at NSTEP 4000
+        work = {}
+        for name in ("small", args.mesh):
+            wdb, wdb_obs, wrec, wev = make_workload(name, NR, 6000 + len(work))
+            work[name] = (wdb, wdb_obs, wrec,
+                          [S.make_source(x, y, z, mt, f0) for (x, y, z, mt, f0) in wev])
+        picks = []
+        for k in range(NR):
+            name = ("small", args.mesh)[int(rng.integers(2))]
+            kind = "fwd" if rng.random() < 0.6 else "fwdadj"
+            picks.append((name, kind, int(rng.choice(lengths))))
+        # observed data: one batched forward run of 4000 steps per mesh on
+        # its anomaly model, cut to each request's record length
+        obs_m = {}
+        for name, (wdb, wdb_obs, wrec, wsrc) in work.items():
+            ks = [k for k, p_ in enumerate(picks) if p_[0] == name and p_[1] == "fwdadj"]
+            if not ks:
+                continue
+            mo = S.Mesh(wdb_obs)
+            so = S.Simulation(mo, max(lengths), dt, nev=len(ks), use_graph=True,
+                              max_receivers=len(wrec))
+            so.set_sources([wsrc[k] for k in ks])
+            so.set_receivers(wrec)
+            so.iterate_time(1)
+            for q, k in enumerate(ks):
+                obs_m[k] = so.seismograms(q).astype(np.float64)
+            so.close()
+            mo.close()
+        # device cost of each request from the batched run's per-event step
+        # time, scaled by element count, record length and phase share
+        per_ev_step = ms_per_step / (E * NS)
+        fwd_share = sum(fms) / (sum(fms) + sum(ams))
+        def cost(name, kind, ns):
+            w = per_ev_step * ns * work[name][0].nspec / db.nspec
+            return w * (1.0 if kind == "fwdadj" else fwd_share)
+        costs = np.array([cost(*p_) for p_ in picks]) / 1e3          # seconds
+        # Poisson rate: served_load times what one event at a time would
+        # sustain at the batched per-event cost (requests/s)
+        lam = args.served_load / costs.mean()
+        arr = np.cumsum(np.random.default_rng(77).exponential(1.0 / lam, NR))
+        arr -= arr[0]
+        reqs = []
+        for k, (name, kind, ns) in enumerate(picks):
+            wdb, _, wrec, wsrc = work[name]
+            reqs.append(Request(rid=k, mesh=name, kind=kind, nstep=ns, source=wsrc[k],
+                                receivers=wrec,
+                                obs=obs_m[k][:, :, :ns].copy() if kind == "fwdadj" else None,
+                                arrival=float(arr[k])))
+        servers = {name: MeshServer(name, work[name][0], slots=E, nstep_max=max(lengths),
+                                    dt=dt, store=args.store, graph_steps=50,
+                                    max_receivers=len(work[name][2]), policy="group",
+                                    max_wait=2.0)
+                   for name in work}
+        done = Server(servers, quantum=100).run(reqs, timeout=3000)
+        for sv in servers.values():
+            sv.close()
+        st = latency_stats(done)
+        served_mixed = {
+            "requests": NR, "meshes": list(work), "kinds": "60% fwd, 40% fwd+adj",
+            "nstep": list(lengths), "arrivals": "Poisson",
+            "arrival_rate_per_hour": lam * 3600.0, "policy": "8-lane groups per mesh",
+            **st}
+        if "plain" in result:
+            # the plain path, one request at a time in arrival order, with
+            # the plain medium fwd+adj time scaled by the same work ratios
+            scale = result["plain"]["ms_per_event"] / 1e3 / cost(args.mesh, "fwdadj", NS) * 1e3
+            t_free, lat = 0.0, []
+            for a_, c_ in zip(arr, costs):
+                start = max(a_, t_free)
+                t_free = start + c_ * scale
+                lat.append(t_free - a_)
+            served_mixed["plain_fifo_estimate"] = {
+                "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)),
+                "events_per_hour": NR / (t_free - arr[0]) * 3600.0}
+
     nglob = db.nglob
     adj_bytes = algorithmic_bytes(db.nspec, nglob, E, True)
     fwd_bytes = algorithmic_bytes(db.nspec, nglob, E, False)
@@ -557,6 +643,8 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
         line["served"] = served
     if smooth:
         line["smooth"] = smooth
+    if served_mixed:
+        line["served_mixed"] = served_mixed
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
