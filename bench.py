@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--served-mixed", type=int, default=48,
                    help="requests of the mixed served stream (two meshes, forward "
                         "and forward+adjoint, record lengths NSTEP/4 .. NSTEP); 0 skips it")
+    p.add_argument("--mixed-policy", default="lane", choices=["lane", "group"],
+                   help="admission policy of the mixed stream's batched servers")
     p.add_argument("--served-load", type=float, default=1.25,
                    help="Poisson arrival rate as a fraction of batched capacity "
                         "(above 1: a saturated server, throughput-limited)")
@@ -511,17 +513,26 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                                 arrival=float(arr[k])))
         servers = {name: MeshServer(name, work[name][0], slots=E, nstep_max=max(lengths),
                                     dt=dt, store=args.store, graph_steps=50,
-                                    max_receivers=len(work[name][2]), policy="group",
-                                    max_wait=2.0)
+                                    max_receivers=len(work[name][2]),
+                                    policy=args.mixed_policy, max_wait=2.0)
                    for name in work}
-        done = Server(servers, quantum=100).run(reqs, timeout=3000)
-        for sv in servers.values():
+        solo = {name: MeshServer(name, work[name][0], slots=1, nstep_max=max(lengths), dt=dt,
+                                 store=args.store, graph_steps=50,
+                                 max_receivers=len(work[name][2]))
+                for name in work}
+        done = Server(servers, quantum=100, solo=solo).run(reqs, timeout=3000)
+        for sv in list(servers.values()) + list(solo.values()):
             sv.close()
         st = latency_stats(done)
         served_mixed = {
+            "solo_share": sum(r.server == "solo" for r in done) / len(done),
             "requests": NR, "meshes": list(work), "kinds": "60% fwd, 40% fwd+adj",
             "nstep": list(lengths), "arrivals": "Poisson",
-            "arrival_rate_per_hour": lam * 3600.0, "policy": "8-lane groups per mesh",
+            "arrival_rate_per_hour": lam * 3600.0,
+            "policy": (("8-lane groups" if args.mixed_policy == "group" else
+                        "any free lane, forward lanes packed away from adjoint ones")
+                       + " per mesh; a one-lane server per mesh takes requests while "
+                         "the batched one holds fewer than 4"),
             **st}
         if "plain" in result:
             # the plain path, one request at a time in arrival order, with

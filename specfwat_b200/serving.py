@@ -41,6 +41,7 @@ class Request:
     want_kernels: bool = False
     # results
     admitted: float = float("nan")
+    server: str = ""                   # "solo" or "batched" (set on admission)
     done: float = float("nan")
     misfit: float = float("nan")
     seismograms: Optional[np.ndarray] = None
@@ -94,6 +95,7 @@ class MeshServer:
         self.lane_store[lane] = need
         self.store_in_use += need
         req.admitted = now
+        req.server = "solo" if self.slots == 1 else "batched"
 
     def _fits(self, req):
         need = self.sim.lane_store_bytes(req.nstep) if req.kind == "fwdadj" else 0
@@ -124,6 +126,7 @@ class MeshServer:
             self.lane_store[lane] = need
             self.store_in_use += need
             req.admitted = now
+            req.server = "solo" if self.slots == 1 else "batched"
             started += 1
         return started
 
@@ -223,9 +226,30 @@ class Server:
     the number of steps every busy mesh advances between scheduling
     decisions (shortened when a lane completes sooner)."""
 
-    def __init__(self, servers: Dict[str, MeshServer], quantum=100):
+    def __init__(self, servers: Dict[str, MeshServer], quantum=100,
+                 solo: Optional[Dict[str, MeshServer]] = None, solo_below=4):
         self.servers = servers
         self.quantum = quantum
+        # Optional one-lane server per mesh (the plain one-event kernels).
+        # A lone request in an 8-lane group costs the whole group's
+        # launches, about four times the one-event path; so while the
+        # batched server of its mesh holds fewer than `solo_below` requests
+        # (running or queued) and the solo server is free, an arriving
+        # request takes the solo server instead.
+        self.solo = solo or {}
+        self.solo_below = solo_below
+
+    def _route(self, req):
+        batched = self.servers[req.mesh]
+        solo = self.solo.get(req.mesh)
+        if solo is not None and not solo.busy() and not solo.queue:
+            load = sum(1 for r in batched.lanes if r is not None) + len(batched.queue)
+            if load < self.solo_below:
+                return solo
+        return batched
+
+    def _all(self):
+        return list(self.servers.values()) + list(self.solo.values())
 
     def run(self, requests: List[Request], timeout=3600.0):
         pending = sorted(requests, key=lambda r: r.arrival)
@@ -238,11 +262,11 @@ class Server:
             if now > timeout:
                 raise TimeoutError("serving stream did not finish")
             while i < len(pending) and pending[i].arrival <= now:
-                self.servers[pending[i].mesh].queue.append(pending[i])
+                self._route(pending[i]).queue.append(pending[i])
                 i += 1
-            for srv in self.servers.values():
+            for srv in self._all():
                 srv.try_admit(now)
-            busy = [s for s in self.servers.values() if s.busy()]
+            busy = [s for s in self._all() if s.busy()]
             if not busy:
                 if i < len(pending):
                     time.sleep(max(0.0, min(0.01, pending[i].arrival - clock())))

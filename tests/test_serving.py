@@ -118,3 +118,36 @@ def test_store_budget_limits_admission(gpu):
     done = Server({"mini": srv}, quantum=50).run([], timeout=60)
     assert done == []
     srv.close()
+
+
+def test_solo_routing_same_results(gpu):
+    """A request that finds its mesh's batched server nearly empty and the
+    one-lane server free runs on the one-lane server (the plain one-event
+    kernels); the rest queue for the batched server.  A burst of five (one
+    solo, four batched) and two late arrivals; every result equals the
+    request run alone."""
+    rng = np.random.default_rng(12)
+    db = D.build("mini")
+    dt = 0.02
+    reqs = _requests(rng, "mini", db, 7, ["fwdadj", "fwd"], [240, 300], 0.0)
+    for k, r in enumerate(reqs):
+        r.arrival = 0.0 if k < 5 else 0.5   # a burst, then two late ones
+    batched = MeshServer("mini", db, slots=8, nstep_max=300, dt=dt, store="fp32",
+                         graph_steps=20, max_receivers=16)
+    solo = MeshServer("mini", db, slots=1, nstep_max=300, dt=dt, store="fp32",
+                      graph_steps=20, max_receivers=16)
+    srv = Server({"mini": batched}, quantum=40, solo={"mini": solo}, solo_below=2)
+    done = srv.run(reqs, timeout=600)
+    assert len(done) == len(reqs)
+    for r in reqs:
+        a = _alone(db, r, dt)
+        floor = 0.01 * np.linalg.norm(a["seis"]) + 1e-30
+        assert rel(r.seismograms, a["seis"], floor) < SEIS_TOL, r.rid
+        if r.kind == "fwdadj":
+            assert abs(r.misfit - a["misfit"]) <= 1e-4 * abs(a["misfit"]), r.rid
+            for q in range(3):
+                assert rel(r.kernels[q], a["kernels"][q]) < KERN_TOL, (r.rid, q)
+    assert {r.server for r in reqs} == {"solo", "batched"}
+    assert solo.store_in_use == 0 and batched.store_in_use == 0
+    solo.close()
+    batched.close()
