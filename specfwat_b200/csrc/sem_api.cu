@@ -802,10 +802,10 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   *out = nullptr;
   int rc = validate_cfg(c);
   if (rc) return rc;
-  if (!m->h_irreg.empty() && c->kernel_variant > 1)
+  if (!m->h_irreg.empty() && c->kernel_variant > 1 && c->kernel_variant != 11)
     return fail(SEM_ERR_UNSUPPORTED,
                 "kernel_variant %d needs regular elements; this mesh has irregular ones "
-                "(use 0 or 1)",
+                "(use 0, 1 or 11)",
                 c->kernel_variant);
   auto r = new sem_run_s();
   std::unique_ptr<sem_run_s> guard(r);
@@ -1042,8 +1042,9 @@ static int autotune_phase(sem_run* r, bool adj) {
 static int ensure_tuned(sem_run* r) {
   if (r->cfg.kernel_variant != 0 || (r->variant[0] >= 0 && r->variant[1] >= 0)) return SEM_OK;
   if (!r->mesh->h_irreg.empty()) {
-    // irregular elements run the thread-per-point kernel only
-    r->variant[0] = r->variant[1] = 0;
+    // irregular elements: the register-prefetch kernels for batches, the
+    // thread-per-point kernel for one event
+    r->variant[0] = r->variant[1] = r->nev > 1 ? 10 : 0;
     return SEM_OK;
   }
   if (r->nstep < 3) {

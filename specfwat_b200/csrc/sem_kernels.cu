@@ -1297,6 +1297,27 @@ __device__ __forceinline__ void red_v(float* g, const LV<NL>& x) {
   }
 }
 
+// Mapping of GLL point p of a general element: xix, xiy, xiz, etax, etay,
+// etaz, gammax, gammay, gammaz, jacobian (geo_e = the element's row of the
+// mesh's per-point mapping, 8-byte aligned), or the regular element's
+// diagonal mapping when geo_e is null.
+__device__ __forceinline__ void load_geo(const float* geo_e, int p, float xix, float jac,
+                                         float G[10]) {
+  if (geo_e) {
+    const float2* q = reinterpret_cast<const float2*>(geo_e + p * 10);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const float2 v = __ldg(q + k);
+      G[2 * k] = v.x;
+      G[2 * k + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) G[k] = (k % 4 == 0) ? xix : 0.f;
+    G[9] = jac;
+  }
+}
+
 // Shared block of one (field, element): U/B region then A region, each
 // value a run of LB lanes; `ub`/`ab` already include the thread's lane
 // offset.
@@ -1350,7 +1371,7 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
 }
 
 // eta / gamma divergence roles: B -> A.
-template <int LB, int NL>
+template <int LB, int NL, bool GEN = false>
 __device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
   {
     // eta pencil: sigma_{c,y} = (xy, yy, yz) = B0, B1, B2
@@ -1378,14 +1399,15 @@ __device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
       }
   }
   {
-    // gamma pencil: sigma_{c,z} = (xz, yz, zz) = B3, B2, B4
+    // gamma pencil: sigma_{c,z} = (xz, yz, zz) = B3, B2, B4; general
+    // elements: the gamma fluxes of the three components, B3, B4, B5
     LV<NL> v[3][5];
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
       const int p = pi + 5 * pq + 25 * l;
       v[0][l] = lds_v<NL>(b.U(3, p));
-      v[1][l] = lds_v<NL>(b.U(2, p));
-      v[2][l] = lds_v<NL>(b.U(4, p));
+      v[1][l] = lds_v<NL>(b.U(GEN ? 4 : 2, p));
+      v[2][l] = lds_v<NL>(b.U(GEN ? 5 : 4, p));
     }
 #pragma unroll
     for (int k = 0; k < 5; ++k)
@@ -1410,10 +1432,17 @@ __device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
 // deviatoric strain and trace are parked in its own A region at the
 // pencil's points.  MODE 2: adjoint field; the products with the parked
 // backward strain (read from `park`) are returned in kmu / kka.
-template <int LB, int NL, int MODE>
+// GEN: general elements.  The derivatives are mapped with the point's
+// mapping, the stress is formed without scale, and the xi role keeps the
+// xi fluxes J sigma_c . grad(xi) while the eta and gamma fluxes of the
+// three components go to B0..B2 and B3..B5; the strains of MODE 1 / 2 are
+// the physical ones (the caller's kernel-product scale is dt alone).
+template <int LB, int NL, int MODE, bool GEN = false>
 __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, int t,
                                      const float* kap, const float* mu, float fac,
-                                     LV<NL> fx[5][3], LV<NL> kmu[5], LV<NL> kka[5]) {
+                                     LV<NL> fx[5][3], LV<NL> kmu[5], LV<NL> kka[5],
+                                     const float* geo_e = nullptr, float xix = 0.f,
+                                     float jac = 0.f) {
   LV<NL> u[3][5];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -1434,8 +1463,11 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
 #pragma unroll
       for (int q = 0; q < 6; ++q) pk[q] = lds_v<NL>(park.Ar(q, p));
     }
-    LV<NL> o[5];
+    constexpr int NO = GEN ? 6 : 5;
+    LV<NL> o[NO];
     const float kp = kap[p], m = mu[p];
+    float G[10];
+    if (GEN) load_geo(geo_e, p, xix, jac, G);
 #pragma unroll
     for (int n = 0; n < NL; ++n) {
       float g[3][3];
@@ -1448,16 +1480,34 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
         g[c][1] = de[c].v[n];
         g[c][2] = dg[c].v[n];
       }
-      float sig[6];
-      stress_point(g, kp, m, fac, sig);
-      sx[0][i].v[n] = sig[0];
-      sx[1][i].v[n] = sig[3];
-      sx[2][i].v[n] = sig[4];
-      o[0].v[n] = sig[3];
-      o[1].v[n] = sig[1];
-      o[2].v[n] = sig[5];
-      o[3].v[n] = sig[4];
-      o[4].v[n] = sig[2];
+      if constexpr (GEN) {
+        float r[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) r[c][d] = g[c][d];
+        map_gradient(r, G, g);
+        float sig[6], F[9];
+        stress_point(g, kp, m, 1.0f, sig);
+        map_flux(sig, G, F);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          sx[c][i].v[n] = F[c * 3 + 0];
+          o[c].v[n] = F[c * 3 + 1];
+          o[3 + c].v[n] = F[c * 3 + 2];
+        }
+      } else {
+        float sig[6];
+        stress_point(g, kp, m, fac, sig);
+        sx[0][i].v[n] = sig[0];
+        sx[1][i].v[n] = sig[3];
+        sx[2][i].v[n] = sig[4];
+        o[0].v[n] = sig[3];
+        o[1].v[n] = sig[1];
+        o[2].v[n] = sig[5];
+        o[3].v[n] = sig[4];
+        o[4].v[n] = sig[2];
+      }
       if (MODE != 0) {
         const float tr = g[0][0] + g[1][1] + g[2][2];
         const float xx = g[0][0] - tr * (1.0f / 3.0f);
@@ -1481,7 +1531,7 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
       }
     }
 #pragma unroll
-    for (int q = 0; q < 5; ++q) sts_v<NL>(b.U(q, p), o[q]);
+    for (int q = 0; q < NO; ++q) sts_v<NL>(b.U(q, p), o[q]);
     if (MODE == 1) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) sts_v<NL>(b.Ar(q, p), pk[q]);
@@ -1774,9 +1824,12 @@ __global__ void __launch_bounds__(25 * LB / NL) k_forces_vec(StepArgs A, PipeIte
 // strain products for the mu/kappa kernels are formed in registers at each
 // point, with no parking in shared memory.
 
-template <int VL>
+// GEN: general elements, as v_xi (six fluxes to B, physical strains).
+template <int VL, bool GEN = false>
 __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* kap, const float* mu,
-                                        float fac, LV<2> fx[5][3], float kmu[5], float kka[5]) {
+                                        float fac, LV<2> fx[5][3], float kmu[5], float kka[5],
+                                        const float* geo_e = nullptr, float xix = 0.f,
+                                        float jac = 0.f) {
   LV<2> u[3][5];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -1792,9 +1845,12 @@ __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* k
       de[c] = lds_v<2>(b.Ar(c, p));
       dg[c] = lds_v<2>(b.Ar(3 + c, p));
     }
-    LV<2> o[5];
+    constexpr int NO = GEN ? 6 : 5;
+    LV<2> o[NO];
     float ev[2][6];
     const float kp = kap[p], m = mu[p];
+    float G[10];
+    if (GEN) load_geo(geo_e, p, xix, jac, G);
 #pragma unroll
     for (int n = 0; n < 2; ++n) {
       float g[3][3];
@@ -1807,16 +1863,34 @@ __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* k
         g[c][1] = de[c].v[n];
         g[c][2] = dg[c].v[n];
       }
-      float sig[6];
-      stress_point(g, kp, m, fac, sig);
-      sx[0][i].v[n] = sig[0];
-      sx[1][i].v[n] = sig[3];
-      sx[2][i].v[n] = sig[4];
-      o[0].v[n] = sig[3];
-      o[1].v[n] = sig[1];
-      o[2].v[n] = sig[5];
-      o[3].v[n] = sig[4];
-      o[4].v[n] = sig[2];
+      if constexpr (GEN) {
+        float r[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) r[c][d] = g[c][d];
+        map_gradient(r, G, g);
+        float sig[6], F[9];
+        stress_point(g, kp, m, 1.0f, sig);
+        map_flux(sig, G, F);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          sx[c][i].v[n] = F[c * 3 + 0];
+          o[c].v[n] = F[c * 3 + 1];
+          o[3 + c].v[n] = F[c * 3 + 2];
+        }
+      } else {
+        float sig[6];
+        stress_point(g, kp, m, fac, sig);
+        sx[0][i].v[n] = sig[0];
+        sx[1][i].v[n] = sig[3];
+        sx[2][i].v[n] = sig[4];
+        o[0].v[n] = sig[3];
+        o[1].v[n] = sig[1];
+        o[2].v[n] = sig[5];
+        o[3].v[n] = sig[4];
+        o[4].v[n] = sig[2];
+      }
       const float tr = g[0][0] + g[1][1] + g[2][2];
       ev[n][0] = g[0][0] - tr * (1.0f / 3.0f);
       ev[n][1] = g[1][1] - tr * (1.0f / 3.0f);
@@ -1831,7 +1905,7 @@ __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* k
              2.0f * (ev[0][2] * ev[1][2] + ev[0][3] * ev[1][3] + ev[0][4] * ev[1][4]);
     kka[i] = ev[0][5] * ev[1][5];
 #pragma unroll
-    for (int q = 0; q < 5; ++q) sts_v<2>(b.U(q, p), o[q]);
+    for (int q = 0; q < NO; ++q) sts_v<2>(b.U(q, p), o[q]);
   }
 #pragma unroll
   for (int i = 0; i < 5; ++i)
@@ -2046,24 +2120,25 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair(StepArgs A, PipeItem
 // is computed, stored to shared memory at the top of the next iteration),
 // so the displacement region is single-buffered: 40 KB less shared memory
 // per 8 events, twice the resident blocks.
-template <int LB>
+template <int LB, bool GEN = false>
 struct PairRLayout {
   static constexpr int VL = 2 * LB;
   static constexpr int NE = NGLL3;
+  static constexpr int PPU = GEN ? 6 * NGLL3 : PP_U;               // U, then 5 (6) values
   static constexpr int OFF_IB = 0;                                  // int [3][NE]
   static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);               // [2][2][NE]
-  static constexpr int OFF_U = al4(OFF_KM + 4 * NE);                // [PP_U][VL]
-  static constexpr int OFF_A = al4(OFF_U + PP_U * VL);              // [PP_A][VL]
+  static constexpr int OFF_U = al4(OFF_KM + 4 * NE);                // [PPU][VL]
+  static constexpr int OFF_A = al4(OFF_U + PPU * VL);               // [PP_A][VL]
   static constexpr int OFF_K = al4(OFF_A + PP_A * VL);              // [2][2][NE][LB]
   static constexpr int TOTAL = OFF_K + 4 * NE * LB;
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
 
-template <int LB>
+template <int LB, bool GEN = false>
 __global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeItems items) {
   constexpr int VL = 2 * LB;
   constexpr int NT = 25 * LB;
-  using LY = PairRLayout<LB>;
+  using LY = PairRLayout<LB, GEN>;
   constexpr int NE = NGLL3;
   constexpr int LWLOG = 3;
   extern __shared__ float sm[];
@@ -2174,7 +2249,9 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeIt
   load_u(w, 0);
 
   const float fac = A.m.jac * A.m.xix * A.m.xix;
-  const float dtk = A.dt * A.m.xix * A.m.xix;
+  // kernel products: raw reference derivatives (times xix^2) or, for
+  // general elements, physical strains
+  const float dtk = GEN ? A.dt : A.dt * A.m.xix * A.m.xix;
   for (int k = 0; w < nitems; ++k, w += gridDim.x) {
     const int buf = k & 1;
     const int ibs = k % 3;
@@ -2210,7 +2287,12 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeIt
     __syncthreads();
     LV<2> fx[5][3];
     float kmu[5], kka[5];
-    pair_xi<VL>(b, t, kap, mu, fac, fx, kmu, kka);
+    const float* geo_e = nullptr;
+    if (GEN && e < nspec) {
+      const int ir = A.m.irreg[e];
+      if (ir >= 0) geo_e = A.m.geo + (size_t)ir * NGLL3 * 10;
+    }
+    pair_xi<VL, GEN>(b, t, kap, mu, fac, fx, kmu, kka, geo_e, A.m.xix, A.m.jac);
     if ((fl & 2) && e < nspec) {
       const float* kb = sK + buf * 2 * NE * LB;
       const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3) << LWLOG);
@@ -2223,7 +2305,7 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeIt
       }
     }
     __syncthreads();
-    v_div_eg<VL, 2>(b, pi, pq);
+    v_div_eg<VL, 2, GEN>(b, pi, pq);
     __syncthreads();
     if (e < nspec && (fl & 1)) {
       const size_t fb = fbase<LWLOG>(A, lg);
@@ -2233,15 +2315,15 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeIt
   cp_wait_all();
 }
 
-template <int LB>
+template <int LB, bool GEN = false>
 static void forces_adjpair_r_cfg(const StepArgs& a, cudaStream_t st) {
   constexpr int NT = 25 * LB;
-  constexpr size_t BYTES = PairRLayout<LB>::BYTES;
+  constexpr size_t BYTES = PairRLayout<LB, GEN>::BYTES;
   static int blocks_per_sm = 0, sms = 0;
   if (!blocks_per_sm) {
-    cudaFuncSetAttribute(k_forces_adjpair_r<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_forces_adjpair_r<LB, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_adjpair_r<LB>, NT,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_adjpair_r<LB, GEN>, NT,
                                                   BYTES);
     int dev = 0;
     cudaGetDevice(&dev);
@@ -2253,29 +2335,30 @@ static void forces_adjpair_r_cfg(const StepArgs& a, cudaStream_t st) {
   int gx = blocks_per_sm * sms;
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
-  k_forces_adjpair_r<LB><<<gx, NT, BYTES, st>>>(a, items);
+  k_forces_adjpair_r<LB, GEN><<<gx, NT, BYTES, st>>>(a, items);
 }
 
 // Forward-phase element kernel with 2 events per thread and the next
 // element's gather prefetched into registers (single-buffered shared
 // displacement), LB events per block.  LB is at most the 8-lane sector
 // group, so a work item never spans two groups of a group map.
-template <int LB>
+template <int LB, bool GEN = false>
 struct FwdRLayout {
   static constexpr int NE = NGLL3;
+  static constexpr int PPU = GEN ? 6 * NGLL3 : PP_U;   // U, then 5 (6) values
   static constexpr int OFF_IB = 0;                      // int [3][NE]
   static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);   // [2][2][NE]
-  static constexpr int OFF_U = al4(OFF_KM + 4 * NE);    // [PP_U][LB]
-  static constexpr int OFF_A = al4(OFF_U + PP_U * LB);  // [PP_A][LB]
+  static constexpr int OFF_U = al4(OFF_KM + 4 * NE);    // [PPU][LB]
+  static constexpr int OFF_A = al4(OFF_U + PPU * LB);   // [PP_A][LB]
   static constexpr int TOTAL = OFF_A + PP_A * LB;
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
 
-template <int LB, bool COLOURED>
+template <int LB, bool COLOURED, bool GEN = false>
 __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeItems items) {
   constexpr int NL = 2;
   constexpr int NT = 25 * LB / NL;
-  using LY = FwdRLayout<LB>;
+  using LY = FwdRLayout<LB, GEN>;
   constexpr int NE = NGLL3;
   constexpr int LWLOG = 3;
   extern __shared__ float sm[];
@@ -2399,15 +2482,20 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     int lg0, g, fl[NL];
     const int anyf = flags(w, lg0, g, fl);
     const bool valid = g < ngr;
+    const float* geo_e = nullptr;
+    if (GEN && valid) {
+      const int ir = A.m.irreg[A.m.order[g]];
+      if (ir >= 0) geo_e = A.m.geo + (size_t)ir * NGLL3 * 10;
+    }
     const float* kap = sKM + buf * 2 * NE;
     const float* mu = kap + NE;
     PBuf<LB> b{sU + lane, sA + lane};
     v_grad_eg<LB, NL>(b, pi, pq);
     __syncthreads();
     LV<NL> fx[5][3], km[1], kk[1];
-    v_xi<LB, NL, 0>(b, b, t, kap, mu, fac, fx, km, kk);
+    v_xi<LB, NL, 0, GEN>(b, b, t, kap, mu, fac, fx, km, kk, geo_e, A.m.xix, A.m.jac);
     __syncthreads();
-    v_div_eg<LB, NL>(b, pi, pq);
+    v_div_eg<LB, NL, GEN>(b, pi, pq);
     __syncthreads();
     if (valid && anyf)
       v_scatter<LB, NL, !COLOURED>(b, t, fx, sIB + ibs * NE, A.f1.a + fbase<LWLOG>(A, lg0), fl, 1);
@@ -2415,16 +2503,16 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
   cp_wait_all();
 }
 
-template <int LB, bool COLOURED>
+template <int LB, bool COLOURED, bool GEN = false>
 static int forces_fwd_r_cfg(const StepArgs& a, cudaStream_t st) {
   constexpr int NT = 25 * LB / 2;
-  constexpr size_t BYTES = FwdRLayout<LB>::BYTES;
+  constexpr size_t BYTES = FwdRLayout<LB, GEN>::BYTES;
   static int blocks_per_sm = 0, sms = 0;
   if (!blocks_per_sm) {
-    cudaFuncSetAttribute(k_forces_fwd_r<LB, COLOURED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_fwd_r<LB, COLOURED>, NT,
-                                                  BYTES);
+    cudaFuncSetAttribute(k_forces_fwd_r<LB, COLOURED, GEN>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
+                                                  k_forces_fwd_r<LB, COLOURED, GEN>, NT, BYTES);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2436,7 +2524,7 @@ static int forces_fwd_r_cfg(const StepArgs& a, cudaStream_t st) {
     int gx = blocks_per_sm * sms;
     if (gx > items.count()) gx = items.count();
     if (gx < 1) gx = 1;
-    k_forces_fwd_r<LB, COLOURED><<<gx, NT, BYTES, st>>>(ac, items);
+    k_forces_fwd_r<LB, COLOURED, GEN><<<gx, NT, BYTES, st>>>(ac, items);
     return 1;
   };
   if (!COLOURED) return launch(a, a.m.nspec);
@@ -2506,8 +2594,14 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
 //   per thread and register prefetch (8 events per block).
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
   if (a.m.geo) {
-    // a mesh with irregular elements: the thread-per-point kernel with the
-    // general mapping, for every variant
+    // a mesh with irregular elements: the register-prefetch kernels with
+    // the general mapping (variant 10, batched), else the thread-per-point
+    // kernel with the general mapping
+    if (a.variant == 10 && a.nev > 1) {
+      if (!adj) return forces_fwd_r_cfg<8, false, true>(a, st);
+      forces_adjpair_r_cfg<8, true>(a, st);
+      return 1;
+    }
     if (a.nev == 1) {
       if (adj)
         forces_cfg<1, 128, true, true>(a, st);

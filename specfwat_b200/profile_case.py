@@ -33,8 +33,15 @@ def main(argv=None):
     p.add_argument("--smooth", type=int, default=0,
                    help="smooth this many element fields instead")
     p.add_argument("--smooth-steps", type=int, default=0)
+    p.add_argument("--topo", type=float, default=0.0,
+                   help="hill topography height (m): every element irregular")
     a = p.parse_args(argv)
-    db = D.build(a.mesh)
+    if a.topo:
+        box = D.config_box(a.mesh)
+        db = D.make_box(box, topo=D.hill_topography(box, a.topo, 0.25 * box.lx))
+        db = db.with_model(*D.background_model(db, seed=1234))
+    else:
+        db = D.build(a.mesh)
     if a.smooth:
         from .postproc import smooth_sem_pde
         mesh = S.Mesh(db)

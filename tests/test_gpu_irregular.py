@@ -2,7 +2,8 @@
 
 A mesh with topography (every element irregular: per-point mapping
 derivatives and Jacobian, read_mesh_databases.f90:168-181) runs the
-thread-per-point element kernel with the general mapping.  Checked here:
+thread-per-point element kernel (one event) or the register-prefetch
+kernels (batches) with the general mapping.  Checked here:
 - seismograms within relative L2 1e-4 of the FP32 and FP64 oracle runs;
 - event kernels within 1e-3;
 - several events batched equal each event alone;
@@ -65,17 +66,23 @@ def test_topography_forward_matches_oracle(gpu, topo_case, variant):
     mesh.close()
 
 
-def test_topography_adjoint_kernels_match_oracle(gpu, topo_case):
+@pytest.mark.parametrize("nev", [1, 3])
+def test_topography_adjoint_kernels_match_oracle(gpu, topo_case, nev):
+    """nev 1: the thread-per-point kernel; nev 3 (the same event in every
+    lane): the batched register-prefetch kernels with the general mapping."""
     db, rec, mt, sxyz, nstep, dt, obs = topo_case
     mesh = S.Mesh(db)
-    sim = S.Simulation(mesh, nstep, dt, max_receivers=len(rec))
-    sim.set_sources([S.make_source(*sxyz, mt, 1.0)])
+    sim = S.Simulation(mesh, nstep, dt, nev=nev, max_receivers=len(rec))
+    sim.set_sources([S.make_source(*sxyz, mt, 1.0)] * nev)
     sim.set_receivers(rec)
     sim.iterate_time(1, save_forward=True)
-    syn = sim.seismograms(0)
-    misfit = sim.measure_l2(0, obs, 0.05, 1)
+    syn = sim.seismograms(nev - 1)
+    for e in range(nev - 1):
+        sim.measure_l2(e, obs, 0.05, 1)
+    misfit = sim.measure_l2(nev - 1, obs, 0.05, 1)
     sim.iterate_time(3)
-    kg = sim.save_adjoint_kernels(0)
+    assert sim.kernel_variants() == ((11, 11) if nev > 1 else (1, 1))
+    kg = sim.save_adjoint_kernels(nev - 1)
     src = Oracle.source(*sxyz, mt, 1.0)
     res = {}
     for prec in (4, 8):
@@ -138,5 +145,5 @@ def test_regular_only_variants_refused(gpu, topo_case):
     db, rec, *_ = topo_case
     mesh = S.Mesh(db)
     with pytest.raises(_lib.SemError, match="regular elements"):
-        S.Simulation(mesh, 100, 0.02, nev=8, max_receivers=len(rec), kernel_variant=11)
+        S.Simulation(mesh, 100, 0.02, nev=8, max_receivers=len(rec), kernel_variant=5)
     mesh.close()
