@@ -2135,7 +2135,7 @@ struct PairRLayout {
 };
 
 template <int LB, bool GEN = false>
-__global__ void __launch_bounds__(25 * LB) k_forces_adjpair_r(StepArgs A, PipeItems items) {
+__global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(StepArgs A, PipeItems items) {
   constexpr int VL = 2 * LB;
   constexpr int NT = 25 * LB;
   using LY = PairRLayout<LB, GEN>;
