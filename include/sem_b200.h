@@ -375,6 +375,38 @@ int sem_smooth_pde(sem_mesh *mesh, const sem_smooth_cfg *cfg, int nfield,
                    const float *dat_in, const int *is_cpml, float *dat_out,
                    sem_smooth_stats *stats);
 
+/* Approximate Hessian kernel (SPECFEM's APPROXIMATE_HESS_KL, read by
+ * PostFlow%sum_precond / apply_precond as hess_kernel,
+ * src/postproc/post_processing.f90:164-230).  Enabled before a
+ * sim_type 3 run, the adjoint run also accumulates per GLL point
+ *     hess = 2 * sum_it DT * (adjoint accel . backward accel).
+ * Batched runs (sem_iterate_time) only; lanes driven by sem_lane_* do not
+ * hand it back.  Costs 8 bytes per point and event and step. */
+int sem_set_approximate_hessian(sem_run *run, int enable);
+/* hess_kernel of event ev: out[nspec][125]. */
+int sem_save_hessian_kernel(sem_run *run, int ev, double *out);
+/* FP64 sum over the run's events of hess (abs_each = 0) or |hess| (1):
+ * out[nspec][125]. */
+int sem_sum_hessian(sem_run *run, int abs_each, double *out);
+
+/* Preconditioner of PostFlow%apply_precond (post_processing.f90:164-197)
+ * from the event-summed Hessian (n values; sem_sum_hessian over all
+ * batches): precond_type 1 takes hess_sum = sum |hess|, 0 takes
+ * |sum hess|; then invert_hess (post_processing.f90:333-372): normalise by
+ * the maximum (all ones when it is below 1e-18), invert with
+ * THRESHOLD_HESS = 1e-3, normalise by the maximum.  The kernels are
+ * multiplied by precond.  Computed on the device in FP64; precond FP32. */
+int sem_hessian_precond(const double *hess_sum, long long n, int precond_type,
+                        float *precond);
+/* Depth preconditioner zprecond_gll (src/postproc/zprecond.f90:11-71),
+ * precond_type 2 (1/|z|) or 3 (1/sqrt|z|): the profile on the model
+ * grid's depth levels zlev[nz] (strictly ascending; z = 1e-8 above the
+ * surface, z + 1e-8 below), linearly interpolated to the GLL points'
+ * z, times nevents, normalised, inverted, normalised.  Points outside
+ * [zlev[0], zlev[nz-1]] take the end values.  precond[nspec][125]. */
+int sem_depth_precond(sem_mesh *mesh, const double *zlev, int nz, int precond_type,
+                      int nevents, float *precond);
+
 /* FP32 FMA throughput of the current device in TFLOP/s (an FMA counts
  * as 2 flops), the best of 5 timed launches of independent fmaf chains on
  * every SM; *ms (may be null) is that launch's time.  No reference

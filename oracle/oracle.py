@@ -62,6 +62,7 @@ def lib():
         L.oracle_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
+        L.oracle_get_hessian.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_energy.restype = C.c_double
         L.oracle_energy.argtypes = [C.c_void_p]
         L.oracle_get_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -180,6 +181,14 @@ class Oracle:
         if want_adjoint_seis:
             out.append(aseis)
         return out[0] if len(out) == 1 else tuple(out)
+
+    def hessian(self):
+        """hess_kernel [nspec, 5, 5, 5] of the last ``adjoint`` run: twice
+        the sum over steps of DT * (adjoint accel . backward accel)."""
+        out = np.zeros((self.db.nspec, 5, 5, 5), np.float64)
+        if lib().oracle_get_hessian(self._h, out.ctypes.data):
+            raise RuntimeError("no adjoint run")
+        return out
 
     def field(self, which):
         n = self.db.nglob * 3
@@ -464,3 +473,60 @@ def measure_waveform(syn, obs, dt, t0, obs_tbeg, obs_dt, bands, windows,
         comb = np.stack([-rr * np.sin(b) - tt * np.cos(b),
                          -rr * np.cos(b) + tt * np.sin(b), z], axis=1)
     return mis.sum((1, 2)), comb, mis
+
+
+# --------------------------------------------------------------------------
+# Kernel preconditioners (src/postproc/post_processing.f90:164-197,333-372;
+# src/postproc/zprecond.f90:11-71), vectorised FP64 restatements.
+# --------------------------------------------------------------------------
+
+THRESHOLD_HESS = 1e-3   # src/shared/config.f90:42
+
+
+def invert_hess(h):
+    """``invert_hess`` (post_processing.f90:333-372): normalise by max|h|
+    (all ones when it is below 1e-18), invert where |h| > THRESHOLD_HESS
+    (1/THRESHOLD_HESS elsewhere), normalise by max|h| again."""
+    h = np.asarray(h, np.float64)
+    mx = np.abs(h).max()
+    h = np.ones_like(h) if mx < 1e-18 else h / mx
+    safe = np.where(np.abs(h) > THRESHOLD_HESS, h, 1.0)
+    h = np.where(np.abs(h) > THRESHOLD_HESS, 1.0 / safe, 1.0 / THRESHOLD_HESS)
+    return h / np.abs(h).max()
+
+
+def hessian_precond(hess_sum, precond_type=1):
+    """``apply_precond`` PRECOND_TYPE 0 (|sum hess|) or 1 (sum |hess| given)
+    followed by ``invert_hess`` (post_processing.f90:171-185)."""
+    h = np.asarray(hess_sum, np.float64)
+    if precond_type == 0:
+        h = np.abs(h)
+    return invert_hess(h)
+
+
+def depth_profile(zlev, precond_type):
+    """``get_1d_precond`` (zprecond.f90:11-32): 1e-8 above the surface,
+    z + 1e-8 below; 1/|z| (type 2) or 1/sqrt|z| (type 3)."""
+    z = np.asarray(zlev, np.float64)
+    zl = np.where(z > 0.0, 1e-8, z + 1e-8)
+    return 1.0 / np.sqrt(zl * zl) if precond_type == 2 else 1.0 / np.sqrt(np.sqrt(zl * zl))
+
+
+def interp1_clamped(x, v, xq):
+    """``interp1`` (src/shared/utils.f90:889-910) on ascending levels:
+    linear between the bracketing levels, the end value at and above the
+    last level.  Below the first level the Fortran reads x(0); here the
+    first value is taken."""
+    return np.interp(np.asarray(xq, np.float64), np.asarray(x, np.float64),
+                     np.asarray(v, np.float64))
+
+
+def depth_precond(db, zlev, precond_type, nevents):
+    """``zprecond_gll`` (zprecond.f90:34-71) on the mesh ``db``:
+    [nspec, 5, 5, 5]."""
+    prof = depth_profile(zlev, precond_type)
+    z = np.asarray(db.zstore, np.float64)[np.asarray(db.ibool).reshape(db.nspec, 5, 5, 5)]
+    h = interp1_clamped(zlev, prof, z) * nevents
+    h = h / np.abs(h).max()
+    h = 1.0 / h
+    return h / np.abs(h).max()

@@ -350,6 +350,9 @@ struct Solver {
   std::vector<T> stf;                // [nstep]
   // kernels
   std::vector<T> rho_kl_glob, mu_kl, kappa_kl;
+  // approximate Hessian sum_j DT a_adj . a_bwd per global point
+  // (APPROXIMATE_HESS_KL; read as hess_kernel by post_processing.f90:175)
+  std::vector<T> hess_kl_glob;
 
   explicit Solver(const oracle_mesh& mm, int nth) : m(mm), nthreads(nth) {
     g = make_gll();
@@ -711,6 +714,7 @@ struct Solver {
     bv = fin_v;
     ba = fin_a;
     rho_kl_glob.assign(m.nglob, 0);
+    hess_kl_glob.assign(m.nglob, 0);
     mu_kl.assign(ne, 0);
     kappa_kl.assign(ne, 0);
     std::vector<T> eps_a(ne * 6), eps_b(ne * 6), scratch(n3);
@@ -739,6 +743,7 @@ struct Solver {
       for (int ig = 0; ig < m.nglob; ++ig) {
         size_t q = (size_t)ig * 3;
         rho_kl_glob[ig] += tdt * (a[q] * bu[q] + a[q + 1] * bu[q + 1] + a[q + 2] * bu[q + 2]);
+        hess_kl_glob[ig] += tdt * (a[q] * ba[q] + a[q + 1] * ba[q + 1] + a[q + 2] * ba[q + 2]);
       }
 #pragma omp parallel for schedule(static) num_threads(nthreads)
       for (size_t ep = 0; ep < ne; ++ep) {
@@ -997,6 +1002,21 @@ int oracle_adjoint(void* p, int nrec, const double* rxyz, const double* adj, dou
   if (!h || !adj || !kern) return 1;
   return h->prec == 4 ? h->s32->adjoint(nrec, rxyz, adj, kern, bseis, aseis)
                       : h->s64->adjoint(nrec, rxyz, adj, kern, bseis, aseis);
+}
+
+// hess_kernel of the last adjoint run, out[nspec*125]: twice the
+// accumulated sum at each element point (the approximate Hessian's scaling
+// by 2; a positive factor cancels in the preconditioner).
+int oracle_get_hessian(void* p, double* out) {
+  auto* h = (Handle*)p;
+  if (!h || !out) return 1;
+  auto copy = [&](auto& s) {
+    if (s.hess_kl_glob.empty()) return 2;
+    const size_t ne = (size_t)s.m.nspec * 125;
+    for (size_t ep = 0; ep < ne; ++ep) out[ep] = 2.0 * (double)s.hess_kl_glob[s.m.ibool[ep]];
+    return 0;
+  };
+  return h->prec == 4 ? copy(*h->s32) : copy(*h->s64);
 }
 
 double oracle_energy(void* p) {

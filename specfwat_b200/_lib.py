@@ -34,6 +34,8 @@ EXPORTS = (
     "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
     "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
     "sem_smooth_pde", "sem_measure_waveform", "sem_measure_waveform_dev",
+    "sem_set_approximate_hessian", "sem_save_hessian_kernel", "sem_sum_hessian",
+    "sem_hessian_precond", "sem_depth_precond",
 )
 MEAS_MAX_BANDS = 4
 SMOOTH_MAP_CUBE = 0
@@ -167,6 +169,11 @@ def load():
                                            fp, fp]),
         "sem_measure_waveform_dev": (C.c_int, [vp, ip, ip, dp, C.POINTER(MeasCfg), vp,
                                                vp, vp, vp, vp, vp]),
+        "sem_set_approximate_hessian": (C.c_int, [vp, ip]),
+        "sem_save_hessian_kernel": (C.c_int, [vp, ip, fp]),
+        "sem_sum_hessian": (C.c_int, [vp, ip, fp]),
+        "sem_hessian_precond": (C.c_int, [fp, C.c_longlong, ip, fp]),
+        "sem_depth_precond": (C.c_int, [vp, fp, ip, ip, ip, fp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

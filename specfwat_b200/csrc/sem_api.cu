@@ -399,6 +399,9 @@ struct sem_run_s {
   DevArray<unsigned char> store;
   DevArray<float> scale;
   DevArray<float> k_rho, k_mu, k_kappa;
+  DevArray<float> k_hess;          // approximate Hessian [nglob][nevp]
+  bool hess_on = false;            // accumulate it in adjoint runs
+  bool hess_done = false;          // the last adjoint run accumulated it
   DevArray<double> kout, ksum;
   DevArray<double> obs, taper, simpw, misfit_rc, obs_ev;
   double taper_pct_cached = -1.0;
@@ -443,7 +446,7 @@ struct sem_run_s {
     a.m = mesh->view();
     a.f1 = {u1.p, v1.p, a1.p};
     a.f2 = adjoint ? Fields{u2.p, v2.p, a2.p} : Fields{nullptr, nullptr, nullptr};
-    a.k = {k_rho.p, k_mu.p, k_kappa.p};
+    a.k = {k_rho.p, k_mu.p, k_kappa.p, hess_on ? k_hess.p : nullptr};
     a.lanes = lanes.p;
     a.minv = minv.p;
     a.nev = nev;
@@ -983,6 +986,10 @@ static int ensure_adjoint_buffers(sem_run* r) {
     CKM(r->k_mu.alloc(ne * nev), "mu kernel");
     CKM(r->k_kappa.alloc(ne * nev), "kappa kernel");
   }
+  if (r->hess_on && !r->k_hess.p) {
+    CKM(r->k_hess.alloc(ng * nev), "Hessian kernel");
+    CK(cudaMemsetAsync(r->k_hess.p, 0, r->k_hess.bytes(), r->stream));
+  }
   return SEM_OK;
 }
 
@@ -1155,6 +1162,8 @@ int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
     CK(cudaMemsetAsync(r->k_rho.p, 0, r->k_rho.bytes(), r->stream));
     CK(cudaMemsetAsync(r->k_mu.p, 0, r->k_mu.bytes(), r->stream));
     CK(cudaMemsetAsync(r->k_kappa.p, 0, r->k_kappa.bytes(), r->stream));
+    if (r->hess_on) CK(cudaMemsetAsync(r->k_hess.p, 0, r->k_hess.bytes(), r->stream));
+    r->hess_done = r->hess_on;
     r->fill_lanes(PH_ADJ, 0);
     CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
                        r->stream));
@@ -1421,6 +1430,48 @@ int sem_sum_kernels_device(sem_run* r, double* dev_out) {
   return SEM_OK;
 }
 
+int sem_set_approximate_hessian(sem_run* r, int enable) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  r->hess_on = enable != 0;
+  if (r->hess_on && r->k_rho.p) {
+    // adjoint buffers exist already (an earlier adjoint run or lane start)
+    int rc = ensure_adjoint_buffers(r);
+    if (rc) return rc;
+  }
+  return SEM_OK;
+}
+
+int sem_save_hessian_kernel(sem_run* r, int ev, double* out) {
+  if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  if (!r->adj_done || !r->hess_done)
+    return fail(SEM_ERR_STATE, "no adjoint run with the approximate Hessian has completed");
+  const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+  if (!r->kout.p) CKM(r->kout.alloc(6 * ne), "kernel output");
+  launch_finalize_hessian(r->mesh->view(), r->k_hess.p, r->lm, ev, r->kout.p, nullptr, 0,
+                          r->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, r->kout.p, ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_sum_hessian(sem_run* r, int abs_each, double* out) {
+  if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (!r->adj_done || !r->hess_done)
+    return fail(SEM_ERR_STATE, "no adjoint run with the approximate Hessian has completed");
+  const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+  if (!r->ksum.p) CKM(r->ksum.alloc(6 * ne), "kernel sum");
+  CK(cudaMemsetAsync(r->ksum.p, 0, ne * 8, r->stream));
+  for (int e = 0; e < r->nev; ++e)
+    launch_finalize_hessian(r->mesh->view(), r->k_hess.p, r->lm, e, nullptr, r->ksum.p,
+                            abs_each != 0, r->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, r->ksum.p, ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
 int sem_set_stream(sem_run* r, void* stream) {
   if (!r) return fail(SEM_ERR_ARG, "null run");
   CK(cudaStreamSynchronize(r->stream));
@@ -1633,7 +1684,8 @@ int sem_lane_start_adjoint(sem_run* r, int lane, const double* obs, double taper
   const Fields f1{r->u1.p, r->v1.p, r->a1.p}, f2{r->u2.p, r->v2.p, r->a2.p};
   launch_lane_copy(f1, f2, r->mesh->nglob, r->lm, lane, r->stream);
   launch_lane_zero(f1, r->mesh->nglob, r->lm, lane, r->stream);
-  launch_lane_zero_acc({r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->mesh->nglob,
+  launch_lane_zero_acc({r->k_rho.p, r->k_mu.p, r->k_kappa.p, r->hess_on ? r->k_hess.p : nullptr},
+                       r->mesh->nglob,
                        (size_t)r->mesh->nspec * NGLL3, r->lm, lane, r->stream);
   CK(cudaGetLastError());
   if (misfit) {

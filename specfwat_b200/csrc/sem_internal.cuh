@@ -76,6 +76,7 @@ struct KernAcc {
   float* rho_glob;   // [nglob][nev]
   float* mu;         // [nspec*125][nev]
   float* kappa;      // [nspec*125][nev]
+  float* hess_glob;  // [nglob][nev] approximate Hessian, or null (not accumulated)
 };
 
 // Per-event arrays use a lane-group layout: event lanes are grouped by
@@ -132,6 +133,10 @@ int launch_advance(LaneDesc* lanes, int nev, int k, cudaStream_t st);
 int launch_finalize_kernels(const MeshView& m, const float* rho,
                             const KernAcc& k, LaneMap lm, int lane,
                             double* out6, double* sum6, cudaStream_t st);
+// hess_kernel of one lane in element layout: out[ep] = 2 hess_glob[ibool[ep]]
+// (written when out is not null), sum[ep] += that value or its magnitude
+int launch_finalize_hessian(const MeshView& m, const float* hess_glob, LaneMap lm, int lane,
+                            double* out, double* sum, int abs_each, cudaStream_t st);
 int launch_measure_l2(const float* seis, const double* obs, const double* taper,
                       const double* simpw, int nrec, int nstep, float* adj_out,
                       double* misfit_rc, cudaStream_t st);

@@ -2954,6 +2954,9 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
       }
     }
     A.k.rho_glob[A.gi(ig, lg)] += dt * (a[0] * bu[0] + a[1] * bu[1] + a[2] * bu[2]);
+    // approximate Hessian: adjoint acceleration . backward acceleration
+    if (A.k.hess_glob)
+      A.k.hess_glob[A.gi(ig, lg)] += dt * (a[0] * ba[0] + a[1] * ba[1] + a[2] * ba[2]);
     if (pred) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -3045,6 +3048,28 @@ int launch_finalize_kernels(const MeshView& m, const float* rho, const KernAcc& 
   return 1;
 }
 
+// hess_kernel: twice the accumulated sum, mapped from global to element
+// points (the factor 2 of the approximate Hessian's scaling; a positive
+// factor cancels in the preconditioner's normalisations).
+__global__ void k_finalize_hess(MeshView m, const float* __restrict__ hess_glob, LaneMap lm,
+                                int lane, double* __restrict__ out, double* __restrict__ sum,
+                                int abs_each) {
+  const size_t ne = (size_t)m.nspec * NGLL3;
+  const size_t ep = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ep >= ne) return;
+  const double h = 2.0 * (double)hess_glob[lm.p((size_t)m.ibool[ep], lane, (size_t)m.nglob)];
+  if (out) out[ep] = h;
+  if (sum) sum[ep] += abs_each ? fabs(h) : h;
+}
+
+int launch_finalize_hessian(const MeshView& m, const float* hess_glob, LaneMap lm, int lane,
+                            double* out, double* sum, int abs_each, cudaStream_t st) {
+  const size_t ne = (size_t)m.nspec * NGLL3;
+  k_finalize_hess<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, hess_glob, lm, lane, out, sum,
+                                                                 abs_each);
+  return 1;
+}
+
 // ---------------------------------------------------------------------------
 // L2 waveform misfit and adjoint source in FP64
 // ---------------------------------------------------------------------------
@@ -3118,7 +3143,10 @@ int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane, cudaStrea
 
 __global__ void k_lane_zero_acc(KernAcc k, int nglob, size_t ne, LaneMap lm, int lane) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < (size_t)nglob) k.rho_glob[lm.p(i, lane, (size_t)nglob)] = 0.f;
+  if (i < (size_t)nglob) {
+    k.rho_glob[lm.p(i, lane, (size_t)nglob)] = 0.f;
+    if (k.hess_glob) k.hess_glob[lm.p(i, lane, (size_t)nglob)] = 0.f;
+  }
   if (i < ne) {
     k.mu[lm.p(i, lane, ne)] = 0.f;
     k.kappa[lm.p(i, lane, ne)] = 0.f;

@@ -244,6 +244,24 @@ class Simulation:
         check(_lib.load().sem_sum_kernels(self._h, out.ctypes.data))
         return out
 
+    # approximate Hessian (APPROXIMATE_HESS_KL; hess_kernel)
+    def set_approximate_hessian(self, enable: bool = True):
+        """Accumulate hess = 2 sum DT accel_adj . accel_bwd in the next
+        adjoint runs (enable before ``iterate_time(3)``)."""
+        check(_lib.load().sem_set_approximate_hessian(self._h, int(bool(enable))))
+
+    def hessian_kernel(self, ev: int = 0) -> np.ndarray:
+        """hess_kernel of event ``ev``: [nspec, 5, 5, 5] FP64."""
+        out = np.zeros((self.mesh.nspec, 5, 5, 5), np.float64)
+        check(_lib.load().sem_save_hessian_kernel(self._h, ev, out.ctypes.data))
+        return out
+
+    def sum_hessian(self, abs_each: bool = True) -> np.ndarray:
+        """FP64 sum over the events of |hess| (``abs_each``) or hess."""
+        out = np.zeros((self.mesh.nspec, 5, 5, 5), np.float64)
+        check(_lib.load().sem_sum_hessian(self._h, int(bool(abs_each)), out.ctypes.data))
+        return out
+
     # -- serving primitives (one event per lane, lanes advance together) --
     def lane_store_bytes(self, nstep: int) -> int:
         return int(_lib.load().sem_lane_store_bytes(self._h, nstep))

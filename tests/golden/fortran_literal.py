@@ -8,6 +8,9 @@ the golden vectors in this directory:
 * ``window_taper`` src/shared/signal.f90:419-491
 * ``calc_adjoint_source`` (L2, one window)
                    src/preproc/adjoint_sources/waveform_misfit.f90:15-64
+* ``invert_hess``  src/postproc/post_processing.f90:333-372 (FP32)
+* ``interp1_0``    src/shared/utils.f90:889-910
+* ``get_1d_precond``, ``zprecond_gll`` src/postproc/zprecond.f90:11-71 (FP32)
 """
 import math
 
@@ -384,3 +387,83 @@ def interpolate_func_dp(syn, t1, dt1, npt1, t2, dt2, npt2):
             tt = time - ((ii - 1) * dt1 + t1)
             syn1[i - 1] = (syn[ii + 1 - 1] - syn[ii - 1]) * tt / dt1 + syn[ii - 1]
     return syn1
+
+
+def invert_hess(hess):
+    """Element by element in FP32, as the Fortran array statements run."""
+    import numpy as np
+    f = np.float32
+    h = [f(x) for x in hess]
+    maxh = f(0.0)
+    for x in h:
+        maxh = max(maxh, f(abs(x)))
+    if maxh < f(1.0e-18):
+        h = [f(1.0) for _ in h]
+    else:
+        h = [f(x / maxh) for x in h]
+    thr = f(1.0e-3)
+    h = [f(f(1.0) / x) if abs(x) > thr else f(f(1.0) / thr) for x in h]
+    maxh = f(0.0)
+    for x in h:
+        maxh = max(maxh, f(abs(x)))
+    return [f(x / maxh) for x in h]
+
+
+def interp1_0(x, v, xq):
+    """1-based masked minloc/maxloc as written; returns None where the
+    Fortran would read x(0) (xq below the first level)."""
+    n = len(x)
+    x1 = 0
+    best = None
+    for i in range(1, n + 1):
+        if xq >= x[i - 1] and (best is None or xq - x[i - 1] < best):
+            best, x1 = xq - x[i - 1], i
+    x2 = 0
+    best = None
+    for i in range(1, n + 1):
+        if xq < x[i - 1] and (best is None or xq - x[i - 1] > best):
+            best, x2 = xq - x[i - 1], i
+    if x2 != 0:
+        if x1 == 0:
+            return None
+        vn = abs(x[x2 - 1] - x[x1 - 1])
+        vq = v[x1 - 1] * (x[x2 - 1] - xq) + v[x2 - 1] * (xq - x[x1 - 1])
+        return vq / vn
+    if xq <= x[0]:
+        return v[0]
+    if xq >= x[n - 1]:
+        return v[n - 1]
+    return None
+
+
+def get_1d_precond(zgrid, precond_type):
+    import numpy as np
+    f = np.float32
+    zl = []
+    for z in zgrid:
+        if f(z) > f(0.0):
+            q = f(1.0e-8)
+        else:
+            q = f(f(z) + f(1.0e-8))
+        if precond_type == 2:
+            q = f(f(1.0) / f(np.sqrt(f(q * q))))
+        elif precond_type == 3:
+            q = f(f(1.0) / f(np.sqrt(f(np.sqrt(f(q * q))))))
+        zl.append(q)
+    return zl
+
+
+def zprecond_gll(ibool, zstore, zgrid, precond_type, nevents):
+    """ibool: flat 1-based element-point -> global point; returns the flat
+    FP32 preconditioner."""
+    import numpy as np
+    f = np.float32
+    zl = [float(q) for q in get_1d_precond(zgrid, precond_type)]
+    zg = [float(z) for z in zgrid]
+    h = [f(interp1_0(zg, zl, float(zstore[ig - 1]))) for ig in ibool]
+    h = [f(x * f(nevents)) for x in h]
+    maxh = max(f(abs(x)) for x in h)
+    h = [f(x / maxh) for x in h]
+    h = [f(f(1.0) / x) for x in h]
+    maxh = max(f(abs(x)) for x in h)
+    return [f(x / maxh) for x in h]
