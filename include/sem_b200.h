@@ -375,6 +375,24 @@ int sem_smooth_pde(sem_mesh *mesh, const sem_smooth_cfg *cfg, int nfield,
                    const float *dat_in, const int *is_cpml, float *dat_out,
                    sem_smooth_stats *stats);
 
+/* Incident wavefield injected on the absorbing faces of event ev's
+ * forward run: FK injection (COUPLE_WITH_INJECTION_TECHNIQUE with
+ * INJECTION_TECHNIQUE_TYPE 3, prepare_timerun_fwat.f90:104-117), fed with
+ * the arrays read_fk_coupling_file loads (src/shared/fk_coupling.f90:396-439).
+ * veloc, tract: [nt][nf*25][3] FP32, the reference's Veloc_FK and
+ * Tract_FK(NDIM, npt, k0 : k0+nt-1) with npt ordered face by face as
+ * ipt_table (fk_coupling.f90:299-327); sample k is at time
+ * k * np_resamp * DT (the reference uses k0 = -NP_RESAMP).  Step it takes
+ * the 4-point Lagrange interpolant at it / np_resamp (the sample itself
+ * when np_resamp divides it).  The absorbing term becomes
+ *     accel -= (Stacey(v - veloc) - tract) * jacobian2Dw
+ * with tract = sigma . n for the outward normal; the boundary store saves
+ * that term, so the backward reconstruction replays it.  An event with an
+ * injection needs no point source.  veloc = NULL removes it.  Batched runs
+ * (sem_iterate_time) only. */
+int sem_set_injection(sem_run *run, int ev, const float *veloc, const float *tract, int nt,
+                      int np_resamp, int k0);
+
 /* Approximate Hessian kernel (SPECFEM's APPROXIMATE_HESS_KL, read by
  * PostFlow%sum_precond / apply_precond as hess_kernel,
  * src/postproc/post_processing.f90:164-230).  Enabled before a

@@ -63,6 +63,8 @@ def lib():
                                      C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
         L.oracle_get_hessian.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_set_injection.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                           C.c_void_p, C.c_void_p]
         L.oracle_energy.restype = C.c_double
         L.oracle_energy.argtypes = [C.c_void_p]
         L.oracle_get_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -181,6 +183,21 @@ class Oracle:
         if want_adjoint_seis:
             out.append(aseis)
         return out[0] if len(out) == 1 else tuple(out)
+
+    def set_injection(self, veloc, tract, np_resamp=1, k0=0):
+        """FK injection on the absorbing faces for the next forward runs:
+        ``[nt, nf*25, 3]`` incident velocity and traction (sigma . n,
+        outward normal), sample ``k`` at time ``(k + k0) * np_resamp * dt``;
+        ``veloc=None`` removes it."""
+        if veloc is None:
+            lib().oracle_set_injection(self._h, 0, 1, 0, None, None)
+            return
+        v = np.ascontiguousarray(veloc, np.float64)
+        t = np.ascontiguousarray(tract, np.float64)
+        assert v.shape == t.shape and v.shape[1:] == (self.db.nfaces * 25, 3)
+        if lib().oracle_set_injection(self._h, v.shape[0], int(np_resamp), int(k0),
+                                      v.ctypes.data, t.ctypes.data):
+            raise RuntimeError("oracle_set_injection failed")
 
     def hessian(self):
         """hess_kernel [nspec, 5, 5, 5] of the last ``adjoint`` run: twice

@@ -353,6 +353,10 @@ struct Solver {
   // approximate Hessian sum_j DT a_adj . a_bwd per global point
   // (APPROXIMATE_HESS_KL; read as hess_kernel by post_processing.f90:175)
   std::vector<T> hess_kl_glob;
+  // FK injection (forward runs): [inj_nt][nf*25][3] incident velocity and
+  // traction, sample k at time (k + inj_k0) * inj_np * dt
+  std::vector<double> inj_v, inj_t;
+  int inj_nt = 0, inj_np = 1, inj_k0 = 0;
 
   explicit Solver(const oracle_mesh& mm, int nth) : m(mm), nthreads(nth) {
     g = make_gll();
@@ -541,7 +545,35 @@ struct Solver {
 
   // Stacey traction from velocity vel; acc -= jw t.  mode 0: absorb,
   // mode 1: absorb and save record `rec`, mode 2: subtract stored record.
-  void stacey(const std::vector<T>& vel, std::vector<T>& acc, int mode, int rec) {
+  // Incident velocity and traction of face point fp at step it: the 4-point
+  // Lagrange interpolant in time of the stored samples, indices clamped.
+  void injected(int it, size_t fp, T vi[3], T ti[3]) const {
+    const size_t npt = (size_t)m.nf * NG2;
+    const int i1 = it / inj_np - inj_k0;
+    const double x = (double)(it % inj_np) / inj_np;
+    const double w[4] = {-x * (x - 1) * (x - 2) / 6, (x + 1) * (x - 1) * (x - 2) / 2,
+                         -(x + 1) * x * (x - 2) / 2, (x + 1) * x * (x - 1) / 6};
+    double sv[3] = {0, 0, 0}, st[3] = {0, 0, 0};
+    for (int q = 0; q < 4; ++q) {
+      const int k = std::min(std::max(i1 - 1 + q, 0), inj_nt - 1);
+      for (int c = 0; c < 3; ++c) {
+        sv[c] += w[q] * inj_v[((size_t)k * npt + fp) * 3 + c];
+        st[c] += w[q] * inj_t[((size_t)k * npt + fp) * 3 + c];
+      }
+    }
+    for (int c = 0; c < 3; ++c) {
+      vi[c] = (T)sv[c];
+      ti[c] = (T)st[c];
+    }
+  }
+
+  // Stacey faces.  mode 0: absorb; 1: absorb and save the boundary term
+  // in store[rec]; 2: subtract store[rec].  it_inj >= 0: the forward step
+  // whose incident field is injected (absorb the velocity relative to it,
+  // add its traction).
+  void stacey(const std::vector<T>& vel, std::vector<T>& acc, int mode, int rec,
+              int it_inj = -1) {
+    const bool inject = it_inj >= 0 && !inj_v.empty();
     for (int f = 0; f < m.nf; ++f) {
       int e = m.f_ispec[f];
       for (int p = 0; p < NG2; ++p) {
@@ -555,12 +587,14 @@ struct Solver {
           continue;
         }
         const T* n = &nrm[((size_t)f * NG2 + p) * 3];
-        T vx = vel[ig * 3 + 0], vy = vel[ig * 3 + 1], vz = vel[ig * 3 + 2];
+        T vi[3] = {0, 0, 0}, ti[3] = {0, 0, 0};
+        if (inject) injected(it_inj, (size_t)f * NG2 + p, vi, ti);
+        T vx = vel[ig * 3 + 0] - vi[0], vy = vel[ig * 3 + 1] - vi[1], vz = vel[ig * 3 + 2] - vi[2];
         T vn = vx * n[0] + vy * n[1] + vz * n[2];
         T rvp = rho_vp[(size_t)e * NG3 + lp], rvs = rho_vs[(size_t)e * NG3 + lp];
-        T tx = rvp * vn * n[0] + rvs * (vx - vn * n[0]);
-        T ty = rvp * vn * n[1] + rvs * (vy - vn * n[1]);
-        T tz = rvp * vn * n[2] + rvs * (vz - vn * n[2]);
+        T tx = rvp * vn * n[0] + rvs * (vx - vn * n[0]) - ti[0];
+        T ty = rvp * vn * n[1] + rvs * (vy - vn * n[1]) - ti[1];
+        T tz = rvp * vn * n[2] + rvs * (vz - vn * n[2]) - ti[2];
         T wgt = jw[(size_t)f * NG2 + p];
         T sx = tx * wgt, sy = ty * wgt, sz = tz * wgt;
         acc[ig * 3 + 0] -= sx;
@@ -687,7 +721,7 @@ struct Solver {
     for (int it = 0; it < nstep; ++it) {
       predictor(u, v, a, dt);
       forces(u, a, nullptr);
-      stacey(v, a, save ? 1 : 0, it);
+      stacey(v, a, save ? 1 : 0, it, it);
       add_source(a, it);
       corrector(v, a, dt);
       if (seis) record(u, seis, it);
@@ -1017,6 +1051,30 @@ int oracle_get_hessian(void* p, double* out) {
     return 0;
   };
   return h->prec == 4 ? copy(*h->s32) : copy(*h->s64);
+}
+
+// FK injection for the next forward runs: [nt][nf*25][3] velocity and
+// traction, sample k at time (k + k0) * np_resamp * dt; veloc = null clears.
+int oracle_set_injection(void* p, int nt, int np_resamp, int k0, const double* veloc,
+                         const double* tract) {
+  auto* h = (Handle*)p;
+  if (!h) return 1;
+  auto set = [&](auto& s) {
+    if (!veloc) {
+      s.inj_v.clear();
+      s.inj_t.clear();
+      return 0;
+    }
+    if (!tract || nt < 1 || np_resamp < 1) return 2;
+    const size_t n = (size_t)nt * s.m.nf * 25 * 3;
+    s.inj_v.assign(veloc, veloc + n);
+    s.inj_t.assign(tract, tract + n);
+    s.inj_nt = nt;
+    s.inj_np = np_resamp;
+    s.inj_k0 = k0;
+    return 0;
+  };
+  return h->prec == 4 ? set(*h->s32) : set(*h->s64);
 }
 
 double oracle_energy(void* p) {

@@ -35,7 +35,7 @@ EXPORTS = (
     "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
     "sem_smooth_pde", "sem_measure_waveform", "sem_measure_waveform_dev",
     "sem_set_approximate_hessian", "sem_save_hessian_kernel", "sem_sum_hessian",
-    "sem_hessian_precond", "sem_depth_precond",
+    "sem_hessian_precond", "sem_depth_precond", "sem_set_injection",
 )
 MEAS_MAX_BANDS = 4
 SMOOTH_MAP_CUBE = 0
@@ -174,6 +174,7 @@ def load():
         "sem_sum_hessian": (C.c_int, [vp, ip, fp]),
         "sem_hessian_precond": (C.c_int, [fp, C.c_longlong, ip, fp]),
         "sem_depth_precond": (C.c_int, [vp, fp, ip, ip, ip, fp]),
+        "sem_set_injection": (C.c_int, [vp, ip, fp, fp, ip, ip, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -416,6 +416,13 @@ struct sem_run_s {
   DevArray<int> gmap;             // serving: active 8-lane groups
   std::vector<int> src_ispec, nrec;
   std::vector<char> have_src, have_rec, have_adj;
+  // FK injection per event: one device allocation holding the velocity and
+  // traction samples, and its shape
+  struct Injection {
+    float* buf = nullptr;
+    int nt = 0, np = 1, k0 = 0;
+  };
+  std::vector<Injection> inj;
   bool fwd_saved = false, adj_done = false;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int variant[2] = {-1, -1};  // element-kernel variant per phase (fwd, adj)
@@ -423,6 +430,8 @@ struct sem_run_s {
   long long last_launches = 0;
 
   ~sem_run_s() {
+    for (auto& j : inj)
+      if (j.buf) cudaFree(j.buf);
     for (size_t l = 0; l < lane_store.size(); ++l) {
       if (lane_store[l]) cudaFreeAsync(lane_store[l], stream);
       if (lane_scale[l]) cudaFreeAsync(lane_scale[l], stream);
@@ -481,6 +490,14 @@ struct sem_run_s {
       L.adj = adj.p + (size_t)e * nrec_max * 3 * ns;
       L.store = store.p ? store.p + (size_t)e * store_bytes_per_event() : nullptr;
       L.scale = scale.p ? scale.p + (size_t)e * ns * mesh->nf : nullptr;
+      if (e < (int)inj.size() && inj[e].buf) {
+        const size_t npt3 = (size_t)mesh->nf * 25 * 3;
+        L.inj_v = inj[e].buf;
+        L.inj_t = inj[e].buf + (size_t)inj[e].nt * npt3;
+        L.inj_nt = inj[e].nt;
+        L.inj_np = inj[e].np;
+        L.inj_k0 = inj[e].k0;
+      }
     }
   }
 };
@@ -879,6 +896,7 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   r->src_ispec.assign(nev, -1);
   r->nrec.assign(nev, 0);
   r->have_src.assign(nev, 0);
+  r->inj.assign(nev, sem_run_s::Injection{});
   r->have_rec.assign(nev, 0);
   r->have_adj.assign(nev, 0);
   CK(cudaStreamSynchronize(r->stream));
@@ -1127,8 +1145,8 @@ int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
   const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nevp;
   if (sim_type == 1) {
     for (int e = 0; e < r->nev; ++e)
-      if (!r->have_src[e] || !r->have_rec[e])
-        return fail(SEM_ERR_STATE, "event %d has no source or receivers", e);
+      if (!(r->have_src[e] || r->inj[e].buf) || !r->have_rec[e])
+        return fail(SEM_ERR_STATE, "event %d has no source, injection or receivers", e);
     int trc = ensure_tuned(r);
     if (trc) return trc;
     if (save_forward) {
@@ -1468,6 +1486,51 @@ int sem_sum_hessian(sem_run* r, int abs_each, double* out) {
                             abs_each != 0, r->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, r->ksum.p, ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return SEM_OK;
+}
+
+int sem_set_injection(sem_run* r, int ev, const float* veloc, const float* tract, int nt,
+                      int np_resamp, int k0) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  if (r->lanes_mode) return fail(SEM_ERR_STATE, "run is driven lane by lane (sem_lane_*)");
+  auto& j = r->inj[ev];
+  if (!veloc) {
+    if (j.buf) {
+      CK(cudaStreamSynchronize(r->stream));
+      cudaFree(j.buf);
+    }
+    j = sem_run_s::Injection{};
+    return SEM_OK;
+  }
+  if (!tract) return fail(SEM_ERR_ARG, "null traction");
+  if (r->mesh->nf == 0) return fail(SEM_ERR_STATE, "the mesh has no absorbing faces");
+  if (nt < 1 || np_resamp < 1) return fail(SEM_ERR_ARG, "nt and np_resamp must be >= 1");
+  const size_t npt3 = (size_t)r->mesh->nf * 25 * 3;
+  const size_t n = (size_t)nt * npt3;
+  for (const float* a : {veloc, tract})
+    for (size_t i = 0; i < n; ++i)
+      if (!std::isfinite(a[i])) return fail(SEM_ERR_ARG, "non-finite injected value at %zu", i);
+  if (j.buf && j.nt != nt) {
+    CK(cudaStreamSynchronize(r->stream));
+    cudaFree(j.buf);
+    j.buf = nullptr;
+  }
+  if (!j.buf) {
+    cudaError_t e = cudaMalloc((void**)&j.buf, 2 * n * sizeof(float));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      j.buf = nullptr;
+      return fail(SEM_ERR_NOMEM, "device allocation of the injected field failed: %s",
+                  cudaGetErrorString(e));
+    }
+  }
+  j.nt = nt;
+  j.np = np_resamp;
+  j.k0 = k0;
+  CK(cudaMemcpyAsync(j.buf, veloc, n * 4, cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(j.buf + n, tract, n * 4, cudaMemcpyHostToDevice, r->stream));
   CK(cudaStreamSynchronize(r->stream));
   return SEM_OK;
 }

@@ -39,6 +39,12 @@ struct LaneDesc {
   const float* adj;      // [nrec][3][nstep] adjoint sources, forward time
   void* store;           // [nstep][nf][25][3] float or half
   float* scale;          // [nstep][nf] per-face FP16 scale
+  // incident wavefield on the absorbing faces (forward phase), or null:
+  // [inj_nt][nf*25][3] velocity and traction, sample k at time
+  // (k + inj_k0) * inj_np * DT
+  const float* inj_v;
+  const float* inj_t;
+  int inj_nt, inj_np, inj_k0, inj_pad;
 };
 
 struct MeshView {

@@ -2717,6 +2717,33 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
 // Stacey absorbing faces: traction, boundary store save / replay
 // ---------------------------------------------------------------------------
 
+// Incident velocity and traction of face point fp at step it: the 4-point
+// Lagrange interpolant of the samples at it / inj_np (exact when inj_np
+// divides it), sample indices clamped to the stored range.
+__device__ __forceinline__ void injected(const LaneDesc* L, int it, int fp, int npt, float vi[3],
+                                         float ti[3]) {
+  const int i1 = it / L->inj_np - L->inj_k0;
+  const float x = (float)(it % L->inj_np) / (float)L->inj_np;
+  float w[4];
+  w[0] = -x * (x - 1.f) * (x - 2.f) * (1.f / 6.f);
+  w[1] = (x + 1.f) * (x - 1.f) * (x - 2.f) * 0.5f;
+  w[2] = -(x + 1.f) * x * (x - 2.f) * 0.5f;
+  w[3] = (x + 1.f) * x * (x - 1.f) * (1.f / 6.f);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) vi[c] = ti[c] = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q != 1 && x == 0.f) continue;
+    const int k = min(max(i1 - 1 + q, 0), L->inj_nt - 1);
+    const size_t b = ((size_t)k * npt + fp) * 3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      vi[c] = fmaf(w[q], L->inj_v[b + c], vi[c]);
+      ti[c] = fmaf(w[q], L->inj_t[b + c], ti[c]);
+    }
+  }
+}
+
 // Block of 128 threads = FPB faces x (32 point slots x LBB lanes).
 template <int LBB>
 __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
@@ -2755,15 +2782,19 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
     ig = (size_t)A.m.f_iglob[fp];
     if (absorb) {
       const float nx = A.m.f_n[fp * 3 + 0], ny = A.m.f_n[fp * 3 + 1], nz = A.m.f_n[fp * 3 + 2];
-      const float vx = A.f1.v[A.fi(ig, 0, lg)];
-      const float vy = A.f1.v[A.fi(ig, 1, lg)];
-      const float vz = A.f1.v[A.fi(ig, 2, lg)];
+      float vi[3] = {0.f, 0.f, 0.f}, ti[3] = {0.f, 0.f, 0.f};
+      if (L->phase == PH_FWD && L->inj_v) injected(L, it, fp, nf * NGLL2, vi, ti);
+      // FK injection: Stacey on the velocity relative to the incident field,
+      // plus the incident traction
+      const float vx = A.f1.v[A.fi(ig, 0, lg)] - vi[0];
+      const float vy = A.f1.v[A.fi(ig, 1, lg)] - vi[1];
+      const float vz = A.f1.v[A.fi(ig, 2, lg)] - vi[2];
       const float vn = vx * nx + vy * ny + vz * nz;
       const float rvp = A.m.f_rvp[fp], rvs = A.m.f_rvs[fp];
       const float jw = A.m.f_jw[fp];
-      sv[0] = (rvp * vn * nx + rvs * (vx - vn * nx)) * jw;
-      sv[1] = (rvp * vn * ny + rvs * (vy - vn * ny)) * jw;
-      sv[2] = (rvp * vn * nz + rvs * (vz - vn * nz)) * jw;
+      sv[0] = (rvp * vn * nx + rvs * (vx - vn * nx) - ti[0]) * jw;
+      sv[1] = (rvp * vn * ny + rvs * (vy - vn * ny) - ti[1]) * jw;
+      sv[2] = (rvp * vn * nz + rvs * (vz - vn * nz) - ti[2]) * jw;
 #pragma unroll
       for (int c = 0; c < 3; ++c) atomicAdd(&A.f1.a[A.fi(ig, c, lg)], -sv[c]);
       if (save && A.store_fp16) {

@@ -244,6 +244,21 @@ class Simulation:
         check(_lib.load().sem_sum_kernels(self._h, out.ctypes.data))
         return out
 
+    # FK injection on the absorbing faces
+    def set_injection(self, ev: int, veloc, tract, np_resamp: int = 1, k0: int = 0):
+        """Incident velocity and traction on the absorbing face points of
+        event ``ev``: ``[nt, nf*25, 3]`` each (Veloc_FK / Tract_FK), sample
+        ``k`` at time ``(k + k0) * np_resamp * dt``.  ``veloc=None`` removes
+        the injection."""
+        if veloc is None:
+            check(_lib.load().sem_set_injection(self._h, ev, None, None, 0, 1, 0))
+            return
+        v = np.ascontiguousarray(veloc, np.float32)
+        t = np.ascontiguousarray(tract, np.float32)
+        assert v.shape == t.shape and v.ndim == 3 and v.shape[2] == 3
+        check(_lib.load().sem_set_injection(self._h, ev, v.ctypes.data, t.ctypes.data,
+                                            v.shape[0], int(np_resamp), int(k0)))
+
     # approximate Hessian (APPROXIMATE_HESS_KL; hess_kernel)
     def set_approximate_hessian(self, enable: bool = True):
         """Accumulate hess = 2 sum DT accel_adj . accel_bwd in the next
