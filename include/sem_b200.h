@@ -30,6 +30,15 @@
  *     src/postproc/post_processing.f90:108-149
  *   FinalizeSpecfem / prepare_cleanup_device          sem_release_run,
  *     src/specfem_interface/specfem_api.f90:298-369    sem_release_mesh
+ *   Veloc_FK / Tract_FK (FK injection)                sem_set_injection
+ *     src/shared/fk_coupling.f90:71-439
+ *   hess_kernel (APPROXIMATE_HESS_KL) and its sum      sem_set_approximate_hessian,
+ *     src/postproc/post_processing.f90:171-218         sem_save_hessian_kernel,
+ *                                                     sem_sum_hessian
+ *   invert_hess / zprecond_gll                        sem_hessian_precond,
+ *     post_processing.f90:333-372, zprecond.f90:34-71  sem_depth_precond
+ *   smooth_sem_pde                                    sem_smooth_pde
+ *     src/postproc/smooth.f90:7-437
  *
  * Conventions
  *  - Every function returns SEM_OK (0) or a negative sem_status; the reason
