@@ -12,6 +12,8 @@ backward reconstruction.  Checked against the exact half-space plane wave
 - the adjoint run after an injected forward: kernels within 1e-3 of the
   FP32 and FP64 oracle (the backward field replays the injected boundary
   term);
+- a two-layer box driven by the layered field (``LayeredPlaneWave``):
+  receivers within 2e-3 of that field and 1e-4 of the FP64 oracle;
 - argument errors and an event with neither source nor injection.
 """
 import numpy as np
@@ -142,3 +144,22 @@ def test_injection_errors(gpu, case):
         sim.iterate_time(1)                       # event 1 has neither
     sim.close()
     mesh.close()
+
+
+def test_layered_box_reproduces_the_layered_field(gpu):
+    from specfwat_b200.injection import LayeredPlaneWave
+    layers = ([4500.0, VP], [2600.0, VS], [2400.0, RHO], [4000.0])
+    box = D.BoxSpec(10, 10, 6, h=2000.0)
+    db = D.make_box(box)
+    zc = db.zstore[db.ibool].reshape(db.nspec, 125).mean(axis=1)
+    top = (zc > -4000.0)[:, None, None, None]
+    ones = np.ones(db.ibool.shape)
+    db = db.with_model(*[np.where(top, q[0], q[1]) * ones for q in layers[:3]])
+    rec = np.concatenate([D.surface_receivers(box, 4), [[7e3, 9e3, -2e3], [13e3, 11e3, -9e3]]])
+    L = LayeredPlaneWave(*layers, 15.0, 30.0, "SV", f0=0.2, t0=5.0, x0=(10e3, 10e3, -12e3))
+    v, t = injection_arrays(db, L, NSTEP, DT)
+    (seis,), _ = device(db, rec, [("inject", v, t, 1, 0)])
+    ana = np.transpose(L.displacement(rec, np.arange(NSTEP) * DT), (1, 2, 0))
+    assert rel(seis, ana) < 2e-3
+    o, _ = oracle_run(db, rec, v, t, 8)
+    assert rel(seis, o) < 1e-4

@@ -14,7 +14,12 @@ that field.  Checked here:
   incidence, within relative L2 1e-3 (2e-4 reached); a one-step time shift
   of the injected samples is 60x worse, so the check resolves one step;
 - resampled injection (every 4th step, k0 = -4, cubic interpolation);
-- exact backward reconstruction with the injection in the boundary store.
+- exact backward reconstruction with the injection in the boundary store;
+- the layered-model field (``LayeredPlaneWave``, FK3D's role): equal to
+  the closed form for one layer and for identical layers (1e-12); zero
+  free-surface traction and continuity across an interface with an
+  evanescent P layer; injected on a two-layer box, the oracle's receivers
+  match it within 2e-3 (4e-4 and 9e-4 reached).
 """
 import os
 
@@ -100,3 +105,78 @@ def test_backward_reconstruction_with_injection():
     o, seis = run(db, rec, v, t, save=True)
     _, bseis = o.adjoint(rec, np.zeros_like(seis), want_backward_seis=True)
     assert rel(bseis, seis) < 1e-10
+
+
+# --------------------------------------------------------------------------
+# layered incident field (FK3D's job): LayeredPlaneWave
+# --------------------------------------------------------------------------
+
+LAYERS = ([4500.0, VP], [2600.0, VS], [2400.0, RHO], [4000.0])
+
+
+@pytest.mark.parametrize("kind", ["P", "SV"])
+def test_layered_solver_reduces_to_the_halfspace(kind):
+    from specfwat_b200.injection import LayeredPlaneWave
+    xs = np.array([[3e3, 4e3, 0.0], [15e3, 2e3, -3e3], [9e3, 9e3, -11e3]])
+    nrm = np.array([[1.0, 0, 0], [0, -1.0, 0], [0, 0, -1.0]])
+    t = np.arange(800) * DT
+    hs = wave(kind)
+    th = 20.0 if kind == "P" else 15.0
+    for lay in (([VP], [VS], [RHO], []),
+                ([VP] * 3, [VS] * 3, [RHO] * 3, [2000.0, 5000.0])):
+        L = LayeredPlaneWave(*lay, th, 30.0, kind, f0=0.2, t0=5.0, x0=(10e3, 10e3, -12e3))
+        for a, b in ((hs.displacement(xs, t), L.displacement(xs, t)),
+                     (hs.velocity(xs, t), L.velocity(xs, t)),
+                     (hs.traction(xs, nrm, t), L.traction(xs, nrm, t))):
+            assert np.abs(a - b).max() < 1e-12 * np.abs(a).max()
+
+
+def test_layered_boundary_conditions_with_an_evanescent_layer():
+    """A fast layer (vp 8000 over a 6000 half-space) at 55 degrees: P is
+    evanescent in it.  Free-surface traction vanishes and displacement and
+    vertical traction are continuous across the interface."""
+    from specfwat_b200.injection import LayeredPlaneWave
+    L = LayeredPlaneWave([8000.0, VP], [4600.0, VS], [3000.0, RHO], [3000.0], 55.0, 10.0, "P",
+                         f0=0.2, t0=5.0, x0=(0.0, 0.0, -10e3))
+    t = np.arange(1000) * DT
+    up = np.array([[0.0, 0.0, 1.0]] * 2)
+    top = np.array([[1e3, 2e3, 0.0], [5e3, -3e3, 0.0]])
+    side = np.array([[1.0, 0.0, 0.0]] * 2)
+    assert np.isfinite(L.displacement(top, t)).all()
+    scale = np.abs(L.traction(top, side, t)).max()
+    assert np.abs(L.traction(top, up, t)).max() < 1e-9 * scale
+    eps = 1e-3
+    above = np.array([[2e3, 1e3, -3000.0 + eps]])
+    below = np.array([[2e3, 1e3, -3000.0 - eps]])
+    ua, ub = L.displacement(above, t), L.displacement(below, t)
+    assert np.abs(ua - ub).max() < 1e-6 * np.abs(ua).max()
+    ta, tb = L.traction(above, up[:1], t), L.traction(below, up[:1], t)
+    assert np.abs(ta - tb).max() < 1e-6 * np.abs(ta).max()
+
+
+def layered_box():
+    box = D.BoxSpec(10, 10, 6, h=2000.0)
+    db = D.make_box(box)
+    zc = db.zstore[db.ibool].reshape(db.nspec, 125).mean(axis=1)
+    top = (zc > -LAYERS[3][0])[:, None, None, None]
+    ones = np.ones(db.ibool.shape)
+    db = db.with_model(*[np.where(top, q[0], q[1]) * ones for q in LAYERS[:3]])
+    return box, db
+
+
+@pytest.mark.parametrize("kind", ["P", "SV"])
+def test_oracle_reproduces_the_layered_plane_wave(kind):
+    """Layer boundary at an element boundary (4 km); the layered field
+    injected on the faces must be the interior solution."""
+    from specfwat_b200.injection import LayeredPlaneWave
+    box, db = layered_box()
+    rec = np.concatenate([D.surface_receivers(box, 4), [[7e3, 9e3, -2e3], [13e3, 11e3, -9e3]]])
+    th = 20.0 if kind == "P" else 15.0
+    L = LayeredPlaneWave(*LAYERS, th, 30.0, kind, f0=0.2, t0=5.0, x0=(10e3, 10e3, -12e3))
+    nstep = 900
+    v, t = injection_arrays(db, L, nstep, DT)
+    o = Oracle(db, precision=8, nthreads=NTH)
+    o.set_injection(v, t)
+    seis = o.forward(DT, nstep, Oracle.source(10e3, 10e3, -6e3, ZERO_MT, 1.0), rec)
+    ana = np.transpose(L.displacement(rec, np.arange(nstep) * DT), (1, 2, 0))
+    assert rel(seis, ana) < 2e-3
