@@ -464,6 +464,8 @@ struct sem_run_s {
     a.store_fp16 = cfg.store_kind == SEM_STORE_FP16;
     a.nrec_max = nrec_max;
     a.lm = lm;
+    a.inject = 0;
+    for (const auto& j : inj) a.inject |= j.buf != nullptr;
     // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined;
     // 0 = chosen by the autotuner per phase
     const int v = variant[adjoint ? 1 : 0];

@@ -118,6 +118,7 @@ struct StepArgs {
   LaneMap lm;            // lane-group layout of the per-event arrays
   const int* gmap;       // serving: active 8-lane groups (device), or null
   int ngmap;
+  int inject;            // some lane has an FK injection (LaneDesc::inj_v)
   __device__ __forceinline__ size_t fi(size_t ig, int c, int lg) const {
     return lm.f(ig, c, lg, (size_t)m.nglob);
   }

@@ -2745,7 +2745,9 @@ __device__ __forceinline__ void injected(const LaneDesc* L, int it, int fp, int 
 }
 
 // Block of 128 threads = FPB faces x (32 point slots x LBB lanes).
-template <int LBB>
+// INJ: lanes may carry an FK injection (a separate instantiation, so that
+// runs without one keep the plain kernel's registers).
+template <int LBB, bool INJ>
 __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
   constexpr int FPB = 128 / (32 * LBB);
   __shared__ unsigned s_max[FPB * LBB];
@@ -2783,7 +2785,7 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
     if (absorb) {
       const float nx = A.m.f_n[fp * 3 + 0], ny = A.m.f_n[fp * 3 + 1], nz = A.m.f_n[fp * 3 + 2];
       float vi[3] = {0.f, 0.f, 0.f}, ti[3] = {0.f, 0.f, 0.f};
-      if (L->phase == PH_FWD && L->inj_v) injected(L, it, fp, nf * NGLL2, vi, ti);
+      if (INJ && L->phase == PH_FWD && L->inj_v) injected(L, it, fp, nf * NGLL2, vi, ti);
       // FK injection: Stacey on the velocity relative to the incident field,
       // plus the incident traction
       const float vx = A.f1.v[A.fi(ig, 0, lg)] - vi[0];
@@ -2844,13 +2846,22 @@ int launch_boundary(const StepArgs& a, bool adj, cudaStream_t st) {
   if (a.m.nf > 0) {
     if (a.nev == 1) {
       dim3 grid((a.m.nf + 3) / 4, 1);
-      k_stacey<1><<<grid, 128, 0, st>>>(a);
+      if (a.inject)
+        k_stacey<1, true><<<grid, 128, 0, st>>>(a);
+      else
+        k_stacey<1, false><<<grid, 128, 0, st>>>(a);
     } else if (a.nev == 2) {
       dim3 grid((a.m.nf + 1) / 2, 1);
-      k_stacey<2><<<grid, 128, 0, st>>>(a);
+      if (a.inject)
+        k_stacey<2, true><<<grid, 128, 0, st>>>(a);
+      else
+        k_stacey<2, false><<<grid, 128, 0, st>>>(a);
     } else {
       dim3 grid(a.m.nf, (a.nev + 3) / 4);
-      k_stacey<4><<<grid, 128, 0, st>>>(a);
+      if (a.inject)
+        k_stacey<4, true><<<grid, 128, 0, st>>>(a);
+      else
+        k_stacey<4, false><<<grid, 128, 0, st>>>(a);
     }
     ++n;
   }
@@ -2941,8 +2952,10 @@ __global__ void __launch_bounds__(128) k_points(StepArgs A) {
 // Newmark corrector (this step) + predictor (next step)
 // ---------------------------------------------------------------------------
 
-// One thread per (point, lane), lanes of a group fastest.
-template <bool ADJ>
+// One thread per (point, lane), lanes of a group fastest.  HESS: also
+// accumulate the approximate Hessian (a separate instantiation, so that the
+// plain adjoint update keeps its code).
+template <bool ADJ, bool HESS = false>
 __global__ void __launch_bounds__(256) k_update(StepArgs A) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nev = A.nev;
@@ -2986,8 +2999,7 @@ __global__ void __launch_bounds__(256) k_update(StepArgs A) {
     }
     A.k.rho_glob[A.gi(ig, lg)] += dt * (a[0] * bu[0] + a[1] * bu[1] + a[2] * bu[2]);
     // approximate Hessian: adjoint acceleration . backward acceleration
-    if (A.k.hess_glob)
-      A.k.hess_glob[A.gi(ig, lg)] += dt * (a[0] * ba[0] + a[1] * ba[1] + a[2] * ba[2]);
+    if (HESS) A.k.hess_glob[A.gi(ig, lg)] += dt * (a[0] * ba[0] + a[1] * ba[1] + a[2] * ba[2]);
     if (pred) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -3027,7 +3039,9 @@ int launch_update(const StepArgs& a, bool adj, cudaStream_t st) {
   const size_t n = (size_t)a.m.nglob * ng * lw;
   if (n == 0) return 0;
   const unsigned blocks = (unsigned)((n + 255) / 256);
-  if (adj)
+  if (adj && a.k.hess_glob)
+    k_update<true, true><<<blocks, 256, 0, st>>>(a);
+  else if (adj)
     k_update<true><<<blocks, 256, 0, st>>>(a);
   else
     k_update<false><<<blocks, 256, 0, st>>>(a);
