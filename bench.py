@@ -460,7 +460,7 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
     # four record lengths arriving as a Poisson stream --------------------
     served_mixed = None
     if args.served_mixed > 0 and world == 1:
-        from specfwat_b200.serving import MeshServer, Request, Server, latency_stats
+        from specfwat_b200.serving import MeshServer, Request, Server, StepCosts, latency_stats
         NR = args.served_mixed
         rng = np.random.default_rng(4242)
         lengths = tuple(NS * q // 4 for q in (1, 2, 3, 4))   # 1000 .. 4000 at NSTEP 4000
@@ -520,7 +520,20 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
                                  store=args.store, graph_steps=50,
                                  max_receivers=len(work[name][2]))
                 for name in work}
-        done = Server(servers, quantum=100, solo=solo).run(reqs, timeout=3000)
+        # routing costs from this run's own timings: the batched step per
+        # active 8-lane group and the plain one-event step, per phase,
+        # scaled to each mesh by its element count
+        step_costs = None
+        if "plain" in result:
+            pf = sum(result["plain"]["kernel_ms_fwd"].values()) / 1e3
+            pa = sum(result["plain"]["kernel_ms_adj"].values()) / 1e3
+            groups = max(1, E // 8)
+            gf, ga = sum(fms) / 1e3 / groups, sum(ams) / 1e3 / groups
+            step_costs = {}
+            for name in work:
+                w_ = work[name][0].nspec / db.nspec
+                step_costs[name] = StepCosts(pf * w_, pa * w_, gf * w_, ga * w_)
+        done = Server(servers, quantum=100, solo=solo, costs=step_costs).run(reqs, timeout=3000)
         for sv in list(servers.values()) + list(solo.values()):
             sv.close()
         st = latency_stats(done)
@@ -530,9 +543,10 @@ def _run_ours(args, torch, S, dist, world, rank, local, dev, stream):
             "nstep": list(lengths), "arrivals": "Poisson",
             "arrival_rate_per_hour": lam * 3600.0,
             "policy": (("8-lane groups" if args.mixed_policy == "group" else
-                        "any free lane, forward lanes packed away from adjoint ones")
-                       + " per mesh; a one-lane server per mesh takes requests while "
-                         "the batched one holds fewer than 4"),
+                        "any free lane in the fullest forward-only group")
+                       + " per mesh; a one-lane server per mesh takes each request "
+                       + ("predicted to finish there first (measured step costs)"
+                          if step_costs else "while the batched one holds fewer than 4")),
             **st}
         if "plain" in result:
             # the plain path, one request at a time in arrival order, with

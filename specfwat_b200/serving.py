@@ -52,6 +52,28 @@ class Request:
         return self.done - self.arrival
 
 
+@dataclasses.dataclass
+class StepCosts:
+    """Device seconds per step on one mesh, for routing: one event alone on
+    the plain path, and one active 8-lane group of the batched run (a
+    batched step costs about this times its active groups), forward and
+    adjoint phase."""
+    plain_fwd: float
+    plain_adj: float
+    group_fwd: float
+    group_adj: float
+
+    def plain(self, kind, nsteps_fwd, nsteps_adj=None):
+        """Plain-path seconds of nsteps_fwd forward steps, plus (fwd+adj
+        requests) nsteps_adj adjoint steps (default: as many)."""
+        na = nsteps_fwd if nsteps_adj is None else nsteps_adj
+        return nsteps_fwd * self.plain_fwd + (na * self.plain_adj if kind == "fwdadj" else 0.0)
+
+    def group(self, kind, nsteps):
+        """Batched seconds of a request in one active group."""
+        return nsteps * (self.group_fwd + (self.group_adj if kind == "fwdadj" else 0.0))
+
+
 class MeshServer:
     """One resident mesh and its lane-batched run."""
 
@@ -117,8 +139,9 @@ class MeshServer:
                 break
             self.queue.popleft()
             # prefer a lane whose 8-lane group runs no adjoint field, so
-            # forward lanes share the cheaper one-field launches
-            lane = min(free, key=lambda l: (self._adj_in_group(l), l))
+            # forward lanes share the cheaper one-field launches; then the
+            # fullest group, so that fewer groups are launched
+            lane = min(free, key=lambda l: (self._adj_in_group(l), -self._busy_in_group(l), l))
             self.sim.lane_start_forward(lane, req.source, req.receivers, req.nstep,
                                         save_forward=req.kind == "fwdadj")
             self.lanes[lane] = req
@@ -151,6 +174,57 @@ class MeshServer:
                 break
             started += n
         return started
+
+    def _busy_in_group(self, lane):
+        g = lane // 8
+        return sum(1 for l in range(8 * g, min(8 * g + 8, self.slots))
+                   if self.lanes[l] is not None)
+
+    def active_groups(self):
+        return len({l // 8 for l, r in enumerate(self.lanes) if r is not None})
+
+    def groups_after_admit(self):
+        """Active 8-lane groups once one more request is admitted (it goes
+        to an active group when one has a free lane), or None when no lane
+        is free."""
+        free = [l for l, r in enumerate(self.lanes) if r is None]
+        if not free:
+            return None
+        g = self.active_groups()
+        return g if any(self._busy_in_group(l) for l in free) else g + 1
+
+    def lane_free_times(self, costs: StepCosts):
+        """Sorted seconds until each busy lane frees, at the current number
+        of active groups (for the batched server)."""
+        g = max(1, self.active_groups())
+        out = []
+        for lane, req in enumerate(self.lanes):
+            if req is None:
+                continue
+            ph, st, ns = self.sim.lane_status(lane)
+            left = max(0, ns - st)
+            if ph == PH_FWD:
+                t = left * costs.group_fwd + (req.nstep * costs.group_adj
+                                              if req.kind == "fwdadj" else 0.0)
+            else:
+                t = left * costs.group_adj
+            out.append(t * g)
+        return sorted(out)
+
+    def backlog(self, costs: StepCosts):
+        """Plain-path seconds of the work queued and running here (for the
+        one-lane server)."""
+        t = sum(costs.plain(r.kind, r.nstep) for r in self.queue)
+        for lane, req in enumerate(self.lanes):
+            if req is None:
+                continue
+            ph, st, ns = self.sim.lane_status(lane)
+            left = max(0, ns - st)
+            if ph == PH_FWD:
+                t += costs.plain(req.kind, left, req.nstep)
+            elif ph == PH_ADJ:
+                t += left * costs.plain_adj
+        return t
 
     def _adj_in_group(self, lane):
         g = lane // 8
@@ -227,26 +301,47 @@ class Server:
     decisions (shortened when a lane completes sooner)."""
 
     def __init__(self, servers: Dict[str, MeshServer], quantum=100,
-                 solo: Optional[Dict[str, MeshServer]] = None, solo_below=4):
+                 solo: Optional[Dict[str, MeshServer]] = None, solo_below=4,
+                 costs: Optional[Dict[str, StepCosts]] = None):
         self.servers = servers
         self.quantum = quantum
         # Optional one-lane server per mesh (the plain one-event kernels).
         # A lone request in an 8-lane group costs the whole group's
-        # launches, about four times the one-event path; so while the
-        # batched server of its mesh holds fewer than `solo_below` requests
-        # (running or queued) and the solo server is free, an arriving
-        # request takes the solo server instead.
+        # launches, about four times the one-event path.  Without step
+        # costs: while the batched server of its mesh holds fewer than
+        # `solo_below` requests (running or queued) and the solo server is
+        # free, an arriving request takes the solo server.  With step costs
+        # per mesh: the request goes where it is predicted to finish first,
+        # the solo server's backlog plus its plain time against its batched
+        # time at the group count its admission leaves (plus the wait for
+        # a lane when none is free).  A short burst is then served mostly
+        # one event at a time and a sustained load mostly batched.
         self.solo = solo or {}
         self.solo_below = solo_below
+        self.costs = costs or {}
 
     def _route(self, req):
         batched = self.servers[req.mesh]
         solo = self.solo.get(req.mesh)
-        if solo is not None and not solo.busy() and not solo.queue:
-            load = sum(1 for r in batched.lanes if r is not None) + len(batched.queue)
-            if load < self.solo_below:
-                return solo
-        return batched
+        if solo is None:
+            return batched
+        c = self.costs.get(req.mesh)
+        if c is None:
+            if not solo.busy() and not solo.queue:
+                load = sum(1 for r in batched.lanes if r is not None) + len(batched.queue)
+                if load < self.solo_below:
+                    return solo
+            return batched
+        t_solo = solo.backlog(c) + c.plain(req.kind, req.nstep)
+        g = batched.groups_after_admit()
+        if g is not None and not batched.queue:
+            t_batched = c.group(req.kind, req.nstep) * g
+        else:
+            # wait for a lane: the (queued + 1)-th lane to free
+            free_at = batched.lane_free_times(c) or [0.0]
+            wait = free_at[min(len(batched.queue), len(free_at) - 1)]
+            t_batched = wait + c.group(req.kind, req.nstep) * max(1, batched.active_groups())
+        return solo if t_solo <= t_batched else batched
 
     def _all(self):
         return list(self.servers.values()) + list(self.solo.values())
