@@ -1450,15 +1450,37 @@ int sem_sum_kernels_device(sem_run* r, double* dev_out) {
   return SEM_OK;
 }
 
+// A captured step graph holds the kernel instantiations and the step
+// arguments of its capture (the Hessian update and accumulator, the
+// injecting Stacey kernel); a switch that changes them drops the graphs,
+// and the next run of each phase captures its graph again.
+static int drop_graphs(sem_run* r) {
+  if (!r->gexec[0] && !r->gexec[1]) return SEM_OK;
+  CK(cudaStreamSynchronize(r->stream));
+  for (auto& g : r->gexec)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  return SEM_OK;
+}
+
+static bool any_injection(const sem_run* r) {
+  for (const auto& j : r->inj)
+    if (j.buf) return true;
+  return false;
+}
+
 int sem_set_approximate_hessian(sem_run* r, int enable) {
   if (!r) return fail(SEM_ERR_ARG, "null run");
+  const bool was = r->hess_on;
   r->hess_on = enable != 0;
   if (r->hess_on && r->k_rho.p) {
     // adjoint buffers exist already (an earlier adjoint run or lane start)
     int rc = ensure_adjoint_buffers(r);
     if (rc) return rc;
   }
-  return SEM_OK;
+  return was != r->hess_on ? drop_graphs(r) : SEM_OK;
 }
 
 int sem_save_hessian_kernel(sem_run* r, int ev, double* out) {
@@ -1498,13 +1520,14 @@ int sem_set_injection(sem_run* r, int ev, const float* veloc, const float* tract
   if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
   if (r->lanes_mode) return fail(SEM_ERR_STATE, "run is driven lane by lane (sem_lane_*)");
   auto& j = r->inj[ev];
+  const bool before = any_injection(r);
   if (!veloc) {
     if (j.buf) {
       CK(cudaStreamSynchronize(r->stream));
       cudaFree(j.buf);
     }
     j = sem_run_s::Injection{};
-    return SEM_OK;
+    return before != any_injection(r) ? drop_graphs(r) : SEM_OK;
   }
   if (!tract) return fail(SEM_ERR_ARG, "null traction");
   if (r->mesh->nf == 0) return fail(SEM_ERR_STATE, "the mesh has no absorbing faces");
@@ -1534,7 +1557,7 @@ int sem_set_injection(sem_run* r, int ev, const float* veloc, const float* tract
   CK(cudaMemcpyAsync(j.buf, veloc, n * 4, cudaMemcpyHostToDevice, r->stream));
   CK(cudaMemcpyAsync(j.buf + n, tract, n * 4, cudaMemcpyHostToDevice, r->stream));
   CK(cudaStreamSynchronize(r->stream));
-  return SEM_OK;
+  return before ? SEM_OK : drop_graphs(r);
 }
 
 int sem_set_stream(sem_run* r, void* stream) {

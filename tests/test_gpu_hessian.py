@@ -156,3 +156,24 @@ def test_depth_precond_matches_oracle(gpu, ptype):
     with pytest.raises(_lib.SemError, match="depth forms"):
         depth_precond(mesh, zlev, 1, 5)
     mesh.close()
+
+
+def test_hessian_enabled_after_a_captured_adjoint_graph(gpu, box_case):
+    """The adjoint step graph is captured by a first adjoint run without the
+    Hessian; switching it on must take effect in the next adjoint run."""
+    db, rec, srcs, obs = box_case
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, NSTEP, DT, nev=1, max_receivers=len(rec), use_graph=True,
+                       graph_steps=40)
+    sim.set_sources([S.make_source(*srcs[0])])
+    sim.set_receivers(rec)
+    for hess in (False, True):
+        sim.iterate_time(1, save_forward=True)
+        sim.measure_l2(0, obs[0], 0.05, 1)
+        sim.set_approximate_hessian(hess)
+        sim.iterate_time(3)
+    h = sim.hessian_kernel(0)
+    sim.close()
+    mesh.close()
+    ref = oracle_hessians(db, rec, srcs[0], obs[0], 8)
+    assert rel(h, ref) < KERN_TOL

@@ -163,3 +163,29 @@ def test_layered_box_reproduces_the_layered_field(gpu):
     assert rel(seis, ana) < 2e-3
     o, _ = oracle_run(db, rec, v, t, 8)
     assert rel(seis, o) < 1e-4
+
+
+def test_injection_set_after_a_captured_forward_graph(gpu, case):
+    """A forward step graph captured without an injection is dropped when
+    one is set, so the next forward run injects."""
+    box, db, rec, waves = case
+    w = waves["P"]
+    v, t = injection_arrays(db, w, NSTEP, DT)
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, NSTEP, DT, nev=1, max_receivers=len(rec), use_graph=True,
+                       graph_steps=40)
+    sim.set_sources([S.make_source(*SRC_XYZ, ZERO_MT, 1.0)])
+    sim.set_receivers(rec)
+    sim.iterate_time(1)
+    assert np.abs(sim.seismograms(0)).max() == 0.0
+    sim.set_injection(0, v, t)
+    sim.iterate_time(1)
+    seis = sim.seismograms(0)
+    sim.set_injection(0, None, None)
+    sim.iterate_time(1)
+    after = sim.seismograms(0)
+    sim.close()
+    mesh.close()
+    ana = np.transpose(w.displacement(rec, np.arange(NSTEP) * DT), (1, 2, 0))
+    assert rel(seis, ana) < 1e-3
+    assert np.abs(after).max() == 0.0
