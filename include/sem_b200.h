@@ -398,7 +398,9 @@ int sem_smooth_pde(sem_mesh *mesh, const sem_smooth_cfg *cfg, int nfield,
  * with tract = sigma . n for the outward normal; the boundary store saves
  * that term, so the backward reconstruction replays it.  An event with an
  * injection needs no point source.  veloc = NULL removes it.  Batched runs
- * (sem_iterate_time) only. */
+ * (sem_iterate_time) only.  Setting the first injection or removing the last
+ * one drops the run's captured step graphs, so that the next run of each
+ * phase captures the matching kernels. */
 int sem_set_injection(sem_run *run, int ev, const float *veloc, const float *tract, int nt,
                       int np_resamp, int k0);
 
@@ -408,7 +410,8 @@ int sem_set_injection(sem_run *run, int ev, const float *veloc, const float *tra
  * sim_type 3 run, the adjoint run also accumulates per GLL point
  *     hess = 2 * sum_it DT * (adjoint accel . backward accel).
  * Batched runs (sem_iterate_time) only; lanes driven by sem_lane_* do not
- * hand it back.  Costs 8 bytes per point and event and step. */
+ * hand it back.  Costs 8 bytes per point and event and step.  Changing the
+ * switch drops the run's captured step graphs (recaptured at the next run). */
 int sem_set_approximate_hessian(sem_run *run, int enable);
 /* hess_kernel of event ev: out[nspec][125]. */
 int sem_save_hessian_kernel(sem_run *run, int ev, double *out);
