@@ -5,7 +5,8 @@ cannot be run here, so the oracle is pinned by properties the continuous
 and discrete problems must have: energy conservation, exact time
 reversibility of the backward reconstruction, the analytic full-space
 moment-tensor Green's function, agreement of the adjoint kernels with
-finite differences of the misfit, and FP32/FP64 agreement.
+finite differences of the misfit, FP32/FP64 agreement, and source-receiver
+reciprocity.
 """
 import os
 
@@ -170,3 +171,37 @@ def test_golden_forward_regression():
     seis = Oracle(db, precision=8, nthreads=1).forward(
         0.02, 200, Oracle.source(8000.0, 8000.0, -6000.0, gold["mt"], 1.0), gold["rec"])
     assert np.allclose(seis, gold["seis"], rtol=1e-12, atol=1e-20)
+
+
+@pytest.mark.parametrize("topo", [False, True])
+def test_source_receiver_reciprocity(topo):
+    """A point force in direction i at x_a recorded in direction j at x_b
+    equals a force in j at x_b recorded in i at x_a.  The adjoint run
+    injects the force (an adjoint source at a receiver, with the same
+    Lagrange weights that record it), and the discrete operator is
+    symmetric: diagonal mass with the Stacey term folded in, symmetric
+    stiffness (regular and general mapping alike) and symmetric Stacey
+    damping.  So the two traces agree to round-off in FP64."""
+    box = D.BoxSpec(5, 5, 4)
+    db = D.make_box(box, topo=D.hill_topography(box, 2000.0, 6000.0) if topo else None)
+    db = db.with_model(*D.background_model(db, seed=21))
+    rec = np.array([[6300.0, 7100.0, -5200.0], [13700.0, 12900.0, -9800.0]])
+    n, dt = 300, 0.02
+    g = np.exp(-((np.arange(n) * dt - 1.5) / 0.4) ** 2)
+    mt = D.random_moment_tensor(np.random.default_rng(2))
+
+    def force_run(r, c):
+        o = Oracle(db, precision=8, nthreads=NTH)
+        o.forward(dt, n, Oracle.source(9000., 11000., -7000., mt, 1.0), rec, save_forward=True)
+        adj = np.zeros((2, 3, n))
+        adj[r, c] = g[::-1]              # injected in adjoint time order
+        _, aseis = o.adjoint(rec, adj, want_adjoint_seis=True)
+        return aseis
+
+    at_a = [force_run(0, i) for i in range(3)]
+    at_b = [force_run(1, j) for j in range(3)]
+    for i in range(3):
+        for j in range(3):
+            ab, ba = at_a[i][1, j], at_b[j][0, i]
+            assert np.abs(ab).max() > 0
+            assert np.abs(ab - ba).max() <= 1e-12 * np.abs(ab).max(), (i, j)
