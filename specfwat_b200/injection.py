@@ -317,3 +317,73 @@ class LayeredPlaneWave:
 
     def traction(self, xyz, normals, t):
         return self._fields(xyz, t, normals, what="t")
+
+
+def read_fkmodel(path):
+    """The keyword file the reference names ``src_rec/FKmodel_<event>``
+    (``read_fk_model``, src/shared/fk_coupling.f90:12-59): ``NLAYER n``,
+    ``LAYER i rho vp vs ztop`` per layer from the top (the last one the
+    half-space, its ``ztop`` the half-space's top), ``INCIDENT_WAVE p|sv``,
+    ``BACK_AZIMUTH`` and ``TAKE_OFF`` in degrees, ``FREQUENCY_MAX``,
+    ``TIME_WINDOW``, and optionally ``FREQUENCY_SAMPLING``, ``AMPLITUDE``,
+    ``ORIGIN_WAVEFRONT x y z`` and ``ORIGIN_TIME``.  ``#`` starts a
+    comment.  Returns a dict with those values (layers as arrays)."""
+    d = {"layers": {}}
+    with open(path) as f:
+        for raw in f:
+            line = raw.split("#", 1)[0].strip()
+            if not line:
+                continue
+            key, *vals = line.split()
+            key = key.upper()
+            if key == "LAYER":
+                i, rho, vp, vs, ztop = vals[:5]
+                d["layers"][int(i)] = (float(rho), float(vp), float(vs), float(ztop))
+            elif key == "NLAYER":
+                d["nlayer"] = int(vals[0])
+            elif key == "INCIDENT_WAVE":
+                d["wave"] = vals[0].upper()
+            elif key == "ORIGIN_WAVEFRONT":
+                d["origin_wavefront"] = tuple(float(v) for v in vals[:3])
+            elif key in ("BACK_AZIMUTH", "TAKE_OFF", "FREQUENCY_MAX", "FREQUENCY_SAMPLING",
+                         "TIME_WINDOW", "AMPLITUDE", "ORIGIN_TIME"):
+                d[key.lower()] = float(vals[0])
+    n = d.get("nlayer", len(d["layers"]))
+    if sorted(d["layers"]) != list(range(1, n + 1)):
+        raise ValueError(f"{path}: LAYER lines 1..{n} expected, got {sorted(d['layers'])}")
+    lay = np.array([d["layers"][i] for i in range(1, n + 1)], np.float64)
+    if np.any(np.diff(lay[:, 3]) >= 0):
+        raise ValueError(f"{path}: layer tops must decrease downward")
+    d["rho"], d["vp"], d["vs"], d["ztop"] = lay[:, 0], lay[:, 1], lay[:, 2], lay[:, 3]
+    for k in ("wave", "back_azimuth", "take_off"):
+        if k not in d:
+            raise ValueError(f"{path}: {k.upper()} missing")
+    if d["wave"] not in ("P", "SV"):
+        raise ValueError(f"{path}: INCIDENT_WAVE must be p or sv")
+    return d
+
+
+def plane_wave_from_fkmodel(fk, x0=None, t0=None):
+    """``LayeredPlaneWave`` of an ``read_fkmodel`` dict.
+
+    - The propagation azimuth measured from +x (east) counter-clockwise is
+      ``-90 - BACK_AZIMUTH`` degrees (a wave from the back azimuth travels
+      the opposite way).
+    - The layer thicknesses are the differences of the layer tops; the free
+      surface is the first layer's top.
+    - ``FREQUENCY_MAX`` sets the Gaussian time function's ``f0``.  The
+      reference's FK code (absent here) defines its own wavelet.
+    - ``ORIGIN_WAVEFRONT`` and ``ORIGIN_TIME`` give ``x0`` and ``t0`` unless
+      passed here; without either the call fails.
+    """
+    if x0 is None:
+        if "origin_wavefront" not in fk:
+            raise ValueError("no ORIGIN_WAVEFRONT in the file: pass x0")
+        x0 = fk["origin_wavefront"]
+    if t0 is None:
+        t0 = fk.get("origin_time", 0.0)
+    h = -np.diff(fk["ztop"])
+    return LayeredPlaneWave(fk["vp"], fk["vs"], fk["rho"], h, fk["take_off"],
+                            -90.0 - fk["back_azimuth"], fk["wave"],
+                            f0=fk.get("frequency_max", 0.2), t0=t0, x0=x0,
+                            z_top=float(fk["ztop"][0]), amplitude=fk.get("amplitude", 1.0))
