@@ -80,14 +80,22 @@ def read_external_mesh(path, *, ocean_load=False, pml=False, stacey=True, anisot
     lists; arrays are flat (Fortran order) except the counts."""
     r = _Records(path)
     d = {}
+
+    def sized(name, arr, n, hint=""):
+        if arr.size != n:
+            raise ValueError(f"{path}: record {name} holds {arr.size} values, {n} expected"
+                             + (f" ({hint})" if hint else ""))
+        return arr
+
     try:
         # :158-189
         d["NSPEC_AB"] = r.int()
         d["NGLOB_AB"] = r.int()
         d["NSPEC_IRREGULAR"] = r.int()
-        d["ibool"] = r.i4()
+        ne = d["NSPEC_AB"] * NGLL3
+        d["ibool"] = sized("ibool", r.i4(), ne)
         for k in ("xstore", "ystore", "zstore"):
-            d[k] = r.f4()
+            d[k] = sized(k, r.f4(), d["NGLOB_AB"])
         d["irregular_element_number"] = r.i4()
         d["xix_regular"] = float(r.f4()[0])
         d["jacobian_regular"] = float(r.f4()[0])
@@ -191,12 +199,14 @@ def read_external_mesh(path, *, ocean_load=False, pml=False, stacey=True, anisot
             for k in ("c11", "c12", "c13", "c14", "c15", "c16", "c22", "c23", "c24", "c25",
                       "c26", "c33", "c34", "c35", "c36", "c44", "c45", "c46", "c55", "c56",
                       "c66"):
-                d[k + "store"] = r.f4()
-        d["ispec_is_inner"] = r.logical()
+                d[k + "store"] = sized(k + "store", r.f4(), ne, "check the ANISOTROPY switch")
+        # no check word follows: the sizes catch a wrong ANISOTROPY switch
+        d["ispec_is_inner"] = sized("ispec_is_inner", r.logical(), d["NSPEC_AB"],
+                                    "check the ANISOTROPY switch")
         for kind, present in (("acoustic", acoustic), ("elastic", elastic),
                               ("poroelastic", poro)):
             if present:
-                inner_outer = r.i4()
+                inner_outer = sized(f"nspec_inner/outer_{kind}", r.i4(), 2)
                 d[f"nspec_inner_{kind}"], d[f"nspec_outer_{kind}"] = (int(inner_outer[0]),
                                                                       int(inner_outer[1]))
                 n = d[f"num_phase_ispec_{kind}"] = r.int()
@@ -271,12 +281,33 @@ class _Writer:
         self.f.close()
 
 
-def write_external_mesh(path, db: Database, *, dt=None, free_surface=None):
+CPML_ARRAYS = ("d_store_x", "d_store_y", "d_store_z", "k_store_x", "k_store_y", "k_store_z",
+               "alpha_store_x", "alpha_store_y", "alpha_store_z")
+ANISO_NAMES = ("c11", "c12", "c13", "c14", "c15", "c16", "c22", "c23", "c24", "c25", "c26",
+               "c33", "c34", "c35", "c36", "c44", "c45", "c46", "c55", "c56", "c66")
+IBELM_NAMES = ("ibelm_xmin", "ibelm_xmax", "ibelm_ymin", "ibelm_ymax", "ibelm_bottom",
+               "ibelm_top")
+
+
+def write_external_mesh(path, db: Database, *, dt=None, free_surface=None, ocean_load=None,
+                        cpml=None, interfaces=None, anisotropy=None, ibelm=None):
     """Write an elastic single-slice database in the record order
-    read_mesh_databases.f90 reads (no PML, no MPI interfaces, isotropic,
-    Stacey on).  ``rmassx/y/z`` carry the Stacey term ``dt/2 C`` when
-    ``dt`` is given, else the plain mass.  ``free_surface``: optional
-    (ispec, ijk, jw, normal) of the free-surface faces, 0-based."""
+    read_mesh_databases.f90 reads (Stacey on).  ``rmassx/y/z`` carry the
+    Stacey term ``dt/2 C`` when ``dt`` is given, else the plain mass.
+
+    Optional record groups, each read only under the matching switch of
+    ``read_external_mesh`` (indices 0-based here, written 1-based):
+    - ``free_surface``: (ispec, ijk, jw, normal) of the free-surface faces;
+    - ``ocean_load``: ``rmass_ocean_load`` [nglob] (APPROXIMATE_OCEAN_LOAD);
+    - ``cpml``: dict with ``NSPEC_CPML``, the three ``CPML_width_*``,
+      ``min_distance_between_CPML_parameter``, ``CPML_regions``,
+      ``CPML_to_spec``, ``is_CPML`` [nspec], the nine damping arrays and
+      ``points_interface_PML_elastic`` (PML_CONDITIONS; the Stacey mass
+      records are then absent, as the reader expects);
+    - ``interfaces``: (my_neighbors, nibool, ibool_interfaces) of the MPI
+      interfaces;
+    - ``anisotropy``: dict ``c11`` .. ``c66`` of element arrays (ANISOTROPY);
+    - ``ibelm``: dict ``ibelm_xmin`` .. ``ibelm_top`` of element lists."""
     nspec, nglob = db.nspec, db.nglob
     nirr = db.nspec_irregular
     w = _Writer(path)
@@ -302,8 +333,26 @@ def write_external_mesh(path, db: Database, *, dt=None, free_surface=None):
         w.i4(np.zeros(nspec))           # ispec_is_poroelastic
         w.i4([9999])
         w.f4(db.rmass)
+        if ocean_load is not None:
+            w.f4(ocean_load)
         w.f4(np.asarray(db.rho_vp).reshape(-1))
         w.f4(np.asarray(db.rho_vs).reshape(-1))
+        if cpml is not None:
+            w.i4([cpml["NSPEC_CPML"]])
+            for k in ("CPML_width_x", "CPML_width_y", "CPML_width_z",
+                      "min_distance_between_CPML_parameter"):
+                w.f4([cpml[k]])
+            if cpml["NSPEC_CPML"] > 0:
+                w.i4(cpml["CPML_regions"])
+                w.i4(np.asarray(cpml["CPML_to_spec"]) + 1)
+                w.i4(np.asarray(cpml["is_CPML"], np.int32))
+                for k in CPML_ARRAYS:
+                    w.f4(np.asarray(cpml[k]).reshape(-1))
+                pts = np.asarray(cpml.get("points_interface_PML_elastic", []), np.int64)
+                w.i4([0])                       # nglob_interface_PML_acoustic
+                w.i4([pts.size])                # nglob_interface_PML_elastic
+                if pts.size:
+                    w.i4(pts + 1)
         nf = db.nfaces
         w.i4([nf])
         if nf > 0:
@@ -324,11 +373,16 @@ def write_external_mesh(path, db: Database, *, dt=None, free_surface=None):
                 for c in range(3):
                     term = 0.5 * dt * db.abs_jw * (rvp * n[..., c] ** 2 + rvs * (1 - n[..., c] ** 2))
                     np.add.at(rm[:, c], ig.reshape(-1), term.reshape(-1))
-            for c in range(3):
-                w.f4(rm[:, c])
+            if cpml is None:
+                for c in range(3):
+                    w.f4(rm[:, c])
         w.i4([9998])
-        for _ in range(6):              # nspec2D_xmin .. NSPEC2D_TOP
-            w.i4([0])
+        ib = ibelm or {}
+        for k in IBELM_NAMES:           # nspec2D_xmin .. NSPEC2D_TOP
+            w.i4([len(ib.get(k, []))])
+        for k in IBELM_NAMES:
+            if len(ib.get(k, [])):
+                w.i4(np.asarray(ib[k]) + 1)
         if free_surface is not None:
             fs_ispec, fs_ijk, fs_jw, fs_n = free_surface
             w.i4([len(fs_ispec)])
@@ -342,9 +396,20 @@ def write_external_mesh(path, db: Database, *, dt=None, free_surface=None):
         w.i4([0])                       # coupling acoustic-poroelastic
         w.i4([0])                       # coupling elastic-poroelastic
         w.i4([9997])
-        w.i4([0])                       # num_interfaces_ext_mesh
-        w.i4([0])                       # max_nibool_interfaces_ext_mesh
+        if interfaces is not None:
+            nb, nib, ibi = interfaces
+            w.i4([len(nb)])
+            w.i4([int(np.max(nib))])
+            w.i4(nb)
+            w.i4(nib)
+            w.i4(np.asarray(ibi).reshape(-1) + 1)
+        else:
+            w.i4([0])                   # num_interfaces_ext_mesh
+            w.i4([0])                   # max_nibool_interfaces_ext_mesh
         w.i4([9996])
+        if anisotropy is not None:
+            for k in ANISO_NAMES:
+                w.f4(np.asarray(anisotropy[k]).reshape(-1))
         w.i4(np.ones(nspec))            # ispec_is_inner
         w.i4([nspec, 0])                # nspec_inner_elastic, nspec_outer_elastic
         w.i4([nspec])                   # num_phase_ispec_elastic

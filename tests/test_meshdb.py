@@ -84,3 +84,59 @@ def test_wrong_switches_and_broken_files(tmp_path):
     short.write_bytes(path.read_bytes()[:1000])
     with pytest.raises(ValueError):
         read_external_mesh(short)
+
+
+def test_optional_record_groups(tmp_path):
+    """Ocean load, C-PML, element face lists, MPI interfaces and anisotropy
+    records, each read under the reference's switch; the solver's
+    conversion refuses the C-PML and anisotropic slices."""
+    _, dbs = box_dbs()
+    db = dbs["regular"]
+    ne = db.nspec * 125
+    rng = np.random.default_rng(1)
+    ocean = rng.random(db.nglob).astype(np.float32)
+    ncp = 5
+    cpml = {"NSPEC_CPML": ncp, "CPML_width_x": 4000.0, "CPML_width_y": 4000.0,
+            "CPML_width_z": 2000.0, "min_distance_between_CPML_parameter": 100.0,
+            "CPML_regions": np.arange(1, ncp + 1), "CPML_to_spec": np.arange(ncp),
+            "is_CPML": np.arange(db.nspec) < ncp,
+            "points_interface_PML_elastic": np.arange(7)}
+    for k in ("d_store_x", "d_store_y", "d_store_z", "k_store_x", "k_store_y", "k_store_z",
+              "alpha_store_x", "alpha_store_y", "alpha_store_z"):
+        cpml[k] = rng.random(ncp * 125).astype(np.float32)
+    interfaces = ([1, 2], [3, 2], np.array([[0, 1, 2], [5, 6, 0]]))
+    aniso = {k: rng.random(ne).astype(np.float32) for k in
+             ("c11", "c12", "c13", "c14", "c15", "c16", "c22", "c23", "c24", "c25", "c26",
+              "c33", "c34", "c35", "c36", "c44", "c45", "c46", "c55", "c56", "c66")}
+    ibelm = {"ibelm_xmin": [0, 3], "ibelm_top": [7, 8, 9]}
+    path = tmp_path / "m.bin"
+    write_external_mesh(path, db, ocean_load=ocean, cpml=cpml, interfaces=interfaces,
+                        anisotropy=aniso, ibelm=ibelm)
+    rec = read_external_mesh(path, ocean_load=True, pml=True, anisotropy=True)
+    assert np.array_equal(rec["rmass_ocean_load"], ocean)
+    assert rec["NSPEC_CPML"] == ncp and rec["CPML_width_z"] == 2000.0
+    assert np.array_equal(rec["CPML_to_spec"], np.arange(1, ncp + 1))
+    assert np.array_equal(rec["is_CPML"], cpml["is_CPML"])
+    assert np.array_equal(rec["alpha_store_y"], cpml["alpha_store_y"])
+    assert np.array_equal(rec["points_interface_PML_elastic"], np.arange(1, 8))
+    assert "rmassx" not in rec                       # no Stacey mass under C-PML
+    assert rec["nspec2D_xmin"] == 2 and rec["NSPEC2D_TOP"] == 3
+    assert np.array_equal(rec["ibelm_top"], [8, 9, 10]) and "ibelm_ymin" not in rec
+    assert rec["num_interfaces_ext_mesh"] == 2 and rec["max_nibool_interfaces_ext_mesh"] == 3
+    assert np.array_equal(rec["ibool_interfaces_ext_mesh"], [1, 2, 3, 6, 7, 1])
+    assert np.array_equal(rec["c46store"], aniso["c46"])
+    assert rec["num_phase_ispec_elastic"] == db.nspec
+    with pytest.raises(ValueError, match="C-PML"):
+        to_database(rec)
+    # the same file read with a switch off stops at a check word
+    for kw in ({"ocean_load": False, "pml": True, "anisotropy": True},
+               {"ocean_load": True, "pml": False, "anisotropy": True}):
+        with pytest.raises(ValueError):
+            read_external_mesh(path, **kw)
+    # past the last check word: the record sizes catch the ANISOTROPY switch
+    with pytest.raises(ValueError, match="ANISOTROPY"):
+        read_external_mesh(path, ocean_load=True, pml=True, anisotropy=False)
+    plain = tmp_path / "plain.bin"
+    write_external_mesh(plain, db)
+    with pytest.raises(ValueError, match="ANISOTROPY"):
+        read_external_mesh(plain, anisotropy=True)
