@@ -11,6 +11,11 @@ the golden vectors in this directory:
 * ``invert_hess``  src/postproc/post_processing.f90:333-372 (FP32)
 * ``interp1_0``    src/shared/utils.f90:889-910
 * ``get_1d_precond``, ``zprecond_gll`` src/postproc/zprecond.f90:11-71 (FP32)
+* ``coswin``, ``create_taper``  src/postproc/taper_3D_mod.f90 (FP32)
+* ``locate_bissection``, ``interp3``  src/shared/utils.f90:1089-1159,1490-1525
+* ``project_sem2fd``: compute_interpolation_coeff_FD_SEM + Project_model_
+  SEM2FD_grid (src/shared/projection_on_FD_grid_mod_fwat.f90:186-596), one
+  slice, regular elements (reference coordinates linear in x, y, z)
 """
 import math
 
@@ -467,3 +472,147 @@ def zprecond_gll(ibool, zstore, zgrid, precond_type, nevents):
     h = [f(f(1.0) / x) for x in h]
     maxh = max(f(abs(x)) for x in h)
     return [f(x / maxh) for x in h]
+
+
+def coswin(n, opt):
+    import numpy as np
+    f = np.float32
+    nn = 2 * n + 1
+    win = [f(0.5) - f(0.5) * f(np.cos(f(2.0) * f(3.1415926535) * f(i - 1) / f(nn - 1)))
+           for i in range(1, nn + 1)]
+    return win[0:n] if opt == 1 else win[n + 1:nn]
+
+
+def create_taper(taph1, taph2, tapz1, tapz2, hx, hy, hz, nx, ny, nz):
+    import numpy as np
+    f = np.float32
+    xt = [f(0.0)] * (nx + 1)
+    yt = [f(0.0)] * (ny + 1)
+    zt = [f(0.0)] * (nz + 1)
+    nh1 = int(np.floor(f(taph1) / f(hx)))
+    nh2 = int(np.floor(f(taph2) / f(hx)))
+    x1, x2, x3, x4 = nh1 + 1, nh1 + nh2 + 1, nx - nh1 - nh2, nx - nh1
+    for q, v in zip(range(x1, x2), coswin(nh2, 1)):
+        xt[q] = v
+    for q, v in zip(range(x3 + 1, x4 + 1), coswin(nh2, 0)):
+        xt[q] = v
+    for q in range(x2, x3 + 1):
+        xt[q] = f(1.0)
+    nh1 = int(np.floor(f(taph1) / f(hy)))
+    nh2 = int(np.floor(f(taph2) / f(hy)))
+    y1, y2, y3, y4 = nh1 + 1, nh1 + nh2 + 1, ny - nh1 - nh2, ny - nh1
+    for q, v in zip(range(y1, y2), coswin(nh2, 1)):
+        yt[q] = v
+    for q, v in zip(range(y3 + 1, y4 + 1), coswin(nh2, 0)):
+        yt[q] = v
+    for q in range(y2, y3 + 1):
+        yt[q] = f(1.0)
+    nh1 = int(np.floor(f(tapz1) / f(hz)))
+    nh2 = int(np.floor(f(tapz2) / f(hz)))
+    z1 = nh1 + nh2 + 1
+    for q, v in zip(range(nh1 + 1, z1), coswin(nh2, 1)):
+        zt[q] = v
+    for q in range(z1, nz + 1):
+        zt[q] = f(1.0)
+    out = np.zeros((nx, ny, nz), np.float32)
+    for k in range(1, nz + 1):
+        for j in range(1, ny + 1):
+            for i in range(1, nx + 1):
+                out[i - 1, j - 1, k - 1] = xt[i] * yt[j] * zt[k]
+    return out
+
+
+def locate_bissection(valx, n, x):
+    if x < valx[0] or x > valx[n - 1]:
+        return -1
+    jl, ju = 0, n + 1
+    while ju - jl > 1:
+        jm = (ju + jl) // 2
+        if x >= valx[jm - 1]:
+            jl = jm
+        else:
+            ju = jm
+    if x == valx[0]:
+        return 1
+    if x == valx[n - 1]:
+        return n - 1
+    return jl
+
+
+def interp3(valx, valy, valz, valin, x, y, z):
+    nx, ny, nz = len(valx), len(valy), len(valz)
+    indx = locate_bissection(valx, nx, x)
+    indy = locate_bissection(valy, ny, y)
+    indz = locate_bissection(valz, nz, z)
+    kx = min(max(indx, 1), nx - 1)
+    ky = min(max(indy, 1), ny - 1)
+    kz = min(max(indz, 1), nz - 1)
+    X = lambda q: valx[q - 1]  # noqa: E731
+    Y = lambda q: valy[q - 1]  # noqa: E731
+    Z = lambda q: valz[q - 1]  # noqa: E731
+    V = lambda a, b, c: valin[a - 1][b - 1][c - 1]  # noqa: E731
+    xix1, yiy1, ziz1 = x - X(kx), y - Y(ky), z - Z(kz)
+    xix2, yiy2, ziz2 = x - X(kx + 1), y - Y(ky + 1), z - Z(kz + 1)
+    x1x2, y1y2, z1z2 = 1.0 / (X(kx) - X(kx + 1)), 1.0 / (Y(ky) - Y(ky + 1)), 1.0 / (Z(kz) - Z(kz + 1))
+    x2x1, y2y1, z2z1 = 1.0 / (X(kx + 1) - X(kx)), 1.0 / (Y(ky + 1) - Y(ky)), 1.0 / (Z(kz + 1) - Z(kz))
+    return (xix2 * yiy2 * ziz2 * x1x2 * y1y2 * z1z2 * V(kx, ky, kz)
+            + xix2 * yiy2 * ziz1 * x1x2 * y1y2 * z2z1 * V(kx, ky, kz + 1)
+            + xix2 * yiy1 * ziz2 * x1x2 * y2y1 * z1z2 * V(kx, ky + 1, kz)
+            + xix2 * yiy1 * ziz1 * x1x2 * y2y1 * z2z1 * V(kx, ky + 1, kz + 1)
+            + xix1 * yiy2 * ziz2 * x2x1 * y1y2 * z1z2 * V(kx + 1, ky, kz)
+            + xix1 * yiy2 * ziz1 * x2x1 * y1y2 * z2z1 * V(kx + 1, ky, kz + 1)
+            + xix1 * yiy1 * ziz2 * x2x1 * y2y1 * z1z2 * V(kx + 1, ky + 1, kz)
+            + xix1 * yiy1 * ziz1 * x2x1 * y2y1 * z2z1 * V(kx + 1, ky + 1, kz + 1))
+
+
+def project_sem2fd(ibool, xstore, ystore, zstore, nspec, data, ox, oy, oz, hx, hy, hz,
+                   nx, ny, nz):
+    """ibool: flat 1-based (i fastest); data: flat element values in the
+    same order.  Returns the grid as nested lists [nx][ny][nz]."""
+    import math
+    xg = [-1.0, -math.sqrt(3.0 / 7.0), 0.0, math.sqrt(3.0 / 7.0), 1.0]
+
+    def lag(x):
+        out = []
+        for i in range(5):
+            v = 1.0
+            for m in range(5):
+                if m != i:
+                    v *= (x - xg[m]) / (xg[i] - xg[m])
+            out.append(v)
+        return out
+    found = {}
+    for ispec in range(1, nspec + 1):
+        xs = [xstore[ibool[(ispec - 1) * 125 + q] - 1] for q in range(125)]
+        ys = [ystore[ibool[(ispec - 1) * 125 + q] - 1] for q in range(125)]
+        zs = [zstore[ibool[(ispec - 1) * 125 + q] - 1] for q in range(125)]
+        xmin, xmax, ymin, ymax = min(xs), max(xs), min(ys), max(ys)
+        zmin, zmax = min(zs), max(zs)
+        kmin, kmax = int(1 + (zmin - oz) / hz), int(1 + (zmax - oz) / hz)
+        jmin, jmax = int(1 + (ymin - oy) / hy), int(1 + (ymax - oy) / hy)
+        imin, imax = int(1 + (xmin - ox) / hx), int(1 + (xmax - ox) / hx)
+        for kfd in range(kmin, kmax + 1):
+            zfd = oz + (kfd - 1) * hz
+            for jfd in range(jmin, jmax + 1):
+                yfd = oy + (jfd - 1) * hy
+                for ifd in range(imin, imax + 1):
+                    xfd = ox + (ifd - 1) * hx
+                    if not (1 <= ifd <= nx and 1 <= jfd <= ny and 1 <= kfd <= nz):
+                        continue
+                    xi = 2.0 * (xfd - xmin) / (xmax - xmin) - 1.0
+                    eta = 2.0 * (yfd - ymin) / (ymax - ymin) - 1.0
+                    gam = 2.0 * (zfd - zmin) / (zmax - zmin) - 1.0
+                    if abs(xi) < 1.05 and abs(eta) < 1.05 and abs(gam) < 1.05:
+                        if (ifd, jfd, kfd) not in found:
+                            found[(ifd, jfd, kfd)] = (ispec, xi, eta, gam)
+    grid = [[[0.0] * nz for _ in range(ny)] for _ in range(nx)]
+    for (ifd, jfd, kfd), (ispec, xi, eta, gam) in found.items():
+        hxis, hetas, hgams = lag(xi), lag(eta), lag(gam)
+        val = 0.0
+        for kgg in range(5):
+            for jgg in range(5):
+                for igg in range(5):
+                    val += hxis[igg] * hetas[jgg] * hgams[kgg] * \
+                        data[(ispec - 1) * 125 + igg + 5 * jgg + 25 * kgg]
+        grid[ifd - 1][jfd - 1][kfd - 1] = val
+    return grid
