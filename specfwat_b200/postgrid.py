@@ -27,6 +27,8 @@ they do here too, on the arrays the device hands back.
   the smallest and largest distance between neighbouring GLL points along
   the element directions; ``taper_kernel_grid`` spaces its mask by their
   mean.
+- ``zprecond_grid`` is the depth preconditioner on the grid
+  (src/postproc/zprecond.f90:73-100), as ``sum_precond`` uses it.
 """
 from __future__ import annotations
 
@@ -193,3 +195,21 @@ def taper_kernel_grid(db, grid_kernels, x0, h, n, h_suppress, h_buffer, v_suppre
     X, Y, Z = np.meshgrid(gx, gy, gz, indexing="ij")
     mask = tap.interp(X, Y, Z)
     return np.asarray(grid_kernels) * mask, mask
+
+
+def zprecond_grid(zgrid, nx, ny, precond_type, nevents):
+    """``zprecond_grid`` (src/postproc/zprecond.f90:73-100): the depth
+    preconditioner on the model grid, [nx, ny, nz] FP32.  The 1-D profile
+    of ``get_1d_precond`` (:11-32) on the levels ``zgrid`` (1e-8 above the
+    surface, z + 1e-8 below; 1/|z| for type 2, 1/sqrt|z| for type 3),
+    repeated over x and y, times the event count, normalised, inverted and
+    normalised."""
+    if precond_type not in (2, 3):
+        raise ValueError("the depth forms are PRECOND_TYPE 2 and 3")
+    z = np.asarray(zgrid, np.float64)
+    zl = np.where(z > 0.0, 1e-8, z + 1e-8)
+    zl = 1.0 / np.sqrt(zl * zl) if precond_type == 2 else 1.0 / np.sqrt(np.sqrt(zl * zl))
+    h = np.broadcast_to(zl, (nx, ny, z.size)) * float(nevents)
+    h = h / np.abs(h).max()
+    h = 1.0 / h
+    return (h / np.abs(h).max()).astype(np.float32)

@@ -123,3 +123,21 @@ def test_mesh_distances_and_taper_kernel_grid():
     assert np.all(mask[0] == 0.0) and np.all(mask[:, :, 0] == 0.0)
     assert mask[16, 16, -1] == 1.0                  # no taper at the free surface
     assert 0.0 < mask[3, 16, 16] < 1.0              # the cosine ramp
+
+
+@pytest.mark.parametrize("ptype", [2, 3])
+def test_zprecond_grid_matches_literal(ptype):
+    from specfwat_b200.postgrid import zprecond_grid
+    zg = np.linspace(-30000.0, 2000.0, 17)
+    ours = zprecond_grid(zg, 4, 3, ptype, 6)
+    zl = np.array(F.get_1d_precond(zg, ptype), np.float32)
+    h = np.broadcast_to(zl, (4, 3, zg.size)).astype(np.float32) * np.float32(6)
+    h = h / np.abs(h).max()
+    h = np.float32(1.0) / h
+    lit = h / np.abs(h).max()
+    assert ours.shape == (4, 3, 17)
+    assert np.abs(ours - lit).max() <= 2e-6
+    # deeper levels get the larger preconditioner
+    assert np.all(np.diff(ours[0, 0][zg < 0]) < 0)
+    with pytest.raises(ValueError):
+        zprecond_grid(zg, 2, 2, 1, 1)
