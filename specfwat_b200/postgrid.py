@@ -12,12 +12,14 @@ they do here too, on the arrays the device hands back.
   ``Project_model_SEM2FD_grid`` (src/shared/projection_on_FD_grid_mod_fwat.f90:
   186-596) for one slice: elements in order; each element's grid
   candidates from its GLL bounding box, index ranges truncated as the
-  Fortran integer assignment does; a candidate is taken by the first
-  element in which its reference coordinates are all within 1.05 (so a
-  point up to 2.5% of an element beyond its face can be extrapolated from
-  it); its value is the element's 5x5x5 Lagrange interpolant there.  Points
-  no element takes stay 0.  Regular (axis-aligned cube) elements only,
-  where the reference's Newton location is exact and linear.
+  Fortran integer assignment does; the candidate's reference coordinates
+  from ``locate_point_in_element`` (:935-1125), whose Newton iterations
+  clamp them to [-1, 1], so the 1.05 acceptance always holds and a
+  candidate is taken by the first element whose range holds it (a point
+  just outside an element takes the value on the element's face); its
+  value is the element's 5x5x5 Lagrange interpolant there.  Points no
+  element takes stay 0.  Regular (axis-aligned cube) elements only, where
+  that Newton location is exact and linear.
 - ``Taper3D`` restates ``taper_cls``: a separable mask on a grid of
   spacing ``hx, hy, hz`` over the mesh's extent, zero for ``taph1`` from
   each side and the bottom, a half cosine over the next ``taph2``, one
@@ -79,7 +81,8 @@ def gll2grid(db, gll, x0, h, n):
                 break
             c = x0[d] + idx * h[d]
             rng.append(idx)
-            ref.append(2.0 * (c - lo) / (hi - lo) - 1.0)
+            # the locator's Newton steps clamp to the element
+            ref.append(np.clip(2.0 * (c - lo) / (hi - lo) - 1.0, -1.0, 1.0))
         if len(rng) < 3:
             continue
         ok = [np.abs(r) < 1.05 for r in ref]

@@ -15,7 +15,8 @@ the golden vectors in this directory:
 * ``locate_bissection``, ``interp3``  src/shared/utils.f90:1089-1159,1490-1525
 * ``project_sem2fd``: compute_interpolation_coeff_FD_SEM + Project_model_
   SEM2FD_grid (src/shared/projection_on_FD_grid_mod_fwat.f90:186-596), one
-  slice, regular elements (reference coordinates linear in x, y, z)
+  slice, regular elements (reference coordinates linear in x, y, z, clamped
+  to [-1, 1] as locate_point_in_element's iterations do, :935-1125)
 """
 import math
 
@@ -599,9 +600,11 @@ def project_sem2fd(ibool, xstore, ystore, zstore, nspec, data, ox, oy, oz, hx, h
                     xfd = ox + (ifd - 1) * hx
                     if not (1 <= ifd <= nx and 1 <= jfd <= ny and 1 <= kfd <= nz):
                         continue
-                    xi = 2.0 * (xfd - xmin) / (xmax - xmin) - 1.0
-                    eta = 2.0 * (yfd - ymin) / (ymax - ymin) - 1.0
-                    gam = 2.0 * (zfd - zmin) / (zmax - zmin) - 1.0
+                    # locate_point_in_element: Newton steps (exact for
+                    # these affine elements), each clamped to [-1, 1]
+                    xi = min(max(2.0 * (xfd - xmin) / (xmax - xmin) - 1.0, -1.0), 1.0)
+                    eta = min(max(2.0 * (yfd - ymin) / (ymax - ymin) - 1.0, -1.0), 1.0)
+                    gam = min(max(2.0 * (zfd - zmin) / (zmax - zmin) - 1.0, -1.0), 1.0)
                     if abs(xi) < 1.05 and abs(eta) < 1.05 and abs(gam) < 1.05:
                         if (ifd, jfd, kfd) not in found:
                             found[(ifd, jfd, kfd)] = (ispec, xi, eta, gam)

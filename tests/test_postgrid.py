@@ -1,9 +1,10 @@
 """Kernels on the model grid: ``specfwat_b200.postgrid``.
 
 - ``gll2grid`` equals a line-by-line transcription of the reference's
-  projection loop (first element wins, 1.05 acceptance, truncated index
-  ranges; tests/golden/fortran_literal.py) on a grid that is not aligned
-  with the elements, including points outside the mesh;
+  projection loop (first element wins, locator coordinates clamped to the
+  element, truncated index ranges; tests/golden/fortran_literal.py) on a
+  grid that is not aligned with the elements, including points outside
+  the mesh;
 - it reproduces a field that is a polynomial of degree <= 4 per element
   exactly at any grid point;
 - ``create_taper`` and the trilinear ``Taper3D.interp`` equal FP32
@@ -40,16 +41,16 @@ def test_gll2grid_matches_literal_loop():
                            db.zstore, db.nspec, data.reshape(-1), *x0, *h, *n)
     lit = np.asarray(lit, np.float64)
     assert np.abs(ours - lit).max() <= 1e-6 * np.abs(lit).max()
-    # x = -700, -150 (xi -1.15), y = -300, z = -4200 and z = +30 lie
-    # outside and stay zero; every point inside is filled
-    assert np.all(ours[:2] == 0.0) and np.all(ours[:, 0] == 0.0)
-    assert np.all(ours[:, :, 0] == 0.0) and np.all(ours[:, :, -1] == 0.0)
-    assert np.all(ours[2:, 1:, 1:-1] != 0.0)
+    # x = -700 and z = +30 are no element's candidates and stay zero;
+    # x = -150 is a candidate of the first elements through the truncated
+    # index range and takes their value on the face x = 0
+    assert np.all(ours[0] == 0.0) and np.all(ours[:, :, -1] == 0.0)
+    assert np.all(ours[1:, :, :-1] != 0.0)
 
 
-def test_gll2grid_extrapolates_within_the_acceptance():
-    """x = -40 m lies 2% of an element outside the first element (xi = -1.04)
-    and is taken from it by extrapolation, as the reference's 1.05 rule does."""
+def test_gll2grid_clamps_to_the_element_face():
+    """x = -40 m lies outside the first elements; it is their candidate and
+    takes their value on the face x = 0, since the locator clamps xi to -1."""
     db = small_box()
     rng = np.random.default_rng(4)
     data = rng.standard_normal((db.nspec, 5, 5, 5))
@@ -59,7 +60,8 @@ def test_gll2grid_extrapolates_within_the_acceptance():
                                       db.ystore, db.zstore, db.nspec, data.reshape(-1),
                                       *x0, *h, *n), np.float64)
     assert np.abs(ours - lit).max() <= 1e-6 * np.abs(lit).max()
-    assert np.all(ours[0] != 0.0)
+    face = gll2grid(db, data, (0.0, 35.0, -3980.0), (550.0, 610.0, 470.0), (1, 7, 9))
+    assert np.array_equal(ours[0], face[0])
 
 
 def test_gll2grid_is_exact_for_element_polynomials():
