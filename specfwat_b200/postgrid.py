@@ -18,8 +18,11 @@ they do here too, on the arrays the device hands back.
   candidate is taken by the first element whose range holds it (a point
   just outside an element takes the value on the element's face); its
   value is the element's 5x5x5 Lagrange interpolant there.  Points no
-  element takes stay 0.  Regular (axis-aligned cube) elements only, where
-  that Newton location is exact and linear.
+  element takes stay 0.  The locator starts from the nearest of the 27
+  interior GLL nodes and takes ``NUM_ITER = 4`` Newton steps on the
+  element's NGNOD anchor nodes (8: GLL corners; 27: corners, edge, face
+  and centre nodes); on regular (affine) elements it is exact and the
+  linear formula is used directly.
 - ``Taper3D`` restates ``taper_cls``: a separable mask on a grid of
   spacing ``hx, hy, hz`` over the mesh's extent, zero for ``taph1`` from
   each side and the bottom, a half cosine over the next ``taph2``, one
@@ -56,13 +59,58 @@ def _element_boxes(db):
     return [(a.min(axis=1), a.max(axis=1)) for a in xyz]
 
 
-def gll2grid(db, gll, x0, h, n):
+NUM_ITER = 4
+
+
+def _shape(u, m):
+    """1-D Lagrange shape functions on m = 2 ([-1, 1]) or 3 ([-1, 0, 1])
+    nodes at u [n]: values and derivatives [n, m]."""
+    u = np.asarray(u, np.float64)
+    if m == 2:
+        return np.stack([0.5 * (1 - u), 0.5 * (1 + u)], 1), \
+            np.stack([np.full_like(u, -0.5), np.full_like(u, 0.5)], 1)
+    return np.stack([0.5 * u * (u - 1), 1 - u * u, 0.5 * u * (u + 1)], 1), \
+        np.stack([u - 0.5, -2 * u, u + 0.5], 1)
+
+
+def locate_in_element(nodes, targets, ngnod=8, niter=NUM_ITER):
+    """``locate_point_in_element`` (projection_on_FD_grid_mod_fwat.f90:
+    935-1125) for one element: ``nodes`` [5, 5, 5, 3] GLL point coordinates
+    ([k][j][i]), ``targets`` [n, 3]; returns (xi, eta, gamma) [n, 3] after
+    the initial guess at the nearest interior GLL node and ``niter`` Newton
+    steps on the anchor-node mapping, each clamped to [-1, 1]."""
+    t = np.asarray(targets, np.float64).reshape(-1, 3)
+    inner = nodes[1:4, 1:4, 1:4].reshape(-1, 3)                    # k, j, i order
+    best = np.argmin(((t[:, None, :] - inner[None]) ** 2).sum(-1), axis=1)
+    k, j, i = np.unravel_index(best, (3, 3, 3))
+    ref = np.stack([XG[i + 1], XG[j + 1], XG[k + 1]], 1)
+    sel = [0, 4] if ngnod == 8 else [0, 2, 4]
+    m = len(sel)
+    anc = nodes[np.ix_(sel, sel, sel)]                              # [c][b][a][3]
+    for _ in range(niter):
+        (la, da), (lb, db_), (lc, dc) = (_shape(ref[:, q], m) for q in range(3))
+        x = np.einsum("na,nb,nc,cbad->nd", la, lb, lc, anc)
+        jac = np.stack([np.einsum("na,nb,nc,cbad->nd", da, lb, lc, anc),
+                        np.einsum("na,nb,nc,cbad->nd", la, db_, lc, anc),
+                        np.einsum("na,nb,nc,cbad->nd", la, lb, dc, anc)], axis=2)
+        ref = np.clip(ref + np.linalg.solve(jac, (t - x)[..., None])[..., 0], -1.0, 1.0)
+    return ref
+
+
+def gll2grid(db, gll, x0, h, n, ngnod=8):
     """Project element values ``gll`` [nspec, 5, 5, 5] (Fortran dat(i,j,k,
     ispec) order, i fastest: [ispec][k][j][i]) onto the grid
-    ``x0[d] + i h[d]``, i < n[d]; returns [nx, ny, nz] FP32."""
-    if getattr(db, "geo", None) is not None:
-        raise ValueError("gll2grid takes regular elements only")
+    ``x0[d] + i h[d]``, i < n[d]; returns [nx, ny, nz] FP32.  ``ngnod``:
+    anchor nodes of the mesher's elements (8 or 27), used on irregular
+    elements."""
+    if ngnod not in (8, 27):
+        raise ValueError("ngnod must be 8 or 27")
     g = np.asarray(gll, np.float64).reshape(db.nspec, 5, 5, 5)
+    irr = getattr(db, "irregular", None)
+    irregular = (np.zeros(db.nspec, bool) if getattr(db, "geo", None) is None or irr is None
+                 else np.asarray(irr) >= 0)
+    ib5 = np.asarray(db.ibool).reshape(db.nspec, 5, 5, 5)
+    xyz = np.stack([np.asarray(a, np.float64) for a in (db.xstore, db.ystore, db.zstore)], 1)
     x0 = np.asarray(x0, np.float64)
     h = np.asarray(h, np.float64)
     n = np.asarray(n, np.int64)
@@ -85,17 +133,24 @@ def gll2grid(db, gll, x0, h, n):
             ref.append(np.clip(2.0 * (c - lo) / (hi - lo) - 1.0, -1.0, 1.0))
         if len(rng) < 3:
             continue
-        ok = [np.abs(r) < 1.05 for r in ref]
-        ix, iy, iz = (r[o] for r, o in zip(rng, ok))
-        if ix.size == 0 or iy.size == 0 or iz.size == 0:
-            continue
-        hx, hy, hz = (lagrange5(r[o]) for r, o in zip(ref, ok))
+        ix, iy, iz = rng
         sub = np.ix_(ix, iy, iz)
         take = ~found[sub]
         if not take.any():
             continue
-        # sum_k sum_j sum_i hx_i hy_j hz_k g[e, k, j, i]
-        val = np.einsum("ai,bj,ck,kji->abc", hx, hy, hz, g[e])
+        if not irregular[e]:
+            # affine element: the clamped linear coordinates are what the
+            # locator's Newton steps reach; the 1.05 test always holds
+            hx, hy, hz = (lagrange5(r) for r in ref)
+            # sum_k sum_j sum_i hx_i hy_j hz_k g[e, k, j, i]
+            val = np.einsum("ai,bj,ck,kji->abc", hx, hy, hz, g[e])
+        else:
+            gx, gy, gz = (x0[d] + rng[d] * h[d] for d in range(3))
+            P = np.stack(np.meshgrid(gx, gy, gz, indexing="ij"), -1).reshape(-1, 3)
+            r = locate_in_element(xyz[ib5[e]], P, ngnod)
+            w = np.einsum("ni,nj,nk->nkji", lagrange5(r[:, 0]), lagrange5(r[:, 1]),
+                          lagrange5(r[:, 2]))
+            val = np.einsum("nkji,kji->n", w, g[e]).reshape(take.shape)
         blk = out[sub]
         blk[take] = val[take]
         out[sub] = blk

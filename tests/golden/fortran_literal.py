@@ -17,6 +17,8 @@ the golden vectors in this directory:
   SEM2FD_grid (src/shared/projection_on_FD_grid_mod_fwat.f90:186-596), one
   slice, regular elements (reference coordinates linear in x, y, z, clamped
   to [-1, 1] as locate_point_in_element's iterations do, :935-1125)
+* ``locate_point_in_element`` (:935-1125) with NGNOD = 8 and NUM_ITER = 4,
+  and ``project_sem2fd_located`` using it for every element
 """
 import math
 
@@ -608,6 +610,107 @@ def project_sem2fd(ibool, xstore, ystore, zstore, nspec, data, ox, oy, oz, hx, h
                     if abs(xi) < 1.05 and abs(eta) < 1.05 and abs(gam) < 1.05:
                         if (ifd, jfd, kfd) not in found:
                             found[(ifd, jfd, kfd)] = (ispec, xi, eta, gam)
+    grid = [[[0.0] * nz for _ in range(ny)] for _ in range(nx)]
+    for (ifd, jfd, kfd), (ispec, xi, eta, gam) in found.items():
+        hxis, hetas, hgams = lag(xi), lag(eta), lag(gam)
+        val = 0.0
+        for kgg in range(5):
+            for jgg in range(5):
+                for igg in range(5):
+                    val += hxis[igg] * hetas[jgg] * hgams[kgg] * \
+                        data[(ispec - 1) * 125 + igg + 5 * jgg + 25 * kgg]
+        grid[ifd - 1][jfd - 1][kfd - 1] = val
+    return grid
+
+
+def _inv3(m):
+    a, b, c = m[0]
+    d, e, f = m[1]
+    g, h, i = m[2]
+    det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g)
+    return [[(e * i - f * h) / det, (c * h - b * i) / det, (b * f - c * e) / det],
+            [(f * g - d * i) / det, (a * i - c * g) / det, (c * d - a * f) / det],
+            [(d * h - e * g) / det, (b * g - a * h) / det, (a * e - b * d) / det]]
+
+
+def locate_point_in_element(ex, ey, ez, xt, yt, zt, niter=4):
+    """ex, ey, ez: the element's 125 GLL point coordinates, i fastest."""
+    import math
+    xg = [-1.0, -math.sqrt(3.0 / 7.0), 0.0, math.sqrt(3.0 / 7.0), 1.0]
+    P = lambda i, j, k: (i - 1) + 5 * (j - 1) + 25 * (k - 1)  # noqa: E731
+    distmin = float("inf")
+    ig = jg = kg = 1
+    for k in range(2, 5):
+        for j in range(2, 5):
+            for i in range(2, 5):
+                q = P(i, j, k)
+                dist = (xt - ex[q]) ** 2 + (yt - ey[q]) ** 2 + (zt - ez[q]) ** 2
+                if dist < distmin:
+                    distmin, ig, jg, kg = dist, i, j, k
+    xi, eta, gam = xg[ig - 1], xg[jg - 1], xg[kg - 1]
+    corners = [(a, b, c) for c in (0, 1) for b in (0, 1) for a in (0, 1)]
+    anc = [P(1 + 4 * a, 1 + 4 * b, 1 + 4 * c) for (a, b, c) in corners]
+    for _ in range(niter):
+        x = y = z = 0.0
+        J = [[0.0] * 3 for _ in range(3)]
+        for (a, b, c), q in zip(corners, anc):
+            sa, sb, sc = (1 - 2 * a), (1 - 2 * b), (1 - 2 * c)
+            la = 0.5 * (1 - sa * xi)
+            lb = 0.5 * (1 - sb * eta)
+            lc = 0.5 * (1 - sc * gam)
+            dla, dlb, dlc = -0.5 * sa, -0.5 * sb, -0.5 * sc
+            n = la * lb * lc
+            dn = (dla * lb * lc, la * dlb * lc, la * lb * dlc)
+            x += n * ex[q]
+            y += n * ey[q]
+            z += n * ez[q]
+            for e_ in range(3):
+                J[0][e_] += dn[e_] * ex[q]
+                J[1][e_] += dn[e_] * ey[q]
+                J[2][e_] += dn[e_] * ez[q]
+        inv = _inv3(J)
+        dx, dy, dz = -(x - xt), -(y - yt), -(z - zt)
+        xi += inv[0][0] * dx + inv[0][1] * dy + inv[0][2] * dz
+        eta += inv[1][0] * dx + inv[1][1] * dy + inv[1][2] * dz
+        gam += inv[2][0] * dx + inv[2][1] * dy + inv[2][2] * dz
+        xi, eta, gam = (min(max(v, -1.0), 1.0) for v in (xi, eta, gam))
+    return xi, eta, gam
+
+
+def project_sem2fd_located(ibool, xstore, ystore, zstore, nspec, data, ox, oy, oz, hx, hy,
+                           hz, nx, ny, nz):
+    """As project_sem2fd, with locate_point_in_element for every element."""
+    import math
+    xg = [-1.0, -math.sqrt(3.0 / 7.0), 0.0, math.sqrt(3.0 / 7.0), 1.0]
+
+    def lag(x):
+        out = []
+        for i in range(5):
+            v = 1.0
+            for m in range(5):
+                if m != i:
+                    v *= (x - xg[m]) / (xg[i] - xg[m])
+            out.append(v)
+        return out
+    found = {}
+    for ispec in range(1, nspec + 1):
+        ex = [xstore[ibool[(ispec - 1) * 125 + q] - 1] for q in range(125)]
+        ey = [ystore[ibool[(ispec - 1) * 125 + q] - 1] for q in range(125)]
+        ez = [zstore[ibool[(ispec - 1) * 125 + q] - 1] for q in range(125)]
+        kmin, kmax = int(1 + (min(ez) - oz) / hz), int(1 + (max(ez) - oz) / hz)
+        jmin, jmax = int(1 + (min(ey) - oy) / hy), int(1 + (max(ey) - oy) / hy)
+        imin, imax = int(1 + (min(ex) - ox) / hx), int(1 + (max(ex) - ox) / hx)
+        for kfd in range(kmin, kmax + 1):
+            for jfd in range(jmin, jmax + 1):
+                for ifd in range(imin, imax + 1):
+                    if not (1 <= ifd <= nx and 1 <= jfd <= ny and 1 <= kfd <= nz):
+                        continue
+                    if (ifd, jfd, kfd) in found:
+                        continue
+                    loc = locate_point_in_element(ex, ey, ez, ox + (ifd - 1) * hx,
+                                                  oy + (jfd - 1) * hy, oz + (kfd - 1) * hz)
+                    if all(abs(v) < 1.05 for v in loc):
+                        found[(ifd, jfd, kfd)] = (ispec,) + tuple(loc)
     grid = [[[0.0] * nz for _ in range(ny)] for _ in range(nx)]
     for (ifd, jfd, kfd), (ispec, xi, eta, gam) in found.items():
         hxis, hetas, hgams = lag(xi), lag(eta), lag(gam)

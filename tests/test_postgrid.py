@@ -78,11 +78,55 @@ def test_gll2grid_is_exact_for_element_polynomials():
     assert np.abs(grid - ref).max() <= 1e-5 * np.abs(ref).max()
 
 
-def test_irregular_mesh_refused():
-    box = D.BoxSpec(2, 2, 2)
-    db = D.make_box(box, topo=D.hill_topography(box, 1000.0, 3000.0))
-    with pytest.raises(ValueError, match="regular"):
-        gll2grid(db, np.zeros((db.nspec, 5, 5, 5)), (0, 0, 0), (1000, 1000, 1000), (3, 3, 3))
+def test_gll2grid_topography_matches_literal_locator():
+    """All elements irregular: every candidate is located by the Newton
+    iteration on the 8 anchor nodes, as in the transcription."""
+    box = D.BoxSpec(3, 2, 2, h=2000.0)
+    db = D.make_box(box, topo=D.hill_topography(box, 1200.0, 2500.0))
+    assert db.nspec_irregular == db.nspec
+    rng = np.random.default_rng(6)
+    data = rng.standard_normal((db.nspec, 5, 5, 5))
+    x0, h, n = (-300.0, 120.0, -4100.0), (610.0, 560.0, 700.0), (11, 8, 9)
+    ours = gll2grid(db, data, x0, h, n)
+    lit = np.asarray(F.project_sem2fd_located(
+        (db.ibool.reshape(-1) + 1).tolist(), db.xstore, db.ystore, db.zstore, db.nspec,
+        data.reshape(-1), *x0, *h, *n), np.float64)
+    assert np.abs(ours - lit).max() <= 1e-5 * np.abs(lit).max()
+    assert np.count_nonzero(ours) > 0.5 * ours.size
+
+
+def test_gll2grid_newton_path_equals_linear_path():
+    """A regular box flagged irregular takes the Newton locator, which must
+    land where the linear formula does."""
+    db = small_box()
+    rng = np.random.default_rng(7)
+    data = rng.standard_normal((db.nspec, 5, 5, 5))
+    x0, h, n = (-700.0, -300.0, -4200.0), (550.0, 610.0, 470.0), (13, 8, 10)
+    a = gll2grid(db, data, x0, h, n)
+    b = gll2grid(D.as_irregular(db), data, x0, h, n)
+    assert np.abs(a - b).max() <= 1e-5 * np.abs(a).max()
+
+
+def test_gll2grid_linear_field_on_topography():
+    """A linear field on a topography mesh.  Most grid points come back to
+    the interpolation accuracy; a few do not, by the reference's rule: on a
+    deformed mesh element bounding boxes overlap, and the first element
+    whose box holds a point takes it at the clamped (face) coordinate even
+    when the point lies in the next element."""
+    box = D.BoxSpec(4, 4, 3, h=2000.0)
+    db = D.make_box(box, topo=D.hill_topography(box, 800.0, 3000.0))
+    ib = db.ibool.reshape(-1)
+    f = lambda x, y, z: 1.0 + 2e-5 * x - 3e-5 * y + 4e-5 * z  # noqa: E731
+    data = f(*(np.asarray(a, np.float64)[ib] for a in (db.xstore, db.ystore, db.zstore)))
+    x0, h, n = (500.0, 500.0, -5500.0), (700.0, 700.0, 600.0), (10, 10, 9)
+    grid = gll2grid(db, data.reshape(db.nspec, 5, 5, 5), x0, h, n, ngnod=27)
+    gx, gy, gz = (x0[d] + np.arange(n[d]) * h[d] for d in range(3))
+    X, Y, Z = np.meshgrid(gx, gy, gz, indexing="ij")
+    ref = f(X, Y, Z)
+    err = np.abs(grid - ref)
+    assert np.median(err) < 1e-4 and np.percentile(err, 95) < 1e-3 and err.max() < 5e-3
+    with pytest.raises(ValueError, match="ngnod"):
+        gll2grid(db, data.reshape(db.nspec, 5, 5, 5), x0, h, n, ngnod=20)
 
 
 @pytest.mark.parametrize("args", [(3000.0, 5000.0, 2000.0, 4000.0, 500.0, 500.0, 400.0, 41, 37, 30),
