@@ -96,3 +96,46 @@ def apply_precond(kernels, precond):
     """``ker_data(:,:,:,:,iker) * total_hess`` for every kernel
     (post_processing.f90:193-195): ``kernels`` [..., nspec, 5, 5, 5]."""
     return np.asarray(kernels) * np.asarray(precond, np.float64)
+
+
+KERNEL_ISO = ("alpha", "beta", "rhop")     # src/shared/config.f90:35
+RHO_SCALING_FAC = 0.33                     # src/shared/config.f90:42
+_SIX = ("rho", "mu", "kappa", "rhop", "beta", "alpha")
+
+
+def gradient_on_grid(mesh, db, kernels6, x0, h, n, sigma_h, sigma_v, *, precond=None,
+                     rho_scaling=False, taper=None, ngnod=8, smooth=None):
+    """The post-processing of ``fwat_post_proc`` for an isotropic model
+    (src/postproc/fwat_post_proc.f90:29-46), from the summed kernels to
+    the gradient on the model grid:
+
+    1. the ``KERNEL_ISO`` kernels alpha, beta, rhop of ``kernels6``
+       [6, nspec, 5, 5, 5] (``Simulation.sum_kernels`` order);
+    2. times ``precond`` [nspec, 5, 5, 5] when given (``apply_precond``);
+    3. each smoothed on the device (``pde_smooth``: ``smooth_sem_pde``) and
+       projected onto the grid ``x0 + i h``, i < n (``gll2grid``); with
+       ``rho_scaling`` the rhop grid is the beta grid times 0.33 instead
+       (USE_RHO_SCALING, post_processing.f90:262-264);
+    4. times the boundary taper when ``taper`` = (h_suppress, h_buffer,
+       v_suppress, v_buffer) is given (``taper_kernel_grid``).
+
+    Returns [3, nx, ny, nz] in KERNEL_ISO order.  ``smooth`` replaces the
+    device smoother (a function of [nfield, nspec, 5, 5, 5] arrays)."""
+    from .postgrid import gll2grid, taper_kernel_grid
+    k6 = np.asarray(kernels6, np.float64)
+    ker = np.stack([k6[_SIX.index(k)] for k in KERNEL_ISO])
+    if precond is not None:
+        ker = ker * np.asarray(precond, np.float64)
+    nsm = 2 if rho_scaling else 3
+    if smooth is None:
+        def smooth(d):
+            return smooth_sem_pde(mesh, d, sigma_h, sigma_v)[0]
+    sm = np.asarray(smooth(ker[:nsm].astype(np.float32)), np.float64).reshape(
+        (nsm,) + ker.shape[1:])
+    grid = [gll2grid(db, sm[i], x0, h, n, ngnod) for i in range(nsm)]
+    if rho_scaling:
+        grid.append(grid[1] * np.float32(RHO_SCALING_FAC))
+    grid = np.stack(grid)
+    if taper is not None:
+        grid, _ = taper_kernel_grid(db, grid, x0, h, n, *taper)
+    return grid
