@@ -116,3 +116,22 @@ def test_bad_arguments(gpu):
     with pytest.raises(Exception, match="sigma"):
         smooth_sem_pde(mesh, dat, -1.0, 3000.0)
     mesh.close()
+
+
+def test_gradient_on_grid_with_the_device_smoother(gpu):
+    """The post-processing chain through the device smoother: each kernel's
+    grid equals the oracle-smoothed kernel projected the same way."""
+    from specfwat_b200.postgrid import gll2grid
+    from specfwat_b200.postproc import gradient_on_grid
+    db = box_db(5, 4, 3)
+    mesh = S.Mesh(db)
+    k6 = fields(db, 6, seed=9).astype(np.float64)
+    x0, h, n = (0.0, 0.0, -12000.0), (1000.0, 1000.0, 1000.0), (21, 17, 13)
+    grid = gradient_on_grid(mesh, db, k6, x0, h, n, 7000.0, 3500.0)
+    dmin = (1.0 - np.sqrt(3.0 / 7.0)) / db.xix_regular
+    ref, _, _ = Oracle(db, precision=4).smooth_pde(k6[[5, 4, 3]].astype(np.float32),
+                                                    7000.0, 3500.0, dmin)
+    for i in range(3):
+        g_ref = gll2grid(db, ref[i], x0, h, n)
+        assert rel(grid[i], g_ref) < 1e-4, i
+    mesh.close()
