@@ -139,3 +139,29 @@ def gradient_on_grid(mesh, db, kernels6, x0, h, n, sigma_h, sigma_v, *, precond=
     if taper is not None:
         grid, _ = taper_kernel_grid(db, grid, x0, h, n, *taper)
     return grid
+
+
+def hessian_on_grid(mesh, db, hess_sum, x0, h, n, sigma_h, sigma_v, precond_type=1, *,
+                    zgrid=None, nevents=1, ngnod=8, smooth=None):
+    """``PostFlow%sum_precond`` (src/postproc/post_processing.f90:199-230):
+    the preconditioner on the model grid, normalised to a maximum of 1.
+
+    - PRECOND_TYPE 0 and 1: ``invert_hess`` of the event-summed Hessian
+      (``hessian_precond``, on the device), smoothed on the device,
+      projected onto the grid and divided by its largest magnitude;
+    - PRECOND_TYPE 2 and 3: ``zprecond_grid`` on the grid's depth levels
+      ``zgrid`` (defaults to ``x0[2] + k h[2]``) for ``nevents`` events.
+
+    ``smooth`` replaces the device smoother."""
+    from .postgrid import gll2grid, zprecond_grid
+    if precond_type in (2, 3):
+        z = (np.asarray(zgrid, np.float64) if zgrid is not None
+             else x0[2] + np.arange(n[2]) * h[2])
+        return zprecond_grid(z, n[0], n[1], precond_type, nevents)
+    inv = hessian_precond(hess_sum, precond_type)
+    if smooth is None:
+        def smooth(d):
+            return smooth_sem_pde(mesh, d, sigma_h, sigma_v)[0]
+    sm = np.asarray(smooth(inv.reshape(db.nspec, 5, 5, 5)), np.float64)
+    gm = gll2grid(db, sm, x0, h, n, ngnod).astype(np.float64)
+    return (gm / np.abs(gm).max()).astype(np.float32)

@@ -135,3 +135,26 @@ def test_gradient_on_grid_with_the_device_smoother(gpu):
         g_ref = gll2grid(db, ref[i], x0, h, n)
         assert rel(grid[i], g_ref) < 1e-4, i
     mesh.close()
+
+
+def test_hessian_on_grid(gpu):
+    """sum_precond on the device: invert, smooth, project, normalise; and the
+    depth forms on the grid."""
+    from oracle import oracle as O
+    from specfwat_b200.postgrid import gll2grid, zprecond_grid
+    from specfwat_b200.postproc import hessian_on_grid
+    db = box_db(5, 4, 3)
+    mesh = S.Mesh(db)
+    hs = np.abs(fields(db, 1, seed=12)[0].astype(np.float64)) + 0.1
+    x0, h, n = (0.0, 0.0, -12000.0), (1000.0, 1000.0, 1000.0), (21, 17, 13)
+    g = hessian_on_grid(mesh, db, hs, x0, h, n, 7000.0, 3500.0, 1)
+    inv = O.hessian_precond(hs, 1).astype(np.float32)
+    dmin = (1.0 - np.sqrt(3.0 / 7.0)) / db.xix_regular
+    ref, _, _ = Oracle(db, precision=4).smooth_pde(inv, 7000.0, 3500.0, dmin)
+    gr = gll2grid(db, ref, x0, h, n).astype(np.float64)
+    gr /= np.abs(gr).max()
+    assert np.abs(g).max() == pytest.approx(1.0)
+    assert rel(g, gr) < 1e-4
+    z = hessian_on_grid(mesh, db, None, x0, h, n, 0.0, 0.0, 2, nevents=4)
+    assert np.array_equal(z, zprecond_grid(x0[2] + np.arange(n[2]) * h[2], n[0], n[1], 2, 4))
+    mesh.close()
