@@ -5,7 +5,8 @@ data-path collective.  The only exchange is the cross-event kernel sum
 (the reference's ``PostFlow%sum_kernel``, ``post_processing.f90:108-149``),
 done here as one FP64 all-reduce of the summed rho/mu/kappa kernels per
 batch; the derived rhop/beta/alpha kernels are linear in them and are
-formed after the reduction by whoever needs them.
+formed after the reduction by whoever needs them.  With the approximate
+Hessian on, its event sum is reduced the same way.
 """
 from __future__ import annotations
 
@@ -30,6 +31,18 @@ def reduce_kernel_sum(ksum, group=None):
         raise TypeError("kernel sums are reduced in FP64")
     dist.all_reduce(ksum[:3], op=dist.ReduceOp.SUM, group=group)
     return ksum
+
+
+def reduce_hessian_sum(hsum, group=None):
+    """Sum a rank's event-summed Hessian (``Simulation.sum_hessian``; sum of
+    |hess| for PRECOND_TYPE 1, of hess for type 0) over all ranks in place,
+    in FP64, before the preconditioner is formed
+    (``PostFlow%apply_precond``, post_processing.f90:171-185)."""
+    import torch.distributed as dist
+    if hsum.dtype.itemsize != 8:
+        raise TypeError("Hessian sums are reduced in FP64")
+    dist.all_reduce(hsum, op=dist.ReduceOp.SUM, group=group)
+    return hsum
 
 
 def derived_kernels(k3, mu, kappa):

@@ -1,5 +1,5 @@
-"""Multi-rank host logic on CPU: event sharding and the FP64 kernel-sum
-all-reduce, run as two gloo ranks."""
+"""Multi-rank host logic on CPU: event sharding and the FP64 kernel-sum and
+Hessian-sum all-reduces, run as two gloo ranks."""
 import os
 import socket
 
@@ -9,8 +9,8 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from specfwat_b200.shard import (derived_kernels, events_of, reduce_kernel_sum,
-                                 shard_events)
+from specfwat_b200.shard import (derived_kernels, events_of, reduce_hessian_sum,
+                                 reduce_kernel_sum, shard_events)
 
 
 def test_shard_covers_all_events_once():
@@ -76,3 +76,47 @@ def test_two_ranks_sum_equals_single_rank(tmp_path):
     d = derived_kernels(got[:3], mu, kap)
     for q in range(3):
         assert np.allclose(d[q], ref[3 + q], rtol=1e-9, atol=1e-30)
+
+
+def _hessian_sum_for(events, abs_each):
+    """One rank's event-summed approximate Hessian from the CPU oracle."""
+    from specfwat_b200 import database as D
+    from oracle.oracle import Oracle, l2_adjoint_source
+    db = D.build("tiny")
+    rec = D.surface_receivers(db.box, 2)
+    total = np.zeros((db.nspec, 5, 5, 5))
+    for (x, y, z, seed) in events:
+        mt = D.random_moment_tensor(np.random.default_rng(seed))
+        o = Oracle(db, precision=8, nthreads=1)
+        syn = o.forward(0.02, 120, Oracle.source(x, y, z, mt, 1.0), rec, save_forward=True)
+        _, adj = l2_adjoint_source(syn, 0.5 * syn, 0.02)
+        o.adjoint(rec, adj)
+        h = o.hessian()
+        total += np.abs(h) if abs_each else h
+    return total
+
+
+def _hess_rank_main(rank, world, port, events, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        h = torch.from_numpy(_hessian_sum_for(events_of(events, rank, world), True).copy())
+        reduce_hessian_sum(h)
+        if rank == 0:
+            np.save(out, h.numpy())
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_hessian_sum_equals_single_rank(tmp_path):
+    events = [(4000.0 + 800 * i, 5000.0, -4000.0 - 500 * i, 200 + i) for i in range(3)]
+    out = str(tmp_path / "h.npy")
+    mp.start_processes(_hess_rank_main, args=(2, _free_port(), events, out), nprocs=2,
+                       join=True, start_method="spawn")
+    two = np.load(out)
+    one = _hessian_sum_for(events, True)
+    assert np.abs(one).max() > 0
+    assert np.allclose(two, one, rtol=1e-12, atol=0)
+    with pytest.raises(TypeError):
+        reduce_hessian_sum(torch.zeros(4, dtype=torch.float32))
