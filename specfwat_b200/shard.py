@@ -3,10 +3,11 @@
 Events are independent, so N GPUs run N disjoint event sets with no
 data-path collective.  The only exchange is the cross-event kernel sum
 (the reference's ``PostFlow%sum_kernel``, ``post_processing.f90:108-149``),
-done here as one FP64 all-reduce of the summed rho/mu/kappa kernels per
-batch; the derived rhop/beta/alpha kernels are linear in them and are
-formed after the reduction by whoever needs them.  With the approximate
-Hessian on, its event sum is reduced the same way.
+done here as one FP64 all-reduce of the six summed kernels per batch
+(rho, mu, kappa and the derived rhop, beta, alpha).  The derived rows are
+linear in the primary ones at fixed model, so the sum of the ranks' derived
+rows equals the rows derived from the summed primary kernels.  With the
+approximate Hessian on, its event sum is reduced the same way.
 """
 from __future__ import annotations
 
@@ -23,13 +24,16 @@ def shard_events(n_events: int, rank: int, world: int) -> range:
 
 
 def reduce_kernel_sum(ksum, group=None):
-    """Sum the primary kernels (rho, mu, kappa: rows 0-2 of a [6, ...]
-    FP64 tensor) over all ranks in place, then rebuild rows 3-5
-    (rhop, beta, alpha) from them is left to the caller."""
+    """Sum a rank's event-summed kernels over all ranks in place: a
+    [6, ...] FP64 tensor with rows rho, mu, kappa, rhop, beta, alpha (the
+    layout of ``sem_sum_kernels``).  All six rows are reduced, so every row
+    of the result is the sum over every rank's events."""
     import torch.distributed as dist
     if ksum.dtype.itemsize != 8:
         raise TypeError("kernel sums are reduced in FP64")
-    dist.all_reduce(ksum[:3], op=dist.ReduceOp.SUM, group=group)
+    if ksum.shape[0] != 6:
+        raise ValueError("kernel sums have six rows (rho, mu, kappa, rhop, beta, alpha)")
+    dist.all_reduce(ksum, op=dist.ReduceOp.SUM, group=group)
     return ksum
 
 
