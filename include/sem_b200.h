@@ -267,9 +267,13 @@ int sem_kernel_variants(sem_run *run, int *fwd, int *adj);
  * until exit) sized for SEM_L2_NOALLOC_MAX_RECEIVERS receivers and
  * SEM_L2_NOALLOC_MAX_STEPS samples; larger requests return SEM_ERR_ARG.
  * Work is queued on `stream` (a cudaStream_t, NULL = legacy default).  The
- * first call on a device looks up that array's device address, so make it
- * before capturing the stream into a CUDA graph.  All calls share the
- * array: calls that overlap on the GPU race and must not be issued. */
+ * first call on a device (and the first after its context was reset) looks
+ * up that array's device address; CUDA loads device code lazily, so that
+ * call is also when the array is placed on the GPU, and on a full device
+ * it returns SEM_ERR_CUDA.  Make one small call at start-up, before a
+ * fixed budget applies and before capturing the stream into a CUDA graph.
+ * All calls share the array: calls that overlap on the GPU race and must
+ * not be issued. */
 #define SEM_L2_NOALLOC_MAX_RECEIVERS 4096
 #define SEM_L2_NOALLOC_MAX_STEPS 32768
 int sem_measure_l2_noalloc(const float *seis_dev, const double *obs_dev,

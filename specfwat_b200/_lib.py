@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsem_b200.so")
 
 SEM_OK = 0
+SEM_ERR_NUMERIC = -6
 STATUS = {
     0: "SEM_OK", -1: "SEM_ERR_ARG", -2: "SEM_ERR_CUDA", -3: "SEM_ERR_NOMEM",
     -4: "SEM_ERR_STATE", -5: "SEM_ERR_UNSUPPORTED", -6: "SEM_ERR_NUMERIC",

@@ -414,6 +414,17 @@ struct sem_run_s {
   bool lanes_mode = false;        // run driven through the sem_lane_* calls
   DevArray<int> flag;
   DevArray<int> gmap;             // serving: active 8-lane groups
+  // periodic stability check (cfg.check_every > 0): per-lane non-finite
+  // flags and the step each flagged lane was stopped at (device), their
+  // pinned host copies for lane-driven runs, and the lane state on the host
+  DevArray<int> lflags, halt_step;
+  int* h_lflags = nullptr;
+  int* h_halt = nullptr;
+  cudaEvent_t check_ev = nullptr;
+  bool check_pending = false;     // a check's flags are on their way to h_lflags
+  int steps_since_check = 0;
+  std::vector<char> lane_failed;
+  std::vector<int> lane_fail_step;
   std::vector<int> src_ispec, nrec;
   std::vector<char> have_src, have_rec, have_adj;
   // FK injection per event: one device allocation holding the velocity and
@@ -441,6 +452,9 @@ struct sem_run_s {
       if (g) cudaGraphExecDestroy(g);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
+    if (check_ev) cudaEventDestroy(check_ev);
+    if (h_lflags) cudaFreeHost(h_lflags);
+    if (h_halt) cudaFreeHost(h_halt);
     if (own_stream) cudaStreamDestroy(own_stream);
     if (mesh) mesh->live_runs--;
   }
@@ -1093,6 +1107,34 @@ static int ensure_tuned(sem_run* r) {
   return SEM_OK;
 }
 
+// Periodic stability check (cfg.check_every > 0).  The per-lane flags and
+// halt steps start cleared (flags 0, halt step -1) for every lane.
+static int ensure_check_buffers(sem_run* r) {
+  if (r->lflags.p) return SEM_OK;
+  CKM(r->lflags.alloc((size_t)r->nev), "stability flags");
+  CKM(r->halt_step.alloc((size_t)r->nev), "stability halt steps");
+  CK(cudaMallocHost((void**)&r->h_lflags, (size_t)r->nev * sizeof(int)));
+  CK(cudaMallocHost((void**)&r->h_halt, (size_t)r->nev * sizeof(int)));
+  CK(cudaEventCreateWithFlags(&r->check_ev, cudaEventDisableTiming));
+  CK(cudaMemsetAsync(r->lflags.p, 0, r->lflags.bytes(), r->stream));
+  CK(cudaMemsetAsync(r->halt_step.p, 0xff, r->halt_step.bytes(), r->stream));
+  r->lane_failed.assign(r->nev, 0);
+  r->lane_fail_step.assign(r->nev, -1);
+  return SEM_OK;
+}
+
+// Queue a scan of the run's fields (the backward field too once it exists)
+// and stop the lanes found non-finite; s_off = steps the kernels have done
+// beyond each lane's device it0.
+static void queue_check(sem_run* r, bool both, int s_off) {
+  launch_check_lanes(r->u1.p, r->mesh->nglob, r->lm.lwlog, r->nevp, r->lanes.p, r->nev,
+                     r->lflags.p, r->stream);
+  if (both && r->u2.p)
+    launch_check_lanes(r->u2.p, r->mesh->nglob, r->lm.lwlog, r->nevp, r->lanes.p, r->nev,
+                       r->lflags.p, r->stream);
+  launch_halt_lanes(r->lanes.p, r->nev, r->lflags.p, r->halt_step.p, s_off, r->stream);
+}
+
 // Queue the step loop of one phase (graphs or per-step launches).
 static int run_loop(sem_run* r, bool adjoint) {
   long long launches = 0;
@@ -1121,17 +1163,30 @@ static int run_loop(sem_run* r, bool adjoint) {
     }
     const int nlaunch = (r->nstep + K - 1) / K;
     const int per_step = (r->mesh->nf > 0 ? 4 : 3);
+    const int ce = r->cfg.check_every;
     for (int g = 0; g < nlaunch; ++g) {
       CK(cudaGraphLaunch(gx, r->stream));
       launches += (long long)K * per_step + 1;
+      // stability check at the first graph boundary at or after every
+      // check_every steps, and after the last graph (each graph advances
+      // the lanes' device it0 by K)
+      if (ce > 0 && (g == nlaunch - 1 || (long long)(g + 1) * K / ce > (long long)g * K / ce)) {
+        queue_check(r, adjoint, 0);
+        launches += adjoint ? 3 : 2;
+      }
     }
   } else {
+    const int ce = r->cfg.check_every;
     for (int s = 0; s < r->nstep; ++s) {
       a.s = s;
       launches += launch_forces(a, adjoint, r->stream);
       launches += launch_boundary(a, adjoint, r->stream);
       launches += launch_points(a, r->stream);
       launches += launch_update(a, adjoint, r->stream);
+      if (ce > 0 && ((s + 1) % ce == 0 || s == r->nstep - 1)) {
+        queue_check(r, adjoint, s + 1);
+        launches += adjoint ? 3 : 2;
+      }
     }
   }
   CK(cudaGetLastError());
@@ -1145,6 +1200,12 @@ int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
   if (r->lanes_mode)
     return fail(SEM_ERR_STATE, "run is driven lane by lane (sem_lane_*); use sem_advance");
   const size_t n3 = (size_t)r->mesh->nglob * 3 * r->nevp;
+  if (r->cfg.check_every > 0 && (sim_type == 1 || sim_type == 3)) {
+    int rc = ensure_check_buffers(r);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(r->lflags.p, 0, r->lflags.bytes(), r->stream));
+    CK(cudaMemsetAsync(r->halt_step.p, 0xff, r->halt_step.bytes(), r->stream));
+  }
   if (sim_type == 1) {
     for (int e = 0; e < r->nev; ++e)
       if (!(r->have_src[e] || r->inj[e].buf) || !r->have_rec[e])
@@ -1195,12 +1256,27 @@ int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
     return fail(SEM_ERR_ARG, "sim_type must be 1 or 3");
   }
   if (r->cfg.check_every > 0) {
-    CK(cudaMemsetAsync(r->flag.p, 0, sizeof(int), r->stream));
-    launch_nonfinite(r->u1.p, n3, r->flag.p, r->stream);
-    int h = 0;
-    CK(cudaMemcpyAsync(&h, r->flag.p, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+    // the checks ran inside the loop; a flagged event stopped at its check
+    std::vector<int> fl(r->nev), hs(r->nev);
+    CK(cudaMemcpyAsync(fl.data(), r->lflags.p, r->lflags.bytes(), cudaMemcpyDeviceToHost,
+                       r->stream));
+    CK(cudaMemcpyAsync(hs.data(), r->halt_step.p, r->halt_step.bytes(), cudaMemcpyDeviceToHost,
+                       r->stream));
     CK(cudaStreamSynchronize(r->stream));
-    if (h) return fail(SEM_ERR_NUMERIC, "non-finite wavefield after sim_type %d", sim_type);
+    int nbad = 0, first = -1;
+    for (int e = 0; e < r->nev; ++e)
+      if (fl[e]) {
+        if (first < 0) first = e;
+        ++nbad;
+      }
+    if (nbad) {
+      r->fwd_saved = false;
+      r->adj_done = false;
+      return fail(SEM_ERR_NUMERIC,
+                  "non-finite wavefield in event %d (%d of %d events) found at step %d of %d "
+                  "(sim_type %d, checked every %d steps); those events stopped there",
+                  first, nbad, r->nev, hs[first], r->nstep, sim_type, r->cfg.check_every);
+    }
   }
   return SEM_OK;
 }
@@ -1736,6 +1812,14 @@ int sem_lane_start_forward(sem_run* r, int lane, const sem_source* src, int nrec
   }
   launch_lane_zero({r->u1.p, r->v1.p, r->a1.p}, r->mesh->nglob, r->lm, lane, r->stream);
   CK(cudaGetLastError());
+  if (r->cfg.check_every > 0) {
+    rc = ensure_check_buffers(r);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(r->lflags.p + lane, 0, sizeof(int), r->stream));
+    CK(cudaMemsetAsync(r->halt_step.p + lane, 0xff, sizeof(int), r->stream));
+    r->lane_failed[lane] = 0;
+    r->lane_fail_step[lane] = -1;
+  }
   LaneDesc& L = r->h_lanes[lane];
   lane_defaults(r, lane);
   L.phase = PH_FWD;
@@ -1791,9 +1875,30 @@ int sem_lane_start_adjoint(sem_run* r, int lane, const double* obs, double taper
   return SEM_OK;
 }
 
+// Lane-driven runs: take in the flags of the last stability check once its
+// copy has landed (without waiting).  A flagged running lane is marked
+// failed and complete, so no further launch works it; sem_lane_status and
+// sem_lane_finish report it.
+static void consume_check(sem_run* r) {
+  if (!r->check_pending || cudaEventQuery(r->check_ev) != cudaSuccess) {
+    cudaGetLastError();  // cudaErrorNotReady is not an error here
+    return;
+  }
+  r->check_pending = false;
+  for (int l = 0; l < r->nev; ++l) {
+    LaneDesc& L = r->h_lanes[l];
+    if (r->h_lflags[l] && !r->lane_failed[l] && L.phase != PH_IDLE) {
+      r->lane_failed[l] = 1;
+      r->lane_fail_step[l] = r->h_halt[l];
+      L.it0 = L.nstep;
+    }
+  }
+}
+
 int sem_advance(sem_run* r, int nsteps) {
   if (!r || nsteps < 1) return fail(SEM_ERR_ARG, "bad argument");
   if (!r->lanes_mode) return fail(SEM_ERR_STATE, "no lane has been started");
+  if (r->cfg.check_every > 0) consume_check(r);
   // 8-lane groups with running events, split by phase: a group with any
   // adjoint lane goes to the two-field kernels, an all-forward group to the
   // one-field kernels
@@ -1850,6 +1955,21 @@ int sem_advance(sem_run* r, int nsteps) {
     }
   }
   CK(cudaGetLastError());
+  if (r->cfg.check_every > 0) {
+    r->steps_since_check += nsteps;
+    // one check in flight at a time; a due check waits for the previous one
+    if (r->steps_since_check >= r->cfg.check_every && !r->check_pending) {
+      queue_check(r, true, nsteps);
+      launches += 3;
+      CK(cudaMemcpyAsync(r->h_lflags, r->lflags.p, r->lflags.bytes(), cudaMemcpyDeviceToHost,
+                         r->stream));
+      CK(cudaMemcpyAsync(r->h_halt, r->halt_step.p, r->halt_step.bytes(),
+                         cudaMemcpyDeviceToHost, r->stream));
+      CK(cudaEventRecord(r->check_ev, r->stream));
+      r->check_pending = true;
+      r->steps_since_check = 0;
+    }
+  }
   for (auto& L : r->h_lanes)
     if (L.phase != PH_IDLE) L.it0 = std::min(L.nstep, L.it0 + nsteps);
   r->last_launches = launches;
@@ -1864,10 +1984,17 @@ int sem_lane_status(sem_run* r, int lane, int* phase, int* step, int* nstep) {
     if (nstep) *nstep = 0;
     return SEM_OK;
   }
+  if (r->cfg.check_every > 0) consume_check(r);
   const LaneDesc& L = r->h_lanes[lane];
   if (phase) *phase = L.phase;
   if (step) *step = L.it0;
   if (nstep) *nstep = L.nstep;
+  if (r->cfg.check_every > 0 && r->lane_failed[lane])
+    return fail(SEM_ERR_NUMERIC,
+                "lane %d: non-finite wavefield found at step %d of its %s run (checked every "
+                "%d steps); the lane stopped there, sem_lane_finish releases it",
+                lane, r->lane_fail_step[lane], L.phase == PH_ADJ ? "adjoint" : "forward",
+                r->cfg.check_every);
   return SEM_OK;
 }
 
@@ -1877,6 +2004,39 @@ int sem_lane_finish(sem_run* r, int lane, float* seis, double* kernels6, double*
   LaneDesc& L = r->h_lanes[lane];
   if (L.phase == PH_IDLE || L.it0 < L.nstep)
     return fail(SEM_ERR_STATE, "lane %d has not completed a run", lane);
+  if (r->cfg.check_every > 0) {
+    // take in the check in flight, then scan the lane's final state, so that
+    // no result leaves a lane unchecked and no flag outlives its request
+    if (r->check_pending) {
+      CK(cudaEventSynchronize(r->check_ev));
+      consume_check(r);
+    }
+    if (!r->lane_failed[lane]) {
+      queue_check(r, true, 0);
+      CK(cudaMemcpyAsync(r->h_lflags, r->lflags.p, r->lflags.bytes(), cudaMemcpyDeviceToHost,
+                         r->stream));
+      CK(cudaMemcpyAsync(r->h_halt, r->halt_step.p, r->halt_step.bytes(),
+                         cudaMemcpyDeviceToHost, r->stream));
+      CK(cudaEventRecord(r->check_ev, r->stream));
+      r->check_pending = true;
+      CK(cudaEventSynchronize(r->check_ev));
+      consume_check(r);
+    }
+  }
+  if (r->cfg.check_every > 0 && r->lane_failed[lane]) {
+    // a lane stopped by the stability check: release it, no results
+    if (r->lane_store[lane]) CK(cudaFreeAsync(r->lane_store[lane], r->stream));
+    if (r->lane_scale[lane]) CK(cudaFreeAsync(r->lane_scale[lane], r->stream));
+    r->lane_store[lane] = nullptr;
+    r->lane_scale[lane] = nullptr;
+    const int at = r->lane_fail_step[lane];
+    const bool adj = L.phase == PH_ADJ;
+    L.phase = PH_IDLE;
+    r->lane_failed[lane] = 0;
+    CK(cudaStreamSynchronize(r->stream));
+    return fail(SEM_ERR_NUMERIC, "lane %d: non-finite wavefield at step %d of its %s run; lane "
+                "released without results", lane, at, adj ? "adjoint" : "forward");
+  }
   if (seis && L.phase == PH_FWD)
     CK(cudaMemcpyAsync(seis, L.seis, (size_t)L.nrec * 3 * L.nstep * 4, cudaMemcpyDeviceToHost,
                        r->stream));

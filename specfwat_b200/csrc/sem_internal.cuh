@@ -152,6 +152,13 @@ int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, LaneMap lm
 int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane,
                      cudaStream_t st);
 int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st);
+// Periodic stability check: flags[lane] |= 1 for running lanes of u (a
+// field of nevp lanes) with a non-finite value; then halt the flagged lanes
+// (phase idle, halt_step = it0 + s_off at the first flag).
+int launch_check_lanes(const float* u, size_t nglob, int lwlog, int nevp, LaneDesc* lanes,
+                       int nev, int* flags, cudaStream_t st);
+int launch_halt_lanes(LaneDesc* lanes, int nev, const int* flags, int* halt_step, int s_off,
+                      cudaStream_t st);
 int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int lane,
                          cudaStream_t st);
 

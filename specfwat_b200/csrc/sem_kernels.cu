@@ -3218,4 +3218,47 @@ int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st) {
   return 1;
 }
 
+// Periodic stability check of a run's wavefield u ([group][point][3][LW]):
+// flags[lane] |= 1 for every running lane that holds a non-finite value.
+// per_group = values per lane group (nglob * 3 * LW).
+__global__ void k_check_lanes(const float* __restrict__ u, size_t n, size_t per_group, int lwlog,
+                              const LaneDesc* __restrict__ lanes, int nev, int* flags) {
+  const size_t lwm = ((size_t)1 << lwlog) - 1;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (!isfinite(u[i])) {
+      const int lane = (int)(((i / per_group) << lwlog) + (i & lwm));
+      if (lane < nev && lanes[lane].phase != PH_IDLE && !flags[lane]) atomicOr(&flags[lane], 1);
+    }
+  }
+}
+
+// Stops the flagged lanes: phase idle, so the remaining launches of the run
+// skip them, and the step reached when the flag was first seen
+// (it0 + s_off, at most the lane's nstep) in halt_step.
+__global__ void k_halt_lanes(LaneDesc* lanes, int nev, const int* __restrict__ flags,
+                             int* halt_step, int s_off) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nev; e += gridDim.x * blockDim.x) {
+    LaneDesc& L = lanes[e];
+    if (flags[e] && L.phase != PH_IDLE) {
+      if (halt_step[e] < 0) halt_step[e] = min(L.it0 + s_off, L.nstep);
+      L.phase = PH_IDLE;
+    }
+  }
+}
+
+int launch_check_lanes(const float* u, size_t nglob, int lwlog, int nevp, LaneDesc* lanes,
+                       int nev, int* flags, cudaStream_t st) {
+  const size_t per_group = nglob * 3 * ((size_t)1 << lwlog);
+  k_check_lanes<<<148 * 4, 256, 0, st>>>(u, per_group * (size_t)(nevp >> lwlog), per_group,
+                                         lwlog, lanes, nev, flags);
+  return 1;
+}
+
+int launch_halt_lanes(LaneDesc* lanes, int nev, const int* flags, int* halt_step, int s_off,
+                      cudaStream_t st) {
+  k_halt_lanes<<<(nev + 127) / 128, 128, 0, st>>>(lanes, nev, flags, halt_step, s_off);
+  return 1;
+}
+
 }  // namespace sem

@@ -14,6 +14,19 @@
 // misfits) before using them, so nothing has to start at zero.  Calls that
 // overlap on the GPU (different streams, or different host threads, at the
 // same time) race on the array and must not be issued.
+//
+// Set-up: the first call in a CUDA context (the first on a device, and the
+// first after the context was torn down and recreated, e.g. by
+// cudaDeviceReset) looks up the array's device address.  CUDA loads device
+// code lazily, so that first call is also when the driver loads this file's
+// device code and places the array (about 608 KiB) on the GPU; on a device
+// with no memory left it fails with SEM_ERR_CUDA.  A caller under a fixed
+// budget makes one small call at start-up, before the budget applies.  Make
+// the first call before any stream capture.  The address is cached per
+// device together with the context's id, so a recreated context is set up
+// again instead of reusing an address from the old one.
+
+#include <cuda.h>  // CUcontext / CUresult types of the two driver calls below
 
 #include <cmath>
 #include <cstdio>
@@ -33,10 +46,41 @@ static __device__ __align__(256) double g_l2_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 128;
 std::mutex g_mu;
-double* g_scratch_addr[kMaxDevices] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id;  // context the address belongs to
+  double* addr;
+};
+ScratchSlot g_slot[kMaxDevices] = {};
 
-// Device address of g_l2_scratch on the current device, looked up once per
-// device (the host-side name of the array is only a stand-in).
+// Unique id of the calling thread's current CUDA context (cuCtxGetId),
+// through the runtime's driver entry points, so the library needs no link
+// to libcuda.
+int current_context_id(unsigned long long* id) {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      cudaGetLastError();
+      return sem::report_error(SEM_ERR_CUDA, "driver context queries are not available");
+    }
+    get_current = (GetCurrent)f1;
+    get_id = (GetId)f2;
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS)
+    return sem::report_error(SEM_ERR_CUDA, "no current CUDA context");
+  return SEM_OK;
+}
+
+// Device address of g_l2_scratch in the current context (the host-side name
+// of the array is only a stand-in), looked up once per device and context.
 int scratch_for_current_device(double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -46,8 +90,19 @@ int scratch_for_current_device(double** out) {
   }
   if (dev < 0 || dev >= kMaxDevices)
     return sem::report_error(SEM_ERR_UNSUPPORTED, "device ordinal %d above %d", dev, kMaxDevices);
+  // makes the device's primary context current if no context is yet
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return sem::report_error(SEM_ERR_CUDA, "cudaSetDevice(%d) failed: %s", dev,
+                             cudaGetErrorString(e));
+  }
+  unsigned long long ctx = 0;
+  int rc = current_context_id(&ctx);
+  if (rc) return rc;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev]) {
+  ScratchSlot& s = g_slot[dev];
+  if (!s.addr || s.ctx_id != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_l2_scratch);
     if (e != cudaSuccess || !p) {
@@ -55,9 +110,10 @@ int scratch_for_current_device(double** out) {
       return sem::report_error(SEM_ERR_CUDA, "cudaGetSymbolAddress of the L2 scratch failed: %s",
                                cudaGetErrorString(e));
     }
-    g_scratch_addr[dev] = (double*)p;
+    s.addr = (double*)p;
+    s.ctx_id = ctx;
   }
-  *out = g_scratch_addr[dev];
+  *out = s.addr;
   return SEM_OK;
 }
 

@@ -46,6 +46,7 @@ class Request:
     misfit: float = float("nan")
     seismograms: Optional[np.ndarray] = None
     kernels: Optional[np.ndarray] = None
+    error: str = ""                    # set when the run was stopped (non-finite field)
 
     @property
     def latency(self):
@@ -80,13 +81,30 @@ class MeshServer:
     def __init__(self, name, db, slots, nstep_max, dt, store="fp16",
                  graph_steps=50, max_receivers=128, store_budget=None,
                  ksum_dev_ptr=0, taper_pct=0.05, taper_type=1, policy="lane",
-                 group=8, max_wait=1.5):
+                 group=8, max_wait=1.5, check_every=0):
+        mesh = S.Mesh(db)
+        sim = S.Simulation(mesh, nstep_max, dt, nev=slots, store=store, use_graph=True,
+                           graph_steps=graph_steps, max_receivers=max_receivers,
+                           check_every=check_every)
+        self._setup(name, mesh, sim, slots, nstep_max, db.nspec, store_budget, ksum_dev_ptr,
+                    taper_pct, taper_type, policy, group, max_wait)
+
+    @classmethod
+    def with_sim(cls, name, sim, slots, nstep_max, nspec, store_budget=None, ksum_dev_ptr=0,
+                 taper_pct=0.05, taper_type=1, policy="lane", group=8, max_wait=1.5):
+        """A server around an existing run object (anything with the lane
+        primitives of ``solver.Simulation``), set up by the same code as a
+        server that makes its own mesh and run."""
+        self = cls.__new__(cls)
+        self._setup(name, None, sim, slots, nstep_max, nspec, store_budget, ksum_dev_ptr,
+                    taper_pct, taper_type, policy, group, max_wait)
+        return self
+
+    def _setup(self, name, mesh, sim, slots, nstep_max, nspec, store_budget, ksum_dev_ptr,
+               taper_pct, taper_type, policy, group, max_wait):
         self.name = name
-        self.mesh = S.Mesh(db)
-        self.sim = S.Simulation(self.mesh, nstep_max, dt, nev=slots,
-                                store=store, use_graph=True,
-                                graph_steps=graph_steps,
-                                max_receivers=max_receivers)
+        self.mesh = mesh
+        self.sim = sim
         self.slots = slots
         self.nstep_max = nstep_max
         self.lanes: List[Optional[Request]] = [None] * slots
@@ -96,7 +114,7 @@ class MeshServer:
         self.lane_store = [0] * slots
         self.ksum_dev_ptr = ksum_dev_ptr
         self.taper = (taper_pct, taper_type)
-        self.nspec = db.nspec
+        self.nspec = nspec
         self.phase = [PH_IDLE] * slots
         # "lane": a request takes any free lane at once.  "group": requests
         # enter an 8-lane group together once the group is free and either a
@@ -258,6 +276,18 @@ class MeshServer:
             ph, st, ns = self.sim.lane_status(lane)
             if ph == PH_IDLE or st < ns:
                 continue
+            if lane in self.sim.lane_errors:
+                # stopped by the stability check: released without results
+                req.error = self.sim.lane_errors[lane]
+                try:
+                    self.sim.lane_finish(lane)
+                except S._lib.SemError as e:
+                    if e.code != S._lib.SEM_ERR_NUMERIC:
+                        raise
+                self._free(lane)
+                req.done = clock()
+                finished.append(req)
+                continue
             if ph == PH_FWD and req.kind == "fwd":
                 req.seismograms = np.zeros((len(req.receivers), 3, req.nstep), np.float32)
                 self.sim.lane_finish(lane, seis_out=req.seismograms)
@@ -287,7 +317,8 @@ class MeshServer:
 
     def close(self):
         self.sim.close()
-        self.mesh.close()
+        if self.mesh is not None:
+            self.mesh.close()
 
 
 class Server:

@@ -131,6 +131,7 @@ class Simulation:
         check(L.sem_prepare_timerun(mesh.handle, C.byref(self.cfg), C.byref(h)))
         self._h = h
         self.nrec = [0] * nev
+        self.lane_errors = {}
 
     # setup_sources_receivers_fwat
     def set_sources(self, sources: Iterable):
@@ -302,13 +303,21 @@ class Simulation:
         check(_lib.load().sem_advance(self._h, int(nsteps)))
 
     def lane_status(self, lane: int):
+        """(phase, steps done, nstep) of a lane.  A lane stopped by the
+        stability check (``check_every``) reports its phase complete and its
+        message is kept in ``lane_errors[lane]`` until ``lane_finish``."""
         ph, st, ns = C.c_int(), C.c_int(), C.c_int()
-        check(_lib.load().sem_lane_status(self._h, lane, C.byref(ph), C.byref(st),
-                                          C.byref(ns)))
+        L = _lib.load()
+        rc = L.sem_lane_status(self._h, lane, C.byref(ph), C.byref(st), C.byref(ns))
+        if rc == _lib.SEM_ERR_NUMERIC:
+            self.lane_errors[lane] = L.sem_last_error().decode()
+        else:
+            check(rc)
         return ph.value, st.value, ns.value
 
     def lane_finish(self, lane: int, seis_out=None, kernels_out=None,
                     ksum_dev_ptr: int = 0):
+        self.lane_errors.pop(lane, None)
         check(_lib.load().sem_lane_finish(
             self._h, lane,
             None if seis_out is None else seis_out.ctypes.data,

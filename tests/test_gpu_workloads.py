@@ -8,7 +8,8 @@
   vs each event alone, FP16 store, and the HBM sizing of 8 events;
 * failure detection: a time step far above the stability limit is
   reported as SEM_ERR_NUMERIC by the device non-finite check, the context
-  stays usable.
+  stays usable; the periodic check stops a run (or a serving lane) at the
+  check after its field goes non-finite and reports the step.
 """
 import os
 
@@ -143,6 +144,136 @@ def test_unstable_time_step_is_reported_not_faulted(gpu):
     ok.iterate_time(1)
     assert np.isfinite(ok.seismograms(0)).all()
     ok.close()
+    mesh.close()
+
+
+def _halt_step(msg):
+    import re
+    m = re.search(r"at step (-?\d+)", msg)
+    assert m, msg
+    return int(m.group(1))
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_blowup_reported_before_nstep(gpu, graph):
+    """check_every scans the wavefield every K steps inside the loop; an
+    event that goes non-finite is stopped at that check and reported with
+    the step, well before NSTEP."""
+    db = D.build("tiny")
+    rec = D.surface_receivers(db.box, 2)
+    mt = D.random_moment_tensor(np.random.default_rng(1))
+    mesh = S.Mesh(db)
+    nstep = 2000
+    sim = S.Simulation(mesh, nstep, 0.8, max_receivers=len(rec), check_every=20,
+                       use_graph=graph, graph_steps=10)
+    sim.set_sources([S.make_source(6000., 6000., -6000., mt, 0.2)])
+    sim.set_receivers(rec)
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.iterate_time(1, save_forward=True)
+    assert ei.value.code == -6
+    at = _halt_step(str(ei.value))
+    assert 0 < at < nstep // 4 and at % 20 == 0, at
+    # the failed forward cannot feed an adjoint run
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.iterate_time(3)
+    assert ei.value.code == -4
+    sim.close()
+    mesh.close()
+
+
+def test_adjoint_overflow_reported_for_its_event_only(gpu):
+    """In SIM 3 the adjoint field is scanned too: one event of a batch whose
+    adjoint source overflows the field is flagged, the other is not."""
+    db = D.build("tiny")
+    rec = D.surface_receivers(db.box, 2)
+    rng = np.random.default_rng(5)
+    mesh = S.Mesh(db)
+    nstep = 300
+    sim = S.Simulation(mesh, nstep, 0.02, nev=2, max_receivers=len(rec), check_every=50,
+                       use_graph=True, graph_steps=25, store="fp16")
+    sim.set_sources([S.make_source(6000. + 1000 * e, 6000., -6000., D.random_moment_tensor(rng),
+                                   1.0) for e in range(2)])
+    sim.set_receivers(rec)
+    sim.iterate_time(1, save_forward=True)
+    syn = [sim.seismograms(e).astype(np.float64) for e in range(2)]
+    sim.set_adjoint_sources(0, syn[0])
+    sim.set_adjoint_sources(1, np.full_like(syn[1], 3.0e38))
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.iterate_time(3)
+    msg = str(ei.value)
+    assert ei.value.code == -6 and "event 1 (1 of 2 events)" in msg, msg
+    assert 0 < _halt_step(msg) < nstep
+    sim.close()
+    mesh.close()
+
+
+def test_serving_lane_stopped_by_check_others_complete(gpu):
+    """Lane-driven runs check their lanes too: a lane whose adjoint field
+    overflows is reported by sem_lane_status and released by
+    sem_lane_finish without results, while a lane running beside it
+    completes with the kernels it has when run alone."""
+    db = D.build("tiny")
+    rec = D.surface_receivers(db.box, 2)
+    rng = np.random.default_rng(9)
+    srcs = [S.make_source(6000. + 1500 * e, 7000., -5000., D.random_moment_tensor(rng), 1.0)
+            for e in range(2)]
+    nstep = 240
+    mesh = S.Mesh(db)
+    # the good request alone
+    alone = S.Simulation(mesh, nstep, 0.02, nev=8, max_receivers=len(rec), check_every=30,
+                         use_graph=True, store="fp16")
+    alone.lane_start_forward(0, srcs[0], rec, nstep, save_forward=True)
+    while alone.lane_status(0)[1] < nstep:
+        alone.advance(40)
+    seis0 = np.zeros((len(rec), 3, nstep), np.float32)
+    alone.lane_finish(0, seis_out=seis0)
+    obs0 = 0.5 * seis0.astype(np.float64)
+    alone.lane_start_adjoint(0, obs0)
+    while alone.lane_status(0)[1] < nstep:
+        alone.advance(40)
+    k_alone = np.zeros((6, db.nspec, 5, 5, 5))
+    alone.lane_finish(0, kernels_out=k_alone)
+    alone.close()
+
+    sim = S.Simulation(mesh, nstep, 0.02, nev=8, max_receivers=len(rec), check_every=30,
+                       use_graph=True, store="fp16")
+    for lane in range(2):
+        sim.lane_start_forward(lane, srcs[lane], rec, nstep, save_forward=True)
+    while sim.lane_status(0)[1] < nstep:
+        sim.advance(40)
+    for lane in range(2):
+        seis = np.zeros((len(rec), 3, nstep), np.float32)
+        sim.lane_finish(lane, seis_out=seis)
+    sim.lane_start_adjoint(0, obs0)
+    sim.lane_start_adjoint(1, np.full((len(rec), 3, nstep), 3.0e38))
+    done = {}
+    for _ in range(100):
+        sim.advance(40)
+        for lane in range(2):
+            if lane in done:
+                continue
+            ph, st, ns = sim.lane_status(lane)
+            if st >= ns:
+                done[lane] = sim.lane_errors.get(lane, "")
+        if len(done) == 2:
+            break
+    assert "non-finite" in done[1], done
+    assert done[0] == "", done
+    with pytest.raises(S._lib.SemError) as ei:
+        sim.lane_finish(1)
+    assert ei.value.code == -6
+    k = np.zeros((6, db.nspec, 5, 5, 5))
+    sim.lane_finish(0, kernels_out=k)
+    for q in range(3):
+        assert rel(k[q], k_alone[q]) < 1e-5
+    # the released lane takes the next request
+    sim.lane_start_forward(1, srcs[1], rec, 60, save_forward=False)
+    while sim.lane_status(1)[1] < 60:
+        sim.advance(30)
+    seis = np.zeros((len(rec), 3, 60), np.float32)
+    sim.lane_finish(1, seis_out=seis)
+    assert np.isfinite(seis).all() and np.abs(seis).max() > 0
+    sim.close()
     mesh.close()
 
 

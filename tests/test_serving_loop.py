@@ -13,8 +13,6 @@ steps, so the scheduling logic runs without a device:
   server.
 The device results of the same loop are checked in tests/test_serving.py.
 """
-from collections import deque
-
 import numpy as np
 import pytest
 
@@ -28,6 +26,7 @@ class FakeSim:
         self.store = 0
         self.max_store = 0
         self.starts = []
+        self.lane_errors = {}
 
     def lane_store_bytes(self, nstep):
         return nstep * 1000
@@ -74,17 +73,8 @@ class FakeSim:
 
 
 def mesh_server(name, slots, budget=None, policy="lane", max_wait=0.05):
-    s = MeshServer.__new__(MeshServer)
-    s.name, s.mesh, s.sim = name, None, FakeSim(slots)
-    s.slots, s.nstep_max = slots, 10000
-    s.lanes = [None] * slots
-    s.queue = deque()
-    s.store_budget, s.store_in_use = budget, 0
-    s.lane_store = [0] * slots
-    s.ksum_dev_ptr, s.taper, s.nspec = 0, (0.05, 1), 1
-    s.phase = [PH_IDLE] * slots
-    s.policy, s.group, s.max_wait = policy, 8, max_wait
-    return s
+    return MeshServer.with_sim(name, FakeSim(slots), slots, 10000, 1, store_budget=budget,
+                               policy=policy, max_wait=max_wait)
 
 
 def stream(n, mesh="m", seed=0, spread=0.02):

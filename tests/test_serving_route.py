@@ -7,7 +7,6 @@ wait for a lane when none is free).  Lanes are packed into the fullest
 group.  Checked with server objects whose run is a stand-in (lane status
 only), so no device is needed.
 """
-from collections import deque
 
 import numpy as np
 import pytest
@@ -20,6 +19,7 @@ C = StepCosts(plain_fwd=0.10e-3, plain_adj=0.20e-3, group_fwd=0.35e-3, group_adj
 class FakeSim:
     def __init__(self, status):
         self.status = status        # lane -> (phase, step, nstep)
+        self.lane_errors = {}
 
     def lane_status(self, lane):
         return self.status.get(lane, (PH_IDLE, 0, 0))
@@ -27,18 +27,13 @@ class FakeSim:
 
 def server(slots, running=()):
     """running: (lane, kind, nstep, phase, step)."""
-    s = MeshServer.__new__(MeshServer)
-    s.slots = slots
-    s.lanes = [None] * slots
-    s.queue = deque()
-    s.phase = [PH_IDLE] * slots
     status = {}
+    s = MeshServer.with_sim("m", FakeSim(status), slots, 10000, 1)
     for lane, kind, ns, ph, st in running:
         s.lanes[lane] = Request(rid=lane, mesh="m", kind=kind, nstep=ns, source=None,
                                 receivers=np.zeros((1, 3)))
         s.phase[lane] = ph
         status[lane] = (ph, st, ns)
-    s.sim = FakeSim(status)
     return s
 
 

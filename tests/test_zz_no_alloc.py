@@ -82,6 +82,17 @@ def test_noalloc_matches_measure_l2(gpu):
         mis_dev.append(mis)
         keep += [seis, ob]
     torch.cuda.synchronize()
+    # a third call, on the set-up device, must not change the device's free
+    # memory: the entry point allocates nothing
+    free0, _ = torch.cuda.mem_get_info(dev)
+    rc = lib.sem_measure_l2_noalloc(
+        C.c_void_p(keep[0].data_ptr()), C.c_void_p(keep[1].data_ptr()), len(rec),
+        nstep, dt, 0.05, 1, C.c_void_p(adj_dev[0].data_ptr()),
+        C.c_void_p(mis_dev[0].data_ptr()), None)
+    _lib.check(rc)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0, (free0, free1)
     for e in range(2):
         m = float(mis_dev[e].cpu().item())
         assert abs(m - ref_misfit[e]) <= 1e-12 * abs(ref_misfit[e])
