@@ -117,7 +117,17 @@ typedef struct {
   int use_graph;      /* 1: replay the step loop as CUDA graphs            */
   int graph_steps;    /* steps per captured graph (0 = default 50)         */
   int max_receivers;  /* receivers per event upper bound (>= 1)            */
-  int check_every;    /* steps between non-finite checks (0 = off)         */
+  int check_every;    /* steps between non-finite checks (0 = off): the
+                         wavefields (adjoint and backward in sim_type 3)
+                         are scanned per event inside the loop, at the
+                         first graph boundary after every check_every
+                         steps; an event found non-finite stops there
+                         and sem_iterate_time returns SEM_ERR_NUMERIC
+                         with the event and step.  Lane-driven runs check
+                         their lanes the same way (sem_lane_status /
+                         sem_lane_finish report SEM_ERR_NUMERIC for the
+                         stopped lane only).  The solver's equivalent is
+                         the check every NTSTEP_BETWEEN_OUTPUT_INFO steps */
   int kernel_variant; /* element kernel: 0 autotuned per phase,
                          1 thread-per-point, 2 pencil decomposition,
                          3 pencil, persistent and cp.async-pipelined,
