@@ -56,6 +56,7 @@ def lib():
         L.oracle_create.restype = C.c_void_p
         L.oracle_create.argtypes = [C.POINTER(OracleMesh), C.c_int, C.c_int]
         L.oracle_destroy.argtypes = [C.c_void_p]
+        L.oracle_set_flush_subnormals.argtypes = [C.c_void_p, C.c_int]
         L.oracle_forward.argtypes = [
             C.c_void_p, C.c_double, C.c_int, C.POINTER(OracleSource), C.c_int,
             C.c_void_p, C.c_void_p, C.c_int]
@@ -88,7 +89,10 @@ def _ptr(a, ct):
 class Oracle:
     """One mesh + model on the CPU, FP32 (``precision=4``) or FP64 (8)."""
 
-    def __init__(self, db, precision=8, nthreads=None, stacey=True):
+    def __init__(self, db, precision=8, nthreads=None, stacey=True, flush_subnormals=False):
+        """``flush_subnormals``: run with FP32 subnormals flushed to zero
+        (x86 FTZ/DAZ), which only changes values below 1.2e-38 and avoids
+        the cores' slow path for them on large FP32 runs."""
         self.db = db
         self.precision = precision
         nthreads = nthreads or os.cpu_count() or 1
@@ -128,6 +132,8 @@ class Oracle:
         self._h = lib().oracle_create(C.byref(self._mesh), precision, nthreads)
         if not self._h:
             raise RuntimeError("oracle_create failed")
+        if flush_subnormals:
+            lib().oracle_set_flush_subnormals(self._h, 1)
         self.nstep = 0
         self.nrec = 0
 

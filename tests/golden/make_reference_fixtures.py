@@ -1,8 +1,9 @@
 """Copies small input files of the reference's toy examples into
 tests/golden/reference_files/ and records the structure of two binary
 files (a model file and a SAC trace) in reference_files/summary.json, for
-the file-format tests.  Run from the repository root where the reference
-tree is available; the tests use only what this writes."""
+the file-format tests.  Usage: python make_reference_fixtures.py
+<SpecFWAT source tree> (or SPECFWAT_REFERENCE_ROOT set); the tests use only
+what this writes."""
 import json
 import os
 import shutil
@@ -11,7 +12,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPECFWAT_REFERENCE_ROOT", "")
+if not REF or not os.path.isdir(REF):
+    sys.exit("usage: make_reference_fixtures.py <SpecFWAT source tree>")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_files")
 os.makedirs(OUT, exist_ok=True)
 

@@ -1,8 +1,8 @@
 """File formats at either side of the solver (specfwat_b200.fileio).
 
 Pinned against the reference's own example files: the CMTSOLUTION and
-STATIONS copies in tests/golden/reference_files/, and, when the reference
-tree is present, a model file (Fortran unformatted record) and a SAC trace
+STATIONS copies in tests/golden/reference_files/, and, when
+SPECFWAT_REFERENCE_ROOT names a SpecFWAT source tree, a model file (Fortran unformatted record) and a SAC trace
 whose structure tests/golden/make_reference_fixtures.py recorded.
 """
 import json
@@ -15,7 +15,9 @@ import pytest
 from specfwat_b200 import fileio as F
 
 HERE = os.path.join(os.path.dirname(__file__), "golden", "reference_files")
-REF = "/root/reference"
+# root of a SpecFWAT source tree, for the checks against its binary example
+# files; skipped when unset
+REF = os.environ.get("SPECFWAT_REFERENCE_ROOT", "")
 SUMMARY = json.load(open(os.path.join(HERE, "summary.json")))
 
 
@@ -34,7 +36,8 @@ def test_cmtsolution_and_stations():
     assert xyz.shape == (len(st), 3) and xyz[0, 0] == pytest.approx(st[0]["lon"])
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF),
+                    reason="SPECFWAT_REFERENCE_ROOT not set to a SpecFWAT source tree")
 def test_reference_model_file_and_sac():
     m = SUMMARY["model_bin"]
     k = F.read_kernel_bin(os.path.join(REF, m["file"]))

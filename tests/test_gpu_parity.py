@@ -165,7 +165,7 @@ def test_graph_equals_stepwise(gpu, small):
 
 
 @pytest.mark.parametrize("nev,variant", [(2, 0), (9, 0), (9, 5), (12, 6), (9, 7), (12, 8),
-                                         (9, 9), (12, 10)])
+                                         (9, 9), (12, 10), (9, 11), (16, 11), (12, 12)])
 def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
@@ -187,6 +187,47 @@ def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev, variant):
         sim.close()
     for q in range(3):
         assert rel_l2(kern["fp16"][q], kern["fp32"][q]) < 5e-3
+
+
+def test_fp64_kernel_sum_over_distinct_events_matches_oracle(gpu):
+    """sem_sum_kernels over a batch of distinct events (own source, own
+    observed data) against the sum of the FP64 oracle's per-event kernels,
+    and against the FP64 sum of the device's own per-event kernels."""
+    db = D.build("mini")
+    rec = D.surface_receivers(db.box, 3)
+    rng = np.random.default_rng(77)
+    nev, nstep, dt = 3, 300, 0.02
+    box = db.box
+    ev = [(rng.uniform(0.3, 0.7) * box.lx, rng.uniform(0.3, 0.7) * box.ly,
+           -rng.uniform(0.2, 0.6) * box.lz, D.random_moment_tensor(rng),
+           rng.uniform(0.8, 1.3)) for _ in range(nev)]
+    obs = [1e-5 * rng.standard_normal((len(rec), 3, nstep)) for _ in range(nev)]
+    mesh = S.Mesh(db)
+    b = S.Simulation(mesh, nstep, dt, nev=nev, store="fp16", use_graph=True,
+                     max_receivers=len(rec), kernel_variant=11)
+    b.set_sources([S.make_source(*e) for e in ev])
+    b.set_receivers(rec)
+    b.iterate_time(1, save_forward=True)
+    for e in range(nev):
+        b.measure_l2(e, obs[e])
+    b.iterate_time(3)
+    ksum = b.sum_kernels()
+    kev = [b.save_adjoint_kernels(e) for e in range(nev)]
+    b.close()
+    mesh.close()
+    osum = np.zeros_like(ksum)
+    for e in range(nev):
+        o = Oracle(db, precision=8)
+        osyn = o.forward(dt, nstep, Oracle.source(*ev[e]), rec, save_forward=True)
+        _, adj = l2_adjoint_source(osyn, obs[e], dt)
+        osum += o.adjoint(rec, adj)
+    dev_sum = np.sum(kev, axis=0)
+    for q in range(6):
+        assert rel_l2(ksum[q], osum[q]) < KERN_TOL, (q, rel_l2(ksum[q], osum[q]))
+        assert rel_l2(ksum[q], dev_sum[q]) < 1e-12, q
+    # distinct events: the sum is not a multiple of any one event's kernel
+    c = np.vdot(ksum[1], kev[0][1]) / np.vdot(kev[0][1], kev[0][1])
+    assert rel_l2(c * kev[0][1], ksum[1]) > 0.05
 
 
 def test_state_errors(gpu, small):
