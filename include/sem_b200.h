@@ -220,6 +220,29 @@ int sem_set_stream(sem_run *run, void *stream);
  * dev_out[6][nspec][125] (e.g. a buffer handed to a collective). */
 int sem_sum_kernels_device(sem_run *run, double *dev_out);
 
+/* Boundary store held partly in host memory (the reference keeps the
+ * whole store on disk: absorb_field.bin, src/specfem_interface/
+ * specfem_api.f90:359-361, deleted at src/preproc/prepare_fwd.f90:376-377).
+ * device_store_bytes = 0 (default): the whole store is in HBM.  > 0: at
+ * most that many device bytes hold the store; < 0: the device memory free
+ * when the store is first allocated, less the kernel-output and
+ * measurement buffers and 1 GiB.  When the store does not fit, it is cut
+ * into chunks of graph_steps steps (all events) and the device keeps D >= 2
+ * chunk slots; during the forward run each chunk that a later chunk will
+ * overwrite is copied to pinned host memory on a copy stream, and during
+ * the adjoint run it comes back into its slot right after the slot's
+ * occupant is replayed, at least one launch ahead of its use.  One
+ * cudaMemcpyAsync per chunk (plus one for the FP16 scales).  Fails with
+ * SEM_ERR_NOMEM when fewer than 2 slots fit or the pinned host memory
+ * cannot be had.  Batched runs (sem_iterate_time) only; changing it drops a
+ * saved forward state.  No counterpart for the call itself. */
+int sem_set_store_spill(sem_run *run, long long device_store_bytes);
+/* Store layout after the first saved forward run: chunk_steps and
+ * device_slots are 0 when the whole store is resident; chunks = chunk
+ * count; device and pinned host bytes of the store. */
+int sem_store_info(sem_run *run, int *chunk_steps, int *device_slots, int *chunks,
+                   long long *device_bytes, long long *host_bytes);
+
 /* Average device time in ms of each kernel of one step - forces, stacey,
  * points, update - measured with CUDA events over nsteps further steps of
  * the current state (sim_type 1 or 3 kernels).  Advances the wavefields. */

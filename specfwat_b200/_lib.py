@@ -32,6 +32,7 @@ EXPORTS = (
     "sem_last_loop_ms", "sem_last_launch_count", "sem_set_observed",
     "sem_set_stream", "sem_sum_kernels_device", "sem_time_kernels",
     "sem_kernel_variants", "sem_measure_l2_noalloc",
+    "sem_set_store_spill", "sem_store_info",
     "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
     "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
     "sem_smooth_pde", "sem_measure_waveform", "sem_measure_waveform_dev",
@@ -176,6 +177,10 @@ def load():
         "sem_hessian_precond": (C.c_int, [fp, C.c_longlong, ip, fp]),
         "sem_depth_precond": (C.c_int, [vp, fp, ip, ip, ip, fp]),
         "sem_set_injection": (C.c_int, [vp, ip, fp, fp, ip, ip, ip]),
+        "sem_set_store_spill": (C.c_int, [vp, C.c_longlong]),
+        "sem_store_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                     C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -398,6 +398,18 @@ struct sem_run_s {
   DevArray<int> rec_ispec;
   DevArray<unsigned char> store;
   DevArray<float> scale;
+  // boundary store host spill (sem_set_store_spill): the store is cut into
+  // chunks of ring_c steps (one graph launch); chunk k lives in device slot
+  // k % ring_d; chunks 0 .. ring_n - ring_d - 1 are copied to pinned host
+  // memory during the forward run and fetched back, one launch ahead,
+  // during the adjoint run.  ring_d == 0: the whole store is resident.
+  long long spill_budget = 0;     // device bytes for the store; 0 = resident, < 0 = auto
+  int ring_c = 0, ring_d = 0, ring_n = 0;
+  unsigned char* h_spill = nullptr;   // [ring_n - ring_d] chunks, pinned
+  float* h_spill_scale = nullptr;
+  size_t h_spill_bytes = 0;
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> ev_chunk, ev_launch;  // per chunk / per launch
   DevArray<float> k_rho, k_mu, k_kappa;
   DevArray<float> k_hess;          // approximate Hessian [nglob][nevp]
   bool hess_on = false;            // accumulate it in adjoint runs
@@ -453,6 +465,12 @@ struct sem_run_s {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (check_ev) cudaEventDestroy(check_ev);
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
+    for (auto e : ev_chunk) cudaEventDestroy(e);
+    for (auto e : ev_launch) cudaEventDestroy(e);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (h_spill) cudaFreeHost(h_spill);
+    if (h_spill_scale) cudaFreeHost(h_spill_scale);
     if (h_lflags) cudaFreeHost(h_lflags);
     if (h_halt) cudaFreeHost(h_halt);
     if (own_stream) cudaStreamDestroy(own_stream);
@@ -462,6 +480,12 @@ struct sem_run_s {
   size_t store_elem() const { return cfg.store_kind == SEM_STORE_FP16 ? 2 : 4; }
   size_t store_bytes_per_event() const {
     return (size_t)nstep * mesh->nf * 75 * store_elem();
+  }
+  bool ring() const { return ring_d > 0; }
+  // one chunk of ring_c records of all events: store bytes and scale floats
+  size_t chunk_store_bytes() const { return (size_t)nev * ring_c * mesh->nf * 75 * store_elem(); }
+  size_t chunk_scale_floats() const {
+    return cfg.store_kind == SEM_STORE_FP16 ? (size_t)nev * ring_c * mesh->nf : 0;
   }
 
   StepArgs args(bool adjoint) const {
@@ -504,8 +528,16 @@ struct sem_run_s {
       L.rec_w = rec_w.p + (size_t)e * nrec_max * 125;
       L.seis = seis.p + (size_t)e * nrec_max * 3 * ns;
       L.adj = adj.p + (size_t)e * nrec_max * 3 * ns;
-      L.store = store.p ? store.p + (size_t)e * store_bytes_per_event() : nullptr;
-      L.scale = scale.p ? scale.p + (size_t)e * ns * mesh->nf : nullptr;
+      if (ring()) {
+        // lane e's rows of slot 0; slot s starts nev * ring_c rows further
+        L.store = store.p ? store.p + (size_t)e * ring_c * mesh->nf * 75 * store_elem() : nullptr;
+        L.scale = scale.p ? scale.p + (size_t)e * ring_c * mesh->nf : nullptr;
+        L.ring_c = ring_c;
+        L.ring_d = ring_d;
+      } else {
+        L.store = store.p ? store.p + (size_t)e * store_bytes_per_event() : nullptr;
+        L.scale = scale.p ? scale.p + (size_t)e * ns * mesh->nf : nullptr;
+      }
       if (e < (int)inj.size() && inj[e].buf) {
         const size_t npt3 = (size_t)mesh->nf * 25 * 3;
         L.inj_v = inj[e].buf;
@@ -1027,8 +1059,83 @@ static int ensure_adjoint_buffers(sem_run* r) {
   return SEM_OK;
 }
 
+// Device bytes reserved beside the store in the automatic spill budget:
+// the FP64 kernel output and sum (6 values per element point each), the
+// measurement buffers and 1 GiB of slack.
+static size_t spill_reserve(const sem_run* r) {
+  const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+  return 2 * 6 * ne * 8 + (size_t)r->nrec_max * 3 * r->nstep * 8 * 2 + ((size_t)1 << 30);
+}
+
+static void release_ring(sem_run* r) {
+  if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
+  if (r->h_spill) cudaFreeHost(r->h_spill);
+  if (r->h_spill_scale) cudaFreeHost(r->h_spill_scale);
+  r->h_spill = nullptr;
+  r->h_spill_scale = nullptr;
+  r->h_spill_bytes = 0;
+  for (auto e : r->ev_chunk) cudaEventDestroy(e);
+  for (auto e : r->ev_launch) cudaEventDestroy(e);
+  r->ev_chunk.clear();
+  r->ev_launch.clear();
+  r->ring_c = r->ring_d = r->ring_n = 0;
+}
+
 static int ensure_store(sem_run* r) {
   if (r->mesh->nf == 0 || r->store.p) return SEM_OK;
+  release_ring(r);
+  const size_t full = r->store_bytes_per_event() * r->nev +
+                      (r->cfg.store_kind == SEM_STORE_FP16
+                           ? (size_t)r->nev * r->nstep * r->mesh->nf * 4 : 0);
+  if (r->spill_budget != 0) {
+    long long budget = r->spill_budget;
+    if (budget < 0) {
+      size_t fr = 0, tot = 0;
+      CK(cudaMemGetInfo(&fr, &tot));
+      budget = (long long)fr - (long long)spill_reserve(r);
+    }
+    r->ring_c = r->cfg.graph_steps;
+    r->ring_n = (r->nstep + r->ring_c - 1) / r->ring_c;
+    const size_t slot = r->chunk_store_bytes() + r->chunk_scale_floats() * 4;
+    const long long d = budget > 0 ? budget / (long long)slot : 0;
+    if ((size_t)budget >= full || d >= r->ring_n) {
+      r->ring_c = r->ring_n = 0;  // fits: resident
+    } else if (d < 2) {
+      r->ring_c = r->ring_n = 0;
+      return fail(SEM_ERR_NOMEM,
+                  "boundary store spill: a device budget of %lld bytes holds %lld chunk slots "
+                  "of %zu bytes; at least 2 are needed",
+                  budget, d, slot);
+    } else {
+      r->ring_d = (int)d;
+    }
+  }
+  if (r->ring()) {
+    const int spilled = r->ring_n - r->ring_d;
+    CKM(r->store.alloc(r->chunk_store_bytes() * r->ring_d), "boundary store ring");
+    if (r->cfg.store_kind == SEM_STORE_FP16)
+      CKM(r->scale.alloc(r->chunk_scale_floats() * r->ring_d), "boundary store ring scales");
+    r->h_spill_bytes = r->chunk_store_bytes() * spilled;
+    cudaError_t e = cudaHostAlloc((void**)&r->h_spill, r->h_spill_bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess && r->chunk_scale_floats())
+      e = cudaHostAlloc((void**)&r->h_spill_scale, r->chunk_scale_floats() * 4 * spilled,
+                        cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      const size_t want = r->h_spill_bytes;
+      release_ring(r);
+      r->store.reset();
+      r->scale.reset();
+      return fail(SEM_ERR_NOMEM, "pinned host memory for the spilled boundary store (%zu bytes): %s",
+                  want, cudaGetErrorString(e));
+    }
+    if (!r->copy_stream) CK(cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking));
+    r->ev_chunk.assign(r->ring_n, nullptr);
+    r->ev_launch.assign(r->ring_n, nullptr);
+    for (auto& ev : r->ev_chunk) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (auto& ev : r->ev_launch) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    return SEM_OK;
+  }
   CKM(r->store.alloc(r->store_bytes_per_event() * r->nev), "boundary store");
   if (r->cfg.store_kind == SEM_STORE_FP16)
     CKM(r->scale.alloc((size_t)r->nev * r->nstep * r->mesh->nf), "boundary store scales");
@@ -1135,10 +1242,70 @@ static void queue_check(sem_run* r, bool both, int s_off) {
   launch_halt_lanes(r->lanes.p, r->nev, r->lflags.p, r->halt_step.p, s_off, r->stream);
 }
 
+// Boundary store ring: the stream work around launch unit g (steps
+// [g K, (g+1) K) of the phase, K = ring_c).  Forward (saving): the unit
+// writes chunk g into slot g % D once the spill of chunk g - D, the slot's
+// previous chunk, has left; chunks below N - D are then spilled to the host
+// on the copy stream.  Adjoint: unit g replays records nstep-1-j for its j,
+// i.e. chunks lo..hi; a spilled chunk k is fetched into slot k % D right
+// after the unit that replays the last record of chunk k + D (the slot's
+// occupant), at least (D - 1) K + 1 steps before chunk k is first needed.
+static int ring_before(sem_run* r, bool adjoint, int g, bool save) {
+  const int K = r->ring_c, D = r->ring_d, N = r->ring_n;
+  if (!adjoint) {
+    if (save && g >= D && g - D < N - D) CK(cudaStreamWaitEvent(r->stream, r->ev_chunk[g - D], 0));
+    return SEM_OK;
+  }
+  const int ns = r->nstep;
+  const int jhi = std::min((g + 1) * K, ns) - 1;
+  const int lo = (ns - 1 - jhi) / K, hi = (ns - 1 - g * K) / K;
+  for (int k = lo; k <= hi && k < N - D; ++k)
+    CK(cudaStreamWaitEvent(r->stream, r->ev_chunk[k], 0));
+  return SEM_OK;
+}
+
+static int ring_after(sem_run* r, bool adjoint, int g, bool save) {
+  const int K = r->ring_c, D = r->ring_d, N = r->ring_n;
+  const size_t cs = r->chunk_store_bytes(), cf = r->chunk_scale_floats();
+  if (!adjoint) {
+    if (!save || g >= N - D) return SEM_OK;
+    CK(cudaEventRecord(r->ev_launch[g], r->stream));
+    CK(cudaStreamWaitEvent(r->copy_stream, r->ev_launch[g], 0));
+    const int slot = g % D;
+    CK(cudaMemcpyAsync(r->h_spill + (size_t)g * cs, r->store.p + (size_t)slot * cs, cs,
+                       cudaMemcpyDeviceToHost, r->copy_stream));
+    if (cf)
+      CK(cudaMemcpyAsync(r->h_spill_scale + (size_t)g * cf, r->scale.p + (size_t)slot * cf,
+                         cf * 4, cudaMemcpyDeviceToHost, r->copy_stream));
+    CK(cudaEventRecord(r->ev_chunk[g], r->copy_stream));
+    return SEM_OK;
+  }
+  bool recorded = false;
+  for (int k = 0; k < N - D; ++k) {
+    // unit replaying record (k + D) K, the last one of chunk k + D
+    const int last_use = (r->nstep - 1 - (k + D) * K) / K;
+    if (last_use != g) continue;
+    if (!recorded) {
+      CK(cudaEventRecord(r->ev_launch[g], r->stream));
+      CK(cudaStreamWaitEvent(r->copy_stream, r->ev_launch[g], 0));
+      recorded = true;
+    }
+    const int slot = k % D;
+    CK(cudaMemcpyAsync(r->store.p + (size_t)slot * cs, r->h_spill + (size_t)k * cs, cs,
+                       cudaMemcpyHostToDevice, r->copy_stream));
+    if (cf)
+      CK(cudaMemcpyAsync(r->scale.p + (size_t)slot * cf, r->h_spill_scale + (size_t)k * cf,
+                         cf * 4, cudaMemcpyHostToDevice, r->copy_stream));
+    CK(cudaEventRecord(r->ev_chunk[k], r->copy_stream));
+  }
+  return SEM_OK;
+}
+
 // Queue the step loop of one phase (graphs or per-step launches).
 static int run_loop(sem_run* r, bool adjoint) {
   long long launches = 0;
   StepArgs a = r->args(adjoint);
+  const bool save = !adjoint && !r->h_lanes.empty() && r->h_lanes[0].save;
   CK(cudaEventRecord(r->e0, r->stream));
   if (r->cfg.use_graph) {
     const int K = r->cfg.graph_steps;
@@ -1164,9 +1331,18 @@ static int run_loop(sem_run* r, bool adjoint) {
     const int nlaunch = (r->nstep + K - 1) / K;
     const int per_step = (r->mesh->nf > 0 ? 4 : 3);
     const int ce = r->cfg.check_every;
+    const bool ring = r->ring() && (adjoint || save);
     for (int g = 0; g < nlaunch; ++g) {
+      if (ring) {
+        int rc = ring_before(r, adjoint, g, save);
+        if (rc) return rc;
+      }
       CK(cudaGraphLaunch(gx, r->stream));
       launches += (long long)K * per_step + 1;
+      if (ring) {
+        int rc = ring_after(r, adjoint, g, save);
+        if (rc) return rc;
+      }
       // stability check at the first graph boundary at or after every
       // check_every steps, and after the last graph (each graph advances
       // the lanes' device it0 by K)
@@ -1177,17 +1353,32 @@ static int run_loop(sem_run* r, bool adjoint) {
     }
   } else {
     const int ce = r->cfg.check_every;
+    const bool ring = r->ring() && (adjoint || save);
+    const int K = ring ? r->ring_c : r->nstep;
     for (int s = 0; s < r->nstep; ++s) {
+      if (ring && s % K == 0) {
+        int rc = ring_before(r, adjoint, s / K, save);
+        if (rc) return rc;
+      }
       a.s = s;
       launches += launch_forces(a, adjoint, r->stream);
       launches += launch_boundary(a, adjoint, r->stream);
       launches += launch_points(a, r->stream);
       launches += launch_update(a, adjoint, r->stream);
+      if (ring && ((s + 1) % K == 0 || s == r->nstep - 1)) {
+        int rc = ring_after(r, adjoint, s / K, save);
+        if (rc) return rc;
+      }
       if (ce > 0 && ((s + 1) % ce == 0 || s == r->nstep - 1)) {
         queue_check(r, adjoint, s + 1);
         launches += adjoint ? 3 : 2;
       }
     }
+  }
+  if (r->copy_stream && r->ring()) {
+    // the phase ends when its copies have too
+    CK(cudaEventRecord(r->ev_launch[0], r->copy_stream));
+    CK(cudaStreamWaitEvent(r->stream, r->ev_launch[0], 0));
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(r->e1, r->stream));
@@ -1640,6 +1831,34 @@ int sem_set_stream(sem_run* r, void* stream) {
   if (!r) return fail(SEM_ERR_ARG, "null run");
   CK(cudaStreamSynchronize(r->stream));
   r->stream = stream ? (cudaStream_t)stream : r->own_stream;
+  return SEM_OK;
+}
+
+int sem_set_store_spill(sem_run* r, long long device_store_bytes) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  if (r->lanes_mode)
+    return fail(SEM_ERR_STATE, "lane-driven runs keep their boundary stores resident");
+  if (device_store_bytes == r->spill_budget) return SEM_OK;
+  CK(cudaStreamSynchronize(r->stream));
+  release_ring(r);
+  r->store.reset();
+  r->scale.reset();
+  r->spill_budget = device_store_bytes;
+  r->fwd_saved = false;  // a saved store of the old layout is gone
+  return SEM_OK;
+}
+
+int sem_store_info(sem_run* r, int* chunk_steps, int* device_slots, int* chunks,
+                   long long* device_bytes, long long* host_bytes) {
+  if (!r) return fail(SEM_ERR_ARG, "null run");
+  const size_t dev = r->store.bytes() + r->scale.bytes();
+  const size_t host = r->h_spill_bytes + (r->h_spill_scale ? r->chunk_scale_floats() * 4 *
+                                                                 (r->ring_n - r->ring_d) : 0);
+  if (chunk_steps) *chunk_steps = r->ring_c;
+  if (device_slots) *device_slots = r->ring_d;
+  if (chunks) *chunks = r->ring_n;
+  if (device_bytes) *device_bytes = (long long)dev;
+  if (host_bytes) *host_bytes = (long long)host;
   return SEM_OK;
 }
 

@@ -30,7 +30,10 @@ struct LaneDesc {
   int save;          // forward phase: write the boundary store
   int src_ispec;
   int nrec;
-  int pad0, pad1;
+  // boundary store ring (host spill): 0 when the whole store is resident;
+  // else records of ring_c steps per chunk in ring_d device slots, record
+  // `it` at row ((it / ring_c) % ring_d) * nev * ring_c + it % ring_c
+  int ring_c, ring_d;
   const float* stf;      // [nstep]      source time function samples
   const float* srcarr;   // [125][3]     moment tensor : grad(phi_abc)
   const int* rec_ispec;  // [nrec]

@@ -2806,15 +2806,23 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
     }
   }
   if (A.store_fp16) __syncthreads();
+  // row of record n in the lane's store (resident: n; ring: its chunk's
+  // device slot, slots nev * ring_c rows apart)
+  auto row_of = [&](int n) -> size_t {
+    if (L->ring_c <= 0) return (size_t)n;
+    const int c = L->ring_c;
+    return (size_t)((n / c) % L->ring_d) * (size_t)nev * c + (size_t)(n % c);
+  };
   if (valid && save) {
-    const size_t base = ((size_t)it * nf + f) * 75 + p * 3;
+    const size_t row = row_of(it);
+    const size_t base = (row * nf + f) * 75 + p * 3;
     if (A.store_fp16) {
       const float mx = __uint_as_float(s_max[fl * LBB + lane]);
       const float inv = mx > 0.f ? 32768.0f / mx : 0.f;
       __half* st = (__half*)L->store;
 #pragma unroll
       for (int c = 0; c < 3; ++c) st[base + c] = __float2half_rn(sv[c] * inv);
-      if (p == 0) L->scale[(size_t)it * nf + f] = mx * (1.0f / 32768.0f);
+      if (p == 0) L->scale[row * nf + f] = mx * (1.0f / 32768.0f);
     } else {
       float* st = (float*)L->store;
 #pragma unroll
@@ -2822,11 +2830,11 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
     }
   }
   if (valid && replay) {
-    const int n = nstep - 1 - it;
-    const size_t base = ((size_t)n * nf + f) * 75 + p * 3;
+    const size_t row = row_of(nstep - 1 - it);
+    const size_t base = (row * nf + f) * 75 + p * 3;
     float val[3];
     if (A.store_fp16) {
-      const float sc = L->scale[(size_t)n * nf + f];
+      const float sc = L->scale[row * nf + f];
       const __half* st = (const __half*)L->store;
 #pragma unroll
       for (int c = 0; c < 3; ++c) val[c] = __half2float(st[base + c]) * sc;

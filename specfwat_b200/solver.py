@@ -279,6 +279,21 @@ class Simulation:
         return out
 
     # -- serving primitives (one event per lane, lanes advance together) --
+    def set_store_spill(self, device_bytes: int):
+        """Hold the boundary store partly in pinned host memory: at most
+        ``device_bytes`` of HBM for it (0: all resident; -1: what is free when
+        the store is allocated, less the output buffers)."""
+        check(_lib.load().sem_set_store_spill(self._h, int(device_bytes)))
+
+    def store_info(self) -> dict:
+        """Layout of the boundary store after the first saved forward run."""
+        c, d, n = C.c_int(), C.c_int(), C.c_int()
+        db, hb = C.c_longlong(), C.c_longlong()
+        check(_lib.load().sem_store_info(self._h, C.byref(c), C.byref(d), C.byref(n),
+                                         C.byref(db), C.byref(hb)))
+        return {"chunk_steps": c.value, "device_slots": d.value, "chunks": n.value,
+                "device_bytes": db.value, "host_bytes": hb.value}
+
     def lane_store_bytes(self, nstep: int) -> int:
         return int(_lib.load().sem_lane_store_bytes(self._h, nstep))
 
