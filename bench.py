@@ -770,6 +770,8 @@ def run_large(args):
     fms = sim.time_kernels(1, 10)
     ams = sim.time_kernels(3, 10)
     sim.close()
+    print(f"large batch: ms {ms}, store {info}, fwd {fms}, adj {ams}", file=sys.stderr,
+          flush=True)
     k = ksum.cpu().numpy()
     finite = bool(np.isfinite(k).all() and np.abs(k[:3]).max() > 0)
     mesh.close()
@@ -789,9 +791,9 @@ def run_large(args):
         "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "large box 96x96x48 el over 384x384x192 km (28,607,425 GLL "
-                               "pts), 3 layers + 3% perturbation, NSTEP %d, dt 0.015 s, "
-                               "100 receivers, fwd + L2 adjoint + adjoint/backward with "
-                               "kernels" % NS,
+                               f"pts), 3 layers + 3 percent perturbation, NSTEP {NS}, dt "
+                               "0.015 s, 100 receivers, fwd + L2 adjoint + adjoint/backward "
+                               "with kernels",
                    "events_per_step": E, "store": "fp16 per-face scaled, host-spill ring",
                    "warmup": "one 100-step batch (autotune, graph capture)",
                    "l2": "inputs larger than L2"},
