@@ -13,6 +13,9 @@ the golden vectors in this directory:
 * ``get_1d_precond``, ``zprecond_gll`` src/postproc/zprecond.f90:11-71 (FP32)
 * ``coswin``, ``create_taper``  src/postproc/taper_3D_mod.f90 (FP32)
 * ``locate_bissection``, ``interp3``  src/shared/utils.f90:1089-1159,1490-1525
+* ``get_nearest_bound_idx``, ``interp3_nearest_simple``  src/shared/utils.f90:
+  1262-1325, and ``model_external_values`` (one GLL point)
+  src/patch/model_external_values.f90:206-273
 * ``project_sem2fd``: compute_interpolation_coeff_FD_SEM + Project_model_
   SEM2FD_grid (src/shared/projection_on_FD_grid_mod_fwat.f90:186-596), one
   slice, regular elements (reference coordinates linear in x, y, z, clamped
@@ -566,6 +569,63 @@ def interp3(valx, valy, valz, valin, x, y, z):
             + xix1 * yiy2 * ziz1 * x2x1 * y1y2 * z2z1 * V(kx + 1, ky, kz + 1)
             + xix1 * yiy1 * ziz2 * x2x1 * y2y1 * z1z2 * V(kx + 1, ky + 1, kz)
             + xix1 * yiy1 * ziz1 * x2x1 * y2y1 * z2z1 * V(kx + 1, ky + 1, kz + 1))
+
+
+def get_nearest_bound_idx(x, x_sem):
+    n = len(x)
+    indx = None   # left undefined by the Fortran for a point inside the axis
+    if x_sem < x[0]:
+        indx = 1
+    elif x_sem > x[n - 1]:
+        indx = n - 1
+    return indx
+
+
+def interp3_nearest_simple(x, y, z, model, x_sem, y_sem, z_sem):
+    nx, ny, nz = len(x), len(y), len(z)
+    min_dist = 1.0e30
+    value = None
+    indx = locate_bissection(x, nx, x_sem)
+    indy = locate_bissection(y, ny, y_sem)
+    indz = locate_bissection(z, nz, z_sem)
+    m = 2
+    if indx != -1:
+        kx = min(max(indx - (m - 1) // 2, 1), nx + 1 - m)
+    else:
+        kx = get_nearest_bound_idx(x, x_sem)
+    if indy != -1:
+        ky = min(max(indy - (m - 1) // 2, 1), ny + 1 - m)
+    else:
+        ky = get_nearest_bound_idx(y, y_sem)
+    if indz != -1:
+        kz = min(max(indz - (m - 1) // 2, 1), nz + 1 - m)
+    else:
+        kz = get_nearest_bound_idx(z, z_sem)
+    for ifd in range(kx, kx + 1 + 1):
+        xfd = x[ifd - 1]
+        for jfd in range(ky, ky + 1 + 1):
+            yfd = y[jfd - 1]
+            for kfd in range(kz, kz + 1 + 1):
+                zfd = z[kfd - 1]
+                dist = math.sqrt((x_sem - xfd) ** 2 + (y_sem - yfd) ** 2 + (z_sem - zfd) ** 2)
+                if dist < min_dist and model[ifd - 1][jfd - 1][kfd - 1] != 0.0:
+                    min_dist = dist
+                    value = model[ifd - 1][jfd - 1][kfd - 1]
+    return value
+
+
+def model_external_values(x, y, z, vp, vs, rho, xsem, ysem, zsem):
+    """vp, vs, rho at one GLL point (model_external_values.f90:206-273)."""
+    if (xsem < x[0] or xsem > x[len(x) - 1] or ysem < y[0] or ysem > y[len(y) - 1]
+            or zsem < z[0] or zsem > z[len(z) - 1]):
+        r = interp3_nearest_simple(x, y, z, rho, xsem, ysem, zsem)
+        p = interp3_nearest_simple(x, y, z, vp, xsem, ysem, zsem)
+        s = interp3_nearest_simple(x, y, z, vs, xsem, ysem, zsem)
+    else:
+        r = interp3(x, y, z, rho, xsem, ysem, zsem)
+        p = interp3(x, y, z, vp, xsem, ysem, zsem)
+        s = interp3(x, y, z, vs, xsem, ysem, zsem)
+    return p, s, r
 
 
 def project_sem2fd(ibool, xstore, ystore, zstore, nspec, data, ox, oy, oz, hx, hy, hz,
