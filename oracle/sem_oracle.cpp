@@ -858,11 +858,14 @@ struct Solver {
 //     weights, ddat -= ...; then ddat *= rvol, dat_glob += ddat, and
 //     points of CPML elements reset to dat_bak = 0 (ZERO_PML)   (smooth.f90:244-370)
 //   * output dat(e) = dat_glob(ibool(e))
-// Regular elements only.  mapping 1 reproduces the reference's regular
-// branch, where all nine derivative terms (xix .. gammaz) are xix_regular
-// (smooth.f90:269-279, get_gradient_element_regular :648-689); mapping 0
-// uses the cube's diagonal mapping (xix = etay = gammaz = xix_regular,
-// zero off the diagonal).
+// Irregular elements (m.irreg[e] >= 0) take their nine mapping terms and
+// Jacobian at each point from m.geo, in the fluxes and in rvol_local
+// (smooth.f90:142-164 and the ispec_irreg branch :255-268).  For regular
+// elements, mapping 1 reproduces the reference's regular branch, where all
+// nine derivative terms (xix .. gammaz) are xix_regular (smooth.f90:269-279,
+// get_gradient_element_regular :648-689); mapping 0 uses the cube's
+// diagonal mapping (xix = etay = gammaz = xix_regular, zero off the
+// diagonal).
 // ---------------------------------------------------------------------------
 
 struct SmoothParams {
@@ -898,22 +901,32 @@ void smooth_run(const oracle_mesh& m, int nfield, const float* dat_in, const int
       DWt[i][l] = (T)(g.w[l] * g.D[l][i]); // hprimewgll_xx(l,i)
     }
   }
-  const T xix = (T)(float)m.xix, jac = (T)(float)m.jac;
+  const T xix = (T)(float)m.xix, jac_reg = (T)(float)m.jac;
   const T cv = (T)q.cv, ch = (T)q.ch;
-  // mapping rows: derivative terms of xi, eta, gamma along x, y, z
-  T M[3][3];
+  // mapping rows of a regular element: derivative terms of xi, eta, gamma
+  // along x, y, z
+  T Mreg[3][3];
   for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) M[a][b] = (mapping == 1 || a == b) ? xix : (T)0;
+    for (int b = 0; b < 3; ++b) Mreg[a][b] = (mapping == 1 || a == b) ? xix : (T)0;
   const size_t ne = (size_t)m.nspec * NG3;
-  std::vector<T> rvol_local(NG3), rvol(m.nglob, (T)0);
-  for (int k = 0; k < NG; ++k)
-    for (int j = 0; j < NG; ++j)
-      for (int i = 0; i < NG; ++i) {
-        const double weight = g.w[i] * g.w[j] * g.w[k];
-        rvol_local[i + NG * j + NG2 * k] = (T)((double)(float)m.jac * weight);
-      }
+  // mapping row of an irregular element, or null
+  auto geo_of = [&](int e) -> const float* {
+    return (m.irreg && m.irreg[e] >= 0) ? m.geo + (size_t)m.irreg[e] * NG3 * 10 : nullptr;
+  };
+  std::vector<T> rvol_local(ne), rvol(m.nglob, (T)0);
+  for (int e = 0; e < m.nspec; ++e) {
+    const float* G = geo_of(e);
+    for (int k = 0; k < NG; ++k)
+      for (int j = 0; j < NG; ++j)
+        for (int i = 0; i < NG; ++i) {
+          const int p = i + NG * j + NG2 * k;
+          const double weight = g.w[i] * g.w[j] * g.w[k];
+          const float jacobianl = G ? G[p * 10 + 9] : (float)m.jac;
+          rvol_local[(size_t)e * NG3 + p] = (T)((double)jacobianl * weight);
+        }
+  }
   for (int e = 0; e < m.nspec; ++e)
-    for (int p = 0; p < NG3; ++p) rvol[m.ibool[e * NG3 + p]] += rvol_local[p];
+    for (int p = 0; p < NG3; ++p) rvol[m.ibool[e * NG3 + p]] += rvol_local[(size_t)e * NG3 + p];
   for (int ig = 0; ig < m.nglob; ++ig) rvol[ig] = (T)1 / rvol[ig];
   std::vector<char> cpml_pt(m.nglob, 0);
   if (is_cpml)
@@ -939,17 +952,26 @@ void smooth_run(const oracle_mesh& m, int nfield, const float* dat_in, const int
     std::fill(dat_glob.begin(), dat_glob.end(), (T)0);
     for (int e = 0; e < m.nspec; ++e)
       for (int p = 0; p < NG3; ++p)
-        dat_glob[m.ibool[e * NG3 + p]] += (T)din[(size_t)e * NG3 + p] * rvol_local[p];
+        dat_glob[m.ibool[e * NG3 + p]] +=
+            (T)din[(size_t)e * NG3 + p] * rvol_local[(size_t)e * NG3 + p];
     for (int ig = 0; ig < m.nglob; ++ig) dat_glob[ig] = dat_glob[ig] * rvol[ig];
     for (int it = 0; it < q.nstep; ++it) {
       std::fill(ddat.begin(), ddat.end(), (T)0);
       for (int e = 0; e < m.nspec; ++e) {
         const int* ib = &m.ibool[(size_t)e * NG3];
+        const float* G = geo_of(e);
         T s[NG3], st1[NG3], st2[NG3], st3[NG3];
         for (int p = 0; p < NG3; ++p) s[p] = dat_glob[ib[p]];
         for (int k = 0; k < NG; ++k)
           for (int j = 0; j < NG; ++j)
             for (int i = 0; i < NG; ++i) {
+              T M[3][3];
+              T jac = jac_reg;
+              const int pq = i + NG * j + NG2 * k;
+              for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                  M[a][b] = G ? (T)G[pq * 10 + 3 * a + b] : Mreg[a][b];
+              if (G) jac = (T)G[pq * 10 + 9];
               T t1 = 0, t2 = 0, t3 = 0;
               for (int l = 0; l < NG; ++l) t1 += s[l + NG * j + NG2 * k] * D[i][l];
               for (int l = 0; l < NG; ++l) t2 += s[i + NG * l + NG2 * k] * D[j][l];

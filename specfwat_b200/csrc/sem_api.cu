@@ -563,6 +563,8 @@ int mesh_smooth_view(const sem_mesh_s* m, SmoothMeshView* out) {
   out->x = m->h_x.data();
   out->y = m->h_y.data();
   out->z = m->h_z.data();
+  out->irreg = m->irreg.p;
+  out->geo = m->geo.p;
   return SEM_OK;
 }
 }  // namespace sem

@@ -199,6 +199,10 @@ struct SmoothMeshView {
   const int* order;       // device [nspec] element traversal order
   const int* h_ibool;     // host copy of ibool
   const float *x, *y, *z; // host [nglob] coordinates
+  // irregular elements (both null when all are regular): device irreg[e] =
+  // -1 or the row of geo [nirr][125][10] (xix..gammaz, jacobian)
+  const int* irreg;
+  const float* geo;
 };
 int mesh_smooth_view(const ::sem_mesh_s* m, SmoothMeshView* out);
 

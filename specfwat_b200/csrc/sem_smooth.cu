@@ -18,12 +18,16 @@
 // volume fit the 126 MB L2, so a step runs from L2.  Steps are replayed from
 // a CUDA graph of 16 steps.
 //
-// Regular elements only.  `mapping` selects the element mapping terms: the
-// reference's regular branch sets all nine (xix .. gammaz) to xix_regular
-// (smooth.f90:269-279, smooth_sem_pde.cu:161-170), which makes the operator
-// a diffusion along (1,1,1) with coefficient 3(cv + 2ch), several times the
-// stability bound that the step count assumes; SEM_SMOOTH_MAP_CUBE uses the
-// cube's diagonal mapping (xix = etay = gammaz = xix_regular).
+// Irregular (deformed) elements take their stored mapping terms and
+// Jacobian at every GLL point, in the fluxes and in the lumped volume
+// rvol_local = jacobian * w_i w_j w_k (smooth.f90:142-164 and its
+// ispec_irreg branch :255-268; smooth_sem_pde.cu:149-160).  For regular
+// elements `mapping` selects the mapping terms: the reference's regular
+// branch sets all nine (xix .. gammaz) to xix_regular (smooth.f90:269-279,
+// smooth_sem_pde.cu:161-170), which makes the operator a diffusion along
+// (1,1,1) with coefficient 3(cv + 2ch), several times the stability bound
+// that the step count assumes; SEM_SMOOTH_MAP_CUBE uses the cube's diagonal
+// mapping (xix = etay = gammaz = xix_regular).
 
 #include <cmath>
 #include <cstdio>
@@ -40,15 +44,31 @@ namespace {
 __constant__ float c_smooth_D[25];
 __constant__ float c_smooth_DWt[25];
 __constant__ float c_smooth_w[5];
+__constant__ double c_smooth_w3[125];  // w_i w_j w_k in FP64, point i + 5j + 25k
 
 struct SmoothArgs {
   int nspec, nglob;
   const int* ibool;   // [nspec*125]
   const int* order;   // [nspec]
-  float M[3][3];      // mapping terms: row xi/eta/gamma, column x/y/z
+  float M[3][3];      // mapping terms of a regular element: row xi/eta/gamma, column x/y/z
   float cv, ch, jac;
   const float* rot;   // [nglob][3] radial unit vector, or null (Cartesian)
+  const int* irreg;   // [nspec] -1 or row of geo; null: all regular
+  const float* geo;   // [nirr][125][10] xix..gammaz, jacobian
 };
+
+// rvol_local of element point q (element q / 125): real(dble(jacobian) *
+// w_i w_j w_k) with the point's own Jacobian in an irregular element.
+__device__ __forceinline__ float smooth_rvl(const int* __restrict__ irreg,
+                                            const float* __restrict__ geo, float jac, size_t q) {
+  const int p = (int)(q % NGLL3);
+  float j = jac;
+  if (irreg) {
+    const int ir = irreg[q / NGLL3];
+    if (ir >= 0) j = geo[((size_t)ir * NGLL3 + p) * 10 + 9];
+  }
+  return (float)((double)j * c_smooth_w3[p]);
+}
 
 template <int F>
 struct Vec;
@@ -112,6 +132,23 @@ __global__ void __launch_bounds__(128) k_smooth_elem(SmoothArgs A, const float* 
   const int pp = act ? p : NGLL3 - 1;
   const int i = pp % 5, j = (pp / 5) % 5, k = pp / 25;
   const int ig = A.ibool[(size_t)e * NGLL3 + pp];
+  // mapping terms and Jacobian at this point
+  float M[3][3], jac = A.jac;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) M[r][c] = A.M[r][c];
+  if (A.irreg) {
+    const int ir = A.irreg[e];
+    if (ir >= 0) {
+      const float* G = A.geo + ((size_t)ir * NGLL3 + pp) * 10;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) M[r][c] = G[3 * r + c];
+      jac = G[9];
+    }
+  }
   {
     float v[F];
     vload<F>(dat + (size_t)ig * F, v);
@@ -136,19 +173,18 @@ __global__ void __launch_bounds__(128) k_smooth_elem(SmoothArgs A, const float* 
       t2 = fmaf(su[f][i + 5 * l + 25 * k], sD[j * 5 + l], t2);
       t3 = fmaf(su[f][i + 5 * j + 25 * l], sD[k * 5 + l], t3);
     }
-    const float dx = t1 * A.M[0][0] + t2 * A.M[1][0] + t3 * A.M[2][0];
-    const float dy = t1 * A.M[0][1] + t2 * A.M[1][1] + t3 * A.M[2][1];
-    const float dz = t1 * A.M[0][2] + t2 * A.M[1][2] + t3 * A.M[2][2];
+    const float dx = t1 * M[0][0] + t2 * M[1][0] + t3 * M[2][0];
+    const float dy = t1 * M[0][1] + t2 * M[1][1] + t3 * M[2][1];
+    const float dz = t1 * M[0][2] + t2 * M[1][2] + t3 * M[2][2];
     const float rg = r0 * dx + r1 * dy + r2 * dz;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float g = A.M[a][0] * dx + A.M[a][1] * dy + A.M[a][2] * dz;
+      const float g = M[a][0] * dx + M[a][1] * dy + M[a][2] * dz;
       float s;
       if (A.rot)
-        s = ((A.cv - A.ch) * (r0 * A.M[a][0] + r1 * A.M[a][1] + r2 * A.M[a][2]) * rg + A.ch * g) *
-            A.jac;
+        s = ((A.cv - A.ch) * (r0 * M[a][0] + r1 * M[a][1] + r2 * M[a][2]) * rg + A.ch * g) * jac;
       else
-        s = ((A.cv - A.ch) * A.M[a][2] * dz + A.ch * g) * A.jac;
+        s = ((A.cv - A.ch) * M[a][2] * dz + A.ch * g) * jac;
       if (act) sf[a][f][p] = s;
     }
   }
@@ -199,11 +235,11 @@ __global__ void k_smooth_update(float* __restrict__ dat, float* __restrict__ dda
 }
 
 // Lumped volume: rvol(iglob) += rvol_local over element points.
-__global__ void k_smooth_volume(const int* __restrict__ ibool, int nspec, const float* rvl,
-                                float* vol) {
+__global__ void k_smooth_volume(const int* __restrict__ ibool, int nspec, const int* irreg,
+                                const float* geo, float jac, float* vol) {
   const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= (size_t)nspec * NGLL3) return;
-  atomicAdd(&vol[ibool[q]], rvl[q % NGLL3]);
+  atomicAdd(&vol[ibool[q]], smooth_rvl(irreg, geo, jac, q));
 }
 
 __global__ void k_smooth_invert(float* v, int n) {
@@ -214,12 +250,12 @@ __global__ void k_smooth_invert(float* v, int n) {
 // Projection of F element fields (field f at din + f*ne) onto the points.
 template <int F>
 __global__ void k_smooth_project(const int* __restrict__ ibool, int nspec, const float* __restrict__ din,
-                                 size_t ne, int nf_live, const float* __restrict__ rvl,
-                                 float* __restrict__ dat) {
+                                 size_t ne, int nf_live, const int* irreg, const float* geo,
+                                 float jac, float* __restrict__ dat) {
   const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= (size_t)nspec * NGLL3) return;
   const int ig = ibool[q];
-  const float w = rvl[q % NGLL3];
+  const float w = smooth_rvl(irreg, geo, jac, q);
   float v[F];
 #pragma unroll
   for (int f = 0; f < F; ++f) v[f] = f < nf_live ? din[f * ne + q] * w : 0.f;
@@ -252,11 +288,11 @@ void launch_step(const SmoothArgs& a, float* dat, float* ddat, const float* rvol
 }
 
 template <int F>
-void launch_project(const SmoothArgs& a, const float* din, size_t ne, int nf_live, const float* rvl,
-                    float* dat, const float* rvol, cudaStream_t st) {
+void launch_project(const SmoothArgs& a, const float* din, size_t ne, int nf_live, float* dat,
+                    const float* rvol, cudaStream_t st) {
   const size_t n = (size_t)a.nspec * NGLL3;
-  k_smooth_project<F><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.ibool, a.nspec, din, ne, nf_live,
-                                                                   rvl, dat);
+  k_smooth_project<F><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+      a.ibool, a.nspec, din, ne, nf_live, a.irreg, a.geo, a.jac, dat);
   k_smooth_scale<F><<<(unsigned)(((size_t)a.nglob * F + 255) / 256), 256, 0, st>>>(dat, rvol, a.nglob);
 }
 
@@ -322,9 +358,32 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
   SmoothMeshView mv{};
   int rc = mesh_smooth_view(mesh, &mv);
   if (rc) return rc;
-  // minimum GLL point distance of a regular element: (xi_1 - xi_0) / xix
-  const double dmin = cfg->distance_min > 0.0 ? cfg->distance_min
-                                              : (1.0 - std::sqrt(3.0 / 7.0)) / (double)mv.xix;
+  // minimum GLL point distance: of a regular element (xi_1 - xi_0) / xix;
+  // with irregular elements, the smallest distance between neighbouring
+  // GLL points along the element's index lines over the whole mesh
+  double dmin = cfg->distance_min;
+  if (!(dmin > 0.0)) {
+    if (mv.irreg) {
+      double d2 = 1e300;
+      for (int e = 0; e < mv.nspec; ++e) {
+        const int* ib = mv.h_ibool + (size_t)e * NGLL3;
+        for (int p = 0; p < NGLL3; ++p) {
+          const int i = p % 5, j = (p / 5) % 5, k = p / 25;
+          const int nb[3] = {i < 4 ? p + 1 : -1, j < 4 ? p + 5 : -1, k < 4 ? p + 25 : -1};
+          for (int q : nb) {
+            if (q < 0) continue;
+            const double dx = (double)mv.x[ib[q]] - mv.x[ib[p]];
+            const double dy = (double)mv.y[ib[q]] - mv.y[ib[p]];
+            const double dz = (double)mv.z[ib[q]] - mv.z[ib[p]];
+            d2 = std::min(d2, dx * dx + dy * dy + dz * dz);
+          }
+        }
+      }
+      dmin = std::sqrt(d2);
+    } else {
+      dmin = (1.0 - std::sqrt(3.0 / 7.0)) / (double)mv.xix;
+    }
+  }
   float cv = 0.f, ch = 0.f;
   double nstep_d = 0.0;
   smooth_params(cfg->sigma_h, cfg->sigma_v, dmin, &cv, &ch, &nstep_d);
@@ -341,6 +400,8 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
   a.cv = cv;
   a.ch = ch;
   a.jac = mv.jac;
+  a.irreg = mv.irreg;
+  a.geo = mv.geo;
   for (int r = 0; r < 3; ++r)
     for (int c = 0; c < 3; ++c)
       a.M[r][c] = (cfg->mapping == SEM_SMOOTH_MAP_REFERENCE || r == c) ? mv.xix : 0.f;
@@ -348,11 +409,10 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
   // host-side set-up: element-point volumes, radial vectors, CPML points
   const double xg[5] = {-1.0, -std::sqrt(3.0 / 7.0), 0.0, std::sqrt(3.0 / 7.0), 1.0};
   const double wg[5] = {0.1, 49.0 / 90.0, 32.0 / 45.0, 49.0 / 90.0, 0.1};
-  std::vector<float> rvl(NGLL3);
+  double w3[NGLL3];
   for (int k = 0; k < 5; ++k)
     for (int j = 0; j < 5; ++j)
-      for (int i = 0; i < 5; ++i)
-        rvl[i + 5 * j + 25 * k] = (float)((double)mv.jac * (wg[i] * wg[j] * wg[k]));
+      for (int i = 0; i < 5; ++i) w3[i + 5 * j + 25 * k] = wg[i] * wg[j] * wg[k];
   {
     // D[i][l] = derivative of the l-th Lagrange polynomial at node i
     float hD[25], hDW[25], hW[5];
@@ -379,6 +439,7 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
     cudaError_t e1 = cudaMemcpyToSymbol(c_smooth_D, hD, sizeof(hD));
     if (e1 == cudaSuccess) e1 = cudaMemcpyToSymbol(c_smooth_DWt, hDW, sizeof(hDW));
     if (e1 == cudaSuccess) e1 = cudaMemcpyToSymbol(c_smooth_w, hW, sizeof(hW));
+    if (e1 == cudaSuccess) e1 = cudaMemcpyToSymbol(c_smooth_w3, w3, sizeof(w3));
     if (e1 != cudaSuccess) {
       cudaGetLastError();
       return report_error(SEM_ERR_CUDA, "smoothing tables: %s", cudaGetErrorString(e1));
@@ -411,19 +472,17 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
   cudaGraphExec_t gexec = nullptr;
   const int F = nfield >= 3 ? 4 : (nfield == 2 ? 2 : 1);
   const size_t ne = (size_t)mv.nspec * NGLL3;
-  DevBuf b_dat, b_ddat, b_rvol, b_rvl, b_rot, b_cpml, b_din;
+  DevBuf b_dat, b_ddat, b_rvol, b_rot, b_cpml, b_din;
   SCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   SCK(cudaEventCreate(&ev0));
   SCK(cudaEventCreate(&ev1));
   SCK(cudaMalloc(&b_dat.p, (size_t)mv.nglob * F * sizeof(float)));
   SCK(cudaMalloc(&b_ddat.p, (size_t)mv.nglob * F * sizeof(float)));
   SCK(cudaMalloc(&b_rvol.p, (size_t)mv.nglob * sizeof(float)));
-  SCK(cudaMalloc(&b_rvl.p, NGLL3 * sizeof(float)));
   SCK(cudaMalloc(&b_din.p, ne * F * sizeof(float)));
   float* dat = (float*)b_dat.p;
   float* ddat = (float*)b_ddat.p;
   float* rvol = (float*)b_rvol.p;
-  float* drvl = (float*)b_rvl.p;
   float* din = (float*)b_din.p;
   const unsigned char* dcpml = nullptr;
   if (!rot.empty()) {
@@ -436,9 +495,9 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
     SCK(cudaMemcpyAsync(b_cpml.p, cpml.data(), cpml.size(), cudaMemcpyHostToDevice, st));
     dcpml = (const unsigned char*)b_cpml.p;
   }
-  SCK(cudaMemcpyAsync(drvl, rvl.data(), NGLL3 * sizeof(float), cudaMemcpyHostToDevice, st));
   SCK(cudaMemsetAsync(rvol, 0, (size_t)mv.nglob * sizeof(float), st));
-  k_smooth_volume<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(a.ibool, a.nspec, drvl, rvol);
+  k_smooth_volume<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(a.ibool, a.nspec, a.irreg, a.geo,
+                                                                 a.jac, rvol);
   k_smooth_invert<<<(mv.nglob + 255) / 256, 256, 0, st>>>(rvol, mv.nglob);
   SCK(cudaGetLastError());
 
@@ -468,11 +527,11 @@ extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfi
     SCK(cudaMemsetAsync(dat, 0, (size_t)mv.nglob * F * sizeof(float), st));
     SCK(cudaMemsetAsync(ddat, 0, (size_t)mv.nglob * F * sizeof(float), st));
     if (F == 4)
-      launch_project<4>(a, din, ne, live, drvl, dat, rvol, st);
+      launch_project<4>(a, din, ne, live, dat, rvol, st);
     else if (F == 2)
-      launch_project<2>(a, din, ne, live, drvl, dat, rvol, st);
+      launch_project<2>(a, din, ne, live, dat, rvol, st);
     else
-      launch_project<1>(a, din, ne, live, drvl, dat, rvol, st);
+      launch_project<1>(a, din, ne, live, dat, rvol, st);
     SCK(cudaEventRecord(ev0, st));
     int left = nstep;
     if (use_graph)

@@ -96,15 +96,24 @@ def l2_adjoint_source(syn, dat, dt, taper_percentage, itaper_type):
 
 def smooth_sem_pde_cpu(dat_in, ibool, xstore, ystore, zstore, xix_regular,
                        jacobian_regular, sigma_h, sigma_v, distance_min_glob,
-                       is_sph, is_cpml=None, nstep=None):
-    """CPU branch of ``smooth_sem_pde`` (src/postproc/smooth.f90:7-437) for
-    regular elements, one field, CUSTOM_REAL = float32.
+                       is_sph, is_cpml=None, nstep=None, irregular_element_number=None,
+                       stores=None):
+    """CPU branch of ``smooth_sem_pde`` (src/postproc/smooth.f90:7-437), one
+    field, CUSTOM_REAL = float32.
 
     ``dat_in`` is dat(NGLLX,NGLLY,NGLLZ,NSPEC) flattened in Fortran order,
     ``ibool`` the same shape with 1-based global numbers, the stores 1-D.
     Returns the smoothed dat in the same layout and ntstep.  ``nstep``
     replaces ntstep (the regular branch diverges within a few tens of
-    steps, so comparisons use a few).
+    steps, so comparisons use a few).  ``irregular_element_number`` [nspec]
+    (0 regular, k >= 1 irregular) and ``stores`` = (xixstore, xiystore,
+    xizstore, etaxstore, etaystore, etazstore, gammaxstore, gammaystore,
+    gammazstore, jacobianstore), each (NGLLX,NGLLY,NGLLZ,NSPEC_IRREGULAR)
+    flattened in Fortran order, select the irregular branch of an element
+    (get_gradient_element :603-646 and the fluxes :255-300).  The Fortran
+    passes xixstore(:,:,:,ispec) to get_gradient_element and reads
+    xixstore(i,j,k,ispec_irreg) for the fluxes; the two are the same row
+    when every element is irregular, the case transcribed here.
     """
     import numpy as np
     f32 = np.float32
@@ -157,6 +166,12 @@ def smooth_sem_pde_cpu(dat_in, ibool, xstore, ystore, zstore, xix_regular,
     if nstep:
         ntstep = nstep
 
+    def irreg_of(ispec):
+        return 0 if irregular_element_number is None else int(irregular_element_number[ispec - 1])
+
+    def store(q, i, j, k, row):        # stores[q](i,j,k,row), 1-based
+        return f32(stores[q][idx(i, j, k, row)])
+
     # rvol  (smooth.f90:142-164)
     nglob = max(ibool)
     rvol = [f32(0)] * (nglob + 1)
@@ -166,7 +181,11 @@ def smooth_sem_pde_cpu(dat_in, ibool, xstore, ystore, zstore, xix_regular,
             for j in range(1, N + 1):
                 for i in range(1, N + 1):
                     weight = wxgll[i - 1] * wxgll[j - 1] * wxgll[k - 1]
-                    jacobianl = f32(jacobian_regular)
+                    ispec_irreg = irreg_of(ispec)
+                    if ispec_irreg != 0:
+                        jacobianl = store(9, i, j, k, ispec_irreg)
+                    else:
+                        jacobianl = f32(jacobian_regular)
                     rvol_local[idx(i, j, k, ispec)] = f32(float(jacobianl) * weight)
                     iglob = ibool[idx(i, j, k, ispec)]
                     rvol[iglob] = f32(rvol[iglob] + rvol_local[idx(i, j, k, ispec)])
@@ -192,8 +211,9 @@ def smooth_sem_pde_cpu(dat_in, ibool, xstore, ystore, zstore, xix_regular,
     for _istep in range(ntstep):                      # smooth.f90:244-370
         ddat_glob = [f32(0)] * (nglob + 1)
         for ispec in range(1, nspec + 1):
+            ispec_irreg = irreg_of(ispec)
             dx, dy, dz = {}, {}, {}
-            for k in range(1, N + 1):                 # get_gradient_element_regular
+            for k in range(1, N + 1):     # get_gradient_element(_regular)
                 for j in range(1, N + 1):
                     for i in range(1, N + 1):
                         t1 = t2 = t3 = f32(0)
@@ -203,14 +223,37 @@ def smooth_sem_pde_cpu(dat_in, ibool, xstore, ystore, zstore, xix_regular,
                             t2 = f32(t2 + f32(dat[idx(i, l, k, ispec)] * hprime_xxT[l][j]))
                         for l in range(1, N + 1):
                             t3 = f32(t3 + f32(dat[idx(i, j, l, ispec)] * hprime_xxT[l][k]))
-                        v = f32(f32(f32(t1 * xix) + f32(t2 * xix)) + f32(t3 * xix))
-                        dx[(i, j, k)] = dy[(i, j, k)] = dz[(i, j, k)] = v
+                        if ispec_irreg != 0:
+                            G = [store(q, i, j, k, ispec_irreg) for q in range(9)]
+                            dx[(i, j, k)] = f32(f32(f32(t1 * G[0]) + f32(t2 * G[3])) + f32(t3 * G[6]))
+                            dy[(i, j, k)] = f32(f32(f32(t1 * G[1]) + f32(t2 * G[4])) + f32(t3 * G[7]))
+                            dz[(i, j, k)] = f32(f32(f32(t1 * G[2]) + f32(t2 * G[5])) + f32(t3 * G[8]))
+                        else:
+                            v = f32(f32(f32(t1 * xix) + f32(t2 * xix)) + f32(t3 * xix))
+                            dx[(i, j, k)] = dy[(i, j, k)] = dz[(i, j, k)] = v
             st1, st2, st3 = {}, {}, {}
             jacobianl = f32(jacobian_regular)
             for k in range(1, N + 1):
                 for j in range(1, N + 1):
                     for i in range(1, N + 1):
                         a, b, c = dx[(i, j, k)], dy[(i, j, k)], dz[(i, j, k)]
+                        if ispec_irreg != 0:
+                            G = [store(q, i, j, k, ispec_irreg) for q in range(10)]
+                            jl = G[9]
+                            sts = []
+                            for r in range(3):
+                                ax_, ay_, az_ = G[3 * r], G[3 * r + 1], G[3 * r + 2]
+                                g = f32(f32(f32(ax_ * a) + f32(ay_ * b)) + f32(az_ * c))
+                                if is_sph:
+                                    rxl, ryl, rzl = rot[idx(i, j, k, ispec)]
+                                    mr = f32(f32(f32(rxl * ax_) + f32(ryl * ay_)) + f32(rzl * az_))
+                                    rdot = f32(f32(f32(rxl * a) + f32(ryl * b)) + f32(rzl * c))
+                                    v = f32(f32(f32(f32(cv - ch) * mr) * rdot) + f32(ch * g))
+                                else:
+                                    v = f32(f32(f32(f32(cv - ch) * az_) * c) + f32(ch * g))
+                                sts.append(f32(v * jl))
+                            st1[(i, j, k)], st2[(i, j, k)], st3[(i, j, k)] = sts
+                            continue
                         if is_sph:
                             rxl, ryl, rzl = rot[idx(i, j, k, ispec)]
                             rdot = f32(f32(f32(rxl * a) + f32(ryl * b)) + f32(rzl * c))

@@ -90,3 +90,70 @@ def test_reference_regular_branch_diverges():
     assert not np.isfinite(out).all() or np.abs(out).max() > 1e6 * np.abs(dat).max()
     ok, _, _ = o.smooth_pde(dat, 6000.0, 3000.0, DMIN, mapping=0, nstep=40)
     assert np.abs(ok).max() < np.abs(dat).max()
+
+
+def _literal_irregular(db, dat, sigma_h, sigma_v, dmin, is_sph, nstep):
+    irr = np.asarray(db.irregular)
+    stores = [db.geo[..., q].reshape(-1).astype(np.float32) for q in range(10)]
+    lit, n2 = F.smooth_sem_pde_cpu(
+        dat.reshape(-1), (db.ibool.reshape(-1) + 1).tolist(), db.xstore, db.ystore, db.zstore,
+        db.xix_regular, db.jacobian_regular, sigma_h, sigma_v, dmin, is_sph, nstep=nstep,
+        irregular_element_number=(irr + 1).tolist(), stores=stores)
+    return np.asarray(lit, np.float64).reshape(dat.shape), n2
+
+
+@pytest.mark.parametrize("is_sph", [False, True])
+def test_oracle_matches_literal_fortran_irregular(is_sph):
+    """Every element irregular (an interior warp of a 2x2x2 box): the mapping
+    terms and Jacobian come from the per-point stores, in the fluxes and in
+    the lumped volume, as in the Fortran's ispec_irreg branch."""
+    box = D.BoxSpec(2, 2, 2, x0=2.0e5 if is_sph else 0.0, y0=1.0e5 if is_sph else 0.0)
+    db = D.make_box(box, warp=D.interior_warp(box, 500.0))
+    assert (np.asarray(db.irregular) >= 0).all()
+    dat = _field(db, 7)
+    o = Oracle(db, precision=4, nthreads=1)
+    out, n, _ = o.smooth_pde(dat, 6000.0, 3000.0, DMIN, is_sph=is_sph, nstep=4)
+    lit, n2 = _literal_irregular(db, dat, 6000.0, 3000.0, DMIN, is_sph, 4)
+    assert n == n2 == 4
+    assert np.abs(out - lit).max() <= 2e-6 * np.abs(lit).max()
+
+
+def test_irregular_mesh_conserves_and_keeps_constants():
+    """On a topography mesh (columns stretched under a hill, every element
+    irregular), the volume integral with each point's own Jacobian is
+    conserved and a constant stays constant."""
+    box = D.BoxSpec(4, 4, 3)
+    db = D.make_box(box, topo=D.hill_topography(box, 1500.0, 4000.0))
+    irr = np.asarray(db.irregular)
+    assert (irr >= 0).all()
+    jac = np.broadcast_to(np.float64(db.jacobian_regular), (db.nspec, 5, 5, 5)).copy()
+    for e in np.nonzero(irr >= 0)[0]:
+        jac[e] = db.geo[irr[e], ..., 9]
+    o = Oracle(db, precision=8, nthreads=2)
+    dat = _field(db, 11)
+    one, _, _ = o.smooth_pde(dat, 8000.0, 4000.0, DMIN, nstep=1)
+    out, _, _ = o.smooth_pde(dat, 8000.0, 4000.0, DMIN, nstep=40)
+    integ = lambda f: float((f * WK * jac).sum())  # noqa: E731
+    scale = float(np.abs(out * WK * jac).sum())
+    assert abs(integ(out) - integ(one)) <= 1e-10 * scale
+    assert out.std() < 0.6 * one.std()
+    c, _, _ = o.smooth_pde(np.full_like(dat, -1.5), 8000.0, 4000.0, DMIN, nstep=30)
+    assert np.abs(c + 1.5).max() < 1e-12
+
+
+def test_mixed_flags_equal_regular():
+    """A regular box with half of its elements flagged irregular (their
+    constant mapping stored per point): regular and irregular branches meet
+    in one mesh and give the cube-mapping result."""
+    import dataclasses
+    db = D.make_box(D.BoxSpec(3, 3, 2))
+    full = D.as_irregular(db)
+    irr = np.full(db.nspec, -1, np.int32)
+    pick = np.arange(0, db.nspec, 2)
+    irr[pick] = np.arange(pick.size)
+    mixed = dataclasses.replace(db, irregular=irr, geo=full.geo[pick].copy())
+    dat = _field(db, 13)
+    a, _, _ = Oracle(db, precision=8, nthreads=1).smooth_pde(dat, 6000.0, 3000.0, DMIN, nstep=20)
+    b, _, _ = Oracle(mixed, precision=8, nthreads=1).smooth_pde(dat, 6000.0, 3000.0, DMIN,
+                                                                nstep=20)
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
