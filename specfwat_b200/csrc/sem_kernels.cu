@@ -1297,6 +1297,37 @@ __device__ __forceinline__ void red_v(float* g, const LV<NL>& x) {
   }
 }
 
+// Packed FP32x2 arithmetic (Blackwell f32x2): two values that share a GLL
+// coefficient - two events of one thread, or the adjoint and backward
+// fields of one event - advance with one instruction issue.  fma.rn on
+// each half, so the results are those of the scalar FMAs.
+__device__ __forceinline__ float2 p2(const LV<2>& x) { return make_float2(x.v[0], x.v[1]); }
+__device__ __forceinline__ LV<2> lv2(float2 x) {
+  LV<2> r;
+  r.v[0] = x.x;
+  r.v[1] = x.y;
+  return r;
+}
+__device__ __forceinline__ float2 splat(float c) { return make_float2(c, c); }
+// a + c x for a compile-time GLL coefficient c (c = 0: no instruction)
+__device__ __forceinline__ float2 cfma2(float c, float2 x, float2 a) {
+  return c == 0.0f ? a : __ffma2_rn(splat(c), x, a);
+}
+// Isotropic stress times fac of two gradients sharing kappa and mu:
+// sig = {xx, yy, zz, xy, xz, yz}.
+__device__ __forceinline__ void stress_point2(const float2 g[3][3], float kap, float mu,
+                                              float fac, float2 sig[6]) {
+  const float l2m = kap + (4.0f / 3.0f) * mu;
+  const float lam = l2m - 2.0f * mu;
+  const float2 L = splat(l2m), M = splat(lam), F = splat(fac), MU = splat(fac * mu);
+  sig[0] = __fmul2_rn(F, __ffma2_rn(L, g[0][0], __fmul2_rn(M, __fadd2_rn(g[1][1], g[2][2]))));
+  sig[1] = __fmul2_rn(F, __ffma2_rn(L, g[1][1], __fmul2_rn(M, __fadd2_rn(g[0][0], g[2][2]))));
+  sig[2] = __fmul2_rn(F, __ffma2_rn(L, g[2][2], __fmul2_rn(M, __fadd2_rn(g[0][0], g[1][1]))));
+  sig[3] = __fmul2_rn(MU, __fadd2_rn(g[0][1], g[1][0]));
+  sig[4] = __fmul2_rn(MU, __fadd2_rn(g[0][2], g[2][0]));
+  sig[5] = __fmul2_rn(MU, __fadd2_rn(g[1][2], g[2][1]));
+}
+
 // Mapping of GLL point p of a general element: xix, xiy, xiz, etax, etay,
 // etaz, gammax, gammay, gammaz, jacobian (geo_e = the element's row of the
 // mesh's per-point mapping, 8-byte aligned), or the regular element's
@@ -1332,40 +1363,69 @@ struct PBuf {
 // eta / gamma derivative roles (pencils (i,k) and (i,j) of thread t).
 template <int LB, int NL>
 __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
+  if constexpr (NL == 2) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    LV<NL> v[5];
+    for (int c = 0; c < 3; ++c) {
+      float2 v[5];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) v[l] = lds_v<NL>(b.U(c, pi + 5 * l + 25 * pq));
+      for (int l = 0; l < 5; ++l) v[l] = p2(lds_v<2>(b.U(c, pi + 5 * l + 25 * pq)));
 #pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      LV<NL> s;
+      for (int j = 0; j < 5; ++j) {
+        float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int n = 0; n < NL; ++n) {
-        float a = 0.f;
-#pragma unroll
-        for (int l = 0; l < 5; ++l) a = cfma(gD(j, l), v[l].v[n], a);
-        s.v[n] = a;
+        for (int l = 0; l < 5; ++l) a = cfma2(gD(j, l), v[l], a);
+        sts_v<2>(b.Ar(c, pi + 5 * j + 25 * pq), lv2(a));
       }
-      sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
     }
-  }
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    LV<NL> v[5];
+    for (int c = 0; c < 3; ++c) {
+      float2 v[5];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) v[l] = lds_v<NL>(b.U(c, pi + 5 * pq + 25 * l));
+      for (int l = 0; l < 5; ++l) v[l] = p2(lds_v<2>(b.U(c, pi + 5 * pq + 25 * l)));
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      LV<NL> s;
+      for (int k = 0; k < 5; ++k) {
+        float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int n = 0; n < NL; ++n) {
-        float a = 0.f;
-#pragma unroll
-        for (int l = 0; l < 5; ++l) a = cfma(gD(k, l), v[l].v[n], a);
-        s.v[n] = a;
+        for (int l = 0; l < 5; ++l) a = cfma2(gD(k, l), v[l], a);
+        sts_v<2>(b.Ar(3 + c, pi + 5 * pq + 25 * k), lv2(a));
       }
-      sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LV<NL> v[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) v[l] = lds_v<NL>(b.U(c, pi + 5 * l + 25 * pq));
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        LV<NL> s;
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma(gD(j, l), v[l].v[n], a);
+          s.v[n] = a;
+        }
+        sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LV<NL> v[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) v[l] = lds_v<NL>(b.U(c, pi + 5 * pq + 25 * l));
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        LV<NL> s;
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma(gD(k, l), v[l].v[n], a);
+          s.v[n] = a;
+        }
+        sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
+      }
     }
   }
 }
@@ -1373,56 +1433,97 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
 // eta / gamma divergence roles: B -> A.
 template <int LB, int NL, bool GEN = false>
 __device__ __forceinline__ void v_div_eg(const PBuf<LB>& b, int pi, int pq) {
-  {
-    // eta pencil: sigma_{c,y} = (xy, yy, yz) = B0, B1, B2
-    LV<NL> v[3][5];
+  if constexpr (NL == 2) {
+    {
+      float2 v[3][5];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) {
-      const int p = pi + 5 * l + 25 * pq;
-      v[0][l] = lds_v<NL>(b.U(0, p));
-      v[1][l] = lds_v<NL>(b.U(1, p));
-      v[2][l] = lds_v<NL>(b.U(2, p));
-    }
-#pragma unroll
-    for (int j = 0; j < 5; ++j)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        LV<NL> s;
-#pragma unroll
-        for (int n = 0; n < NL; ++n) {
-          float a = 0.f;
-#pragma unroll
-          for (int l = 0; l < 5; ++l) a = cfma(gDWt(j, l), v[c][l].v[n], a);
-          s.v[n] = a;
-        }
-        sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
+      for (int l = 0; l < 5; ++l) {
+        const int p = pi + 5 * l + 25 * pq;
+        v[0][l] = p2(lds_v<2>(b.U(0, p)));
+        v[1][l] = p2(lds_v<2>(b.U(1, p)));
+        v[2][l] = p2(lds_v<2>(b.U(2, p)));
       }
-  }
-  {
-    // gamma pencil: sigma_{c,z} = (xz, yz, zz) = B3, B2, B4; general
-    // elements: the gamma fluxes of the three components, B3, B4, B5
-    LV<NL> v[3][5];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) {
-      const int p = pi + 5 * pq + 25 * l;
-      v[0][l] = lds_v<NL>(b.U(3, p));
-      v[1][l] = lds_v<NL>(b.U(GEN ? 4 : 2, p));
-      v[2][l] = lds_v<NL>(b.U(GEN ? 5 : 4, p));
-    }
+      for (int j = 0; j < 5; ++j)
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
+        for (int c = 0; c < 3; ++c) {
+          float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        LV<NL> s;
-#pragma unroll
-        for (int n = 0; n < NL; ++n) {
-          float a = 0.f;
-#pragma unroll
-          for (int l = 0; l < 5; ++l) a = cfma(gDWt(k, l), v[c][l].v[n], a);
-          s.v[n] = a;
+          for (int l = 0; l < 5; ++l) a = cfma2(gDWt(j, l), v[c][l], a);
+          sts_v<2>(b.Ar(c, pi + 5 * j + 25 * pq), lv2(a));
         }
-        sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
+    }
+    {
+      float2 v[3][5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        const int p = pi + 5 * pq + 25 * l;
+        v[0][l] = p2(lds_v<2>(b.U(3, p)));
+        v[1][l] = p2(lds_v<2>(b.U(GEN ? 4 : 2, p)));
+        v[2][l] = p2(lds_v<2>(b.U(GEN ? 5 : 4, p)));
       }
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma2(gDWt(k, l), v[c][l], a);
+          sts_v<2>(b.Ar(3 + c, pi + 5 * pq + 25 * k), lv2(a));
+        }
+    }
+  } else {
+    {
+      // eta pencil: sigma_{c,y} = (xy, yy, yz) = B0, B1, B2
+      LV<NL> v[3][5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        const int p = pi + 5 * l + 25 * pq;
+        v[0][l] = lds_v<NL>(b.U(0, p));
+        v[1][l] = lds_v<NL>(b.U(1, p));
+        v[2][l] = lds_v<NL>(b.U(2, p));
+      }
+#pragma unroll
+      for (int j = 0; j < 5; ++j)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          LV<NL> s;
+#pragma unroll
+          for (int n = 0; n < NL; ++n) {
+            float a = 0.f;
+#pragma unroll
+            for (int l = 0; l < 5; ++l) a = cfma(gDWt(j, l), v[c][l].v[n], a);
+            s.v[n] = a;
+          }
+          sts_v<NL>(b.Ar(c, pi + 5 * j + 25 * pq), s);
+        }
+    }
+    {
+      // gamma pencil: sigma_{c,z} = (xz, yz, zz) = B3, B2, B4; general
+      // elements: the gamma fluxes of the three components, B3, B4, B5
+      LV<NL> v[3][5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        const int p = pi + 5 * pq + 25 * l;
+        v[0][l] = lds_v<NL>(b.U(3, p));
+        v[1][l] = lds_v<NL>(b.U(GEN ? 4 : 2, p));
+        v[2][l] = lds_v<NL>(b.U(GEN ? 5 : 4, p));
+      }
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          LV<NL> s;
+#pragma unroll
+          for (int n = 0; n < NL; ++n) {
+            float a = 0.f;
+#pragma unroll
+            for (int l = 0; l < 5; ++l) a = cfma(gDWt(k, l), v[c][l].v[n], a);
+            s.v[n] = a;
+          }
+          sts_v<NL>(b.Ar(3 + c, pi + 5 * pq + 25 * k), s);
+        }
+    }
   }
 }
 
@@ -1443,111 +1544,153 @@ __device__ __forceinline__ void v_xi(const PBuf<LB>& b, const PBuf<LB>& park, in
                                      LV<NL> fx[5][3], LV<NL> kmu[5], LV<NL> kka[5],
                                      const float* geo_e = nullptr, float xix = 0.f,
                                      float jac = 0.f) {
-  LV<NL> u[3][5];
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int l = 0; l < 5; ++l) u[c][l] = lds_v<NL>(b.U(c, l + 5 * t));
-  LV<NL> sx[3][5];  // sigma_xx, sigma_xy, sigma_xz along the pencil
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const int p = i + 5 * t;
-    LV<NL> de[3], dg[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      de[c] = lds_v<NL>(b.Ar(c, p));
-      dg[c] = lds_v<NL>(b.Ar(3 + c, p));
-    }
-    LV<NL> pk[6];
-    if (MODE == 2) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) pk[q] = lds_v<NL>(park.Ar(q, p));
-    }
-    constexpr int NO = GEN ? 6 : 5;
-    LV<NL> o[NO];
-    const float kp = kap[p], m = mu[p];
-    float G[10];
-    if (GEN) load_geo(geo_e, p, xix, jac, G);
-#pragma unroll
-    for (int n = 0; n < NL; ++n) {
-      float g[3][3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float a = 0.f;
-#pragma unroll
-        for (int l = 0; l < 5; ++l) a = cfma(gD(i, l), u[c][l].v[n], a);
-        g[c][0] = a;
-        g[c][1] = de[c].v[n];
-        g[c][2] = dg[c].v[n];
-      }
-      if constexpr (GEN) {
-        float r[3][3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-          for (int d = 0; d < 3; ++d) r[c][d] = g[c][d];
-        map_gradient(r, G, g);
-        float sig[6], F[9];
-        stress_point(g, kp, m, 1.0f, sig);
-        map_flux(sig, G, F);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          sx[c][i].v[n] = F[c * 3 + 0];
-          o[c].v[n] = F[c * 3 + 1];
-          o[3 + c].v[n] = F[c * 3 + 2];
-        }
-      } else {
-        float sig[6];
-        stress_point(g, kp, m, fac, sig);
-        sx[0][i].v[n] = sig[0];
-        sx[1][i].v[n] = sig[3];
-        sx[2][i].v[n] = sig[4];
-        o[0].v[n] = sig[3];
-        o[1].v[n] = sig[1];
-        o[2].v[n] = sig[5];
-        o[3].v[n] = sig[4];
-        o[4].v[n] = sig[2];
-      }
-      if (MODE != 0) {
-        const float tr = g[0][0] + g[1][1] + g[2][2];
-        const float xx = g[0][0] - tr * (1.0f / 3.0f);
-        const float yy = g[1][1] - tr * (1.0f / 3.0f);
-        const float xy = 0.5f * (g[0][1] + g[1][0]);
-        const float xz = 0.5f * (g[0][2] + g[2][0]);
-        const float yz = 0.5f * (g[1][2] + g[2][1]);
-        if (MODE == 1) {
-          pk[0].v[n] = xx;
-          pk[1].v[n] = yy;
-          pk[2].v[n] = xy;
-          pk[3].v[n] = xz;
-          pk[4].v[n] = yz;
-          pk[5].v[n] = tr;
-        } else {
-          const float bxx = pk[0].v[n], byy = pk[1].v[n];
-          kmu[i].v[n] = xx * bxx + yy * byy + (xx + yy) * (bxx + byy) +
-                        2.0f * (xy * pk[2].v[n] + xz * pk[3].v[n] + yz * pk[4].v[n]);
-          kka[i].v[n] = tr * pk[5].v[n];
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < NO; ++q) sts_v<NL>(b.U(q, p), o[q]);
-    if (MODE == 1) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) sts_v<NL>(b.Ar(q, p), pk[q]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 5; ++i)
+  if constexpr (NL == 2 && MODE == 0 && !GEN) {
+    float2 u[3][5];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int n = 0; n < NL; ++n) {
-        float a = 0.f;
+      for (int l = 0; l < 5; ++l) u[c][l] = p2(lds_v<2>(b.U(c, l + 5 * t)));
+    float2 sx[3][5];
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = cfma(gDWt(i, l), sx[c][l].v[n], a);
-        fx[i][c].v[n] = a;
+    for (int i = 0; i < 5; ++i) {
+      const int p = i + 5 * t;
+      float2 g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = cfma2(gD(i, l), u[c][l], a);
+        g[c][0] = a;
+        g[c][1] = p2(lds_v<2>(b.Ar(c, p)));
+        g[c][2] = p2(lds_v<2>(b.Ar(3 + c, p)));
       }
+      float2 sig[6];
+      stress_point2(g, kap[p], mu[p], fac, sig);
+      sx[0][i] = sig[0];
+      sx[1][i] = sig[3];
+      sx[2][i] = sig[4];
+      sts_v<2>(b.U(0, p), lv2(sig[3]));
+      sts_v<2>(b.U(1, p), lv2(sig[1]));
+      sts_v<2>(b.U(2, p), lv2(sig[5]));
+      sts_v<2>(b.U(3, p), lv2(sig[4]));
+      sts_v<2>(b.U(4, p), lv2(sig[2]));
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = cfma2(gDWt(i, l), sx[c][l], a);
+        fx[i][c] = lv2(a);
+      }
+  } else {
+    LV<NL> u[3][5];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int l = 0; l < 5; ++l) u[c][l] = lds_v<NL>(b.U(c, l + 5 * t));
+    LV<NL> sx[3][5];  // sigma_xx, sigma_xy, sigma_xz along the pencil
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const int p = i + 5 * t;
+      LV<NL> de[3], dg[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        de[c] = lds_v<NL>(b.Ar(c, p));
+        dg[c] = lds_v<NL>(b.Ar(3 + c, p));
+      }
+      LV<NL> pk[6];
+      if (MODE == 2) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) pk[q] = lds_v<NL>(park.Ar(q, p));
+      }
+      constexpr int NO = GEN ? 6 : 5;
+      LV<NL> o[NO];
+      const float kp = kap[p], m = mu[p];
+      float G[10];
+      if (GEN) load_geo(geo_e, p, xix, jac, G);
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        float g[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma(gD(i, l), u[c][l].v[n], a);
+          g[c][0] = a;
+          g[c][1] = de[c].v[n];
+          g[c][2] = dg[c].v[n];
+        }
+        if constexpr (GEN) {
+          float r[3][3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) r[c][d] = g[c][d];
+          map_gradient(r, G, g);
+          float sig[6], F[9];
+          stress_point(g, kp, m, 1.0f, sig);
+          map_flux(sig, G, F);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            sx[c][i].v[n] = F[c * 3 + 0];
+            o[c].v[n] = F[c * 3 + 1];
+            o[3 + c].v[n] = F[c * 3 + 2];
+          }
+        } else {
+          float sig[6];
+          stress_point(g, kp, m, fac, sig);
+          sx[0][i].v[n] = sig[0];
+          sx[1][i].v[n] = sig[3];
+          sx[2][i].v[n] = sig[4];
+          o[0].v[n] = sig[3];
+          o[1].v[n] = sig[1];
+          o[2].v[n] = sig[5];
+          o[3].v[n] = sig[4];
+          o[4].v[n] = sig[2];
+        }
+        if (MODE != 0) {
+          const float tr = g[0][0] + g[1][1] + g[2][2];
+          const float xx = g[0][0] - tr * (1.0f / 3.0f);
+          const float yy = g[1][1] - tr * (1.0f / 3.0f);
+          const float xy = 0.5f * (g[0][1] + g[1][0]);
+          const float xz = 0.5f * (g[0][2] + g[2][0]);
+          const float yz = 0.5f * (g[1][2] + g[2][1]);
+          if (MODE == 1) {
+            pk[0].v[n] = xx;
+            pk[1].v[n] = yy;
+            pk[2].v[n] = xy;
+            pk[3].v[n] = xz;
+            pk[4].v[n] = yz;
+            pk[5].v[n] = tr;
+          } else {
+            const float bxx = pk[0].v[n], byy = pk[1].v[n];
+            kmu[i].v[n] = xx * bxx + yy * byy + (xx + yy) * (bxx + byy) +
+                          2.0f * (xy * pk[2].v[n] + xz * pk[3].v[n] + yz * pk[4].v[n]);
+            kka[i].v[n] = tr * pk[5].v[n];
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NO; ++q) sts_v<NL>(b.U(q, p), o[q]);
+      if (MODE == 1) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sts_v<NL>(b.Ar(q, p), pk[q]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma(gDWt(i, l), sx[c][l].v[n], a);
+          fx[i][c].v[n] = a;
+        }
+  }
 }
 
 // xi role: total force on the pencil and vector scatter-add.
@@ -1585,25 +1728,49 @@ __device__ __forceinline__ void v_scatter(const PBuf<LB>& b, int t, const LV<NL>
     if (q == pk) wk = gW(q);
   }
   const float wjk = wj * wk;
+  if constexpr (NL == 2) {
+    const float2 njk = splat(-wjk);
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const int p = i + 5 * t;
-    const size_t ig = (size_t)ib[p];
-    const float wik = gW(i) * wk, wij = gW(i) * wj;
+    for (int i = 0; i < 5; ++i) {
+      const int p = i + 5 * t;
+      const size_t ig = (size_t)ib[p];
+      const float2 nik = splat(-(gW(i) * wk)), nij = splat(-(gW(i) * wj));
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const LV<NL> e1 = lds_v<NL>(b.Ar(c, p));
-      const LV<NL> e2 = lds_v<NL>(b.Ar(3 + c, p));
-      LV<NL> f;
-#pragma unroll
-      for (int n = 0; n < NL; ++n) {
-        const float v = -(wjk * fx[i][c].v[n] + wik * e1.v[n] + wij * e2.v[n]);
-        f.v[n] = (fl[n] & bit) ? v : 0.f;  // lanes not in this phase add nothing
+      for (int c = 0; c < 3; ++c) {
+        const float2 e1 = p2(lds_v<2>(b.Ar(c, p)));
+        const float2 e2 = p2(lds_v<2>(b.Ar(3 + c, p)));
+        float2 v = __ffma2_rn(nij, e2, __ffma2_rn(nik, e1, __fmul2_rn(njk, p2(fx[i][c]))));
+        // lanes not in this phase add nothing
+        LV<2> f;
+        f.v[0] = (fl[0] & bit) ? v.x : 0.f;
+        f.v[1] = (fl[1] & bit) ? v.y : 0.f;
+        if constexpr (ATOMIC)
+          red_v<2>(&accb[foff<3>((int)ig, c)], f);
+        else
+          rmw_v<2>(&accb[foff<3>((int)ig, c)], f);
       }
-      if constexpr (ATOMIC)
-        red_v<NL>(&accb[foff<3>((int)ig, c)], f);
-      else
-        rmw_v<NL>(&accb[foff<3>((int)ig, c)], f);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const int p = i + 5 * t;
+      const size_t ig = (size_t)ib[p];
+      const float wik = gW(i) * wk, wij = gW(i) * wj;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const LV<NL> e1 = lds_v<NL>(b.Ar(c, p));
+        const LV<NL> e2 = lds_v<NL>(b.Ar(3 + c, p));
+        LV<NL> f;
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          const float v = -(wjk * fx[i][c].v[n] + wik * e1.v[n] + wij * e2.v[n]);
+          f.v[n] = (fl[n] & bit) ? v : 0.f;  // lanes not in this phase add nothing
+        }
+        if constexpr (ATOMIC)
+          red_v<NL>(&accb[foff<3>((int)ig, c)], f);
+        else
+          rmw_v<NL>(&accb[foff<3>((int)ig, c)], f);
+      }
     }
   }
 }
@@ -1830,94 +1997,149 @@ __device__ __forceinline__ void pair_xi(const PBuf<VL>& b, int t, const float* k
                                         float fac, LV<2> fx[5][3], float kmu[5], float kka[5],
                                         const float* geo_e = nullptr, float xix = 0.f,
                                         float jac = 0.f) {
-  LV<2> u[3][5];
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int l = 0; l < 5; ++l) u[c][l] = lds_v<2>(b.U(c, l + 5 * t));
-  LV<2> sx[3][5];
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const int p = i + 5 * t;
-    LV<2> de[3], dg[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      de[c] = lds_v<2>(b.Ar(c, p));
-      dg[c] = lds_v<2>(b.Ar(3 + c, p));
-    }
-    constexpr int NO = GEN ? 6 : 5;
-    LV<2> o[NO];
-    float ev[2][6];
-    const float kp = kap[p], m = mu[p];
-    float G[10];
-    if (GEN) load_geo(geo_e, p, xix, jac, G);
-#pragma unroll
-    for (int n = 0; n < 2; ++n) {
-      float g[3][3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float a = 0.f;
-#pragma unroll
-        for (int l = 0; l < 5; ++l) a = cfma(gD(i, l), u[c][l].v[n], a);
-        g[c][0] = a;
-        g[c][1] = de[c].v[n];
-        g[c][2] = dg[c].v[n];
-      }
-      if constexpr (GEN) {
-        float r[3][3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-          for (int d = 0; d < 3; ++d) r[c][d] = g[c][d];
-        map_gradient(r, G, g);
-        float sig[6], F[9];
-        stress_point(g, kp, m, 1.0f, sig);
-        map_flux(sig, G, F);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          sx[c][i].v[n] = F[c * 3 + 0];
-          o[c].v[n] = F[c * 3 + 1];
-          o[3 + c].v[n] = F[c * 3 + 2];
-        }
-      } else {
-        float sig[6];
-        stress_point(g, kp, m, fac, sig);
-        sx[0][i].v[n] = sig[0];
-        sx[1][i].v[n] = sig[3];
-        sx[2][i].v[n] = sig[4];
-        o[0].v[n] = sig[3];
-        o[1].v[n] = sig[1];
-        o[2].v[n] = sig[5];
-        o[3].v[n] = sig[4];
-        o[4].v[n] = sig[2];
-      }
-      const float tr = g[0][0] + g[1][1] + g[2][2];
-      ev[n][0] = g[0][0] - tr * (1.0f / 3.0f);
-      ev[n][1] = g[1][1] - tr * (1.0f / 3.0f);
-      ev[n][2] = 0.5f * (g[0][1] + g[1][0]);
-      ev[n][3] = 0.5f * (g[0][2] + g[2][0]);
-      ev[n][4] = 0.5f * (g[1][2] + g[2][1]);
-      ev[n][5] = tr;
-    }
-    // adjoint (n = 0) x backward (n = 1) deviatoric products and traces
-    kmu[i] = ev[0][0] * ev[1][0] + ev[0][1] * ev[1][1] +
-             (ev[0][0] + ev[0][1]) * (ev[1][0] + ev[1][1]) +
-             2.0f * (ev[0][2] * ev[1][2] + ev[0][3] * ev[1][3] + ev[0][4] * ev[1][4]);
-    kka[i] = ev[0][5] * ev[1][5];
-#pragma unroll
-    for (int q = 0; q < NO; ++q) sts_v<2>(b.U(q, p), o[q]);
-  }
-#pragma unroll
-  for (int i = 0; i < 5; ++i)
+  if constexpr (!GEN) {
+    // the adjoint (x) and backward (y) fields as one packed pair
+    float2 u[3][5];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int n = 0; n < 2; ++n) {
-        float a = 0.f;
+      for (int l = 0; l < 5; ++l) u[c][l] = p2(lds_v<2>(b.U(c, l + 5 * t)));
+    float2 sx[3][5];
 #pragma unroll
-        for (int l = 0; l < 5; ++l) a = cfma(gDWt(i, l), sx[c][l].v[n], a);
-        fx[i][c].v[n] = a;
+    for (int i = 0; i < 5; ++i) {
+      const int p = i + 5 * t;
+      float2 g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = cfma2(gD(i, l), u[c][l], a);
+        g[c][0] = a;
+        g[c][1] = p2(lds_v<2>(b.Ar(c, p)));
+        g[c][2] = p2(lds_v<2>(b.Ar(3 + c, p)));
       }
+      float2 sig[6];
+      stress_point2(g, kap[p], mu[p], fac, sig);
+      sx[0][i] = sig[0];
+      sx[1][i] = sig[3];
+      sx[2][i] = sig[4];
+      // deviatoric strains and traces of both fields, then the adjoint x
+      // backward products
+      const float2 tr = __fadd2_rn(__fadd2_rn(g[0][0], g[1][1]), g[2][2]);
+      const float2 m3 = splat(-1.0f / 3.0f), h = splat(0.5f);
+      const float2 exx = __ffma2_rn(tr, m3, g[0][0]);
+      const float2 eyy = __ffma2_rn(tr, m3, g[1][1]);
+      const float2 exy = __fmul2_rn(h, __fadd2_rn(g[0][1], g[1][0]));
+      const float2 exz = __fmul2_rn(h, __fadd2_rn(g[0][2], g[2][0]));
+      const float2 eyz = __fmul2_rn(h, __fadd2_rn(g[1][2], g[2][1]));
+      kmu[i] = exx.x * exx.y + eyy.x * eyy.y + (exx.x + eyy.x) * (exx.y + eyy.y) +
+               2.0f * (exy.x * exy.y + exz.x * exz.y + eyz.x * eyz.y);
+      kka[i] = tr.x * tr.y;
+      sts_v<2>(b.U(0, p), lv2(sig[3]));
+      sts_v<2>(b.U(1, p), lv2(sig[1]));
+      sts_v<2>(b.U(2, p), lv2(sig[5]));
+      sts_v<2>(b.U(3, p), lv2(sig[4]));
+      sts_v<2>(b.U(4, p), lv2(sig[2]));
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int l = 0; l < 5; ++l) a = cfma2(gDWt(i, l), sx[c][l], a);
+        fx[i][c] = lv2(a);
+      }
+  } else {
+    LV<2> u[3][5];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int l = 0; l < 5; ++l) u[c][l] = lds_v<2>(b.U(c, l + 5 * t));
+    LV<2> sx[3][5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const int p = i + 5 * t;
+      LV<2> de[3], dg[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        de[c] = lds_v<2>(b.Ar(c, p));
+        dg[c] = lds_v<2>(b.Ar(3 + c, p));
+      }
+      constexpr int NO = GEN ? 6 : 5;
+      LV<2> o[NO];
+      float ev[2][6];
+      const float kp = kap[p], m = mu[p];
+      float G[10];
+      if (GEN) load_geo(geo_e, p, xix, jac, G);
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        float g[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma(gD(i, l), u[c][l].v[n], a);
+          g[c][0] = a;
+          g[c][1] = de[c].v[n];
+          g[c][2] = dg[c].v[n];
+        }
+        if constexpr (GEN) {
+          float r[3][3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) r[c][d] = g[c][d];
+          map_gradient(r, G, g);
+          float sig[6], F[9];
+          stress_point(g, kp, m, 1.0f, sig);
+          map_flux(sig, G, F);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            sx[c][i].v[n] = F[c * 3 + 0];
+            o[c].v[n] = F[c * 3 + 1];
+            o[3 + c].v[n] = F[c * 3 + 2];
+          }
+        } else {
+          float sig[6];
+          stress_point(g, kp, m, fac, sig);
+          sx[0][i].v[n] = sig[0];
+          sx[1][i].v[n] = sig[3];
+          sx[2][i].v[n] = sig[4];
+          o[0].v[n] = sig[3];
+          o[1].v[n] = sig[1];
+          o[2].v[n] = sig[5];
+          o[3].v[n] = sig[4];
+          o[4].v[n] = sig[2];
+        }
+        const float tr = g[0][0] + g[1][1] + g[2][2];
+        ev[n][0] = g[0][0] - tr * (1.0f / 3.0f);
+        ev[n][1] = g[1][1] - tr * (1.0f / 3.0f);
+        ev[n][2] = 0.5f * (g[0][1] + g[1][0]);
+        ev[n][3] = 0.5f * (g[0][2] + g[2][0]);
+        ev[n][4] = 0.5f * (g[1][2] + g[2][1]);
+        ev[n][5] = tr;
+      }
+      // adjoint (n = 0) x backward (n = 1) deviatoric products and traces
+      kmu[i] = ev[0][0] * ev[1][0] + ev[0][1] * ev[1][1] +
+               (ev[0][0] + ev[0][1]) * (ev[1][0] + ev[1][1]) +
+               2.0f * (ev[0][2] * ev[1][2] + ev[0][3] * ev[1][3] + ev[0][4] * ev[1][4]);
+      kka[i] = ev[0][5] * ev[1][5];
+#pragma unroll
+      for (int q = 0; q < NO; ++q) sts_v<2>(b.U(q, p), o[q]);
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          float a = 0.f;
+#pragma unroll
+          for (int l = 0; l < 5; ++l) a = cfma(gDWt(i, l), sx[c][l].v[n], a);
+          fx[i][c].v[n] = a;
+        }
+  }
 }
 
 template <int VL>
@@ -1931,19 +2153,20 @@ __device__ __forceinline__ void pair_scatter(const PBuf<VL>& b, int t, const LV<
     if (q == pj) wj = gW(q);
     if (q == pk) wk = gW(q);
   }
-  const float wjk = wj * wk;
+  const float2 njk = splat(-(wj * wk));
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
     const int p = i + 5 * t;
     const int ig = ib[p];
-    const float wik = gW(i) * wk, wij = gW(i) * wj;
+    const float2 nik = splat(-(gW(i) * wk)), nij = splat(-(gW(i) * wj));
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const LV<2> e1 = lds_v<2>(b.Ar(c, p));
-      const LV<2> e2 = lds_v<2>(b.Ar(3 + c, p));
+      const float2 e1 = p2(lds_v<2>(b.Ar(c, p)));
+      const float2 e2 = p2(lds_v<2>(b.Ar(3 + c, p)));
+      const float2 v = __ffma2_rn(nij, e2, __ffma2_rn(nik, e1, __fmul2_rn(njk, p2(fx[i][c]))));
       const size_t q = foff<3>(ig, c);
-      if (on1) atomicAdd(&accb1[q], -(wjk * fx[i][c].v[0] + wik * e1.v[0] + wij * e2.v[0]));
-      if (on2) atomicAdd(&accb2[q], -(wjk * fx[i][c].v[1] + wik * e1.v[1] + wij * e2.v[1]));
+      if (on1) atomicAdd(&accb1[q], v.x);
+      if (on2) atomicAdd(&accb2[q], v.y);
     }
   }
 }
@@ -2129,8 +2352,7 @@ struct PairRLayout {
   static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);               // [2][2][NE]
   static constexpr int OFF_U = al4(OFF_KM + 4 * NE);                // [PPU][VL]
   static constexpr int OFF_A = al4(OFF_U + PPU * VL);               // [PP_A][VL]
-  static constexpr int OFF_K = al4(OFF_A + PP_A * VL);              // [2][2][NE][LB]
-  static constexpr int TOTAL = OFF_K + 4 * NE * LB;
+  static constexpr int TOTAL = OFF_A + PP_A * VL;
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
 
@@ -2146,7 +2368,6 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
   float* sKM = sm + LY::OFF_KM;
   float* sU = sm + LY::OFF_U;
   float* sA = sm + LY::OFF_A;
-  float* sK = sm + LY::OFF_K;
 
   const int tid = threadIdx.x;
   const int lq = tid % LB;
@@ -2206,17 +2427,6 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
         const size_t ep = (size_t)e * NGLL3 + i;
         cp_async4(km + i, A.m.kappa + ep);
         cp_async4(km + NE + i, A.m.mu + ep);
-      }
-    }
-    if ((fl & 2) && g < nspec) {
-      float* kb = sK + buf * 2 * NE * LB;
-      const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3) << LWLOG);
-#pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        const int p = t + 25 * r;
-        const size_t q = eb + ((size_t)p << LWLOG);
-        cp_async4(kb + p * LB + lq, A.k.mu + q);
-        cp_async4(kb + (NE + p) * LB + lq, A.k.kappa + q);
       }
     }
   };
@@ -2294,14 +2504,15 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     }
     pair_xi<VL, GEN>(b, t, kap, mu, fac, fx, kmu, kka, geo_e, A.m.xix, A.m.jac);
     if ((fl & 2) && e < nspec) {
-      const float* kb = sK + buf * 2 * NE * LB;
+      // mu/kappa kernel products: one writer per element point and lane in
+      // a launch, added in L2 without a round trip through the SM
       const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3) << LWLOG);
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
         const int p = i + 5 * t;
         const size_t q = eb + ((size_t)p << LWLOG);
-        A.k.mu[q] = kb[p * LB + lq] + dtk * kmu[i];
-        A.k.kappa[q] = kb[(NE + p) * LB + lq] + dtk * kka[i];
+        atomicAdd(&A.k.mu[q], dtk * kmu[i]);
+        atomicAdd(&A.k.kappa[q], dtk * kka[i]);
       }
     }
     __syncthreads();
