@@ -69,10 +69,14 @@ def parse():
     p.add_argument("--accuracy-steps", type=int, default=600,
                    help="record length of the after-timing accuracy check against the "
                         "FP64 oracle (0 skips it)")
-    p.add_argument("--workload", default="batched", choices=["batched", "large"],
+    p.add_argument("--serve-requests", type=int, default=200,
+                   help="--workload serve: requests of the stream")
+    p.add_argument("--workload", default="batched", choices=["batched", "large", "serve"],
                    help="batched: the headline line (medium mesh, --events per batch); "
                         "large: the 96x96x48-element layered box, 8 events, NSTEP 6000, "
-                        "dt 0.015 s, FP16 store with the host-spill ring (its own line)")
+                        "dt 0.015 s, FP16 store with the host-spill ring (its own line); "
+                        "serve: a request stream over the small, medium and large meshes "
+                        "(its own line)")
     p.add_argument("--served-load", type=float, default=1.25,
                    help="Poisson arrival rate as a fraction of batched capacity "
                         "(above 1: a saturated server, throughput-limited)")
@@ -910,12 +914,167 @@ def run_large(args):
     return 0
 
 
+def run_serve(args):
+    """Serving stream shaped as the workload list's: requests over the
+    small, medium and large meshes (50/35/15 %), NSTEP uniform on
+    1000-8000, 60 % forward-only and 40 % forward+adjoint, each with its own
+    seeded source and 25 (small) or 100 receivers at random surface
+    positions, arriving as a Poisson stream.  Each mesh stays resident with
+    a lane-batched run (32, 32 and 8 lanes) and a one-lane run; requests go
+    where they are predicted to finish first, are admitted by each mesh's
+    boundary-store budget, and advance in pipelined quanta.  Reports
+    events/hour over the stream's span and p50/p99 latency, beside the
+    plain path (one request at a time, FIFO, each mesh's measured plain
+    step costs) on the same arrivals."""
+    import torch
+    from specfwat_b200 import database as D
+    from specfwat_b200 import solver as S
+    from specfwat_b200.serving import MeshServer, Request, Server, StepCosts, latency_stats
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    NR = args.serve_requests
+    rng = np.random.default_rng(2026)
+    # dt, lanes, receivers per side, store budget of the batched and of the
+    # one-lane server: each budget holds the largest request's store (an
+    # 8000-step large request needs 34 GB), and with the wavefields of all
+    # six runs (about 33 GB) they stay well inside 180 GB
+    spec = {"small": (0.02, 32, 5, 2e9, 1e9), "medium": (0.02, 32, 10, 20e9, 6.2e9),
+            "large": (0.015, 8, 10, 70e9, 35e9)}
+    dbs, obs_dbs = {}, {}
+    for name in spec:
+        db = D.build(name, seed=1234)
+        dbs[name] = db
+        obs_dbs[name] = db.with_model(db.vp, D.gaussian_vs_anomaly(db, db.vs), db.rho)
+    reqs = []
+    for k in range(NR):
+        name = ("small", "medium", "large")[int(rng.choice(3, p=[0.5, 0.35, 0.15]))]
+        kind = "fwd" if rng.random() < 0.6 else "fwdadj"
+        ns = int(rng.integers(1000, 8001))
+        box = dbs[name].box
+        src = S.make_source(rng.uniform(0.15, 0.85) * box.lx, rng.uniform(0.15, 0.85) * box.ly,
+                            -rng.uniform(0.1, 0.45) * box.lz, D.random_moment_tensor(rng),
+                            rng.uniform(0.5, 1.5))
+        nr = spec[name][2] ** 2
+        rec = np.stack([box.x0 + rng.uniform(0.1, 0.9, nr) * box.lx,
+                        box.y0 + rng.uniform(0.1, 0.9, nr) * box.ly, np.zeros(nr)], 1)
+        reqs.append(Request(rid=k, mesh=name, kind=kind, nstep=ns, source=src, receivers=rec))
+    # observed data of the forward+adjoint requests: batched forward runs on
+    # each mesh's anomaly model, every event with its own receivers
+    for name, (dt, lanes, nside, _, _) in spec.items():
+        ks = [r for r in reqs if r.mesh == name and r.kind == "fwdadj"]
+        if not ks:
+            continue
+        mo = S.Mesh(obs_dbs[name])
+        for c0 in range(0, len(ks), 32 if name != "large" else 8):
+            chunk = ks[c0:c0 + (32 if name != "large" else 8)]
+            so = S.Simulation(mo, max(r.nstep for r in chunk), dt, nev=len(chunk),
+                              use_graph=True, max_receivers=nside * nside)
+            so.set_sources([r.source for r in chunk])
+            for e, r in enumerate(chunk):
+                so.set_receivers(r.receivers, ev=e)
+            so.iterate_time(1)
+            for e, r in enumerate(chunk):
+                r.obs = so.seismograms(e)[:, :, :r.nstep].astype(np.float64).copy()
+            so.close()
+        mo.close()
+    # per-mesh step costs: the plain one-event path and one active 8-lane
+    # group of the batched path, forward and adjoint
+    costs, plain_ms = {}, {}
+    for name, (dt, lanes, nside, _, _) in spec.items():
+        m = S.Mesh(dbs[name])
+        rec = D.surface_receivers(dbs[name].box, nside)
+        box = dbs[name].box
+        src = S.make_source(0.5 * box.lx, 0.5 * box.ly, -0.2 * box.lz,
+                            D.random_moment_tensor(rng), 1.0)
+        per = {}
+        for nev in (1, 8):
+            sim = S.Simulation(m, 60, dt, nev=nev, store="fp16", max_receivers=len(rec))
+            sim.set_sources([src] * nev)
+            sim.set_receivers(rec)
+            sim.iterate_time(1, save_forward=True)
+            for e in range(nev):
+                sim.measure_l2(e, np.zeros((len(rec), 3, 60)))
+            sim.iterate_time(3)
+            per[nev] = (sum(sim.time_kernels(1, 20)), sum(sim.time_kernels(3, 20)))
+            sim.close()
+        m.close()
+        plain_ms[name] = per[1]
+        costs[name] = StepCosts(per[1][0] / 1e3, per[1][1] / 1e3, per[8][0] / 1e3,
+                                per[8][1] / 1e3)
+    def plain_s(r):
+        f, a = plain_ms[r.mesh]
+        return r.nstep * (f + (a if r.kind == "fwdadj" else 0.0)) / 1e3
+    work = np.array([plain_s(r) for r in reqs])
+    # arrivals at the rate that keeps the plain path busy 2x over (a load the
+    # batched servers absorb, a queue for the one-at-a-time path)
+    lam = 2.0 / work.mean()
+    arr = np.cumsum(np.random.default_rng(77).exponential(1.0 / lam, NR))
+    arr -= arr[0]
+    for r, a in zip(reqs, arr):
+        r.arrival = float(a)
+    servers = {name: MeshServer(name, dbs[name], slots=spec[name][1], nstep_max=8000,
+                                dt=spec[name][0], store="fp16", graph_steps=50,
+                                max_receivers=spec[name][2] ** 2, store_budget=spec[name][3])
+               for name in spec}
+    solo = {name: MeshServer(name, dbs[name], slots=1, nstep_max=8000, dt=spec[name][0],
+                             store="fp16", graph_steps=50, max_receivers=spec[name][2] ** 2,
+                             store_budget=spec[name][4])
+            for name in spec}
+    clocks = Clocks(0)
+    clocks.start()
+    done = Server(servers, quantum=100, solo=solo, costs=costs).run(reqs, timeout=5400)
+    clk = clocks.stop()
+    for sv in list(servers.values()) + list(solo.values()):
+        sv.close()
+    st = latency_stats(done)
+    t_free, lat = 0.0, []
+    for r in sorted(reqs, key=lambda q: q.arrival):
+        start = max(r.arrival, t_free)
+        t_free = start + plain_s(r)
+        lat.append(t_free - r.arrival)
+    fifo = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "events_per_hour": NR / (t_free - arr[0]) * 3600.0,
+            "how": "each request's plain one-event time from the mesh's measured plain "
+                   "step costs (FP16 store), served one at a time in arrival order"}
+    by_mesh = {}
+    for name in spec:
+        rs = [r for r in done if r.mesh == name]
+        if rs:
+            lt = np.array([r.latency for r in rs])
+            by_mesh[name] = {"n": len(rs), "p50_s": float(np.percentile(lt, 50)),
+                             "p99_s": float(np.percentile(lt, 99)),
+                             "solo_share": sum(r.server == "solo" for r in rs) / len(rs)}
+    line = {
+        "metric": "served fwd and fwd+adj requests/hour over three resident meshes; p50/p99 "
+                  "latency", "value": st["events_per_hour"], "unit": "events/hour",
+        "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+        "config": {"workload": f"{NR} Poisson requests over the small/medium/large meshes "
+                               "(50/35/15 percent), NSTEP uniform 1000-8000, 60 percent "
+                               "forward-only, own source and receivers per request",
+                   "arrival_rate_per_hour": lam * 3600.0,
+                   "lanes": {n: v[1] for n, v in spec.items()},
+                   "store_budget_bytes": {n: {"batched": v[3], "one_lane": v[4]}
+                                          for n, v in spec.items()}},
+        "served": st, "plain_fifo": fifo, "by_mesh": by_mesh,
+        "errors": sum(bool(r.error) for r in done),
+        "step_costs_ms": {n: {"plain_fwd": c.plain_fwd * 1e3, "plain_adj": c.plain_adj * 1e3,
+                              "group_fwd": c.group_fwd * 1e3, "group_adj": c.group_adj * 1e3}
+                          for n, c in costs.items()},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

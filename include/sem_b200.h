@@ -267,6 +267,16 @@ int sem_lane_start_adjoint(sem_run *run, int lane, const double *obs,
 /* Queue nsteps steps for every active lane (lanes that reach their NSTEP
  * stop inside the launches).  Asynchronous. */
 int sem_advance(sem_run *run, int nsteps);
+/* Completion marks on the run's stream, for a scheduler that keeps work
+ * queued on several runs and services whichever finishes first.
+ * sem_mark records a mark after everything queued so far and returns its
+ * token; sem_mark_done returns 1 once the work before it has finished, 0
+ * if not yet (wait = 1 blocks until it has); sem_mark_elapsed gives the
+ * device time in ms between two marks still among the last 16.  No
+ * counterpart in the reference. */
+int sem_mark(sem_run *run, long long *token);
+int sem_mark_done(sem_run *run, long long token, int wait);
+int sem_mark_elapsed(sem_run *run, long long t0, long long t1, double *ms);
 /* phase: 0 idle, 1 forward, 3 adjoint; step: steps done in that phase. */
 int sem_lane_status(sem_run *run, int lane, int *phase, int *step,
                     int *nstep);
@@ -277,6 +287,22 @@ int sem_lane_status(sem_run *run, int lane, int *phase, int *step,
  * any other lane becomes idle.  Blocks until the copies are done. */
 int sem_lane_finish(sem_run *run, int lane, float *seis, double *kernels6,
                     double *ksum_dev);
+
+/* Non-blocking forms for a scheduler that keeps work queued on the run.
+ * sem_lane_finish_async queues what sem_lane_finish does (results to the
+ * host and/or the FP64 device sum, the lane's store freed stream-ordered)
+ * and returns at once; seis / kernels6 should be page-locked host memory
+ * (pageable memory makes the copy wait for the queued work), and must not
+ * be read before sem_lane_ready(run, lane, 0) returns 1 (wait = 1 blocks
+ * until it does).  With check_every > 0 it blocks as sem_lane_finish does.
+ * sem_lane_start_adjoint with misfit = NULL does not wait either;
+ * sem_lane_misfit then queues the copy of the lane's FP64 misfit to
+ * *misfit, readable after sem_lane_ready (at once for pageable memory).
+ * No counterpart in the reference. */
+int sem_lane_finish_async(sem_run *run, int lane, float *seis, double *kernels6,
+                          double *ksum_dev);
+int sem_lane_ready(sem_run *run, int lane, int wait);
+int sem_lane_misfit(sem_run *run, int lane, double *misfit);
 
 /* Element-kernel variants in use for the forward and adjoint phases
  * (1 thread-per-point, 2 pencil, 3 pencil pipelined, 4 pencil pipelined

@@ -437,6 +437,23 @@ struct sem_run_s {
   int steps_since_check = 0;
   std::vector<char> lane_failed;
   std::vector<int> lane_fail_step;
+  // lane-driven runs: pinned host staging, so that a lane's set-up and the
+  // lane table reach the device without draining the stream (a copy from
+  // pageable host memory first waits for all queued work)
+  static constexpr int kStage = 8;
+  unsigned char* h_stage_tab = nullptr;      // [kStage][lane table, group map]
+  size_t stage_tab_bytes = 0;
+  cudaEvent_t stage_ev[kStage] = {};
+  long long stage_next = 0;
+  std::vector<unsigned char*> h_lane_stage;  // per lane: set-up or observed data
+  size_t lane_stage_bytes = 0;
+  std::vector<cudaEvent_t> lane_ev;          // per lane: its staged copies have left
+  std::vector<cudaEvent_t> lane_res_ev;      // per lane: its queued results have landed
+  DevArray<double> lane_misfit;              // [nev] misfit of each lane's last measurement
+  // completion marks (sem_mark): a ring of timing events on the run's stream
+  static constexpr int kMarks = 16;
+  cudaEvent_t mark_ev[kMarks] = {};
+  long long mark_next = 0;        // token of the next mark
   std::vector<int> src_ispec, nrec;
   std::vector<char> have_src, have_rec, have_adj;
   // FK injection per event: one device allocation holding the velocity and
@@ -465,6 +482,17 @@ struct sem_run_s {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (check_ev) cudaEventDestroy(check_ev);
+    for (auto e : mark_ev)
+      if (e) cudaEventDestroy(e);
+    for (auto e : stage_ev)
+      if (e) cudaEventDestroy(e);
+    for (auto e : lane_ev)
+      if (e) cudaEventDestroy(e);
+    for (auto e : lane_res_ev)
+      if (e) cudaEventDestroy(e);
+    if (h_stage_tab) cudaFreeHost(h_stage_tab);
+    for (auto p : h_lane_stage)
+      if (p) cudaFreeHost(p);
     if (copy_stream) cudaStreamSynchronize(copy_stream);
     for (auto e : ev_chunk) cudaEventDestroy(e);
     for (auto e : ev_launch) cudaEventDestroy(e);
@@ -1008,13 +1036,11 @@ int sem_set_sources(sem_run* r, int nev, const sem_source* src) {
   return SEM_OK;
 }
 
-int sem_set_receivers(sem_run* r, int ev, int nrec, const double* xyz) {
-  if (!r || (!xyz && nrec > 0)) return fail(SEM_ERR_ARG, "null argument");
-  if (nrec < 0 || nrec > r->nrec_max)
-    return fail(SEM_ERR_ARG, "nrec %d outside [0, max_receivers=%d]", nrec, r->nrec_max);
-  if (ev < -1 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
-  std::vector<int> isp(r->nrec_max, 0);
-  std::vector<float> w((size_t)r->nrec_max * 125, 0.f);
+// Receiver elements and Lagrange weights of nrec receivers into isp
+// [nrec_max] and w [nrec_max][125] (entries past nrec zero).
+static int receivers_host(sem_run* r, int nrec, const double* xyz, int* isp, float* w) {
+  std::fill(isp, isp + r->nrec_max, 0);
+  std::fill(w, w + (size_t)r->nrec_max * 125, 0.f);
   for (int k = 0; k < nrec; ++k) {
     if (!std::isfinite(xyz[k * 3] + xyz[k * 3 + 1] + xyz[k * 3 + 2]))
       return fail(SEM_ERR_ARG, "receiver %d position is not finite", k);
@@ -1029,6 +1055,18 @@ int sem_set_receivers(sem_run* r, int ev, int nrec, const double* xyz) {
         for (int a = 0; a < 5; ++a)
           w[(size_t)k * 125 + a + 5 * b + 25 * c] = (float)(hx[a] * hy[b] * hz[c]);
   }
+  return SEM_OK;
+}
+
+int sem_set_receivers(sem_run* r, int ev, int nrec, const double* xyz) {
+  if (!r || (!xyz && nrec > 0)) return fail(SEM_ERR_ARG, "null argument");
+  if (nrec < 0 || nrec > r->nrec_max)
+    return fail(SEM_ERR_ARG, "nrec %d outside [0, max_receivers=%d]", nrec, r->nrec_max);
+  if (ev < -1 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
+  std::vector<int> isp(r->nrec_max, 0);
+  std::vector<float> w((size_t)r->nrec_max * 125, 0.f);
+  int rrc = receivers_host(r, nrec, xyz, isp.data(), w.data());
+  if (rrc) return rrc;
   const int e0 = ev < 0 ? 0 : ev, e1 = ev < 0 ? r->nev : ev + 1;
   for (int e = e0; e < e1; ++e) {
     CK(cudaMemcpyAsync(r->rec_ispec.p + (size_t)e * r->nrec_max, isp.data(),
@@ -1507,17 +1545,10 @@ int sem_set_adjoint_sources(sem_run* r, int ev, const double* adj) {
 }
 
 // Taper (src/shared/signal.f90:419-491) and Simpson weights
-// (src/shared/utils.f90:1635-1663, as written there) for nstep samples.
-static int prepare_measure(sem_run* r, double taper_pct, int taper_type, int ns) {
-  if (!r->taper.p) {
-    CKM(r->taper.alloc(r->nstep), "taper");
-    CKM(r->simpw.alloc(r->nstep), "simpson weights");
-    CKM(r->misfit_rc.alloc((size_t)r->nrec_max * 3), "misfits");
-  }
-  if (taper_pct == r->taper_pct_cached && taper_type == r->taper_type_cached &&
-      ns == r->taper_ns_cached)
-    return SEM_OK;
-  std::vector<double> w(ns, 1.0);
+// (src/shared/utils.f90:1635-1663, as written there) for ns samples of dt.
+static void measure_weights(int ns, double dx, double taper_pct, int taper_type, double* w,
+                            double* sw) {
+  for (int i = 0; i < ns; ++i) w[i] = 1.0;
   const int frac = (taper_pct == 0.0 || taper_pct == 1.0) ? (int)(ns * taper_pct / 2.0)
                                                           : (int)(ns * taper_pct / 2.0 + 0.5);
   if (frac > 0) {
@@ -1537,8 +1568,7 @@ static int prepare_measure(sem_run* r, double taper_pct, int taper_type, int ns)
   }
   // The even-count branch weights sample n-1 (1-based) by 1 + 2: the
   // initial sum holds y(n-1) and the loop adds 2 y(i+1) up to i+1 = n-1.
-  std::vector<double> sw(ns, 0.0);
-  const double dx = r->dt;
+  for (int i = 0; i < ns; ++i) sw[i] = 0.0;
   if (ns >= 2) {
     if (ns % 2 == 0) {
       sw[0] += dx / 3.0;
@@ -1556,6 +1586,25 @@ static int prepare_measure(sem_run* r, double taper_pct, int taper_type, int ns)
       for (int i = 3; i <= ns - 2; i += 2) sw[i - 1] += 2.0 * dx / 3.0;
     }
   }
+}
+
+static int prepare_measure_buffers(sem_run* r) {
+  if (!r->taper.p) {
+    CKM(r->taper.alloc(r->nstep), "taper");
+    CKM(r->simpw.alloc(r->nstep), "simpson weights");
+    CKM(r->misfit_rc.alloc((size_t)r->nrec_max * 3), "misfits");
+  }
+  return SEM_OK;
+}
+
+static int prepare_measure(sem_run* r, double taper_pct, int taper_type, int ns) {
+  int rc = prepare_measure_buffers(r);
+  if (rc) return rc;
+  if (taper_pct == r->taper_pct_cached && taper_type == r->taper_type_cached &&
+      ns == r->taper_ns_cached)
+    return SEM_OK;
+  std::vector<double> w(ns), sw(ns);
+  measure_weights(ns, r->dt, taper_pct, taper_type, w.data(), sw.data());
   CK(cudaMemcpyAsync(r->taper.p, w.data(), ns * 8, cudaMemcpyHostToDevice, r->stream));
   CK(cudaMemcpyAsync(r->simpw.p, sw.data(), ns * 8, cudaMemcpyHostToDevice, r->stream));
   CK(cudaStreamSynchronize(r->stream));
@@ -1836,6 +1885,49 @@ int sem_set_stream(sem_run* r, void* stream) {
   return SEM_OK;
 }
 
+int sem_mark(sem_run* r, long long* token) {
+  if (!r || !token) return fail(SEM_ERR_ARG, "null argument");
+  const int slot = (int)(r->mark_next % sem_run_s::kMarks);
+  if (!r->mark_ev[slot]) CK(cudaEventCreate(&r->mark_ev[slot]));
+  CK(cudaEventRecord(r->mark_ev[slot], r->stream));
+  *token = r->mark_next++;
+  return SEM_OK;
+}
+
+// A mark whose slot has been recorded again is older than every mark in
+// flight; the stream runs in order, so it has completed.
+static bool mark_recycled(const sem_run* r, long long token) {
+  return token < r->mark_next - sem_run_s::kMarks;
+}
+
+int sem_mark_done(sem_run* r, long long token, int wait) {
+  if (!r || token < 0 || token >= r->mark_next) return fail(SEM_ERR_ARG, "unknown mark %lld", token);
+  if (mark_recycled(r, token)) return 1;
+  cudaEvent_t e = r->mark_ev[token % sem_run_s::kMarks];
+  if (wait) {
+    CK(cudaEventSynchronize(e));
+    return 1;
+  }
+  const cudaError_t q = cudaEventQuery(e);
+  if (q == cudaSuccess) return 1;
+  if (q == cudaErrorNotReady) {
+    cudaGetLastError();
+    return 0;
+  }
+  return fail(SEM_ERR_CUDA, "mark %lld: %s", token, cudaGetErrorString(q));
+}
+
+int sem_mark_elapsed(sem_run* r, long long t0, long long t1, double* ms) {
+  if (!r || !ms) return fail(SEM_ERR_ARG, "null argument");
+  if (t0 < 0 || t1 < t0 || t1 >= r->mark_next || mark_recycled(r, t0))
+    return fail(SEM_ERR_ARG, "marks %lld..%lld are not both in the ring", t0, t1);
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, r->mark_ev[t0 % sem_run_s::kMarks],
+                          r->mark_ev[t1 % sem_run_s::kMarks]));
+  *ms = f;
+  return SEM_OK;
+}
+
 int sem_set_store_spill(sem_run* r, long long device_store_bytes) {
   if (!r) return fail(SEM_ERR_ARG, "null run");
   if (r->lanes_mode)
@@ -1916,6 +2008,44 @@ int sem_time_kernels(sem_run* r, int sim_type, int nsteps, double* ms4) {
 // serving primitives: one event per lane, lanes advance independently
 // ----------------------------------------------------------------------------
 
+// Event marking that a lane's queued results (async finish, misfit) have
+// landed.
+static int lane_result_event(sem_run* r, int lane, cudaEvent_t* out) {
+  if (r->lane_res_ev.empty()) r->lane_res_ev.assign(r->nev, nullptr);
+  if (!r->lane_res_ev[lane])
+    CK(cudaEventCreateWithFlags(&r->lane_res_ev[lane], cudaEventDisableTiming));
+  *out = r->lane_res_ev[lane];
+  return SEM_OK;
+}
+
+// Pinned staging area of a lane, at least `bytes`, once the lane's earlier
+// staged copies have left it.
+static int lane_stage(sem_run* r, int lane, size_t bytes, unsigned char** out) {
+  if (r->h_lane_stage.empty()) {
+    r->h_lane_stage.assign(r->nev, nullptr);
+    r->lane_ev.assign(r->nev, nullptr);
+  }
+  if (!r->lane_ev[lane])
+    CK(cudaEventCreateWithFlags(&r->lane_ev[lane], cudaEventDisableTiming));
+  else
+    CK(cudaEventSynchronize(r->lane_ev[lane]));
+  // every lane's area has the largest size any lane needs
+  const size_t need = std::max(bytes, r->lane_stage_bytes);
+  if (need > r->lane_stage_bytes) {
+    for (int l = 0; l < r->nev; ++l)
+      if (r->h_lane_stage[l]) {
+        if (r->lane_ev[l]) CK(cudaEventSynchronize(r->lane_ev[l]));
+        cudaFreeHost(r->h_lane_stage[l]);
+        r->h_lane_stage[l] = nullptr;
+      }
+    r->lane_stage_bytes = need;
+  }
+  if (!r->h_lane_stage[lane])
+    CK(cudaMallocHost((void**)&r->h_lane_stage[lane], r->lane_stage_bytes));
+  *out = r->h_lane_stage[lane];
+  return SEM_OK;
+}
+
 static void lane_defaults(sem_run* r, int e) {
   const size_t ns = (size_t)r->nstep;  // per-lane regions are sized for the run's nstep
   LaneDesc& L = r->h_lanes[e];
@@ -1989,7 +2119,18 @@ int sem_lane_start_forward(sem_run* r, int lane, const sem_source* src, int nrec
   lagrange_all(xi3[2], hz, hzd);
   double B[3][3];
   r->mesh->dxi_dx(r->src_ispec[lane], xi3, B);
-  std::vector<float> sa(375), stf(nstep);
+  if (nrec < 0 || nrec > r->nrec_max || (!xyz && nrec > 0))
+    return fail(SEM_ERR_ARG, "nrec %d outside [0, max_receivers=%d]", nrec, r->nrec_max);
+  // source array, time function and receivers staged in pinned memory, so
+  // that the lane starts without waiting for the work queued on the run
+  const size_t nr = r->nrec_max;
+  unsigned char* stage = nullptr;
+  rc = lane_stage(r, lane, (375 + (size_t)r->nstep + nr * 125) * 4 + nr * 4, &stage);
+  if (rc) return rc;
+  float* sa = (float*)stage;
+  float* stf = sa + 375;
+  float* rw = stf + r->nstep;
+  int* isp = (int*)(rw + nr * 125);
   for (int c = 0; c < 5; ++c)
     for (int b = 0; b < 5; ++b)
       for (int a = 0; a < 5; ++a) {
@@ -2003,13 +2144,20 @@ int sem_lane_start_forward(sem_run* r, int lane, const sem_source* src, int nrec
       }
   const double t0 = 1.2 / s.f0 + s.tshift;
   for (int it = 0; it < nstep; ++it) stf[it] = (float)ricker((double)it * r->dt - t0, s.f0);
-  CK(cudaMemcpyAsync(r->srcarr.p + (size_t)lane * 375, sa.data(), 375 * 4,
-                     cudaMemcpyHostToDevice, r->stream));
-  CK(cudaMemcpyAsync(r->stf.p + (size_t)lane * r->nstep, stf.data(), (size_t)nstep * 4,
-                     cudaMemcpyHostToDevice, r->stream));
-  r->have_src[lane] = 1;
-  rc = sem_set_receivers(r, lane, nrec, xyz);
+  rc = receivers_host(r, nrec, xyz, isp, rw);
   if (rc) return rc;
+  CK(cudaMemcpyAsync(r->srcarr.p + (size_t)lane * 375, sa, 375 * 4, cudaMemcpyHostToDevice,
+                     r->stream));
+  CK(cudaMemcpyAsync(r->stf.p + (size_t)lane * r->nstep, stf, (size_t)nstep * 4,
+                     cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->rec_ispec.p + (size_t)lane * nr, isp, nr * sizeof(int),
+                     cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->rec_w.p + (size_t)lane * nr * 125, rw, nr * 125 * sizeof(float),
+                     cudaMemcpyHostToDevice, r->stream));
+  CK(cudaEventRecord(r->lane_ev[lane], r->stream));
+  r->have_src[lane] = 1;
+  r->nrec[lane] = nrec;
+  r->have_rec[lane] = 1;
   // boundary store for the later adjoint run
   if (r->lane_store[lane]) {
     CK(cudaFreeAsync(r->lane_store[lane], r->stream));
@@ -2066,13 +2214,30 @@ int sem_lane_start_adjoint(sem_run* r, int lane, const double* obs, double taper
   if (!(taper_pct >= 0.0 && taper_pct <= 1.0) || taper_type < 1 || taper_type > 4)
     return fail(SEM_ERR_ARG, "invalid taper");
   const int ns = L.nstep, nr = L.nrec;
-  int rc = prepare_measure(r, taper_pct, taper_type, ns);
+  int rc = prepare_measure_buffers(r);
   if (rc) return rc;
   if (!r->obs.p) CKM(r->obs.alloc((size_t)r->nrec_max * 3 * r->nstep), "observed data");
-  CK(cudaMemcpyAsync(r->obs.p, obs, (size_t)nr * 3 * ns * 8, cudaMemcpyHostToDevice,
+  if (!r->lane_misfit.p) CKM(r->lane_misfit.alloc((size_t)r->nev), "lane misfits");
+  // observed data and this record's weights staged in pinned memory, so
+  // that the switch does not wait for the work queued on the run; the
+  // device buffers are shared, and every use is stream-ordered
+  unsigned char* stage = nullptr;
+  rc = lane_stage(r, lane, ((size_t)nr * 3 * ns + 2 * (size_t)ns) * 8, &stage);
+  if (rc) return rc;
+  double* hobs = (double*)stage;
+  double* hw = hobs + (size_t)nr * 3 * ns;
+  double* hsw = hw + ns;
+  std::memcpy(hobs, obs, (size_t)nr * 3 * ns * 8);
+  measure_weights(ns, r->dt, taper_pct, taper_type, hw, hsw);
+  CK(cudaMemcpyAsync(r->obs.p, hobs, (size_t)nr * 3 * ns * 8, cudaMemcpyHostToDevice,
                      r->stream));
+  CK(cudaMemcpyAsync(r->taper.p, hw, (size_t)ns * 8, cudaMemcpyHostToDevice, r->stream));
+  CK(cudaMemcpyAsync(r->simpw.p, hsw, (size_t)ns * 8, cudaMemcpyHostToDevice, r->stream));
+  CK(cudaEventRecord(r->lane_ev[lane], r->stream));
+  r->taper_ns_cached = -1;  // the shared weights now hold this record's
   launch_measure_l2(L.seis, r->obs.p, r->taper.p, r->simpw.p, nr, ns, (float*)L.adj,
                     r->misfit_rc.p, r->stream);
+  launch_sum_series(r->misfit_rc.p, 3 * nr, r->lane_misfit.p + lane, r->stream);
   // backward field starts from this lane's final forward state
   const Fields f1{r->u1.p, r->v1.p, r->a1.p}, f2{r->u2.p, r->v2.p, r->a2.p};
   launch_lane_copy(f1, f2, r->mesh->nglob, r->lm, lane, r->stream);
@@ -2082,17 +2247,26 @@ int sem_lane_start_adjoint(sem_run* r, int lane, const double* obs, double taper
                        (size_t)r->mesh->nspec * NGLL3, r->lm, lane, r->stream);
   CK(cudaGetLastError());
   if (misfit) {
-    std::vector<double> m((size_t)nr * 3);
-    CK(cudaMemcpyAsync(m.data(), r->misfit_rc.p, m.size() * 8, cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(misfit, r->lane_misfit.p + lane, sizeof(double), cudaMemcpyDeviceToHost,
                        r->stream));
     CK(cudaStreamSynchronize(r->stream));
-    double t = 0.0;
-    for (double v : m) t += v;
-    *misfit = t;
   }
   L.phase = PH_ADJ;
   L.it0 = 0;
   L.save = 0;
+  return SEM_OK;
+}
+
+int sem_lane_misfit(sem_run* r, int lane, double* misfit) {
+  if (!r || !misfit || !r->lanes_mode || lane < 0 || lane >= r->nev)
+    return fail(SEM_ERR_ARG, "lane %d is not a serving lane", lane);
+  if (!r->lane_misfit.p) return fail(SEM_ERR_STATE, "no lane has been measured");
+  cudaEvent_t done = nullptr;
+  int rc = lane_result_event(r, lane, &done);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(misfit, r->lane_misfit.p + lane, sizeof(double), cudaMemcpyDeviceToHost,
+                     r->stream));
+  CK(cudaEventRecord(done, r->stream));
   return SEM_OK;
 }
 
@@ -2142,11 +2316,25 @@ int sem_advance(sem_run* r, int nsteps) {
   for (int g = 0; g < ngr; ++g)
     if (has[g] & 2) gmap.push_back(g);
   const int na = (int)gmap.size() - nf;
-  CK(cudaMemcpyAsync(r->lanes.p, r->h_lanes.data(), r->lanes.bytes(), cudaMemcpyHostToDevice,
-                     r->stream));
   if (!r->gmap.p) CKM(r->gmap.alloc((size_t)std::max(1, ngr)), "group map");
-  CK(cudaMemcpyAsync(r->gmap.p, gmap.data(), gmap.size() * sizeof(int), cudaMemcpyHostToDevice,
-                     r->stream));
+  // lane table and group map through a ring of pinned slots, so that the
+  // launches queue behind the work in flight instead of waiting for it
+  if (!r->h_stage_tab) {
+    r->stage_tab_bytes = r->lanes.bytes() + (size_t)std::max(1, ngr) * sizeof(int);
+    CK(cudaMallocHost((void**)&r->h_stage_tab, r->stage_tab_bytes * sem_run_s::kStage));
+    for (auto& e : r->stage_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  {
+    const int slot = (int)(r->stage_next++ % sem_run_s::kStage);
+    CK(cudaEventSynchronize(r->stage_ev[slot]));
+    unsigned char* tab = r->h_stage_tab + (size_t)slot * r->stage_tab_bytes;
+    std::memcpy(tab, r->h_lanes.data(), r->lanes.bytes());
+    std::memcpy(tab + r->lanes.bytes(), gmap.data(), gmap.size() * sizeof(int));
+    CK(cudaMemcpyAsync(r->lanes.p, tab, r->lanes.bytes(), cudaMemcpyHostToDevice, r->stream));
+    CK(cudaMemcpyAsync(r->gmap.p, tab + r->lanes.bytes(), gmap.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, r->stream));
+    CK(cudaEventRecord(r->stage_ev[slot], r->stream));
+  }
   StepArgs af = r->args(false), aa = r->args(true), ab = r->args(na > 0);
   if (lw > 1) {
     af.gmap = r->gmap.p;
@@ -2281,6 +2469,60 @@ int sem_lane_finish(sem_run* r, int lane, float* seis, double* kernels6, double*
   }
   CK(cudaStreamSynchronize(r->stream));
   return SEM_OK;
+}
+
+int sem_lane_finish_async(sem_run* r, int lane, float* seis, double* kernels6,
+                          double* ksum_dev) {
+  if (!r || !r->lanes_mode || lane < 0 || lane >= r->nev)
+    return fail(SEM_ERR_ARG, "lane %d is not a serving lane", lane);
+  // with the stability check on, a lane's last steps are scanned before
+  // its results leave: the blocking form does that
+  if (r->cfg.check_every > 0) return sem_lane_finish(r, lane, seis, kernels6, ksum_dev);
+  LaneDesc& L = r->h_lanes[lane];
+  if (L.phase == PH_IDLE || L.it0 < L.nstep)
+    return fail(SEM_ERR_STATE, "lane %d has not completed a run", lane);
+  cudaEvent_t done = nullptr;
+  int rc = lane_result_event(r, lane, &done);
+  if (rc) return rc;
+  if (seis && L.phase == PH_FWD)
+    CK(cudaMemcpyAsync(seis, L.seis, (size_t)L.nrec * 3 * L.nstep * 4, cudaMemcpyDeviceToHost,
+                       r->stream));
+  if (L.phase == PH_ADJ && (kernels6 || ksum_dev)) {
+    const size_t ne = (size_t)r->mesh->nspec * NGLL3;
+    if (kernels6 && !r->kout.p) CKM(r->kout.alloc(6 * ne), "kernel output");
+    launch_finalize_kernels(r->mesh->view(), r->mesh->rho.p,
+                            {r->k_rho.p, r->k_mu.p, r->k_kappa.p}, r->lm, lane,
+                            kernels6 ? r->kout.p : nullptr, ksum_dev, r->stream);
+    CK(cudaGetLastError());
+    if (kernels6)
+      CK(cudaMemcpyAsync(kernels6, r->kout.p, 6 * ne * 8, cudaMemcpyDeviceToHost, r->stream));
+  }
+  CK(cudaEventRecord(done, r->stream));
+  const bool keep_store = L.phase == PH_FWD && L.save;
+  if (!keep_store) {
+    if (r->lane_store[lane]) CK(cudaFreeAsync(r->lane_store[lane], r->stream));
+    if (r->lane_scale[lane]) CK(cudaFreeAsync(r->lane_scale[lane], r->stream));
+    r->lane_store[lane] = nullptr;
+    r->lane_scale[lane] = nullptr;
+    L.phase = PH_IDLE;
+  }
+  return SEM_OK;
+}
+
+int sem_lane_ready(sem_run* r, int lane, int wait) {
+  if (!r || lane < 0 || lane >= r->nev) return fail(SEM_ERR_ARG, "bad lane");
+  if (r->lane_res_ev.empty() || !r->lane_res_ev[lane]) return 1;
+  if (wait) {
+    CK(cudaEventSynchronize(r->lane_res_ev[lane]));
+    return 1;
+  }
+  const cudaError_t q = cudaEventQuery(r->lane_res_ev[lane]);
+  if (q == cudaSuccess) return 1;
+  if (q == cudaErrorNotReady) {
+    cudaGetLastError();
+    return 0;
+  }
+  return fail(SEM_ERR_CUDA, "lane %d: %s", lane, cudaGetErrorString(q));
 }
 
 int sem_kernel_variants(sem_run* r, int* fwd, int* adj) {

@@ -162,6 +162,8 @@ int launch_check_lanes(const float* u, size_t nglob, int lwlog, int nevp, LaneDe
                        int nev, int* flags, cudaStream_t st);
 int launch_halt_lanes(LaneDesc* lanes, int nev, const int* flags, int* halt_step, int s_off,
                       cudaStream_t st);
+// *out = part[0] + ... + part[n-1], summed in that order
+int launch_sum_series(const double* part, int n, double* out, cudaStream_t st);
 int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int lane,
                          cudaStream_t st);
 

@@ -3437,6 +3437,20 @@ int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st) {
   return 1;
 }
 
+// Sum of n per-series misfits in series order (the order of a host loop)
+// into *out.
+__global__ void k_sum_series(const double* __restrict__ part, int n, double* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double t = 0.0;
+  for (int k = 0; k < n; ++k) t += part[k];
+  *out = t;
+}
+
+int launch_sum_series(const double* part, int n, double* out, cudaStream_t st) {
+  k_sum_series<<<1, 1, 0, st>>>(part, n, out);
+  return 1;
+}
+
 // Periodic stability check of a run's wavefield u ([group][point][3][LW]):
 // flags[lane] |= 1 for every running lane that holds a non-finite value.
 // per_group = values per lane group (nglob * 3 * LW).

@@ -28,6 +28,23 @@ from . import solver as S
 PH_IDLE, PH_FWD, PH_ADJ = 0, 1, 3
 
 
+def _pinned(n, dtype):
+    """A 1-D host array of n elements in page-locked memory (through torch,
+    when a CUDA device is there), so that result copies queue without
+    waiting; pageable numpy memory otherwise."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            t = torch.empty(n, dtype={np.dtype(np.float32): torch.float32,
+                                      np.dtype(np.float64): torch.float64}[np.dtype(dtype)])
+            t = t.pin_memory()
+            a = t.numpy()
+            return a, t
+    except Exception:
+        pass
+    return np.empty(n, dtype), None
+
+
 @dataclasses.dataclass
 class Request:
     rid: int
@@ -124,6 +141,18 @@ class MeshServer:
         self.policy = policy
         self.group = group
         self.max_wait = max_wait
+        # pipelined operation: quanta queued on the run and not yet retired,
+        # (mark before, mark after, steps, forward groups, adjoint groups);
+        # per lane the mark after which its current phase is complete;
+        # results queued to page-locked buffers and not yet collected
+        self.inflight: deque = deque()
+        self.done_tok: List[Optional[int]] = [None] * slots
+        self.pending: Dict[int, tuple] = {}
+        self._bufs: Dict[tuple, tuple] = {}
+        # device ms per step of one active 8-lane group (one lane on a
+        # one-lane server), forward and adjoint, learned from the marks
+        self.step_ms = {"fwd": None, "adj": None}
+        self.quanta = 0
 
     # -- admission ----------------------------------------------------------
     def _admit_one(self, req, lane, now):
@@ -250,32 +279,113 @@ class MeshServer:
                    if self.phase[l] == PH_ADJ)
 
     def busy(self):
-        return any(r is not None for r in self.lanes)
+        return any(r is not None for r in self.lanes) or bool(self.pending)
 
-    def advance(self, nsteps):
-        if self.busy():
-            self.sim.advance(nsteps)
-
-    def remaining(self):
-        """Fewest steps until some active lane completes its phase."""
-        best = None
+    def running(self):
+        """Lanes that still have steps to queue."""
+        out = []
         for lane, req in enumerate(self.lanes):
-            if req is None:
+            if req is None or self.done_tok[lane] is not None:
                 continue
             ph, st, ns = self.sim.lane_status(lane)
             if ph != PH_IDLE and st < ns:
-                best = ns - st if best is None else min(best, ns - st)
-        return best
+                out.append((lane, ph, ns - st))
+        return out
+
+    def _groups(self, run):
+        g = self.group if self.slots > 1 else 1
+        fwd, adj = set(), set()
+        for lane, ph, _ in run:
+            (adj if ph == PH_ADJ else fwd).add(lane // g)
+        return len(fwd - adj), len(adj)
+
+    def advance(self, nsteps):
+        """Queue nsteps steps of every running lane, bracketed by two marks;
+        lanes that complete their phase inside are tagged with the closing
+        mark."""
+        run = self.running()
+        if not run:
+            return
+        nf, na = self._groups(run)
+        t0 = self.sim.mark()
+        self.sim.advance(nsteps)
+        t1 = self.sim.mark()
+        self.inflight.append((t0, t1, nsteps, nf, na))
+        for lane, ph, left in run:
+            if left <= nsteps:
+                self.done_tok[lane] = t1
+
+    def remaining(self):
+        """Fewest steps until a running lane completes its phase."""
+        run = self.running()
+        return min(left for _, _, left in run) if run else None
+
+    def retire(self):
+        """Retire the queued quanta that have finished and learn the step
+        cost from their device time; returns how many retired."""
+        n = 0
+        while self.inflight and self.sim.mark_done(self.inflight[0][1]):
+            t0, t1, steps, nf, na = self.inflight.popleft()
+            n += 1
+            try:
+                ms = self.sim.mark_elapsed(t0, t1) / steps
+            except Exception:
+                continue
+            self._learn(ms, nf, na)
+        return n
+
+    def _learn(self, ms, nf, na, rate=0.3):
+        """Step cost model ms = nf * c_fwd + na * c_adj, fitted online."""
+        cf, ca = self.step_ms["fwd"], self.step_ms["adj"]
+        if na == 0 and nf > 0:
+            v = ms / nf
+            self.step_ms["fwd"] = v if cf is None else (1 - rate) * cf + rate * v
+        elif nf == 0 and na > 0:
+            v = ms / na
+            self.step_ms["adj"] = v if ca is None else (1 - rate) * ca + rate * v
+        elif cf is not None:
+            v = max(0.0, (ms - nf * cf) / na)
+            self.step_ms["adj"] = v if ca is None else (1 - rate) * ca + rate * v
+        self.quanta += 1
+
+    def _buf(self, lane, key, n, dtype):
+        b = self._bufs.get((lane, key))
+        if b is None or b[0].size < n:
+            b = _pinned(n, dtype)
+            self._bufs[(lane, key)] = b
+        return b[0][:n]
+
+    def _collect(self, lane, clock):
+        kind, req, *rest = self.pending.pop(lane)
+        if kind in ("fwd", "seis"):
+            req.seismograms = rest[0].reshape(len(req.receivers), 3, req.nstep).copy()
+        if kind == "seis":
+            return []
+        if kind == "adj":
+            req.misfit = float(rest[0][0])
+            if rest[1] is not None:
+                req.kernels = rest[1].reshape(6, self.nspec, 5, 5, 5).copy()
+        req.done = clock()
+        return [req]
 
     # -- phase transitions ----------------------------------------------------
     def poll(self, clock):
+        """Collect results that have landed, then switch or release the
+        lanes whose phase has completed on the device.  Nothing here waits
+        for the queued work."""
         finished = []
+        for lane in list(self.pending):
+            if self.sim.lane_ready(lane):
+                finished += self._collect(lane, clock)
         for lane, req in enumerate(self.lanes):
-            if req is None:
+            tok = self.done_tok[lane]
+            if req is None or tok is None or not self.sim.mark_done(tok):
                 continue
+            self.done_tok[lane] = None
             ph, st, ns = self.sim.lane_status(lane)
-            if ph == PH_IDLE or st < ns:
-                continue
+            if lane in self.pending:            # an earlier result of this lane first
+                self.sim.lane_ready(lane, wait=True)
+                finished += self._collect(lane, clock)
             if lane in self.sim.lane_errors:
                 # stopped by the stability check: released without results
                 req.error = self.sim.lane_errors[lane]
@@ -288,25 +398,26 @@ class MeshServer:
                 req.done = clock()
                 finished.append(req)
                 continue
-            if ph == PH_FWD and req.kind == "fwd":
-                req.seismograms = np.zeros((len(req.receivers), 3, req.nstep), np.float32)
-                self.sim.lane_finish(lane, seis_out=req.seismograms)
-                self._free(lane)
-                req.done = clock()
-                finished.append(req)
-            elif ph == PH_FWD:
-                req.seismograms = np.zeros((len(req.receivers), 3, req.nstep), np.float32)
-                self.sim.lane_finish(lane, seis_out=req.seismograms)
-                req.misfit = self.sim.lane_start_adjoint(lane, req.obs, *self.taper)
-                self.phase[lane] = PH_ADJ
+            nseis = len(req.receivers) * 3 * req.nstep
+            if ph == PH_FWD:
+                buf = self._buf(lane, "seis", nseis, np.float32)
+                self.sim.lane_finish_async(lane, seis_out=buf)
+                if req.kind == "fwd":
+                    self.pending[lane] = ("fwd", req, buf)
+                    self._free(lane)
+                else:
+                    self.pending[lane] = ("seis", req, buf)
+                    self.sim.lane_start_adjoint(lane, req.obs, *self.taper, want_misfit=False)
+                    self.phase[lane] = PH_ADJ
             elif ph == PH_ADJ:
-                if req.want_kernels:
-                    req.kernels = np.zeros((6, self.nspec, 5, 5, 5), np.float64)
-                self.sim.lane_finish(lane, kernels_out=req.kernels,
-                                     ksum_dev_ptr=self.ksum_dev_ptr)
+                mis = self._buf(lane, "misfit", 1, np.float64)
+                self.sim.lane_misfit(lane, mis)
+                kern = (self._buf(lane, "kern", 6 * self.nspec * 125, np.float64)
+                        if req.want_kernels else None)
+                self.sim.lane_finish_async(lane, kernels_out=kern,
+                                           ksum_dev_ptr=self.ksum_dev_ptr)
+                self.pending[lane] = ("adj", req, mis, kern)
                 self._free(lane)
-                req.done = clock()
-                finished.append(req)
         return finished
 
     def _free(self, lane):
@@ -377,7 +488,28 @@ class Server:
     def _all(self):
         return list(self.servers.values()) + list(self.solo.values())
 
-    def run(self, requests: List[Request], timeout=3600.0):
+    def _online_costs(self, name):
+        """Step costs of a mesh learned from its servers' marks, once both
+        the batched and (if any) the one-lane server have been measured in
+        both phases; None before."""
+        b = self.servers[name].step_ms
+        so = self.solo.get(name)
+        if b["fwd"] is None or b["adj"] is None:
+            return None
+        if so is None:
+            return None
+        p = so.step_ms
+        if p["fwd"] is None or p["adj"] is None:
+            return None
+        return StepCosts(p["fwd"] / 1e3, p["adj"] / 1e3, b["fwd"] / 1e3, b["adj"] / 1e3)
+
+    def run(self, requests: List[Request], timeout=3600.0, depth=2):
+        """Replay a request stream.  Every busy mesh keeps ``depth`` quanta
+        queued on its own stream; the host services whichever mesh has a
+        quantum finished (marks on the run's stream, no device-wide
+        synchronisation), so the GPU always has the next quantum while
+        lanes switch, results come back and requests are admitted.  Step
+        costs for routing are learned online per mesh once measured."""
         pending = sorted(requests, key=lambda r: r.arrival)
         t0 = time.perf_counter()
         clock = lambda: time.perf_counter() - t0  # noqa: E731
@@ -387,26 +519,33 @@ class Server:
             now = clock()
             if now > timeout:
                 raise TimeoutError("serving stream did not finish")
+            for name in self.servers:
+                learned = self._online_costs(name)
+                if learned is not None:
+                    self.costs[name] = learned
             while i < len(pending) and pending[i].arrival <= now:
                 self._route(pending[i]).queue.append(pending[i])
                 i += 1
             for srv in self._all():
                 srv.try_admit(now)
-            busy = [s for s in self._all() if s.busy()]
-            if not busy:
-                if i < len(pending):
-                    time.sleep(max(0.0, min(0.01, pending[i].arrival - clock())))
-                continue
-            for srv in busy:
-                rem = srv.remaining()
-                n = self.quantum if rem is None else max(1, min(self.quantum, rem))
-                srv.advance(n)
-            # one quantum in flight per mesh: new arrivals wait at most one
-            # quantum before they can take a lane
-            for srv in busy:
-                srv.sim.synchronize()
-            for srv in busy:
-                done += srv.poll(clock)
+            for srv in self._all():
+                while len(srv.inflight) < depth:
+                    rem = srv.remaining()
+                    if rem is None:
+                        break
+                    srv.advance(max(1, min(self.quantum, rem)))
+            progressed = False
+            for srv in self._all():
+                progressed |= srv.retire() > 0
+                got = srv.poll(clock)
+                progressed |= bool(got)
+                done += got
+            if not progressed:
+                if not any(srv.inflight or srv.pending for srv in self._all()):
+                    if i < len(pending):
+                        time.sleep(max(0.0, min(0.01, pending[i].arrival - clock())))
+                else:
+                    time.sleep(0.0005)
         return done
 
 

@@ -279,6 +279,24 @@ class Simulation:
         return out
 
     # -- serving primitives (one event per lane, lanes advance together) --
+    def mark(self) -> int:
+        """Token of a completion mark after everything queued so far."""
+        t = C.c_longlong()
+        check(_lib.load().sem_mark(self._h, C.byref(t)))
+        return t.value
+
+    def mark_done(self, token: int, wait: bool = False) -> bool:
+        rc = _lib.load().sem_mark_done(self._h, int(token), int(wait))
+        if rc < 0:
+            check(rc)
+        return rc == 1
+
+    def mark_elapsed(self, t0: int, t1: int) -> float:
+        """Device ms between two marks (both among the last 16)."""
+        ms = C.c_double()
+        check(_lib.load().sem_mark_elapsed(self._h, int(t0), int(t1), C.byref(ms)))
+        return ms.value
+
     def set_store_spill(self, device_bytes: int):
         """Hold the boundary store partly in pinned host memory: at most
         ``device_bytes`` of HBM for it (0: all resident; -1: what is free when
@@ -313,6 +331,29 @@ class Simulation:
             self._h, lane, obs.ctypes.data, float(taper_pct), int(taper_type),
             C.byref(m) if want_misfit else None))
         return m.value if want_misfit else None
+
+    def lane_finish_async(self, lane: int, seis_out=None, kernels_out=None,
+                          ksum_dev_ptr: int = 0):
+        """Queue a lane's results (into page-locked arrays for no waiting);
+        read them after ``lane_ready(lane)``."""
+        self.lane_errors.pop(lane, None)
+        check(_lib.load().sem_lane_finish_async(
+            self._h, lane,
+            None if seis_out is None else seis_out.ctypes.data,
+            None if kernels_out is None else kernels_out.ctypes.data,
+            C.c_void_p(ksum_dev_ptr) if ksum_dev_ptr else None))
+
+    def lane_ready(self, lane: int, wait: bool = False) -> bool:
+        rc = _lib.load().sem_lane_ready(self._h, lane, int(wait))
+        if rc < 0:
+            check(rc)
+        return rc == 1
+
+    def lane_misfit(self, lane: int, out) -> None:
+        """Queue the copy of the lane's FP64 misfit into out[0] (a one-element
+        float64 array, page-locked for no waiting)."""
+        assert out.dtype == np.float64 and out.size >= 1
+        check(_lib.load().sem_lane_misfit(self._h, lane, out.ctypes.data))
 
     def advance(self, nsteps: int):
         check(_lib.load().sem_advance(self._h, int(nsteps)))

@@ -59,11 +59,31 @@ class FakeSim:
             self.store -= self.lane_store_bytes(ns)
         self.state[lane] = [PH_IDLE, 0, 0, False]
 
-    def lane_start_adjoint(self, lane, obs, taper_pct=0.05, taper_type=1):
+    def lane_start_adjoint(self, lane, obs, taper_pct=0.05, taper_type=1, want_misfit=True):
         ph, st, ns, save = self.state[lane]
         assert ph == PH_FWD and st == ns and save
         self.state[lane] = [PH_ADJ, 0, ns, save]
-        return 1.0 + lane
+        return 1.0 + lane if want_misfit else None
+
+    # queued work completes at once in this stand-in
+    def lane_finish_async(self, lane, seis_out=None, kernels_out=None, ksum_dev_ptr=0):
+        self.lane_finish(lane, seis_out, kernels_out, ksum_dev_ptr)
+
+    def lane_ready(self, lane, wait=False):
+        return True
+
+    def lane_misfit(self, lane, out):
+        out[0] = 1.0 + lane
+
+    def mark(self):
+        self.marks = getattr(self, "marks", 0) + 1
+        return self.marks
+
+    def mark_done(self, token, wait=False):
+        return True
+
+    def mark_elapsed(self, t0, t1):
+        return 1.0
 
     def synchronize(self):
         pass
