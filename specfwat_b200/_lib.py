@@ -182,7 +182,7 @@ def load():
         "sem_mark": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "sem_lane_finish_async": (C.c_int, [vp, ip, fp, fp, fp]),
         "sem_lane_ready": (C.c_int, [vp, ip, ip]),
-        "sem_lane_misfit": (C.c_int, [vp, ip, C.POINTER(C.c_double)]),
+        "sem_lane_misfit": (C.c_int, [vp, ip, fp]),
         "sem_mark_done": (C.c_int, [vp, C.c_longlong, ip]),
         "sem_mark_elapsed": (C.c_int, [vp, C.c_longlong, C.c_longlong,
                                        C.POINTER(C.c_double)]),

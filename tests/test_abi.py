@@ -59,3 +59,34 @@ def test_argument_errors_without_device():
     assert lib.sem_iterate_time(None, 1, 0) == -1
     assert lib.sem_measure_l2_noalloc(None, None, 1, 1, 0.1, 0.0, 1, None,
                                       None, None) == -1
+
+
+def test_entry_points_take_their_python_arguments():
+    """Every entry point the Python layer calls with a raw array address or a
+    ctypes reference accepts it (argument conversion happens before the
+    call, so a null handle shows it without a device): each returns
+    SEM_ERR_ARG for the null run instead of raising."""
+    import ctypes as C
+    import numpy as np
+    L = _lib.load()
+    f64 = np.zeros(4)
+    f32 = np.zeros(4, np.float32)
+    t = C.c_longlong()
+    ms = C.c_double()
+    i1, i2, i3 = C.c_int(), C.c_int(), C.c_int()
+    b1, b2 = C.c_longlong(), C.c_longlong()
+    calls = [
+        lambda: L.sem_lane_misfit(None, 0, f64.ctypes.data),
+        lambda: L.sem_lane_finish_async(None, 0, f32.ctypes.data, f64.ctypes.data, None),
+        lambda: L.sem_lane_ready(None, 0, 0),
+        lambda: L.sem_mark(None, C.byref(t)),
+        lambda: L.sem_mark_done(None, 0, 0),
+        lambda: L.sem_mark_elapsed(None, 0, 1, C.byref(ms)),
+        lambda: L.sem_set_store_spill(None, -1),
+        lambda: L.sem_store_info(None, C.byref(i1), C.byref(i2), C.byref(i3), C.byref(b1),
+                                 C.byref(b2)),
+        lambda: L.sem_lane_finish(None, 0, f32.ctypes.data, f64.ctypes.data, None),
+        lambda: L.sem_lane_status(None, 0, C.byref(i1), C.byref(i2), C.byref(i3)),
+    ]
+    for k, call in enumerate(calls):
+        assert call() == -1, k

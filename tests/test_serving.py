@@ -151,3 +151,65 @@ def test_solo_routing_same_results(gpu):
     assert solo.store_in_use == 0 and batched.store_in_use == 0
     solo.close()
     batched.close()
+
+
+def test_async_lane_primitives_match_blocking(gpu):
+    """The non-blocking lane calls a pipelined scheduler uses give what the
+    blocking ones give: sem_lane_finish_async + sem_lane_ready returns the
+    same seismograms as sem_lane_finish, sem_lane_misfit the misfit that
+    sem_lane_start_adjoint returns, and the kernels summed through the
+    asynchronous finish equal the blocking finish's; completion marks
+    finish in order with positive device time between them."""
+    import torch
+    rng = np.random.default_rng(31)
+    db = D.build("mini")
+    reqs = _requests(rng, "mini", db, 2, ["fwdadj"], [240], 0.0)
+    out = {}
+    for mode in ("blocking", "async"):
+        mesh = S.Mesh(db)
+        sim = S.Simulation(mesh, 240, 0.02, nev=8, store="fp16", use_graph=True,
+                           max_receivers=len(reqs[0].receivers))
+        ksum = torch.zeros((6, db.nspec * 125), dtype=torch.float64, device="cuda")
+        for lane, r in enumerate(reqs):
+            sim.lane_start_forward(lane, r.source, r.receivers, r.nstep, save_forward=True)
+        marks = []
+        while sim.lane_status(0)[1] < 240:
+            marks.append(sim.mark())
+            sim.advance(60)
+        marks.append(sim.mark())
+        seis, mis = [], []
+        for lane, r in enumerate(reqs):
+            s = torch.empty(len(r.receivers) * 3 * 240, dtype=torch.float32).pin_memory().numpy()
+            if mode == "blocking":
+                sim.lane_finish(lane, seis_out=s)
+                mis.append(sim.lane_start_adjoint(lane, r.obs))
+            else:
+                sim.lane_finish_async(lane, seis_out=s)
+                sim.lane_start_adjoint(lane, r.obs, want_misfit=False)
+                m = torch.empty(1, dtype=torch.float64).pin_memory().numpy()
+                sim.lane_misfit(lane, m)
+                assert sim.lane_ready(lane, wait=True)
+                mis.append(float(m[0]))
+            seis.append(s.copy())
+        assert sim.mark_done(marks[-1], wait=True)
+        assert all(sim.mark_done(t) for t in marks)
+        assert sim.mark_elapsed(marks[0], marks[-1]) > 0.0
+        while sim.lane_status(0)[1] < 240:
+            sim.advance(60)
+        for lane in range(len(reqs)):
+            if mode == "blocking":
+                sim.lane_finish(lane, ksum_dev_ptr=ksum.data_ptr())
+            else:
+                sim.lane_finish_async(lane, ksum_dev_ptr=ksum.data_ptr())
+                assert sim.lane_ready(lane, wait=True)
+        torch.cuda.synchronize()
+        out[mode] = (seis, mis, ksum.cpu().numpy())
+        sim.close()
+        mesh.close()
+    for a, b in zip(out["blocking"][0], out["async"][0]):
+        assert rel(b, a) < 1e-5
+    # the two runs differ only by the order of atomic adds (~1e-6)
+    for a, b in zip(out["blocking"][1], out["async"][1]):
+        assert abs(a - b) <= 1e-5 * abs(a)
+    for q in range(3):
+        assert rel(out["async"][2][q], out["blocking"][2][q]) < 1e-5
