@@ -143,7 +143,9 @@ typedef struct {
                          with the forward scatter as plain read-modify-
                          writes in one launch per element colour, 13
                          thread per point with xi contractions by warp
-                         shuffles (one event per block)                    */
+                         shuffles (one event per block), 14 forward as 11
+                         and an adjoint kernel sized for three blocks per
+                         SM (divergence summed in shared memory)          */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard
@@ -310,7 +312,8 @@ int sem_lane_misfit(sem_run *run, int lane, double *misfit);
  * per thread, 7 to 10 with the adjoint-phase field pair as a float2,
  * 11 forward with register prefetch, 12 as 11 with colour-ordered
  * non-atomic forward assembly, 13 thread per point with warp-shuffle
- * contractions).  With kernel_variant = 0 the first
+ * contractions, 14 as 11 with the three-blocks-per-SM adjoint kernel).
+ * With kernel_variant = 0 the first
  * sem_iterate_time times the candidates on this run and keeps the fastest
  * per phase; -1 until then. */
 int sem_kernel_variants(sem_run *run, int *fwd, int *adj);

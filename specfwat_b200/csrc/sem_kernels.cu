@@ -2549,6 +2549,323 @@ static void forces_adjpair_r_cfg(const StepArgs& a, cudaStream_t st) {
   k_forces_adjpair_r<LB, GEN><<<gx, NT, BYTES, st>>>(a, items);
 }
 
+// Adjoint element kernel sized for three blocks per SM (variant 14; regular
+// elements, 8 lanes x 2 fields per block).  Same arithmetic as
+// k_forces_adjpair_r, in 72.8 KB of shared memory instead of 91.5 KB:
+// - the displacement takes 3 planes; the stress planes 0-2 overwrite them
+//   at the xi owner's points, planes 3-4 overwrite the eta-derivative slots
+//   0-1 of those points once the owner has read them;
+// - the divergence is summed in shared memory: the xi owner writes
+//   -wjk f_xi into planes A2..A4 of its points, the eta and gamma owners
+//   add -wik f_eta and -wij f_gamma there in two more passes, and the xi
+//   owner scatters the sums, so no flux registers live to the scatter;
+// - kappa/mu are single-buffered, fetched for the next element once this
+//   element's stress is formed.
+struct PairR3Layout {
+  static constexpr int VL = 16;
+  static constexpr int NE = NGLL3;
+  static constexpr int OFF_IB = 0;                          // int [3][NE]
+  static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);       // [2][NE] kappa, mu
+  static constexpr int OFF_U = al4(OFF_KM + 2 * NE);        // [3][NE][VL]
+  static constexpr int OFF_A = al4(OFF_U + 3 * NE * VL);    // [6][NE][VL]
+  static constexpr int TOTAL = OFF_A + 6 * NE * VL;
+  static constexpr size_t BYTES = (size_t)TOTAL * 4;
+};
+
+// xi role of variant 14: gradient, stress and strain products at the
+// pencil's points (as pair_xi), stress components to U0..U2 and A0..A1,
+// and -wjk times the xi divergence to A2..A4.
+__device__ __forceinline__ void pair_xi3(const PBuf<16>& b, int t, const float* kap,
+                                         const float* mu, float fac, float kmu[5], float kka[5]) {
+  float2 u[3][5];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int l = 0; l < 5; ++l) u[c][l] = p2(lds_v<2>(b.U(c, l + 5 * t)));
+  float2 sx[3][5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    float2 g[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) a = cfma2(gD(i, l), u[c][l], a);
+      g[c][0] = a;
+      g[c][1] = p2(lds_v<2>(b.Ar(c, p)));
+      g[c][2] = p2(lds_v<2>(b.Ar(3 + c, p)));
+    }
+    float2 sig[6];
+    stress_point2(g, kap[p], mu[p], fac, sig);
+    sx[0][i] = sig[0];
+    sx[1][i] = sig[3];
+    sx[2][i] = sig[4];
+    const float2 tr = __fadd2_rn(__fadd2_rn(g[0][0], g[1][1]), g[2][2]);
+    const float2 m3 = splat(-1.0f / 3.0f), h = splat(0.5f);
+    const float2 exx = __ffma2_rn(tr, m3, g[0][0]);
+    const float2 eyy = __ffma2_rn(tr, m3, g[1][1]);
+    const float2 exy = __fmul2_rn(h, __fadd2_rn(g[0][1], g[1][0]));
+    const float2 exz = __fmul2_rn(h, __fadd2_rn(g[0][2], g[2][0]));
+    const float2 eyz = __fmul2_rn(h, __fadd2_rn(g[1][2], g[2][1]));
+    kmu[i] = exx.x * exx.y + eyy.x * eyy.y + (exx.x + eyy.x) * (exx.y + eyy.y) +
+             2.0f * (exy.x * exy.y + exz.x * exz.y + eyz.x * eyz.y);
+    kka[i] = tr.x * tr.y;
+    // sigma for the eta pencils: xy, yy, yz; for the gamma pencils xz, yz, zz
+    sts_v<2>(b.U(0, p), lv2(sig[3]));
+    sts_v<2>(b.U(1, p), lv2(sig[1]));
+    sts_v<2>(b.U(2, p), lv2(sig[5]));
+    sts_v<2>(b.Ar(0, p), lv2(sig[4]));
+    sts_v<2>(b.Ar(1, p), lv2(sig[2]));
+  }
+  const int pj = t % 5, pk = t / 5;
+  float wj = 0.f, wk = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q == pj) wj = gW(q);
+    if (q == pk) wk = gW(q);
+  }
+  const float2 njk = splat(-(wj * wk));
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) a = cfma2(gDWt(i, l), sx[c][l], a);
+      sts_v<2>(b.Ar(2 + c, i + 5 * t), lv2(__fmul2_rn(njk, a)));
+    }
+}
+
+// eta (DIR 1) or gamma (DIR 2) role of variant 14 on the pencil (pi, pq):
+// the divergence along the pencil of the three components' fluxes, times
+// -w w of the other two directions, added to A2..A4 at the pencil's points.
+template <int DIR>
+__device__ __forceinline__ void div_add3(const PBuf<16>& b, int pi, int pq) {
+  // point l of the pencil
+  auto pt = [&](int l) { return DIR == 1 ? pi + 5 * l + 25 * pq : pi + 5 * pq + 25 * l; };
+  float2 v[3][5];
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    const int p = pt(l);
+    if (DIR == 1) {                       // sigma_{c,y} = xy, yy, yz
+      v[0][l] = p2(lds_v<2>(b.U(0, p)));
+      v[1][l] = p2(lds_v<2>(b.U(1, p)));
+      v[2][l] = p2(lds_v<2>(b.U(2, p)));
+    } else {                              // sigma_{c,z} = xz, yz, zz
+      v[0][l] = p2(lds_v<2>(b.Ar(0, p)));
+      v[1][l] = p2(lds_v<2>(b.U(2, p)));
+      v[2][l] = p2(lds_v<2>(b.Ar(1, p)));
+    }
+  }
+  float wa = 0.f, wb = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q == pi) wa = gW(q);
+    if (q == pq) wb = gW(q);
+  }
+  const float2 nw = splat(-(wa * wb));
+#pragma unroll
+  for (int j = 0; j < 5; ++j)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) a = cfma2(gDWt(j, l), v[c][l], a);
+      float* d = b.Ar(2 + c, pt(j));
+      sts_v<2>(d, lv2(__ffma2_rn(nw, a, p2(lds_v<2>(d)))));
+    }
+}
+
+__global__ void __maxnreg__(96) k_forces_adjpair_r3(StepArgs A, PipeItems items) {
+  constexpr int LB = 8;
+  constexpr int VL = 2 * LB;
+  constexpr int NT = 25 * LB;
+  using LY = PairR3Layout;
+  constexpr int NE = NGLL3;
+  constexpr int LWLOG = 3;
+  extern __shared__ float sm[];
+  int* sIB = (int*)(sm + LY::OFF_IB);
+  float* sKM = sm + LY::OFF_KM;
+  float* sU = sm + LY::OFF_U;
+  float* sA = sm + LY::OFF_A;
+
+  const int tid = threadIdx.x;
+  const int lq = tid % LB;
+  const int t = tid / LB;
+  const int pi = t % 5, pq = t / 5;
+  const int nev = A.nev;
+  const int nspec = A.m.nspec;
+  const int nitems = items.count();
+
+  bool any = false;
+  for (int l = tid; l < nev; l += NT) {
+    const LaneDesc* L = A.lanes + l;
+    any |= L->phase != PH_IDLE && L->it0 + A.s < L->nstep;
+  }
+  if (!__syncthreads_or(any)) return;
+  if (A.lm.lwlog != LWLOG) return;  // batched layout only
+
+  int c_chunk = -1, c_flag = 0;
+  auto flags = [&](int w, int& lg, int& g) -> int {
+    int chunk;
+    items.decode(w, chunk, g);
+    lg = chunk * LB + lq;
+    if (chunk == c_chunk) return c_flag;
+    int f = 0;
+    if (chunk < items.nchunk && lg < nev) {
+      const LaneDesc* L = A.lanes + lg;
+      const int it = L->it0 + A.s;
+      if (L->phase != PH_IDLE && it < L->nstep) {
+        f = 1;
+        if (L->phase == PH_ADJ) f |= 2 | (it > 0 ? 4 : 0);
+      }
+    }
+    c_chunk = chunk;
+    c_flag = f;
+    return f;
+  };
+  auto issue_ib = [&](int w, int slot) {
+    int* dst = sIB + slot * NE;
+    int chunk = 0, g = 0;
+    if (w < nitems) items.decode(w, chunk, g);
+    for (int i = tid; i < NE; i += NT) {
+      if (w < nitems && g < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      else
+        dst[i] = -1;
+    }
+  };
+  auto issue_km = [&](int w) {
+    if (w >= nitems) return;
+    int chunk, g;
+    items.decode(w, chunk, g);
+    if (g >= nspec) return;
+    const int e = A.m.order[g];
+    for (int i = tid; i < NE; i += NT) {
+      const size_t ep = (size_t)e * NGLL3 + i;
+      cp_async4(sKM + i, A.m.kappa + ep);
+      cp_async4(sKM + NE + i, A.m.mu + ep);
+    }
+  };
+  float pre[2][5][3];
+  auto load_u = [&](int w, int ibslot) {
+    int lg = 0, g = 0, fl = 0;
+    if (w < nitems) fl = flags(w, lg, g);
+    const int* ib = sIB + ibslot * NE;
+    const size_t fb = fbase<LWLOG>(A, lg);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ldg_pred(pre[0][r][c], A.f1.u + fb + foff<LWLOG>(ig, c), (fl & 1) && ig >= 0);
+        ldg_pred(pre[1][r][c], A.f2.u + fb + foff<LWLOG>(ig, c), (fl & 2) && ig >= 0);
+      }
+    }
+  };
+
+  int w = blockIdx.x;
+  issue_ib(w, 0);
+  cp_commit();
+  cp_wait_all();
+  __syncthreads();
+  issue_km(w);
+  issue_ib(w + gridDim.x, 1);
+  cp_commit();
+  load_u(w, 0);
+
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  const float dtk = A.dt * A.m.xix * A.m.xix;
+  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+    const int ibs = k % 3;
+    cp_wait_all();
+    __syncthreads();  // previous element done with U/A; this one's kappa/mu landed
+    {
+      float* ub = sU + 2 * lq;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int p = t + 25 * r;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          LV<2> v;
+          v.v[0] = pre[0][r][c];
+          v.v[1] = pre[1][r][c];
+          sts_v<2>(ub + (c * NGLL3 + p) * VL, v);
+        }
+      }
+    }
+    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    cp_commit();
+    __syncthreads();  // U complete
+    load_u(w + gridDim.x, (k + 1) % 3);
+
+    int lg, g;
+    const int fl = flags(w, lg, g);
+    const int e = g < nspec ? A.m.order[g] : nspec;
+    PBuf<VL> b{sU + 2 * lq, sA + 2 * lq};
+    v_grad_eg<VL, 2>(b, pi, pq);
+    __syncthreads();
+    float kmu[5], kka[5];
+    pair_xi3(b, t, sKM, sKM + NE, fac, kmu, kka);
+    if ((fl & 2) && e < nspec) {
+      const size_t eb = ebase<LWLOG>(A, lg) + (((size_t)e * NGLL3) << LWLOG);
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const size_t q = eb + ((size_t)(i + 5 * t) << LWLOG);
+        atomicAdd(&A.k.mu[q], dtk * kmu[i]);
+        atomicAdd(&A.k.kappa[q], dtk * kka[i]);
+      }
+    }
+    __syncthreads();  // stress and xi sums complete; kappa/mu free
+    issue_km(w + gridDim.x);
+    cp_commit();
+    div_add3<1>(b, pi, pq);
+    __syncthreads();
+    div_add3<2>(b, pi, pq);
+    __syncthreads();
+    if (e < nspec && (fl & 1)) {
+      const int* ib = sIB + ibs * NE;
+      const size_t fb = fbase<LWLOG>(A, lg);
+      const bool on2 = (fl & 4) != 0;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const int p = i + 5 * t;
+        const int ig = ib[p];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float2 v = p2(lds_v<2>(b.Ar(2 + c, p)));
+          const size_t q = fb + foff<LWLOG>(ig, c);
+          atomicAdd(&A.f1.a[q], v.x);
+          if (on2) atomicAdd(&A.f2.a[q], v.y);
+        }
+      }
+    }
+  }
+  cp_wait_all();
+}
+
+static void forces_adjpair_r3_cfg(const StepArgs& a, cudaStream_t st) {
+  constexpr int NT = 200;
+  constexpr size_t BYTES = PairR3Layout::BYTES;
+  static int blocks_per_sm = 0, sms = 0;
+  if (!blocks_per_sm) {
+    cudaFuncSetAttribute(k_forces_adjpair_r3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_adjpair_r3, NT, BYTES);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  PipeItems items = make_items<8>(a, a.m.nspec);
+  if (items.count() == 0) return;
+  int gx = blocks_per_sm * sms;
+  if (gx > items.count()) gx = items.count();
+  if (gx < 1) gx = 1;
+  k_forces_adjpair_r3<<<gx, NT, BYTES, st>>>(a, items);
+}
+
 // Forward-phase element kernel with 2 events per thread and the next
 // element's gather prefetched into registers (single-buffered shared
 // displacement), LB events per block.  LB is at most the 8-lane sector
@@ -2836,6 +3153,11 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
     if (!adj) return a.m.ncolour > 0 ? forces_fwd_r_cfg<8, true>(a, st)
                                      : forces_fwd_r_cfg<8, false>(a, st);
     forces_adjpair_r_cfg<8>(a, st);
+    return 1;
+  }
+  if (a.variant == 13 && a.nev > 1) {
+    if (!adj) return forces_fwd_r_cfg<8, false>(a, st);
+    forces_adjpair_r3_cfg(a, st);
     return 1;
   }
   if ((a.variant >= 6 && a.variant <= 9) && a.nev > 1) {
