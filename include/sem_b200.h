@@ -303,6 +303,14 @@ int sem_lane_finish(sem_run *run, int lane, float *seis, double *kernels6,
  * No counterpart in the reference. */
 int sem_lane_finish_async(sem_run *run, int lane, float *seis, double *kernels6,
                           double *ksum_dev);
+/* Lane compaction: move the request on lane `from` (forward or adjoint, any
+ * step) to the free lane `to`, so that a scheduler can keep requests packed
+ * into few 8-lane groups (each active group costs a share of every step).
+ * Its wavefields, kernel accumulators, source, receivers, seismograms,
+ * adjoint sources and boundary store go with it; the copies queue behind
+ * the work on the run's stream.  Results queued by an earlier async finish
+ * of `from` are not affected.  No counterpart in the reference. */
+int sem_lane_move(sem_run *run, int from, int to);
 int sem_lane_ready(sem_run *run, int lane, int wait);
 int sem_lane_misfit(sem_run *run, int lane, double *misfit);
 

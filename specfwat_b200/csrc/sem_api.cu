@@ -2471,6 +2471,76 @@ int sem_lane_finish(sem_run* r, int lane, float* seis, double* kernels6, double*
   return SEM_OK;
 }
 
+int sem_lane_move(sem_run* r, int from, int to) {
+  if (!r || !r->lanes_mode || from < 0 || from >= r->nev || to < 0 || to >= r->nev || from == to)
+    return fail(SEM_ERR_ARG, "lanes %d -> %d are not two serving lanes of this run", from, to);
+  LaneDesc& F = r->h_lanes[from];
+  LaneDesc& T = r->h_lanes[to];
+  if (F.phase == PH_IDLE) return fail(SEM_ERR_STATE, "lane %d holds no request", from);
+  if (T.phase != PH_IDLE || r->lane_store[to] || r->lane_scale[to])
+    return fail(SEM_ERR_STATE, "lane %d is not free", to);
+  if (r->cfg.check_every > 0 && r->lane_failed[from])
+    return fail(SEM_ERR_STATE, "lane %d was stopped by the stability check", from);
+  // wavefields, kernel accumulators and the per-event arrays, queued behind
+  // the work already on the stream
+  const size_t ng = r->mesh->nglob, ne = (size_t)r->mesh->nspec * NGLL3;
+  launch_lane_move(r->u1.p, r->v1.p, r->a1.p, ng, 3, r->lm, from, to, r->stream);
+  if (F.phase == PH_ADJ) {
+    launch_lane_move(r->u2.p, r->v2.p, r->a2.p, ng, 3, r->lm, from, to, r->stream);
+    launch_lane_move(r->k_rho.p, r->hess_on ? r->k_hess.p : nullptr, nullptr, ng, 1, r->lm, from,
+                     to, r->stream);
+    launch_lane_move(r->k_mu.p, r->k_kappa.p, nullptr, ne, 1, r->lm, from, to, r->stream);
+  }
+  const size_t ns = r->nstep, nr = r->nrec_max;
+  auto d2d = [&](float* base, size_t per) -> cudaError_t {
+    return cudaMemcpyAsync(base + (size_t)to * per, base + (size_t)from * per, per * 4,
+                           cudaMemcpyDeviceToDevice, r->stream);
+  };
+  CK(d2d(r->stf.p, ns));
+  CK(d2d(r->srcarr.p, 375));
+  CK(d2d(r->rec_w.p, nr * 125));
+  CK(d2d(r->seis.p, nr * 3 * ns));
+  CK(d2d(r->adj.p, nr * 3 * ns));
+  CK(cudaMemcpyAsync(r->rec_ispec.p + (size_t)to * nr, r->rec_ispec.p + (size_t)from * nr,
+                     nr * sizeof(int), cudaMemcpyDeviceToDevice, r->stream));
+  if (r->lane_misfit.p)
+    CK(cudaMemcpyAsync(r->lane_misfit.p + to, r->lane_misfit.p + from, sizeof(double),
+                       cudaMemcpyDeviceToDevice, r->stream));
+  if (r->cfg.check_every > 0 && r->lflags.p) {
+    // the target starts with a clear stability flag
+    CK(cudaMemsetAsync(r->lflags.p + to, 0, sizeof(int), r->stream));
+    CK(cudaMemsetAsync(r->halt_step.p + to, 0xff, sizeof(int), r->stream));
+    r->lane_failed[to] = 0;
+    r->lane_fail_step[to] = -1;
+  }
+  CK(cudaGetLastError());
+  // host state: the lane descriptor with the target's array regions
+  const LaneDesc f = F;
+  lane_defaults(r, to);
+  T.phase = f.phase;
+  T.it0 = f.it0;
+  T.nstep = f.nstep;
+  T.save = f.save;
+  T.src_ispec = f.src_ispec;
+  T.nrec = f.nrec;
+  T.store = f.store;
+  T.scale = f.scale;
+  r->lane_store[to] = r->lane_store[from];
+  r->lane_scale[to] = r->lane_scale[from];
+  r->lane_store[from] = nullptr;
+  r->lane_scale[from] = nullptr;
+  r->lane_saved[to] = r->lane_saved[from];
+  r->lane_saved[from] = 0;
+  r->src_ispec[to] = r->src_ispec[from];
+  r->nrec[to] = r->nrec[from];
+  r->have_src[to] = r->have_src[from];
+  r->have_rec[to] = r->have_rec[from];
+  F = LaneDesc{};
+  F.phase = PH_IDLE;
+  lane_defaults(r, from);
+  return SEM_OK;
+}
+
 int sem_lane_finish_async(sem_run* r, int lane, float* seis, double* kernels6,
                           double* ksum_dev) {
   if (!r || !r->lanes_mode || lane < 0 || lane >= r->nev)

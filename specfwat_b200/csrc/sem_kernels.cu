@@ -3721,6 +3721,32 @@ int launch_lane_copy(const Fields& src, const Fields& dst, int nglob, LaneMap lm
   return 1;
 }
 
+// One lane's values of the given per-point arrays (u, v, a of a field, or
+// per-point records with rec values each) moved to another lane of the
+// same run.
+__global__ void k_lane_move(float* __restrict__ x0, float* __restrict__ x1, float* __restrict__ x2,
+                            size_t npts, int rec, LaneMap lm, int from, int to) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts * rec) return;
+  const size_t pnt = i / rec;
+  const int c = (int)(i % rec);
+  // lm.f() with `rec` values per point in place of 3
+  const size_t lw = (size_t)1 << lm.lwlog;
+  const size_t qf = ((((size_t)(from >> lm.lwlog)) * npts + pnt) * rec + c) * lw +
+                    (from & (lw - 1));
+  const size_t qt = ((((size_t)(to >> lm.lwlog)) * npts + pnt) * rec + c) * lw + (to & (lw - 1));
+  x0[qt] = x0[qf];
+  if (x1) x1[qt] = x1[qf];
+  if (x2) x2[qt] = x2[qf];
+}
+
+int launch_lane_move(float* x0, float* x1, float* x2, size_t npts, int rec, LaneMap lm, int from,
+                     int to, cudaStream_t st) {
+  const size_t n = npts * rec;
+  k_lane_move<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x0, x1, x2, npts, rec, lm, from, to);
+  return 1;
+}
+
 int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane, cudaStream_t st) {
   const size_t n = (size_t)nglob * 3;
   k_lane_zero<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f, nglob, lm, lane);

@@ -348,6 +348,49 @@ class MeshServer:
             self.step_ms["adj"] = v if ca is None else (1 - rate) * ca + rate * v
         self.quanta += 1
 
+    def compact(self):
+        """Pack running requests into fewer 8-lane groups (each active group
+        costs a share of every step): while a group of one kind (forward
+        only, or with adjoint lanes) can be emptied into the free lanes of
+        other groups of that kind, its requests move there
+        (``sem_lane_move``).  Requests about to switch phase or with results
+        still to collect stay put.  Returns the number of moves."""
+        g = self.group
+        # the group policy keeps requests admitted together in one group
+        if self.slots <= g or self.policy == "group":
+            return 0
+        moves = 0
+        for kind in (PH_FWD, PH_ADJ):
+            while True:
+                groups = {}
+                for lane, req in enumerate(self.lanes):
+                    if req is None:
+                        continue
+                    groups.setdefault(lane // g, []).append(lane)
+                of_kind = [k for k, ls in groups.items()
+                           if (PH_ADJ in (self.phase[l] for l in ls)) == (kind == PH_ADJ)]
+                if len(of_kind) < 2:
+                    break
+                src = min(of_kind, key=lambda k: (len(groups[k]), -k))
+                movable = [l for l in groups[src]
+                           if self.done_tok[l] is None and l not in self.pending]
+                if len(movable) != len(groups[src]):
+                    break
+                targets = sorted((k for k in of_kind if k != src),
+                                 key=lambda k: -len(groups[k]))
+                free = [l for k in targets for l in range(k * g, (k + 1) * g)
+                        if self.lanes[l] is None and l not in self.pending]
+                if len(free) < len(movable):
+                    break
+                for src_l, dst_l in zip(movable, free):
+                    self.sim.lane_move(src_l, dst_l)
+                    self.lanes[dst_l], self.lanes[src_l] = self.lanes[src_l], None
+                    self.phase[dst_l], self.phase[src_l] = self.phase[src_l], PH_IDLE
+                    self.lane_store[dst_l], self.lane_store[src_l] = self.lane_store[src_l], 0
+                    moves += 1
+        self.moves = getattr(self, "moves", 0) + moves
+        return moves
+
     def _buf(self, lane, key, n, dtype):
         b = self._bufs.get((lane, key))
         if b is None or b[0].size < n:
@@ -444,9 +487,11 @@ class Server:
 
     def __init__(self, servers: Dict[str, MeshServer], quantum=100,
                  solo: Optional[Dict[str, MeshServer]] = None, solo_below=4,
-                 costs: Optional[Dict[str, StepCosts]] = None):
+                 costs: Optional[Dict[str, StepCosts]] = None, compaction=True):
         self.servers = servers
         self.quantum = quantum
+        # pack requests into fewer 8-lane groups as others complete
+        self.compaction = compaction
         # Optional one-lane server per mesh (the plain one-event kernels).
         # A lone request in an 8-lane group costs the whole group's
         # launches, about four times the one-event path.  Without step
@@ -528,6 +573,8 @@ class Server:
                 i += 1
             for srv in self._all():
                 srv.try_admit(now)
+                if self.compaction:
+                    srv.compact()
             for srv in self._all():
                 while len(srv.inflight) < depth:
                     rem = srv.remaining()

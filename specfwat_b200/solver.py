@@ -343,6 +343,14 @@ class Simulation:
             None if kernels_out is None else kernels_out.ctypes.data,
             C.c_void_p(ksum_dev_ptr) if ksum_dev_ptr else None))
 
+    def lane_move(self, src: int, dst: int):
+        """Move the request on lane ``src`` to the free lane ``dst``."""
+        check(_lib.load().sem_lane_move(self._h, int(src), int(dst)))
+        self.nrec[dst] = self.nrec[src]
+        err = self.lane_errors.pop(src, None)
+        if err is not None:
+            self.lane_errors[dst] = err
+
     def lane_ready(self, lane: int, wait: bool = False) -> bool:
         rc = _lib.load().sem_lane_ready(self._h, lane, int(wait))
         if rc < 0:

@@ -65,6 +65,11 @@ class FakeSim:
         self.state[lane] = [PH_ADJ, 0, ns, save]
         return 1.0 + lane if want_misfit else None
 
+    def lane_move(self, src, dst):
+        assert self.state[dst][0] == PH_IDLE and self.state[src][0] != PH_IDLE
+        self.state[dst], self.state[src] = self.state[src], [PH_IDLE, 0, 0, False]
+        self.moves = getattr(self, "moves", 0) + 1
+
     # queued work completes at once in this stand-in
     def lane_finish_async(self, lane, seis_out=None, kernels_out=None, ksum_dev_ptr=0):
         self.lane_finish(lane, seis_out, kernels_out, ksum_dev_ptr)
@@ -168,3 +173,37 @@ def test_busy_lane_start_is_caught_by_the_stand_in():
     sim.lane_start_forward(0, None, None, 10, False)
     with pytest.raises(AssertionError):
         sim.lane_start_forward(0, None, None, 10, False)
+
+
+def test_compaction_packs_running_requests_into_fewer_groups():
+    """Requests spread over three 8-lane groups by completions are packed
+    into fewer groups of the same kind; requests about to switch phase stay
+    where they are; the boundary-store accounting follows the requests."""
+    srv = mesh_server("m", 24)
+    reqs = stream(12, seed=3)
+    for k, r in enumerate(reqs):
+        r.kind, r.nstep = "fwd", 300
+    # lanes 0-1 in group 0, 8-9 in group 1, 16-18 in group 2
+    for lane, r in zip([0, 1, 8, 9, 16, 17, 18], reqs):
+        srv._admit_one(r, lane, 0.0)
+    assert srv.active_groups() == 3
+    srv.done_tok[17] = 5          # about to switch: must not move
+    moved = srv.compact()
+    # the sparsest groups (0, then 1) empty into the fullest (2, which keeps
+    # the pinned lane 17): seven requests in one group
+    assert moved >= 2
+    assert srv.active_groups() < 3
+    assert srv.lanes[17] is reqs[5]
+    busy = [l for l, r in enumerate(srv.lanes) if r is not None]
+    assert len(busy) == 7
+    assert sorted(id(srv.lanes[l]) for l in busy) == sorted(id(r) for r in reqs[:7])
+    for l in busy:
+        assert srv.sim.state[l][0] == PH_FWD
+
+
+def test_mixed_stream_completes_with_compaction():
+    srv = mesh_server("m", 24)
+    reqs = stream(60, seed=7, spread=0.05)
+    done = Server({"m": srv}, quantum=50).run(reqs, timeout=60)
+    check_done(reqs, done, [srv])
+    assert getattr(srv.sim, "moves", 0) > 0
