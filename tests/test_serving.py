@@ -213,3 +213,43 @@ def test_async_lane_primitives_match_blocking(gpu):
         assert abs(a - b) <= 1e-5 * abs(a)
     for q in range(3):
         assert rel(out["async"][2][q], out["blocking"][2][q]) < 1e-5
+
+
+def test_lane_move_keeps_results(gpu):
+    """sem_lane_move in the middle of a forward and of an adjoint run: the
+    moved request (to a lane of another 8-lane group) ends with the
+    seismograms, misfit and kernels it has without the moves."""
+    rng = np.random.default_rng(41)
+    db = D.build("mini")
+    r = _requests(rng, "mini", db, 1, ["fwdadj"], [260], 0.0)[0]
+    out = {}
+    for moved in (False, True):
+        mesh = S.Mesh(db)
+        sim = S.Simulation(mesh, 260, 0.02, nev=16, store="fp16", use_graph=True,
+                           max_receivers=len(r.receivers))
+        lane = 9
+        sim.lane_start_forward(lane, r.source, r.receivers, 260, save_forward=True)
+        sim.advance(110)
+        if moved:
+            sim.lane_move(lane, 2)
+            lane = 2
+        while sim.lane_status(lane)[1] < 260:
+            sim.advance(50)
+        seis = np.zeros((len(r.receivers), 3, 260), np.float32)
+        sim.lane_finish(lane, seis_out=seis)
+        mis = sim.lane_start_adjoint(lane, r.obs)
+        sim.advance(70)
+        if moved:
+            sim.lane_move(lane, 15)
+            lane = 15
+        while sim.lane_status(lane)[1] < 260:
+            sim.advance(50)
+        kern = np.zeros((6, db.nspec, 5, 5, 5))
+        sim.lane_finish(lane, kernels_out=kern)
+        out[moved] = (seis, mis, kern)
+        sim.close()
+        mesh.close()
+    assert rel(out[True][0], out[False][0]) < 1e-5
+    assert abs(out[True][1] - out[False][1]) <= 1e-5 * abs(out[False][1])
+    for q in range(6):
+        assert rel(out[True][2][q], out[False][2][q]) < 1e-4, q
