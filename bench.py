@@ -996,6 +996,8 @@ def run_serve(args):
             for e in range(nev):
                 sim.measure_l2(e, np.zeros((len(rec), 3, 60)))
             sim.iterate_time(3)
+            sim.time_kernels(1, 10)            # first launches load the kernels
+            sim.time_kernels(3, 10)
             per[nev] = (sum(sim.time_kernels(1, 20)), sum(sim.time_kernels(3, 20)))
             sim.close()
         m.close()
@@ -1013,13 +1015,21 @@ def run_serve(args):
     arr -= arr[0]
     for r, a in zip(reqs, arr):
         r.arrival = float(a)
+    # spatial sharing: the large and medium meshes' persistent element
+    # kernels leave SMs free for the others, and the small and medium runs'
+    # streams go first, so that short requests do not queue behind a large
+    # mesh's kernels
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    share = {"small": (0, True), "medium": (sms - 12, True), "large": (sms - 24, False)}
     servers = {name: MeshServer(name, dbs[name], slots=spec[name][1], nstep_max=8000,
                                 dt=spec[name][0], store="fp16", graph_steps=50,
-                                max_receivers=spec[name][2] ** 2, store_budget=spec[name][3])
+                                max_receivers=spec[name][2] ** 2, store_budget=spec[name][3],
+                                sm_limit=share[name][0], high_priority=share[name][1])
                for name in spec}
     solo = {name: MeshServer(name, dbs[name], slots=1, nstep_max=8000, dt=spec[name][0],
                              store="fp16", graph_steps=50, max_receivers=spec[name][2] ** 2,
-                             store_budget=spec[name][4])
+                             store_budget=spec[name][4], sm_limit=share[name][0],
+                             high_priority=share[name][1])
             for name in spec}
     clocks = Clocks(0)
     clocks.start()
@@ -1058,6 +1068,8 @@ def run_serve(args):
                                           for n, v in spec.items()}},
         "served": st, "plain_fifo": fifo, "by_mesh": by_mesh,
         "errors": sum(bool(r.error) for r in done),
+        "sm_share": {n: {"sm_limit": v[0] or sms, "high_priority": v[1]} for n, v in share.items()},
+        "lane_moves": sum(getattr(sv, "moves", 0) for sv in servers.values()),
         "step_costs_ms": {n: {"plain_fwd": c.plain_fwd * 1e3, "plain_adj": c.plain_adj * 1e3,
                               "group_fwd": c.group_fwd * 1e3, "group_adj": c.group_adj * 1e3}
                           for n, c in costs.items()},

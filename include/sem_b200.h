@@ -222,6 +222,15 @@ int sem_set_stream(sem_run *run, void *stream);
  * dev_out[6][nspec][125] (e.g. a buffer handed to a collective). */
 int sem_sum_kernels_device(sem_run *run, double *dev_out);
 
+/* Spatial share of the GPU for runs of different meshes working at once:
+ * the run's persistent element kernels fill at most sm_limit SMs (0: all),
+ * leaving room for the other runs' kernels, and high_priority = 1 puts the
+ * run's own stream at the device's highest stream priority (0: lowest), so
+ * that the blocks of a small mesh's short kernels go ahead of a large
+ * mesh's queued ones.  A stream set with sem_set_stream keeps its own
+ * priority.  No counterpart in the reference. */
+int sem_set_sm_share(sem_run *run, int sm_limit, int high_priority);
+
 /* Boundary store held partly in host memory (the reference keeps the
  * whole store on disk: absorb_field.bin, src/specfem_interface/
  * specfem_api.f90:359-361, deleted at src/preproc/prepare_fwd.f90:376-377).

@@ -34,7 +34,7 @@ EXPORTS = (
     "sem_kernel_variants", "sem_measure_l2_noalloc",
     "sem_set_store_spill", "sem_store_info", "sem_mark", "sem_mark_done",
     "sem_mark_elapsed", "sem_lane_finish_async", "sem_lane_ready", "sem_lane_misfit",
-    "sem_lane_move",
+    "sem_lane_move", "sem_set_sm_share",
     "sem_lane_store_bytes", "sem_lane_start_forward", "sem_lane_start_adjoint",
     "sem_advance", "sem_lane_status", "sem_lane_finish", "sem_fp32_fma_peak",
     "sem_smooth_pde", "sem_measure_waveform", "sem_measure_waveform_dev",
@@ -184,6 +184,7 @@ def load():
         "sem_lane_finish_async": (C.c_int, [vp, ip, fp, fp, fp]),
         "sem_lane_ready": (C.c_int, [vp, ip, ip]),
         "sem_lane_move": (C.c_int, [vp, ip, ip]),
+        "sem_set_sm_share": (C.c_int, [vp, ip, ip]),
         "sem_lane_misfit": (C.c_int, [vp, ip, fp]),
         "sem_mark_done": (C.c_int, [vp, C.c_longlong, ip]),
         "sem_mark_elapsed": (C.c_int, [vp, C.c_longlong, C.c_longlong,

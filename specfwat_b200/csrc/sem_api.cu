@@ -468,6 +468,7 @@ struct sem_run_s {
   int variant[2] = {-1, -1};  // element-kernel variant per phase (fwd, adj)
   double last_ms = 0.0;
   long long last_launches = 0;
+  int sm_limit = 0;   // SMs its persistent element kernels may fill (0: all)
 
   ~sem_run_s() {
     for (auto& j : inj)
@@ -532,6 +533,7 @@ struct sem_run_s {
     a.lm = lm;
     a.inject = 0;
     for (const auto& j : inj) a.inject |= j.buf != nullptr;
+    a.sm_limit = sm_limit;
     // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined;
     // 0 = chosen by the autotuner per phase
     const int v = variant[adjoint ? 1 : 0];
@@ -1953,6 +1955,31 @@ int sem_store_info(sem_run* r, int* chunk_steps, int* device_slots, int* chunks,
   if (chunks) *chunks = r->ring_n;
   if (device_bytes) *device_bytes = (long long)dev;
   if (host_bytes) *host_bytes = (long long)host;
+  return SEM_OK;
+}
+
+int sem_set_sm_share(sem_run* r, int sm_limit, int high_priority) {
+  if (!r || sm_limit < 0) return fail(SEM_ERR_ARG, "bad argument");
+  r->sm_limit = sm_limit;
+  if (r->stream != r->own_stream) return SEM_OK;  // a caller's stream keeps its priority
+  int lo = 0, hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  int cur = 0;
+  CK(cudaStreamGetPriority(r->own_stream, &cur));
+  const int want = high_priority ? hi : lo;
+  if (cur == want) return SEM_OK;
+  cudaStream_t s2 = nullptr;
+  CK(cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, want));
+  // the new stream starts after everything queued on the old one
+  cudaEvent_t e = nullptr;
+  CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CK(cudaEventRecord(e, r->own_stream));
+  CK(cudaStreamWaitEvent(s2, e, 0));
+  CK(cudaEventDestroy(e));
+  CK(cudaStreamSynchronize(r->own_stream));
+  CK(cudaStreamDestroy(r->own_stream));
+  r->own_stream = s2;
+  r->stream = s2;
   return SEM_OK;
 }
 

@@ -122,6 +122,7 @@ struct StepArgs {
   const int* gmap;       // serving: active 8-lane groups (device), or null
   int ngmap;
   int inject;            // some lane has an FK injection (LaneDesc::inj_v)
+  int sm_limit;          // SMs the persistent element kernels may fill (0: all)
   __device__ __forceinline__ size_t fi(size_t ig, int c, int lg) const {
     return lm.f(ig, c, lg, (size_t)m.nglob);
   }

@@ -907,6 +907,13 @@ struct PipeLayout {
   static constexpr size_t BYTES = (size_t)TOTAL * 4;
 };
 
+// SMs a persistent element kernel of this run may fill: the run's share
+// (sem_set_sm_share) or the whole device, so that runs of other meshes on
+// other streams find room beside it.
+__host__ __forceinline__ int sm_share(const StepArgs& a, int sms) {
+  return (a.sm_limit > 0 && a.sm_limit < sms) ? a.sm_limit : sms;
+}
+
 // Work items are (lane chunk, element group) pairs walked chunk-major, so
 // all resident blocks sweep the mesh for one group of event lanes at a
 // time and the working set of shared GLL points stays in L2; the sub-chunks
@@ -1194,7 +1201,7 @@ static void forces_piped_cfg(const StepArgs& a, cudaStream_t st) {
   }
   PipeItems items = make_items<LB>(a, (a.m.nspec + EPB - 1) / EPB);
   if (items.count() == 0) return;
-  int gx = blocks_per_sm * sms;
+  int gx = blocks_per_sm * sm_share(a, sms);
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
   k_forces_piped<LB, EPB, TPE, ADJ><<<gx, NT, LY::BYTES, st>>>(a, items);
@@ -2543,7 +2550,7 @@ static void forces_adjpair_r_cfg(const StepArgs& a, cudaStream_t st) {
   }
   PipeItems items = make_items<LB>(a, a.m.nspec);
   if (items.count() == 0) return;
-  int gx = blocks_per_sm * sms;
+  int gx = blocks_per_sm * sm_share(a, sms);
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
   k_forces_adjpair_r<LB, GEN><<<gx, NT, BYTES, st>>>(a, items);
@@ -2860,7 +2867,7 @@ static void forces_adjpair_r3_cfg(const StepArgs& a, cudaStream_t st) {
   }
   PipeItems items = make_items<8>(a, a.m.nspec);
   if (items.count() == 0) return;
-  int gx = blocks_per_sm * sms;
+  int gx = blocks_per_sm * sm_share(a, sms);
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
   k_forces_adjpair_r3<<<gx, NT, BYTES, st>>>(a, items);
@@ -3049,7 +3056,7 @@ static int forces_fwd_r_cfg(const StepArgs& a, cudaStream_t st) {
   auto launch = [&](const StepArgs& ac, int nel) {
     PipeItems items = make_items<LB>(ac, nel);
     if (items.count() == 0) return 0;
-    int gx = blocks_per_sm * sms;
+    int gx = blocks_per_sm * sm_share(a, sms);
     if (gx > items.count()) gx = items.count();
     if (gx < 1) gx = 1;
     k_forces_fwd_r<LB, COLOURED, GEN><<<gx, NT, BYTES, st>>>(ac, items);
@@ -3083,7 +3090,7 @@ static void forces_adjpair_cfg(const StepArgs& a, cudaStream_t st) {
   }
   PipeItems items = make_items<LB>(a, a.m.nspec);
   if (items.count() == 0) return;
-  int gx = blocks_per_sm * sms;
+  int gx = blocks_per_sm * sm_share(a, sms);
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
   k_forces_adjpair<LB><<<gx, NT, BYTES, st>>>(a, items);
@@ -3106,7 +3113,7 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
   }
   PipeItems items = make_items<LB>(a, a.m.nspec);
   if (items.count() == 0) return;
-  int gx = blocks_per_sm * sms;
+  int gx = blocks_per_sm * sm_share(a, sms);
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
   k_forces_vec<LB, NL, ADJ><<<gx, NT, LY::BYTES, st>>>(a, items);

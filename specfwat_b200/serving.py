@@ -98,13 +98,19 @@ class MeshServer:
     def __init__(self, name, db, slots, nstep_max, dt, store="fp16",
                  graph_steps=50, max_receivers=128, store_budget=None,
                  ksum_dev_ptr=0, taper_pct=0.05, taper_type=1, policy="lane",
-                 group=8, max_wait=1.5, check_every=0):
+                 group=8, max_wait=1.5, check_every=0, sm_limit=0, high_priority=False):
         mesh = S.Mesh(db)
         sim = S.Simulation(mesh, nstep_max, dt, nev=slots, store=store, use_graph=True,
                            graph_steps=graph_steps, max_receivers=max_receivers,
                            check_every=check_every)
+        if high_priority:
+            sim.set_sm_share(0, True)
         self._setup(name, mesh, sim, slots, nstep_max, db.nspec, store_budget, ksum_dev_ptr,
                     taper_pct, taper_type, policy, group, max_wait)
+        # SMs this mesh's persistent element kernels may fill while another
+        # mesh has work (sem_set_sm_share; 0: no limit)
+        self.sm_limit = sm_limit
+        self.high_priority = high_priority
 
     @classmethod
     def with_sim(cls, name, sim, slots, nstep_max, nspec, store_budget=None, ksum_dev_ptr=0,
@@ -153,6 +159,9 @@ class MeshServer:
         # one-lane server), forward and adjoint, learned from the marks
         self.step_ms = {"fwd": None, "adj": None}
         self.quanta = 0
+        self.sm_limit = 0
+        self.high_priority = False
+        self._limit_on = False
 
     # -- admission ----------------------------------------------------------
     def _admit_one(self, req, lane, now):
@@ -298,6 +307,14 @@ class MeshServer:
         for lane, ph, _ in run:
             (adj if ph == PH_ADJ else fwd).add(lane // g)
         return len(fwd - adj), len(adj)
+
+    def share_gpu(self, others_busy):
+        """Apply this mesh's SM limit while another mesh has work queued,
+        and lift it when none has."""
+        on = bool(self.sm_limit) and others_busy
+        if on != self._limit_on:
+            self.sim.set_sm_share(self.sm_limit if on else 0, self.high_priority)
+            self._limit_on = on
 
     def advance(self, nsteps):
         """Queue nsteps steps of every running lane, bracketed by two marks;
@@ -575,7 +592,10 @@ class Server:
                 srv.try_admit(now)
                 if self.compaction:
                     srv.compact()
+            busy = [srv for srv in self._all() if srv.running() or srv.inflight]
             for srv in self._all():
+                srv.share_gpu(any(o is not srv and o.mesh is not srv.mesh and
+                                  o.name != srv.name for o in busy))
                 while len(srv.inflight) < depth:
                     rem = srv.remaining()
                     if rem is None:

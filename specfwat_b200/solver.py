@@ -343,6 +343,11 @@ class Simulation:
             None if kernels_out is None else kernels_out.ctypes.data,
             C.c_void_p(ksum_dev_ptr) if ksum_dev_ptr else None))
 
+    def set_sm_share(self, sm_limit: int = 0, high_priority: bool = False):
+        """Cap the SMs this run's persistent element kernels fill, and set the
+        priority of its own stream (runs of several meshes at once)."""
+        check(_lib.load().sem_set_sm_share(self._h, int(sm_limit), int(high_priority)))
+
     def lane_move(self, src: int, dst: int):
         """Move the request on lane ``src`` to the free lane ``dst``."""
         check(_lib.load().sem_lane_move(self._h, int(src), int(dst)))
