@@ -60,7 +60,7 @@ def parse():
                    help="skip the kernel-smoothing leg")
     p.add_argument("--e2e-steps", type=int, default=1)
     p.add_argument("--store", default="fp16", choices=["fp16", "fp32"])
-    p.add_argument("--served-requests", type=int, default=64)
+    p.add_argument("--served-requests", type=int, default=128)
     p.add_argument("--served-mixed", type=int, default=48,
                    help="requests of the mixed served stream (two meshes, forward "
                         "and forward+adjoint, record lengths NSTEP/4 .. NSTEP); 0 skips it")

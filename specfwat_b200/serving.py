@@ -617,9 +617,19 @@ class Server:
 
 
 def latency_stats(reqs: List[Request]):
+    """Latency percentiles and throughput of a completed stream: over the
+    whole span (first arrival to last completion, ramp-up and drain
+    included) and in steady state (the completions between the 10th and
+    the 90th percentile completion times, over that interval)."""
     lat = np.array([r.latency for r in reqs])
     span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
-    return {"n": len(reqs), "p50_s": float(np.percentile(lat, 50)),
-            "p99_s": float(np.percentile(lat, 99)),
-            "mean_s": float(lat.mean()), "span_s": float(span),
-            "events_per_hour": len(reqs) / span * 3600.0}
+    done = np.sort([r.done for r in reqs])
+    out = {"n": len(reqs), "p50_s": float(np.percentile(lat, 50)),
+           "p99_s": float(np.percentile(lat, 99)),
+           "mean_s": float(lat.mean()), "span_s": float(span),
+           "events_per_hour": len(reqs) / span * 3600.0}
+    if len(done) >= 10:
+        i0, i1 = int(0.1 * (len(done) - 1)), int(0.9 * (len(done) - 1))
+        if done[i1] > done[i0]:
+            out["steady_events_per_hour"] = float((i1 - i0) / (done[i1] - done[i0]) * 3600.0)
+    return out
