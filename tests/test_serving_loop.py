@@ -208,3 +208,19 @@ def test_mixed_stream_completes_with_compaction():
     # every request completes once and every lane and store byte comes back,
     # whatever moves the wall-clock arrivals led to
     check_done(reqs, done, [srv])
+
+
+def test_latency_stats_steady_rate():
+    """Completions every 2 s after a 30 s ramp: the steady rate is 1800/h
+    while the span rate includes the ramp."""
+    from specfwat_b200.serving import latency_stats
+    reqs = []
+    for k in range(50):
+        r = Request(rid=k, mesh="m", kind="fwd", nstep=100, source=None,
+                    receivers=np.zeros((1, 3)), arrival=0.5 * k)
+        r.done = 30.0 + 2.0 * k
+        reqs.append(r)
+    st = latency_stats(reqs)
+    assert st["steady_events_per_hour"] == pytest.approx(1800.0)
+    assert st["events_per_hour"] == pytest.approx(50 / 128.0 * 3600.0)
+    assert st["p50_s"] > 0
