@@ -424,7 +424,6 @@ struct sem_run_s {
   std::vector<float*> lane_scale;
   std::vector<char> lane_saved;   // lane finished a forward with saved store
   bool lanes_mode = false;        // run driven through the sem_lane_* calls
-  DevArray<int> flag;
   DevArray<int> gmap;             // serving: active 8-lane groups
   // periodic stability check (cfg.check_every > 0): per-lane non-finite
   // flags and the step each flagged lane was stopped at (device), their
@@ -971,7 +970,6 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   CKM(r->adj.alloc(nev * nr * 3 * ns), "adjoint sources");
   CK(cudaMemsetAsync(r->seis.p, 0, r->seis.bytes(), r->stream));
   CK(cudaMemsetAsync(r->adj.p, 0, r->adj.bytes(), r->stream));
-  CKM(r->flag.alloc(1), "flag");
   (void)ne;
   r->src_ispec.assign(nev, -1);
   r->nrec.assign(nev, 0);

@@ -159,7 +159,6 @@ int launch_lane_zero(const Fields& f, int nglob, LaneMap lm, int lane,
 // copied to lane `to` (x1, x2 may be null).
 int launch_lane_move(float* x0, float* x1, float* x2, size_t npts, int rec, LaneMap lm, int from,
                      int to, cudaStream_t st);
-int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st);
 // Periodic stability check: flags[lane] |= 1 for running lanes of u (a
 // field of nevp lanes) with a non-finite value; then halt the flagged lanes
 // (phase idle, halt_step = it0 + s_off at the first flag).

@@ -3779,19 +3779,6 @@ int launch_lane_zero_acc(const KernAcc& k, int nglob, size_t ne, LaneMap lm, int
   return 1;
 }
 
-__global__ void k_nonfinite(const float* __restrict__ u, size_t n, int* flag) {
-  bool bad = false;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    bad |= !isfinite(u[i]);
-  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
-}
-
-int launch_nonfinite(const float* u, size_t n, int* flag, cudaStream_t st) {
-  k_nonfinite<<<148 * 4, 256, 0, st>>>(u, n, flag);
-  return 1;
-}
-
 // Sum of n per-series misfits in series order (the order of a host loop)
 // into *out.
 __global__ void k_sum_series(const double* __restrict__ part, int n, double* out) {
