@@ -124,3 +124,35 @@ def test_spill_budget_too_small_is_refused(gpu):
     assert sim.store_info()["device_slots"] == 0
     sim.close()
     mesh.close()
+
+
+def test_sm_share_keeps_results(gpu):
+    """A run whose persistent element kernels are capped to a few SMs and
+    whose stream has the highest priority (sem_set_sm_share) computes the
+    same seismograms and kernels."""
+    db = D.build("mini")
+    rec = D.surface_receivers(db.box, 3)
+    nev, nstep = 9, 200
+    srcs = _events(db, nev, 51)
+    rng = np.random.default_rng(52)
+    obs = [1e-5 * rng.standard_normal((len(rec), 3, nstep)) for _ in range(nev)]
+    mesh = S.Mesh(db)
+    s0, k0, _ = _run(mesh, db, rec, srcs, obs, nstep, "fp16", True, variant=11)
+    sim = S.Simulation(mesh, nstep, 0.02, nev=nev, store="fp16", use_graph=True,
+                       graph_steps=50, max_receivers=len(rec), kernel_variant=11)
+    sim.set_sm_share(16, True)
+    sim.set_sources(srcs)
+    sim.set_receivers(rec)
+    sim.iterate_time(1, save_forward=True)
+    s1 = [sim.seismograms(e) for e in range(nev)]
+    for e in range(nev):
+        sim.measure_l2(e, obs[e])
+    sim.iterate_time(3)
+    k1 = [sim.save_adjoint_kernels(e) for e in range(nev)]
+    sim.set_sm_share(0, False)
+    sim.close()
+    mesh.close()
+    for e in range(nev):
+        assert rel(s1[e], s0[e]) < 1e-5
+        for q in range(3):
+            assert rel(k1[e][q], k0[e][q]) < 1e-4
