@@ -145,7 +145,9 @@ typedef struct {
                          thread per point with xi contractions by warp
                          shuffles (one event per block), 14 forward as 11
                          and an adjoint kernel sized for three blocks per
-                         SM (divergence summed in shared memory)          */
+                         SM (divergence summed in shared memory), 15 a
+                         forward kernel sized for five blocks per SM the
+                         same way and the adjoint kernel of 11           */
 } sem_run_cfg;
 
 /* CMTSOLUTION-style moment-tensor source.  Moment tensor in the Harvard
@@ -329,7 +331,8 @@ int sem_lane_misfit(sem_run *run, int lane, double *misfit);
  * per thread, 7 to 10 with the adjoint-phase field pair as a float2,
  * 11 forward with register prefetch, 12 as 11 with colour-ordered
  * non-atomic forward assembly, 13 thread per point with warp-shuffle
- * contractions, 14 as 11 with the three-blocks-per-SM adjoint kernel).
+ * contractions, 14 as 11 with the three-blocks-per-SM adjoint kernel, 15
+ * the five-blocks-per-SM forward kernel with the adjoint kernel of 11).
  * With kernel_variant = 0 the first
  * sem_iterate_time times the candidates on this run and keeps the fastest
  * per phase; -1 until then. */

@@ -872,8 +872,8 @@ static int validate_cfg(const sem_run_cfg* c) {
   if (c->max_receivers < 1 || c->max_receivers > 100000)
     return fail(SEM_ERR_ARG, "max_receivers must be in [1, 100000]");
   if (c->graph_steps < 0) return fail(SEM_ERR_ARG, "graph_steps must be >= 0");
-  if (c->kernel_variant < 0 || c->kernel_variant > 14)
-    return fail(SEM_ERR_ARG, "kernel_variant must be 0..14");
+  if (c->kernel_variant < 0 || c->kernel_variant > 15)
+    return fail(SEM_ERR_ARG, "kernel_variant must be 0..15");
 
   return SEM_OK;
 }
@@ -924,8 +924,8 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   if (c->kernel_variant == 0) {
     const char* fv = std::getenv("SEM_FORCE_VARIANTS");
     int vf = 0, va = 0;
-    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 14 && va >= 1 &&
-        va <= 14) {
+    if (fv && std::sscanf(fv, "%d,%d", &vf, &va) == 2 && vf >= 1 && vf <= 15 && va >= 1 &&
+        va <= 15) {
       r->variant[0] = vf - 1;
       r->variant[1] = va - 1;
     }
@@ -1187,10 +1187,10 @@ static int ensure_store(sem_run* r) {
 // keep the fastest.  Runs on scratch state before the forward run: the
 // forward zeroes its wavefields and the adjoint run rebuilds its own.
 static int autotune_phase(sem_run* r, bool adj) {
-  const int cands_multi[] = {0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 13};
+  const int cands_multi[] = {0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 13, 14};
   const int cands_single[] = {0, 2, 12};
   const int* cands = r->nev > 1 ? cands_multi : cands_single;
-  const int ncand = r->nev > 1 ? 12 : 3;
+  const int ncand = r->nev > 1 ? 13 : 3;
   const int nsteps = std::max(1, std::min(8, r->nstep - 2));
   r->fill_lanes(adj ? PH_ADJ : PH_FWD, 0);
   for (auto& L : r->h_lanes) L.it0 = 1;

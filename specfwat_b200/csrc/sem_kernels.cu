@@ -2647,8 +2647,8 @@ __device__ __forceinline__ void pair_xi3(const PBuf<16>& b, int t, const float* 
 // eta (DIR 1) or gamma (DIR 2) role of variant 14 on the pencil (pi, pq):
 // the divergence along the pencil of the three components' fluxes, times
 // -w w of the other two directions, added to A2..A4 at the pencil's points.
-template <int DIR>
-__device__ __forceinline__ void div_add3(const PBuf<16>& b, int pi, int pq) {
+template <int DIR, int VL = 16>
+__device__ __forceinline__ void div_add3(const PBuf<VL>& b, int pi, int pq) {
   // point l of the pencil
   auto pt = [&](int l) { return DIR == 1 ? pi + 5 * l + 25 * pq : pi + 5 * pq + 25 * l; };
   float2 v[3][5];
@@ -2871,6 +2871,252 @@ static void forces_adjpair_r3_cfg(const StepArgs& a, cudaStream_t st) {
   if (gx > items.count()) gx = items.count();
   if (gx < 1) gx = 1;
   k_forces_adjpair_r3<<<gx, NT, BYTES, st>>>(a, items);
+}
+
+// Forward element kernel sized for five blocks per SM (variant 15; regular
+// elements, 8 lanes, 2 events per thread, 100 threads): the shared-memory
+// plan of variant 14 for one field - displacement in 3 planes, stress
+// planes 3-4 in the derivative slots of the owner's points, the
+// divergence summed in 3 planes by the xi, eta and gamma owners in turn,
+// single-buffered kappa/mu - 38.5 KB instead of 47.5 KB.
+struct FwdR5Layout {
+  static constexpr int LB = 8;
+  static constexpr int NE = NGLL3;
+  static constexpr int OFF_IB = 0;                          // int [3][NE]
+  static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);       // [2][NE] kappa, mu
+  static constexpr int OFF_U = al4(OFF_KM + 2 * NE);        // [3][NE][LB]
+  static constexpr int OFF_A = al4(OFF_U + 3 * NE * LB);    // [6][NE][LB]
+  static constexpr int TOTAL = OFF_A + 6 * NE * LB;
+  static constexpr size_t BYTES = (size_t)TOTAL * 4;
+};
+
+// xi role of variant 15: gradient and stress of two events at the pencil's
+// points, stress components to U0..U2 and A0..A1, -wjk f_xi to A2..A4.
+__device__ __forceinline__ void fwd_xi5(const PBuf<8>& b, int t, const float* kap,
+                                        const float* mu, float fac) {
+  float2 u[3][5];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int l = 0; l < 5; ++l) u[c][l] = p2(lds_v<2>(b.U(c, l + 5 * t)));
+  float2 sx[3][5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int p = i + 5 * t;
+    float2 g[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) a = cfma2(gD(i, l), u[c][l], a);
+      g[c][0] = a;
+      g[c][1] = p2(lds_v<2>(b.Ar(c, p)));
+      g[c][2] = p2(lds_v<2>(b.Ar(3 + c, p)));
+    }
+    float2 sig[6];
+    stress_point2(g, kap[p], mu[p], fac, sig);
+    sx[0][i] = sig[0];
+    sx[1][i] = sig[3];
+    sx[2][i] = sig[4];
+    sts_v<2>(b.U(0, p), lv2(sig[3]));
+    sts_v<2>(b.U(1, p), lv2(sig[1]));
+    sts_v<2>(b.U(2, p), lv2(sig[5]));
+    sts_v<2>(b.Ar(0, p), lv2(sig[4]));
+    sts_v<2>(b.Ar(1, p), lv2(sig[2]));
+  }
+  const int pj = t % 5, pk = t / 5;
+  float wj = 0.f, wk = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q == pj) wj = gW(q);
+    if (q == pk) wk = gW(q);
+  }
+  const float2 njk = splat(-(wj * wk));
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) a = cfma2(gDWt(i, l), sx[c][l], a);
+      sts_v<2>(b.Ar(2 + c, i + 5 * t), lv2(__fmul2_rn(njk, a)));
+    }
+}
+
+__global__ void __maxnreg__(96) k_forces_fwd_r5(StepArgs A, PipeItems items) {
+  constexpr int LB = 8;
+  constexpr int NL = 2;
+  constexpr int NT = 25 * LB / NL;
+  using LY = FwdR5Layout;
+  constexpr int NE = NGLL3;
+  constexpr int LWLOG = 3;
+  extern __shared__ float sm[];
+  int* sIB = (int*)(sm + LY::OFF_IB);
+  float* sKM = sm + LY::OFF_KM;
+  float* sU = sm + LY::OFF_U;
+  float* sA = sm + LY::OFF_A;
+
+  const int tid = threadIdx.x;
+  const int lq = tid % (LB / NL);
+  const int t = tid / (LB / NL);
+  const int lane = lq * NL;
+  const int pi = t % 5, pq = t / 5;
+  const int nev = A.nev;
+  const int nspec = A.m.nspec;
+  const int nitems = items.count();
+
+  bool any = false;
+  for (int l = tid; l < nev; l += NT) {
+    const LaneDesc* L = A.lanes + l;
+    any |= L->phase != PH_IDLE && L->it0 + A.s < L->nstep;
+  }
+  if (!__syncthreads_or(any)) return;
+  if (A.lm.lwlog != LWLOG) return;  // batched layout only
+
+  int c_chunk = -1, c_fl[NL] = {0, 0};
+  auto flags = [&](int w, int& lg0, int& g, int fl[NL]) -> int {
+    int chunk;
+    items.decode(w, chunk, g);
+    lg0 = chunk * LB + lane;
+    if (chunk != c_chunk) {
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        int f = 0;
+        const int lg = lg0 + n;
+        if (chunk < items.nchunk && lg < nev) {
+          const LaneDesc* L = A.lanes + lg;
+          const int it = L->it0 + A.s;
+          if (L->phase != PH_IDLE && it < L->nstep) f = 1;
+        }
+        c_fl[n] = f;
+      }
+      c_chunk = chunk;
+    }
+    fl[0] = c_fl[0];
+    fl[1] = c_fl[1];
+    return fl[0] | fl[1];
+  };
+  auto issue_ib = [&](int w, int slot) {
+    int* dst = sIB + slot * NE;
+    int chunk = 0, g = 0;
+    if (w < nitems) items.decode(w, chunk, g);
+    for (int i = tid; i < NE; i += NT) {
+      if (w < nitems && g < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      else
+        dst[i] = -1;
+    }
+  };
+  auto issue_km = [&](int w) {
+    if (w >= nitems) return;
+    int chunk, g;
+    items.decode(w, chunk, g);
+    if (g >= nspec) return;
+    const int e = A.m.order[g];
+    for (int i = tid; i < NE; i += NT) {
+      const size_t ep = (size_t)e * NGLL3 + i;
+      cp_async4(sKM + i, A.m.kappa + ep);
+      cp_async4(sKM + NE + i, A.m.mu + ep);
+    }
+  };
+  float2 pre[5][3];
+  auto load_u = [&](int w, int ibslot) {
+    int lg0 = 0, g = 0, fl[NL] = {0, 0}, anyf = 0;
+    if (w < nitems) anyf = flags(w, lg0, g, fl);
+    const int* ib = sIB + ibslot * NE;
+    const float* src = A.f1.u + fbase<LWLOG>(A, lg0);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        ldg_pred(pre[r][c], src + foff<LWLOG>(ig, c), anyf && ig >= 0);
+    }
+  };
+
+  int w = blockIdx.x;
+  issue_ib(w, 0);
+  cp_commit();
+  cp_wait_all();
+  __syncthreads();
+  issue_km(w);
+  issue_ib(w + gridDim.x, 1);
+  cp_commit();
+  load_u(w, 0);
+
+  const float fac = A.m.jac * A.m.xix * A.m.xix;
+  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+    const int ibs = k % 3;
+    cp_wait_all();
+    __syncthreads();  // previous element done with U/A; this one's kappa/mu landed
+    {
+      float* ub = sU + lane;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int p = t + 25 * r;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          *reinterpret_cast<float2*>(ub + (c * NGLL3 + p) * LB) = pre[r][c];
+      }
+    }
+    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    cp_commit();
+    __syncthreads();  // U complete
+    load_u(w + gridDim.x, (k + 1) % 3);
+
+    int lg0, g, fl[NL];
+    const int anyf = flags(w, lg0, g, fl);
+    const bool valid = g < nspec;
+    PBuf<LB> b{sU + lane, sA + lane};
+    v_grad_eg<LB, NL>(b, pi, pq);
+    __syncthreads();
+    fwd_xi5(b, t, sKM, sKM + NE, fac);
+    __syncthreads();  // stress and xi sums complete; kappa/mu free
+    issue_km(w + gridDim.x);
+    cp_commit();
+    div_add3<1, LB>(b, pi, pq);
+    __syncthreads();
+    div_add3<2, LB>(b, pi, pq);
+    __syncthreads();
+    if (valid && anyf) {
+      const int* ib = sIB + ibs * NE;
+      float* accb = A.f1.a + fbase<LWLOG>(A, lg0);
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const int p = i + 5 * t;
+        const int ig = ib[p];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          LV<2> f = lds_v<2>(b.Ar(2 + c, p));
+          if (!(fl[0] & 1)) f.v[0] = 0.f;   // lanes not running add nothing
+          if (!(fl[1] & 1)) f.v[1] = 0.f;
+          red_v<2>(&accb[foff<3>(ig, c)], f);
+        }
+      }
+    }
+  }
+  cp_wait_all();
+}
+
+static int forces_fwd_r5_cfg(const StepArgs& a, cudaStream_t st) {
+  constexpr int NT = 100;
+  constexpr size_t BYTES = FwdR5Layout::BYTES;
+  static int blocks_per_sm = 0, sms = 0;
+  if (!blocks_per_sm) {
+    cudaFuncSetAttribute(k_forces_fwd_r5, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_forces_fwd_r5, NT, BYTES);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  PipeItems items = make_items<8>(a, a.m.nspec);
+  if (items.count() == 0) return 0;
+  int gx = blocks_per_sm * sm_share(a, sms);
+  if (gx > items.count()) gx = items.count();
+  if (gx < 1) gx = 1;
+  k_forces_fwd_r5<<<gx, NT, BYTES, st>>>(a, items);
+  return 1;
 }
 
 // Forward-phase element kernel with 2 events per thread and the next
@@ -3165,6 +3411,11 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
   if (a.variant == 13 && a.nev > 1) {
     if (!adj) return forces_fwd_r_cfg<8, false>(a, st);
     forces_adjpair_r3_cfg(a, st);
+    return 1;
+  }
+  if (a.variant == 14 && a.nev > 1) {
+    if (!adj) return forces_fwd_r5_cfg(a, st);
+    forces_adjpair_r_cfg<8>(a, st);
     return 1;
   }
   if ((a.variant >= 6 && a.variant <= 9) && a.nev > 1) {

@@ -166,7 +166,7 @@ def test_graph_equals_stepwise(gpu, small):
 
 @pytest.mark.parametrize("nev,variant", [(2, 0), (9, 0), (9, 5), (12, 6), (9, 7), (12, 8),
                                          (9, 9), (12, 10), (9, 11), (16, 11), (12, 12),
-                                         (9, 14), (16, 14)])
+                                         (9, 14), (16, 14), (9, 15), (16, 15)])
 def test_batched_adjoint_fp16_store(gpu, mini_adjoint, nev, variant):
     db, rec, mt, sxyz, nstep, dt, obs = mini_adjoint
     mesh = S.Mesh(db)
@@ -248,7 +248,7 @@ def test_state_errors(gpu, small):
     assert ei.value.code == -1
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15])
 def test_batched_adjoint_distinct_events_equal_alone(gpu, variant):
     """Each lane has its own source and observed data: the batched adjoint
     must give every event the kernels it gets alone."""
