@@ -963,6 +963,28 @@ static PipeItems make_items(const StepArgs& a, int ngroups) {
   return it;
 }
 
+// The work items a persistent block has in flight, in shared memory: slot
+// j & 3 holds item w + j * gridDim.x as (element, lane chunk).  One thread
+// decodes an item three iterations before it is computed and fetches its
+// element id from the traversal order by cp.async, so the copies that need
+// the id are addressed without a dependent global load on the way.
+struct ItemRing {
+  int* e;  // [4] element; nspec past the end of the items
+  int* c;  // [4] lane chunk; items.nchunk past the end
+  __device__ __forceinline__ void fill(const PipeItems& items, const int* order, int nspec, int w,
+                                       int slot) const {
+    if (w < items.count()) {
+      int chunk, g;
+      items.decode(w, chunk, g);  // g < items.ngroups, the length of order
+      c[slot] = chunk;
+      cp_async4(e + slot, order + g);
+    } else {
+      c[slot] = items.nchunk;
+      e[slot] = nspec;
+    }
+  }
+};
+
 template <int LB, int EPB, int TPE, bool ADJ>
 __global__ void __launch_bounds__(EPB * TPE * LB) k_forces_piped(StepArgs A, PipeItems items) {
   using LY = PipeLayout<LB, EPB, TPE, ADJ>;
@@ -2347,16 +2369,19 @@ __global__ void __launch_bounds__(25 * LB) k_forces_adjpair(StepArgs A, PipeItem
 
 // As k_forces_adjpair, but the next element's displacement gather is
 // prefetched into registers (plain loads issued before the current element
-// is computed, stored to shared memory at the top of the next iteration),
-// so the displacement region is single-buffered: 40 KB less shared memory
-// per 8 events, twice the resident blocks.
+// is computed, stored to shared memory once the current element's stresses
+// have been read), so the displacement region is single-buffered: 40 KB
+// less shared memory per 8 events, twice the resident blocks.  Four block
+// barriers per element: the gather store shares the top barrier with the
+// copies of the next items, and the items come from an ItemRing.
 template <int LB, bool GEN = false>
 struct PairRLayout {
   static constexpr int VL = 2 * LB;
   static constexpr int NE = NGLL3;
   static constexpr int PPU = GEN ? 6 * NGLL3 : PP_U;               // U, then 5 (6) values
   static constexpr int OFF_IB = 0;                                  // int [3][NE]
-  static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);               // [2][2][NE]
+  static constexpr int OFF_IT = al4(OFF_IB + 3 * NE);               // int [2][4] item ring
+  static constexpr int OFF_KM = al4(OFF_IT + 8);                    // [2][2][NE]
   static constexpr int OFF_U = al4(OFF_KM + 4 * NE);                // [PPU][VL]
   static constexpr int OFF_A = al4(OFF_U + PPU * VL);               // [PP_A][VL]
   static constexpr int TOTAL = OFF_A + PP_A * VL;
@@ -2372,6 +2397,7 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
   constexpr int LWLOG = 3;
   extern __shared__ float sm[];
   int* sIB = (int*)(sm + LY::OFF_IB);
+  const ItemRing ring{(int*)(sm + LY::OFF_IT), (int*)(sm + LY::OFF_IT) + 4};
   float* sKM = sm + LY::OFF_KM;
   float* sU = sm + LY::OFF_U;
   float* sA = sm + LY::OFF_A;
@@ -2383,6 +2409,7 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
   const int nev = A.nev;
   const int nspec = A.m.nspec;
   const int nitems = items.count();
+  const int G = gridDim.x;
 
   bool any = false;
   for (int l = tid; l < nev; l += NT) {
@@ -2392,10 +2419,10 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
   if (!__syncthreads_or(any)) return;
   if (A.lm.lwlog != LWLOG) return;  // batched layout only
 
+  // this thread's lane of a chunk and its flags: 1 running, 2 adjoint
+  // phase, 4 adjoint phase past its first step
   int c_chunk = -1, c_flag = 0;
-  auto flags = [&](int w, int& lg, int& g) -> int {
-    int chunk;
-    items.decode(w, chunk, g);
+  auto flags = [&](int chunk, int& lg) -> int {
     lg = chunk * LB + lq;
     if (chunk == c_chunk) return c_flag;
     int f = 0;
@@ -2411,42 +2438,36 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     c_flag = f;
     return f;
   };
-  auto issue_ib = [&](int w, int slot) {
+  // ibool row of element e into slot `slot` (-1 past the end)
+  auto issue_ib = [&](int e, int slot) {
     int* dst = sIB + slot * NE;
-    int chunk = 0, g = 0;
-    if (w < nitems) items.decode(w, chunk, g);
     for (int i = tid; i < NE; i += NT) {
-      if (w < nitems && g < nspec)
-        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      if (e < nspec)
+        cp_async4(dst + i, A.m.ibool + (size_t)e * NGLL3 + i);
       else
         dst[i] = -1;
     }
   };
-  // kappa, mu and kernel accumulators of item w: cp.async into buffer buf
-  auto issue_km = [&](int w, int buf) {
-    if (w >= nitems) return;
-    int lg, g;
-    const int fl = flags(w, lg, g);
+  // kappa and mu of element e into buffer buf
+  auto issue_km = [&](int e, int buf) {
+    if (e >= nspec) return;
     float* km = sKM + buf * 2 * NE;
-    const int e = g < nspec ? A.m.order[g] : 0;
     for (int i = tid; i < NE; i += NT) {
-      if (g < nspec) {
-        const size_t ep = (size_t)e * NGLL3 + i;
-        cp_async4(km + i, A.m.kappa + ep);
-        cp_async4(km + NE + i, A.m.mu + ep);
-      }
+      const size_t ep = (size_t)e * NGLL3 + i;
+      cp_async4(km + i, A.m.kappa + ep);
+      cp_async4(km + NE + i, A.m.mu + ep);
     }
   };
-  // displacement gather of item w into registers (ibool from slot ibslot)
+  // displacement gather of an item into registers (ibool from slot ibslot)
   float pre[2][5][3];
-  auto load_u = [&](int w, int ibslot) {
-    int lg = 0, g = 0, fl = 0;
-    if (w < nitems) fl = flags(w, lg, g);
+  auto load_u = [&](int chunk, int ibslot) {
+    int lg;
+    const int fl = flags(chunk, lg);
     const int* ib = sIB + ibslot * NE;
     const size_t fb = fbase<LWLOG>(A, lg);
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
+      const int ig = ib[t + 25 * r];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         ldg_pred(pre[0][r][c], A.f1.u + fb + foff<LWLOG>(ig, c), (fl & 1) && ig >= 0);
@@ -2454,49 +2475,55 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
       }
     }
   };
+  auto store_u = [&]() {
+    float* ub = sU + 2 * lq;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int p = t + 25 * r;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        LV<2> v;
+        v.v[0] = pre[0][r][c];
+        v.v[1] = pre[1][r][c];
+        sts_v<2>(ub + (c * NGLL3 + p) * VL, v);
+      }
+    }
+  };
 
   int w = blockIdx.x;
-  issue_ib(w, 0);
+  if (tid == 0)
+    for (int j = 0; j < 3; ++j) ring.fill(items, A.m.order, nspec, w + j * G, j);
   cp_commit();
   cp_wait_all();
   __syncthreads();
-  issue_km(w, 0);
-  issue_ib(w + gridDim.x, 1);
+  issue_ib(ring.e[0], 0);
   cp_commit();
-  load_u(w, 0);
+  cp_wait_all();
+  __syncthreads();
+  issue_km(ring.e[0], 0);
+  issue_ib(ring.e[1], 1);
+  cp_commit();
+  load_u(ring.c[0], 0);
+  store_u();
 
   const float fac = A.m.jac * A.m.xix * A.m.xix;
   // kernel products: raw reference derivatives (times xix^2) or, for
   // general elements, physical strains
   const float dtk = GEN ? A.dt : A.dt * A.m.xix * A.m.xix;
-  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+  for (int k = 0; w < nitems; ++k, w += G) {
     const int buf = k & 1;
     const int ibs = k % 3;
     cp_wait_all();
-    __syncthreads();  // previous item done with U/A/K; this item's copies landed
-    {
-      float* ub = sU + 2 * lq;
-#pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        const int p = t + 25 * r;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          LV<2> v;
-          v.v[0] = pre[0][r][c];
-          v.v[1] = pre[1][r][c];
-          sts_v<2>(ub + (c * NGLL3 + p) * VL, v);
-        }
-      }
-    }
-    issue_km(w + gridDim.x, buf ^ 1);
-    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    __syncthreads();  // U holds this item's displacement, its copies landed, the last scatter is done
+    if (tid == 0) ring.fill(items, A.m.order, nspec, w + 3 * G, (k + 3) & 3);
+    issue_km(ring.e[(k + 1) & 3], buf ^ 1);
+    issue_ib(ring.e[(k + 2) & 3], (k + 2) % 3);
     cp_commit();
-    __syncthreads();  // U complete
-    load_u(w + gridDim.x, (k + 1) % 3);  // next item's gather, consumed next iteration
+    load_u(ring.c[(k + 1) & 3], (k + 1) % 3);  // next item's gather, stored after this item's divergence
 
-    int lg, g;
-    const int fl = flags(w, lg, g);
-    const int e = g < nspec ? A.m.order[g] : nspec;
+    int lg;
+    const int fl = flags(ring.c[k & 3], lg);
+    const int e = ring.e[k & 3];
     const float* kap = sKM + buf * 2 * NE;
     const float* mu = kap + NE;
     PBuf<VL> b{sU + 2 * lq, sA + 2 * lq};
@@ -2524,7 +2551,8 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     }
     __syncthreads();
     v_div_eg<VL, 2, GEN>(b, pi, pq);
-    __syncthreads();
+    __syncthreads();  // U's stresses read: it takes the next displacement
+    store_u();
     if (e < nspec && (fl & 1)) {
       const size_t fb = fbase<LWLOG>(A, lg);
       pair_scatter<VL>(b, t, fx, sIB + ibs * NE, A.f1.a + fb, A.f2.a + fb, true, (fl & 4) != 0);
@@ -3121,14 +3149,17 @@ static int forces_fwd_r5_cfg(const StepArgs& a, cudaStream_t st) {
 
 // Forward-phase element kernel with 2 events per thread and the next
 // element's gather prefetched into registers (single-buffered shared
-// displacement), LB events per block.  LB is at most the 8-lane sector
-// group, so a work item never spans two groups of a group map.
+// displacement, stored once the current element's stresses have been
+// read), LB events per block.  LB is at most the 8-lane sector group, so a
+// work item never spans two groups of a group map.  Four block barriers per
+// element, items from an ItemRing.
 template <int LB, bool GEN = false>
 struct FwdRLayout {
   static constexpr int NE = NGLL3;
   static constexpr int PPU = GEN ? 6 * NGLL3 : PP_U;   // U, then 5 (6) values
   static constexpr int OFF_IB = 0;                      // int [3][NE]
-  static constexpr int OFF_KM = al4(OFF_IB + 3 * NE);   // [2][2][NE]
+  static constexpr int OFF_IT = al4(OFF_IB + 3 * NE);   // int [2][4] item ring
+  static constexpr int OFF_KM = al4(OFF_IT + 8);        // [2][2][NE]
   static constexpr int OFF_U = al4(OFF_KM + 4 * NE);    // [PPU][LB]
   static constexpr int OFF_A = al4(OFF_U + PPU * LB);   // [PP_A][LB]
   static constexpr int TOTAL = OFF_A + PP_A * LB;
@@ -3144,6 +3175,7 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
   constexpr int LWLOG = 3;
   extern __shared__ float sm[];
   int* sIB = (int*)(sm + LY::OFF_IB);
+  const ItemRing ring{(int*)(sm + LY::OFF_IT), (int*)(sm + LY::OFF_IT) + 4};
   float* sKM = sm + LY::OFF_KM;
   float* sU = sm + LY::OFF_U;
   float* sA = sm + LY::OFF_A;
@@ -3154,8 +3186,11 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
   const int lane = lq * NL;
   const int pi = t % 5, pq = t / 5;
   const int nev = A.nev;
-  const int ngr = items.ngroups;  // elements of this launch (one colour, or all)
+  // element ids index the mesh arrays (with colouring, `order` is this
+  // colour's part of the colour order); nspec marks an item past the end
+  const int nel = A.m.nspec;
   const int nitems = items.count();
+  const int G = gridDim.x;
 
   bool any = false;
   for (int l = tid; l < nev; l += NT) {
@@ -3165,10 +3200,9 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
   if (!__syncthreads_or(any)) return;
   if (A.lm.lwlog != LWLOG) return;  // batched layout only
 
+  // running flags of this thread's two lanes of a chunk
   int c_chunk = -1, c_fl[NL] = {0, 0};
-  auto flags = [&](int w, int& lg0, int& g, int fl[NL]) -> int {
-    int chunk;
-    items.decode(w, chunk, g);
+  auto flags = [&](int chunk, int& lg0, int fl[NL]) -> int {
     lg0 = chunk * LB + lane;
     if (chunk != c_chunk) {
 #pragma unroll
@@ -3188,84 +3222,86 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     fl[1] = c_fl[1];
     return fl[0] | fl[1];
   };
-  auto issue_ib = [&](int w, int slot) {
+  // ibool row of element e into slot `slot` (-1 past the end)
+  auto issue_ib = [&](int e, int slot) {
     int* dst = sIB + slot * NE;
-    int chunk = 0, g = 0;
-    if (w < nitems) items.decode(w, chunk, g);
     for (int i = tid; i < NE; i += NT) {
-      if (w < nitems && g < ngr)
-        cp_async4(dst + i, A.m.ibool + (size_t)A.m.order[g] * NGLL3 + i);
+      if (e < nel)
+        cp_async4(dst + i, A.m.ibool + (size_t)e * NGLL3 + i);
       else
         dst[i] = -1;
     }
   };
-  auto issue_km = [&](int w, int buf) {
-    if (w >= nitems) return;
-    int chunk, g;
-    items.decode(w, chunk, g);
+  // kappa and mu of element e into buffer buf
+  auto issue_km = [&](int e, int buf) {
+    if (e >= nel) return;
     float* km = sKM + buf * 2 * NE;
-    const int e = g < ngr ? A.m.order[g] : 0;
     for (int i = tid; i < NE; i += NT) {
-      if (g < ngr) {
-        const size_t ep = (size_t)e * NGLL3 + i;
-        cp_async4(km + i, A.m.kappa + ep);
-        cp_async4(km + NE + i, A.m.mu + ep);
-      }
+      const size_t ep = (size_t)e * NGLL3 + i;
+      cp_async4(km + i, A.m.kappa + ep);
+      cp_async4(km + NE + i, A.m.mu + ep);
     }
   };
   float2 pre[5][3];
-  auto load_u = [&](int w, int ibslot) {
-    int lg0 = 0, g = 0, fl[NL] = {0, 0}, anyf = 0;
-    if (w < nitems) anyf = flags(w, lg0, g, fl);
+  auto load_u = [&](int chunk, int ibslot) {
+    int lg0, fl[NL];
+    const int anyf = flags(chunk, lg0, fl);
     const int* ib = sIB + ibslot * NE;
     const float* src = A.f1.u + fbase<LWLOG>(A, lg0);
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-      const int ig = (w < nitems) ? ib[t + 25 * r] : -1;
+      const int ig = ib[t + 25 * r];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
         ldg_pred(pre[r][c], src + foff<LWLOG>(ig, c), anyf && ig >= 0);
     }
   };
+  auto store_u = [&]() {
+    float* ub = sU + lane;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int p = t + 25 * r;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        *reinterpret_cast<float2*>(ub + (c * NGLL3 + p) * LB) = pre[r][c];
+    }
+  };
 
   int w = blockIdx.x;
-  issue_ib(w, 0);
+  if (tid == 0)
+    for (int j = 0; j < 3; ++j) ring.fill(items, A.m.order, nel, w + j * G, j);
   cp_commit();
   cp_wait_all();
   __syncthreads();
-  issue_km(w, 0);
-  issue_ib(w + gridDim.x, 1);
+  issue_ib(ring.e[0], 0);
   cp_commit();
-  load_u(w, 0);
+  cp_wait_all();
+  __syncthreads();
+  issue_km(ring.e[0], 0);
+  issue_ib(ring.e[1], 1);
+  cp_commit();
+  load_u(ring.c[0], 0);
+  store_u();
 
   const float fac = A.m.jac * A.m.xix * A.m.xix;
-  for (int k = 0; w < nitems; ++k, w += gridDim.x) {
+  for (int k = 0; w < nitems; ++k, w += G) {
     const int buf = k & 1;
     const int ibs = k % 3;
     cp_wait_all();
-    __syncthreads();
-    {
-      float* ub = sU + lane;
-#pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        const int p = t + 25 * r;
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          *reinterpret_cast<float2*>(ub + (c * NGLL3 + p) * LB) = pre[r][c];
-      }
-    }
-    issue_km(w + gridDim.x, buf ^ 1);
-    issue_ib(w + 2 * gridDim.x, (k + 2) % 3);
+    __syncthreads();  // U holds this item's displacement, its copies landed, the last scatter is done
+    if (tid == 0) ring.fill(items, A.m.order, nel, w + 3 * G, (k + 3) & 3);
+    issue_km(ring.e[(k + 1) & 3], buf ^ 1);
+    issue_ib(ring.e[(k + 2) & 3], (k + 2) % 3);
     cp_commit();
-    __syncthreads();
-    load_u(w + gridDim.x, (k + 1) % 3);
+    load_u(ring.c[(k + 1) & 3], (k + 1) % 3);
 
-    int lg0, g, fl[NL];
-    const int anyf = flags(w, lg0, g, fl);
-    const bool valid = g < ngr;
+    int lg0, fl[NL];
+    const int anyf = flags(ring.c[k & 3], lg0, fl);
+    const int e = ring.e[k & 3];
+    const bool valid = e < nel;
     const float* geo_e = nullptr;
     if (GEN && valid) {
-      const int ir = A.m.irreg[A.m.order[g]];
+      const int ir = A.m.irreg[e];
       if (ir >= 0) geo_e = A.m.geo + (size_t)ir * NGLL3 * 10;
     }
     const float* kap = sKM + buf * 2 * NE;
@@ -3277,7 +3313,8 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     v_xi<LB, NL, 0, GEN>(b, b, t, kap, mu, fac, fx, km, kk, geo_e, A.m.xix, A.m.jac);
     __syncthreads();
     v_div_eg<LB, NL, GEN>(b, pi, pq);
-    __syncthreads();
+    __syncthreads();  // U's stresses read: it takes the next displacement
+    store_u();
     if (valid && anyf)
       v_scatter<LB, NL, !COLOURED>(b, t, fx, sIB + ibs * NE, A.f1.a + fbase<LWLOG>(A, lg0), fl, 1);
   }
