@@ -1389,8 +1389,10 @@ struct PBuf {
   __device__ __forceinline__ float* Ar(int q, int p) const { return ab + (q * 125 + p) * LB; }
 };
 
-// eta / gamma derivative roles (pencils (i,k) and (i,j) of thread t).
-template <int LB, int NL>
+// eta / gamma derivative roles (pencils (i,k) and (i,j) of thread t);
+// GAMMA false: the eta role only (the gamma role taken from registers by
+// grad_gamma_regs).
+template <int LB, int NL, bool GAMMA = true>
 __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
   if constexpr (NL == 2) {
 #pragma unroll
@@ -1406,6 +1408,7 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
         sts_v<2>(b.Ar(c, pi + 5 * j + 25 * pq), lv2(a));
       }
     }
+    if constexpr (GAMMA) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       float2 v[5];
@@ -1419,7 +1422,9 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
         sts_v<2>(b.Ar(3 + c, pi + 5 * pq + 25 * k), lv2(a));
       }
     }
+    }
   } else {
+    static_assert(GAMMA, "the eta-only role is packed (NL == 2)");
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       LV<NL> v[5];
@@ -1457,6 +1462,22 @@ __device__ __forceinline__ void v_grad_eg(const PBuf<LB>& b, int pi, int pq) {
       }
     }
   }
+}
+
+// Gamma derivative role from registers: thread t's gamma pencil (points
+// t + 25 l, l = 0..4) is the displacement it gathered itself, v[l][c], so
+// its derivatives need no shared-memory loads.
+template <int LB>
+__device__ __forceinline__ void grad_gamma_regs(const PBuf<LB>& b, int t, const float2 v[5][3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < 5; ++l) a = cfma2(gD(k, l), v[l][c], a);
+      sts_v<2>(b.Ar(3 + c, t + 25 * k), lv2(a));
+    }
 }
 
 // eta / gamma divergence roles: B -> A.
@@ -2459,7 +2480,9 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     }
   };
   // displacement gather of an item into registers (ibool from slot ibslot)
-  float pre[2][5][3];
+  // (adjoint, backward) displacement of points t + 25 r: the thread's
+  // gamma pencil
+  float2 pre[5][3];
   auto load_u = [&](int chunk, int ibslot) {
     int lg;
     const int fl = flags(chunk, lg);
@@ -2470,8 +2493,8 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
       const int ig = ib[t + 25 * r];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        ldg_pred(pre[0][r][c], A.f1.u + fb + foff<LWLOG>(ig, c), (fl & 1) && ig >= 0);
-        ldg_pred(pre[1][r][c], A.f2.u + fb + foff<LWLOG>(ig, c), (fl & 2) && ig >= 0);
+        ldg_pred(pre[r][c].x, A.f1.u + fb + foff<LWLOG>(ig, c), (fl & 1) && ig >= 0);
+        ldg_pred(pre[r][c].y, A.f2.u + fb + foff<LWLOG>(ig, c), (fl & 2) && ig >= 0);
       }
     }
   };
@@ -2481,12 +2504,7 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     for (int r = 0; r < 5; ++r) {
       const int p = t + 25 * r;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        LV<2> v;
-        v.v[0] = pre[0][r][c];
-        v.v[1] = pre[1][r][c];
-        sts_v<2>(ub + (c * NGLL3 + p) * VL, v);
-      }
+      for (int c = 0; c < 3; ++c) sts_v<2>(ub + (c * NGLL3 + p) * VL, lv2(pre[r][c]));
     }
   };
 
@@ -2515,6 +2533,8 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     const int ibs = k % 3;
     cp_wait_all();
     __syncthreads();  // U holds this item's displacement, its copies landed, the last scatter is done
+    PBuf<VL> b{sU + 2 * lq, sA + 2 * lq};
+    grad_gamma_regs<VL>(b, t, pre);  // before the next gather replaces pre
     if (tid == 0) ring.fill(items, A.m.order, nspec, w + 3 * G, (k + 3) & 3);
     issue_km(ring.e[(k + 1) & 3], buf ^ 1);
     issue_ib(ring.e[(k + 2) & 3], (k + 2) % 3);
@@ -2526,8 +2546,7 @@ __global__ void __launch_bounds__(25 * LB, LB == 8 ? 2 : 4) k_forces_adjpair_r(S
     const int e = ring.e[k & 3];
     const float* kap = sKM + buf * 2 * NE;
     const float* mu = kap + NE;
-    PBuf<VL> b{sU + 2 * lq, sA + 2 * lq};
-    v_grad_eg<VL, 2>(b, pi, pq);
+    v_grad_eg<VL, 2, false>(b, pi, pq);
     __syncthreads();
     LV<2> fx[5][3];
     float kmu[5], kka[5];
@@ -3289,6 +3308,8 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     const int ibs = k % 3;
     cp_wait_all();
     __syncthreads();  // U holds this item's displacement, its copies landed, the last scatter is done
+    PBuf<LB> b{sU + lane, sA + lane};
+    grad_gamma_regs<LB>(b, t, pre);  // before the next gather replaces pre
     if (tid == 0) ring.fill(items, A.m.order, nel, w + 3 * G, (k + 3) & 3);
     issue_km(ring.e[(k + 1) & 3], buf ^ 1);
     issue_ib(ring.e[(k + 2) & 3], (k + 2) % 3);
@@ -3306,8 +3327,7 @@ __global__ void __launch_bounds__(25 * LB / 2) k_forces_fwd_r(StepArgs A, PipeIt
     }
     const float* kap = sKM + buf * 2 * NE;
     const float* mu = kap + NE;
-    PBuf<LB> b{sU + lane, sA + lane};
-    v_grad_eg<LB, NL>(b, pi, pq);
+    v_grad_eg<LB, NL, false>(b, pi, pq);
     __syncthreads();
     LV<NL> fx[5][3], km[1], kk[1];
     v_xi<LB, NL, 0, GEN>(b, b, t, kap, mu, fac, fx, km, kk, geo_e, A.m.xix, A.m.jac);
