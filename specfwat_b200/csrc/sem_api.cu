@@ -464,6 +464,10 @@ struct sem_run_s {
   std::vector<Injection> inj;
   bool fwd_saved = false, adj_done = false;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  // graph branches of the lane groups past the first: one stream each, and
+  // the events that fork them from `stream` and join them back
+  std::vector<cudaStream_t> chain_st;
+  std::vector<cudaEvent_t> chain_ev;
   int variant[2] = {-1, -1};  // element-kernel variant per phase (fwd, adj)
   double last_ms = 0.0;
   long long last_launches = 0;
@@ -479,6 +483,8 @@ struct sem_run_s {
     if (stream) cudaStreamSynchronize(stream);
     for (auto& g : gexec)
       if (g) cudaGraphExecDestroy(g);
+    for (auto c : chain_st) cudaStreamDestroy(c);
+    for (auto e : chain_ev) cudaEventDestroy(e);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (check_ev) cudaEventDestroy(check_ev);
@@ -533,6 +539,7 @@ struct sem_run_s {
     a.inject = 0;
     for (const auto& j : inj) a.inject |= j.buf != nullptr;
     a.sm_limit = sm_limit;
+    a.ring_nev = nev;
     // public 1 = thread-per-point, 2 = pencil, 3 = pencil pipelined;
     // 0 = chosen by the autotuner per phase
     const int v = variant[adjoint ? 1 : 0];
@@ -1342,6 +1349,48 @@ static int ring_after(sem_run* r, bool adjoint, int g, bool save) {
 }
 
 // Queue the step loop of one phase (graphs or per-step launches).
+// Step arguments of lane group g (lanes 8g .. 8g+7) of a batched run as a
+// run of its own: every per-lane array starts at the group's block of the
+// lane-group layout, so the kernels see lanes 0..7 of one group.
+static StepArgs group_args(const sem_run* r, const StepArgs& a, int g) {
+  StepArgs ag = a;
+  const int lw = 1 << a.lm.lwlog;
+  const size_t fg = (size_t)g * r->mesh->nglob * 3 * lw;   // field values of a group
+  const size_t pg = (size_t)g * r->mesh->nglob * lw;       // per-point values
+  const size_t eg = (size_t)g * r->mesh->nspec * 125 * lw; // per element point
+  auto off = [](float* p, size_t o) { return p ? p + o : p; };
+  ag.f1 = {off(a.f1.u, fg), off(a.f1.v, fg), off(a.f1.a, fg)};
+  ag.f2 = {off(a.f2.u, fg), off(a.f2.v, fg), off(a.f2.a, fg)};
+  ag.k = {off(a.k.rho_glob, pg), off(a.k.mu, eg), off(a.k.kappa, eg), off(a.k.hess_glob, pg)};
+  ag.lanes = a.lanes + (size_t)g * lw;
+  ag.nev = std::min(lw, a.nev - g * lw);
+  ag.gmap = nullptr;
+  ag.ngmap = 0;
+  return ag;
+}
+
+// Lane groups captured as separate graph branches: the groups' events are
+// independent, so one group's update (HBM-bound) can run while another
+// group's element kernel (bound by shared memory and latency) holds the SMs.
+static int chain_groups(const sem_run* r) {
+  if (r->lm.lwlog != 3 || r->nev <= 8 || r->mesh->nglob == 0) return 1;
+  return (r->nev + 7) / 8;
+}
+
+static int ensure_chains(sem_run* r, int G) {
+  while ((int)r->chain_st.size() < G - 1) {
+    cudaStream_t c;
+    CK(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
+    r->chain_st.push_back(c);
+  }
+  while ((int)r->chain_ev.size() < G) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    r->chain_ev.push_back(e);
+  }
+  return SEM_OK;
+}
+
 static int run_loop(sem_run* r, bool adjoint) {
   long long launches = 0;
   StepArgs a = r->args(adjoint);
@@ -1352,14 +1401,32 @@ static int run_loop(sem_run* r, bool adjoint) {
     cudaGraphExec_t& gx = r->gexec[adjoint ? 1 : 0];
     if (!gx) {
       cudaGraph_t g;
-      CK(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
-      for (int s = 0; s < K; ++s) {
-        a.s = s;
-        launch_forces(a, adjoint, r->stream);
-        launch_boundary(a, adjoint, r->stream);
-        launch_points(a, r->stream);
-        launch_update(a, adjoint, r->stream);
+      const int G = chain_groups(r);
+      if (G > 1) {
+        int rc = ensure_chains(r, G);
+        if (rc) return rc;
       }
+      CK(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
+      if (G > 1) {
+        CK(cudaEventRecord(r->chain_ev[0], r->stream));
+        for (int c = 1; c < G; ++c) CK(cudaStreamWaitEvent(r->chain_st[c - 1], r->chain_ev[0], 0));
+      }
+      for (int c = 0; c < G; ++c) {
+        cudaStream_t st = c == 0 ? r->stream : r->chain_st[c - 1];
+        StepArgs ac = G > 1 ? group_args(r, a, c) : a;
+        for (int s = 0; s < K; ++s) {
+          ac.s = s;
+          launch_forces(ac, adjoint, st);
+          launch_boundary(ac, adjoint, st);
+          launch_points(ac, st);
+          launch_update(ac, adjoint, st);
+        }
+      }
+      if (G > 1)
+        for (int c = 1; c < G; ++c) {
+          CK(cudaEventRecord(r->chain_ev[c], r->chain_st[c - 1]));
+          CK(cudaStreamWaitEvent(r->stream, r->chain_ev[c], 0));
+        }
       launch_advance(r->lanes.p, r->nev, K, r->stream);
       cudaError_t ce = cudaStreamEndCapture(r->stream, &g);
       if (ce != cudaSuccess) return fail(SEM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
@@ -1369,7 +1436,7 @@ static int run_loop(sem_run* r, bool adjoint) {
         return fail(SEM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
     }
     const int nlaunch = (r->nstep + K - 1) / K;
-    const int per_step = (r->mesh->nf > 0 ? 4 : 3);
+    const int per_step = (r->mesh->nf > 0 ? 4 : 3) * chain_groups(r);
     const int ce = r->cfg.check_every;
     const bool ring = r->ring() && (adjoint || save);
     for (int g = 0; g < nlaunch; ++g) {

@@ -123,6 +123,7 @@ struct StepArgs {
   int ngmap;
   int inject;            // some lane has an FK injection (LaneDesc::inj_v)
   int sm_limit;          // SMs the persistent element kernels may fill (0: all)
+  int ring_nev;          // lanes of the whole run: the boundary-store ring's slot pitch
   __device__ __forceinline__ size_t fi(size_t ig, int c, int lg) const {
     return lm.f(ig, c, lg, (size_t)m.nglob);
   }

@@ -3655,11 +3655,11 @@ __global__ void __launch_bounds__(128) k_stacey(StepArgs A) {
   }
   if (A.store_fp16) __syncthreads();
   // row of record n in the lane's store (resident: n; ring: its chunk's
-  // device slot, slots nev * ring_c rows apart)
+  // device slot, slots ring_nev * ring_c rows apart)
   auto row_of = [&](int n) -> size_t {
     if (L->ring_c <= 0) return (size_t)n;
     const int c = L->ring_c;
-    return (size_t)((n / c) % L->ring_d) * (size_t)nev * c + (size_t)(n % c);
+    return (size_t)((n / c) % L->ring_d) * (size_t)A.ring_nev * c + (size_t)(n % c);
   };
   if (valid && save) {
     const size_t row = row_of(it);
@@ -3808,11 +3808,13 @@ __global__ void __launch_bounds__(128) k_points(StepArgs A) {
 // Newmark corrector (this step) + predictor (next step)
 // ---------------------------------------------------------------------------
 
-// One thread per (point, lane), lanes of a group fastest.  HESS: also
-// accumulate the approximate Hessian (a separate instantiation, so that the
-// plain adjoint update keeps its code).
+// One thread per (point, lane), lanes of a group fastest, in 128-thread
+// blocks.  HESS: also accumulate the approximate Hessian (a separate
+// instantiation, so that the plain adjoint update keeps its code).
+constexpr int kUpdThreads = 128;
+
 template <bool ADJ, bool HESS = false>
-__global__ void __launch_bounds__(256) k_update(StepArgs A) {
+__global__ void __launch_bounds__(kUpdThreads) k_update(StepArgs A) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nev = A.nev;
   const int lwlog = A.lm.lwlog;
@@ -3894,13 +3896,16 @@ int launch_update(const StepArgs& a, bool adj, cudaStream_t st) {
   const size_t ng = a.gmap ? (size_t)a.ngmap : (size_t)((a.nev + lw - 1) / lw);
   const size_t n = (size_t)a.m.nglob * ng * lw;
   if (n == 0) return 0;
-  const unsigned blocks = (unsigned)((n + 255) / 256);
+  // 128-thread blocks fit beside two resident blocks of the adjoint element
+  // kernel, so the update of one lane group can run under another group's
+  // element kernel
+  const unsigned blocks = (unsigned)((n + kUpdThreads - 1) / kUpdThreads);
   if (adj && a.k.hess_glob)
-    k_update<true, true><<<blocks, 256, 0, st>>>(a);
+    k_update<true, true><<<blocks, kUpdThreads, 0, st>>>(a);
   else if (adj)
-    k_update<true><<<blocks, 256, 0, st>>>(a);
+    k_update<true><<<blocks, kUpdThreads, 0, st>>>(a);
   else
-    k_update<false><<<blocks, 256, 0, st>>>(a);
+    k_update<false><<<blocks, kUpdThreads, 0, st>>>(a);
   return 1;
 }
 
