@@ -39,6 +39,13 @@
  *     post_processing.f90:333-372, zprecond.f90:34-71  sem_depth_precond
  *   smooth_sem_pde                                    sem_smooth_pde
  *     src/postproc/smooth.f90:7-437
+ *   gll2grid (Project_model_SEM2FD_grid)              sem_grid_project
+ *     src/grid/model_grid_data.f90:183-198,
+ *     src/shared/projection_on_FD_grid_mod_fwat.f90:186-596,935-1125
+ *   PostFlow%taper_kernel_grid (taper_cls)            sem_grid_taper
+ *     src/postproc/post_processing.f90:283-325, taper_3D_mod.f90
+ *   zprecond_grid                                     sem_grid_zprecond
+ *     src/postproc/zprecond.f90:73-100
  *
  * Conventions
  *  - Every function returns SEM_OK (0) or a negative sem_status; the reason
@@ -522,6 +529,52 @@ int sem_hessian_precond(const double *hess_sum, long long n, int precond_type,
  * [zlev[0], zlev[nz-1]] take the end values.  precond[nspec][125]. */
 int sem_depth_precond(sem_mesh *mesh, const double *zlev, int nz, int precond_type,
                       int nevents, float *precond);
+
+/* Regular model grid of the kernels: points x0[d] + i h[d], i < n[d],
+ * grid arrays [nx][ny][nz] (z fastest, the C view of the reference's
+ * Fortran (nz, ny, nx) arrays).  ngnod: anchor nodes of the mesher's
+ * elements (8 or 27), used to locate grid points in irregular elements. */
+typedef struct {
+  double x0[3];
+  double h[3];
+  int n[3];
+  int ngnod;
+} sem_grid_desc;
+
+/* Projection of element fields onto the grid (gll2grid), on the device in
+ * FP64: a grid point belongs to the first element (lowest index) whose
+ * candidate index range, from its GLL points' bounding box with the
+ * reference's truncation, holds it; its value is that element's 5x5x5
+ * Lagrange interpolant at the point's reference coordinates, clamped to
+ * [-1, 1] (affine elements: linear in the box; irregular elements: the
+ * reference locator's start at the nearest interior GLL node and four
+ * Newton steps on the anchor nodes).  Points no element takes are 0.
+ * fields[nfield][nspec][125] FP32, out[nfield][nx][ny][nz] FP32. */
+int sem_grid_project(sem_mesh *mesh, const sem_grid_desc *grid, int nfield,
+                     const float *fields, float *out);
+
+/* Taper widths of taper_kernel_grid (m): zero for *_suppress from the
+ * sides (h) and the bottom (v), a half cosine over the next *_buffer,
+ * one inside; no taper at the surface. */
+typedef struct {
+  double h_suppress, h_buffer, v_suppress, v_buffer;
+} sem_grid_taper_cfg;
+
+/* taper_kernel_grid on the device: the mask lives on a grid of spacing
+ * (smallest + largest GLL point distance) / 2 over the mesh's extent and is
+ * interpolated trilinearly at the grid points (0 outside its box);
+ * grid_fields[nfield][nx][ny][nz] are multiplied by it in place, and mask
+ * (may be null) receives it [nx][ny][nz] in FP64.  nfield may be 0 when
+ * mask is given.  Widths beyond half the mesh are refused (SEM_ERR_ARG). */
+int sem_grid_taper(sem_mesh *mesh, const sem_grid_desc *grid, const sem_grid_taper_cfg *taper,
+                   int nfield, float *grid_fields, double *mask);
+
+/* zprecond_grid on the device: the depth preconditioner, precond_type 2
+ * (1/|z|) or 3 (1/sqrt|z|), of the levels zlev[nz] (NULL: the grid's
+ * x0[2] + k h[2]) for nevents events, normalised, inverted, normalised,
+ * repeated over x and y: out[nx][ny][nz] FP32. */
+int sem_grid_zprecond(const sem_grid_desc *grid, const double *zlev, int precond_type,
+                      int nevents, float *out);
 
 /* FP32 FMA throughput of the current device in TFLOP/s (an FMA counts
  * as 2 flops), the best of 5 timed launches of independent fmaf chains on

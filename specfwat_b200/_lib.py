@@ -40,6 +40,7 @@ EXPORTS = (
     "sem_smooth_pde", "sem_measure_waveform", "sem_measure_waveform_dev",
     "sem_set_approximate_hessian", "sem_save_hessian_kernel", "sem_sum_hessian",
     "sem_hessian_precond", "sem_depth_precond", "sem_set_injection",
+    "sem_grid_project", "sem_grid_taper", "sem_grid_zprecond",
 )
 MEAS_MAX_BANDS = 4
 SMOOTH_MAP_CUBE = 0
@@ -116,6 +117,16 @@ class SmoothStats(C.Structure):
                 ("distance_min", C.c_double), ("step_ms", C.c_double)]
 
 
+class GridDesc(C.Structure):
+    _fields_ = [("x0", C.c_double * 3), ("h", C.c_double * 3), ("n", C.c_int * 3),
+                ("ngnod", C.c_int)]
+
+
+class GridTaperCfg(C.Structure):
+    _fields_ = [("h_suppress", C.c_double), ("h_buffer", C.c_double),
+                ("v_suppress", C.c_double), ("v_buffer", C.c_double)]
+
+
 _lib = None
 
 
@@ -189,6 +200,10 @@ def load():
         "sem_mark_done": (C.c_int, [vp, C.c_longlong, ip]),
         "sem_mark_elapsed": (C.c_int, [vp, C.c_longlong, C.c_longlong,
                                        C.POINTER(C.c_double)]),
+        "sem_grid_project": (C.c_int, [vp, C.POINTER(GridDesc), ip, fp, fp]),
+        "sem_grid_taper": (C.c_int, [vp, C.POINTER(GridDesc), C.POINTER(GridTaperCfg), ip,
+                                     fp, fp]),
+        "sem_grid_zprecond": (C.c_int, [C.POINTER(GridDesc), fp, ip, ip, fp]),
         "sem_store_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int), C.POINTER(C.c_longlong),
                                      C.POINTER(C.c_longlong)]),

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsem_b200.so")
 SOURCES = ["sem_api.cu", "sem_kernels.cu", "sem_noalloc.cu", "sem_probe.cu", "sem_smooth.cu",
-           "sem_measure.cu", "sem_precond.cu"]
+           "sem_measure.cu", "sem_precond.cu", "sem_grid.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -113,14 +113,15 @@ def gradient_on_grid(mesh, db, kernels6, x0, h, n, sigma_h, sigma_v, *, precond=
        [6, nspec, 5, 5, 5] (``Simulation.sum_kernels`` order);
     2. times ``precond`` [nspec, 5, 5, 5] when given (``apply_precond``);
     3. each smoothed on the device (``pde_smooth``: ``smooth_sem_pde``) and
-       projected onto the grid ``x0 + i h``, i < n (``gll2grid``); with
-       ``rho_scaling`` the rhop grid is the beta grid times 0.33 instead
-       (USE_RHO_SCALING, post_processing.f90:262-264);
-    4. times the boundary taper when ``taper`` = (h_suppress, h_buffer,
-       v_suppress, v_buffer) is given (``taper_kernel_grid``).
+       projected onto the grid ``x0 + i h``, i < n, on the device
+       (``gll2grid``); with ``rho_scaling`` the rhop grid is the beta grid
+       times 0.33 instead (USE_RHO_SCALING, post_processing.f90:262-264);
+    4. times the boundary taper, on the device, when ``taper`` =
+       (h_suppress, h_buffer, v_suppress, v_buffer) is given
+       (``taper_kernel_grid``).
 
-    Returns [3, nx, ny, nz] in KERNEL_ISO order.  ``smooth`` replaces the
-    device smoother (a function of [nfield, nspec, 5, 5, 5] arrays)."""
+    Returns [3, nx, ny, nz] FP32 in KERNEL_ISO order.  ``smooth`` replaces
+    the device smoother (a function of [nfield, nspec, 5, 5, 5] arrays)."""
     from .postgrid import gll2grid, taper_kernel_grid
     k6 = np.asarray(kernels6, np.float64)
     ker = np.stack([k6[_SIX.index(k)] for k in KERNEL_ISO])
@@ -132,12 +133,12 @@ def gradient_on_grid(mesh, db, kernels6, x0, h, n, sigma_h, sigma_v, *, precond=
             return smooth_sem_pde(mesh, d, sigma_h, sigma_v)[0]
     sm = np.asarray(smooth(ker[:nsm].astype(np.float32)), np.float64).reshape(
         (nsm,) + ker.shape[1:])
-    grid = [gll2grid(db, sm[i], x0, h, n, ngnod) for i in range(nsm)]
+    grid = list(gll2grid(mesh, sm, x0, h, n, ngnod))
     if rho_scaling:
         grid.append(grid[1] * np.float32(RHO_SCALING_FAC))
     grid = np.stack(grid)
     if taper is not None:
-        grid, _ = taper_kernel_grid(db, grid, x0, h, n, *taper)
+        grid, _ = taper_kernel_grid(mesh, grid, x0, h, n, *taper)
     return grid
 
 
@@ -147,10 +148,11 @@ def hessian_on_grid(mesh, db, hess_sum, x0, h, n, sigma_h, sigma_v, precond_type
     the preconditioner on the model grid, normalised to a maximum of 1.
 
     - PRECOND_TYPE 0 and 1: ``invert_hess`` of the event-summed Hessian
-      (``hessian_precond``, on the device), smoothed on the device,
-      projected onto the grid and divided by its largest magnitude;
-    - PRECOND_TYPE 2 and 3: ``zprecond_grid`` on the grid's depth levels
-      ``zgrid`` (defaults to ``x0[2] + k h[2]``) for ``nevents`` events.
+      (``hessian_precond``), smoothed, projected onto the grid (all three
+      on the device) and divided by its largest magnitude;
+    - PRECOND_TYPE 2 and 3: ``zprecond_grid`` (on the device) on the
+      grid's depth levels ``zgrid`` (defaults to ``x0[2] + k h[2]``) for
+      ``nevents`` events.
 
     ``smooth`` replaces the device smoother."""
     from .postgrid import gll2grid, zprecond_grid
@@ -162,6 +164,6 @@ def hessian_on_grid(mesh, db, hess_sum, x0, h, n, sigma_h, sigma_v, precond_type
     if smooth is None:
         def smooth(d):
             return smooth_sem_pde(mesh, d, sigma_h, sigma_v)[0]
-    sm = np.asarray(smooth(inv.reshape(db.nspec, 5, 5, 5)), np.float64)
-    gm = gll2grid(db, sm, x0, h, n, ngnod).astype(np.float64)
+    sm = np.asarray(smooth(inv.reshape(db.nspec, 5, 5, 5)), np.float32)
+    gm = gll2grid(mesh, sm, x0, h, n, ngnod).astype(np.float64)
     return (gm / np.abs(gm).max()).astype(np.float32)

@@ -121,7 +121,7 @@ def test_bad_arguments(gpu):
 def test_gradient_on_grid_with_the_device_smoother(gpu):
     """The post-processing chain through the device smoother: each kernel's
     grid equals the oracle-smoothed kernel projected the same way."""
-    from specfwat_b200.postgrid import gll2grid
+    from oracle.postgrid import gll2grid
     from specfwat_b200.postproc import gradient_on_grid
     db = box_db(5, 4, 3)
     mesh = S.Mesh(db)
@@ -141,7 +141,7 @@ def test_hessian_on_grid(gpu):
     """sum_precond on the device: invert, smooth, project, normalise; and the
     depth forms on the grid."""
     from oracle import oracle as O
-    from specfwat_b200.postgrid import gll2grid, zprecond_grid
+    from oracle.postgrid import gll2grid, zprecond_grid
     from specfwat_b200.postproc import hessian_on_grid
     db = box_db(5, 4, 3)
     mesh = S.Mesh(db)
@@ -156,7 +156,8 @@ def test_hessian_on_grid(gpu):
     assert np.abs(g).max() == pytest.approx(1.0)
     assert rel(g, gr) < 1e-4
     z = hessian_on_grid(mesh, db, None, x0, h, n, 0.0, 0.0, 2, nevents=4)
-    assert np.array_equal(z, zprecond_grid(x0[2] + np.arange(n[2]) * h[2], n[0], n[1], 2, 4))
+    zref = zprecond_grid(x0[2] + np.arange(n[2]) * h[2], n[0], n[1], 2, 4)
+    assert z.shape == zref.shape and np.abs(z - zref).max() <= 1e-7
     mesh.close()
 
 

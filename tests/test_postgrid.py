@@ -1,4 +1,6 @@
-"""Kernels on the model grid: ``specfwat_b200.postgrid``.
+"""Kernels on the model grid: the CPU restatement ``oracle.postgrid``
+that the device's ``sem_grid_*`` entry points are checked against
+(``tests/test_gpu_grid.py``), pinned here to the reference's loops.
 
 - ``gll2grid`` equals a line-by-line transcription of the reference's
   projection loop (first element wins, locator coordinates clamped to the
@@ -20,8 +22,8 @@ import numpy as np
 import pytest
 
 from specfwat_b200 import database as D
-from specfwat_b200.postgrid import (Taper3D, create_taper, gll2grid, mesh_distances,
-                                    taper_kernel_grid)
+from oracle.postgrid import (Taper3D, create_taper, gll2grid, mesh_distances,
+                             taper_kernel_grid)
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import fortran_literal as F  # noqa: E402
@@ -173,7 +175,7 @@ def test_mesh_distances_and_taper_kernel_grid():
 
 @pytest.mark.parametrize("ptype", [2, 3])
 def test_zprecond_grid_matches_literal(ptype):
-    from specfwat_b200.postgrid import zprecond_grid
+    from oracle.postgrid import zprecond_grid
     zg = np.linspace(-30000.0, 2000.0, 17)
     ours = zprecond_grid(zg, 4, 3, ptype, 6)
     zl = np.array(F.get_1d_precond(zg, ptype), np.float32)
@@ -187,34 +189,3 @@ def test_zprecond_grid_matches_literal(ptype):
     assert np.all(np.diff(ours[0, 0][zg < 0]) < 0)
     with pytest.raises(ValueError):
         zprecond_grid(zg, 2, 2, 1, 1)
-
-
-def test_gradient_on_grid_chain():
-    """The order of fwat_post_proc: precondition, smooth, project, scale
-    rhop from beta, taper (the smoother replaced by a stand-in here)."""
-    from specfwat_b200.postproc import RHO_SCALING_FAC, gradient_on_grid
-    db = D.make_box(D.BoxSpec(4, 4, 2, h=2000.0))
-    rng = np.random.default_rng(8)
-    k6 = rng.standard_normal((6, db.nspec, 5, 5, 5))
-    pre = rng.uniform(0.5, 1.5, (db.nspec, 5, 5, 5))
-    x0, h, n = (0.0, 0.0, -4000.0), (500.0, 500.0, 500.0), (17, 17, 9)
-    calls = []
-
-    def half(d):                      # stand-in smoother: records and halves
-        calls.append(d.shape)
-        return 0.5 * d
-
-    g = gradient_on_grid(None, db, k6, x0, h, n, 1.0, 1.0, precond=pre, smooth=half)
-    assert calls == [(3, db.nspec, 5, 5, 5)]
-    for i, k in enumerate((5, 4, 3)):                 # alpha, beta, rhop
-        ref = gll2grid(db, 0.5 * k6[k] * pre, x0, h, n)
-        assert np.allclose(g[i], ref, rtol=1e-5, atol=1e-6)
-    calls.clear()
-    tap = (500.0, 1000.0, 500.0, 1000.0)
-    g2 = gradient_on_grid(None, db, k6, x0, h, n, 1.0, 1.0, rho_scaling=True, taper=tap,
-                          smooth=half)
-    assert calls == [(2, db.nspec, 5, 5, 5)]
-    beta = gll2grid(db, 0.5 * k6[4], x0, h, n)
-    _, mask = taper_kernel_grid(db, np.ones((1,) + n), x0, h, n, *tap)
-    assert np.allclose(g2[1], beta * mask, rtol=1e-5, atol=1e-6)
-    assert np.allclose(g2[2], beta * np.float32(RHO_SCALING_FAC) * mask, rtol=1e-5, atol=1e-6)
