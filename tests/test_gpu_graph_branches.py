@@ -4,9 +4,10 @@ With graphs, a batch of more than 8 events captures each lane group's steps
 as a branch of its own, with every per-lane array offset to the group's
 block of the lane-group layout. The same batch launched step by step
 runs on one stream over all lanes. The two must agree for every lane:
-- a group handed the wrong block of the fields, the kernel accumulators
-  or the lane table breaks its lanes by far more than the order of the
-  atomic scatter-adds does (about 1e-6 relative between two runs);
+- a group handed the wrong block of the fields, the kernel or Hessian
+  accumulators or the lane table breaks its lanes by far more than the
+  order of the atomic scatter-adds does (about 1e-6 relative between two
+  runs);
 - a partly filled last group must not touch lanes past the batch.
 
 Distinct events per lane, so that lanes of different groups cannot stand in
@@ -35,11 +36,13 @@ def _batch(mesh, rec, srcs, obs, nstep, graph, variant):
     seis = [sim.seismograms(e) for e in range(nev)]
     for e in range(nev):
         sim.measure_l2(e, obs[e])
+    sim.set_approximate_hessian()
     sim.iterate_time(3)
     kern = [sim.save_adjoint_kernels(e) for e in range(nev)]
+    hess = [sim.hessian_kernel(e) for e in range(nev)]
     ksum = sim.sum_kernels()
     sim.close()
-    return seis, kern, ksum
+    return seis, kern, ksum, hess
 
 
 @pytest.mark.parametrize("nev,variant", [(20, 11), (17, 5)])
@@ -54,13 +57,14 @@ def test_group_branches_match_step_launches(gpu, nev, variant):
     nstep = 260  # not a multiple of the 50-step graph
     obs = [1e-5 * rng.standard_normal((len(rec), 3, nstep)) for _ in range(nev)]
     mesh = S.Mesh(db)
-    s0, k0, sum0 = _batch(mesh, rec, srcs, obs, nstep, False, variant)
-    s1, k1, sum1 = _batch(mesh, rec, srcs, obs, nstep, True, variant)
+    s0, k0, sum0, h0 = _batch(mesh, rec, srcs, obs, nstep, False, variant)
+    s1, k1, sum1, h1 = _batch(mesh, rec, srcs, obs, nstep, True, variant)
     mesh.close()
     for e in range(nev):
         assert rel(s1[e], s0[e]) < 1e-5, (e, rel(s1[e], s0[e]))
         for q in range(6):
             assert rel(k1[e][q], k0[e][q]) < 1e-4, (e, q, rel(k1[e][q], k0[e][q]))
+        assert rel(h1[e], h0[e]) < 1e-4, (e, rel(h1[e], h0[e]))
     for q in range(6):
         assert rel(sum1[q], sum0[q]) < 1e-4
     # the lanes are distinct events: no two of them carry the same kernel
