@@ -632,6 +632,7 @@ int sem_device_info(int* sm_count, long long* hbm_bytes, int* cc_major, int* cc_
 }
 
 int sem_prepare_mesh(const sem_mesh_desc* d, sem_mesh** out) {
+  NvtxPhase ph("sem_prepare_mesh");
   if (!d || !out) return fail(SEM_ERR_ARG, "null argument");
   *out = nullptr;
   if (d->nspec <= 0 || d->nglob <= 0) return fail(SEM_ERR_ARG, "nspec and nglob must be > 0");
@@ -904,6 +905,7 @@ long long sem_run_bytes(const sem_mesh* m, const sem_run_cfg* c) {
 }
 
 int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
+  NvtxPhase ph("sem_prepare_timerun");
   if (!m || !out) return fail(SEM_ERR_ARG, "null argument");
   *out = nullptr;
   int rc = validate_cfg(c);
@@ -926,7 +928,7 @@ int sem_prepare_timerun(sem_mesh* m, const sem_run_cfg* c, sem_run** out) {
   r->dt = c->dt;
   r->nrec_max = c->max_receivers;
   // SEM_FORCE_VARIANTS="f,a" pins the autotuned element-kernel variants
-  // (public numbering 1..6) for the forward and adjoint phases, so that a
+  // (public numbering 1..15) for the forward and adjoint phases, so that a
   // profiler run replays the choice made by an unprofiled run.
   if (c->kernel_variant == 0) {
     const char* fv = std::getenv("SEM_FORCE_VARIANTS");
@@ -1494,6 +1496,7 @@ static int run_loop(sem_run* r, bool adjoint) {
 }
 
 int sem_iterate_time(sem_run* r, int sim_type, int save_forward) {
+  NvtxPhase ph(sim_type == 3 ? "sem_iterate_time adjoint" : "sem_iterate_time forward");
   if (!r) return fail(SEM_ERR_ARG, "null run");
   if (r->lanes_mode)
     return fail(SEM_ERR_STATE, "run is driven lane by lane (sem_lane_*); use sem_advance");
@@ -1694,6 +1697,7 @@ int sem_set_observed(sem_run* r, int ev, const double* obs) {
 
 int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int taper_type,
                    double* misfit) {
+  NvtxPhase ph("sem_measure_l2");
   if (!r) return fail(SEM_ERR_ARG, "null run");
   if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
   if (!(taper_pct >= 0.0 && taper_pct <= 1.0))
@@ -1734,6 +1738,7 @@ int sem_measure_l2(sem_run* r, int ev, const double* obs, double taper_pct, int 
 int sem_measure_waveform(sem_run* r, int ev, const sem_meas_cfg* cfg, const double* obs,
                          const double* windows, const double* baz, double* misfit_band,
                          double* misfit_trace) {
+  NvtxPhase ph("sem_measure_waveform");
   if (!r || !cfg || !obs || !windows) return fail(SEM_ERR_ARG, "null argument");
   if (ev < 0 || ev >= r->nev) return fail(SEM_ERR_ARG, "event %d out of range", ev);
   if (cfg->rotate && !baz) return fail(SEM_ERR_ARG, "rotate needs the back-azimuths");
@@ -1807,6 +1812,7 @@ int sem_save_adjoint_kernels(sem_run* r, int ev, double* out) {
 }
 
 int sem_sum_kernels(sem_run* r, double* out) {
+  NvtxPhase ph("sem_sum_kernels");
   if (!r || !out) return fail(SEM_ERR_ARG, "null argument");
   if (!r->adj_done) return fail(SEM_ERR_STATE, "no adjoint run has completed");
   const size_t ne = (size_t)r->mesh->nspec * NGLL3;
@@ -1823,6 +1829,7 @@ int sem_sum_kernels(sem_run* r, double* out) {
 }
 
 int sem_sum_kernels_device(sem_run* r, double* dev_out) {
+  NvtxPhase ph("sem_sum_kernels_device");
   if (!r || !dev_out) return fail(SEM_ERR_ARG, "null argument");
   if (!r->adj_done) return fail(SEM_ERR_STATE, "no adjoint run has completed");
   const size_t ne = (size_t)r->mesh->nspec * NGLL3;
@@ -2383,6 +2390,7 @@ static void consume_check(sem_run* r) {
 }
 
 int sem_advance(sem_run* r, int nsteps) {
+  NvtxPhase ph("sem_advance");
   if (!r || nsteps < 1) return fail(SEM_ERR_ARG, "bad argument");
   if (!r->lanes_mode) return fail(SEM_ERR_STATE, "no lane has been started");
   if (r->cfg.check_every > 0) consume_check(r);

@@ -504,6 +504,7 @@ using namespace sem;
 
 extern "C" int sem_grid_project(sem_mesh* mesh, const sem_grid_desc* grid, int nfield,
                                 const float* fields, float* out) {
+  NvtxPhase ph("sem_grid_project");
   if (!mesh || !fields || !out) return report_error(SEM_ERR_ARG, "null argument");
   if (nfield < 1 || nfield > 64) return report_error(SEM_ERR_ARG, "nfield must be in [1, 64]");
   GridGeom g{};
@@ -541,6 +542,7 @@ extern "C" int sem_grid_project(sem_mesh* mesh, const sem_grid_desc* grid, int n
 extern "C" int sem_grid_taper(sem_mesh* mesh, const sem_grid_desc* grid,
                               const sem_grid_taper_cfg* taper, int nfield, float* grid_fields,
                               double* mask) {
+  NvtxPhase ph("sem_grid_taper");
   if (!mesh || !taper || (!grid_fields && nfield > 0) || (!mask && nfield == 0))
     return report_error(SEM_ERR_ARG, "null argument");
   if (nfield < 0 || nfield > 64) return report_error(SEM_ERR_ARG, "nfield must be in [0, 64]");

@@ -3,6 +3,7 @@
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstddef>
 #include <cstdint>
@@ -215,5 +216,15 @@ int mesh_smooth_view(const ::sem_mesh_s* m, SmoothMeshView* out);
 
 // Sets the per-thread error message returned by sem_last_error().
 int report_error(int code, const char* fmt, ...);
+
+// NVTX range over one C-ABI call (what a profiler's timeline shows as the
+// phase: forward run, measurement, kernel sum, smoothing, ...); a no-op
+// unless a profiler is attached.
+struct NvtxPhase {
+  explicit NvtxPhase(const char* name) { nvtxRangePushA(name); }
+  ~NvtxPhase() { nvtxRangePop(); }
+  NvtxPhase(const NvtxPhase&) = delete;
+  NvtxPhase& operator=(const NvtxPhase&) = delete;
+};
 
 }  // namespace sem

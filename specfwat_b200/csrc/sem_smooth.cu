@@ -349,6 +349,7 @@ using namespace sem;
 extern "C" int sem_smooth_pde(sem_mesh* mesh, const sem_smooth_cfg* cfg, int nfield,
                               const float* dat_in, const int* is_cpml, float* dat_out,
                               sem_smooth_stats* stats) {
+  NvtxPhase ph("sem_smooth_pde");
   if (!mesh || !cfg || !dat_in || !dat_out) return report_error(SEM_ERR_ARG, "null argument");
   if (nfield < 1) return report_error(SEM_ERR_ARG, "nfield must be >= 1");
   if (!(cfg->sigma_h >= 0.0) || !(cfg->sigma_v >= 0.0))
