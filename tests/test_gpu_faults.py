@@ -3,8 +3,8 @@ stays usable after each.
 
 - The mesh upload refuses a corrupt ibool, a non-finite or negative
   material, a zero density and a non-positive mass point (SEM_ERR_ARG).
-- A run larger than the device is refused with SEM_ERR_NOMEM: the first
-  wavefield array alone exceeds the device.
+- A run larger than the device is refused with SEM_ERR_NOMEM when its
+  wavefields are allocated, and what was allocated is released.
 - Malformed requests are refused before any launch (SEM_ERR_ARG):
   - an event index past the batch;
   - more receivers than the run holds;
@@ -77,7 +77,7 @@ def test_run_larger_than_the_device_is_refused(gpu):
     import torch
     db = D.build("medium")
     mesh = S.Mesh(db)
-    nev = 8192       # one wavefield array of 8192 events: 206 GB
+    nev = 4096       # the run's limit; its three forward fields alone take 309 GB
     cfg = _lib.RunCfg(nev, 4000, 0.02, _lib.SEM_STORE_FP16, 1, 50, 4, 0, 0)
     need = _lib.load().sem_run_bytes(mesh.handle, C.byref(cfg))
     _, total = torch.cuda.mem_get_info()
