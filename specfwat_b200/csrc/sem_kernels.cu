@@ -3431,16 +3431,20 @@ static void forces_vec_cfg(const StepArgs& a, cudaStream_t st) {
 //   displacement prefetched into registers, 10 forward phase with 2 events
 //   per thread and register prefetch (8 events per block).
 int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
+  // the kernel follows the wavefield layout, not the lane count: a lane
+  // group of a batch (lane-group layout) that holds one event still takes
+  // the batch's kernels, whose lanes past the batch are idle
+  const bool batched = a.lm.lwlog != 0;
   if (a.m.geo) {
     // a mesh with irregular elements: the register-prefetch kernels with
     // the general mapping (variant 10, batched), else the thread-per-point
     // kernel with the general mapping
-    if (a.variant == 10 && a.nev > 1) {
+    if (a.variant == 10 && batched) {
       if (!adj) return forces_fwd_r_cfg<8, false, true>(a, st);
       forces_adjpair_r_cfg<8, true>(a, st);
       return 1;
     }
-    if (a.nev == 1) {
+    if (!batched) {
       if (adj)
         forces_cfg<1, 128, true, true>(a, st);
       else
@@ -3454,28 +3458,28 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
     return 1;
   }
   if (a.variant == 12 && !a.gmap) return adj ? forces_shfl_cfg<true>(a, st) : forces_shfl_cfg<false>(a, st);
-  if (a.variant == 10 && a.nev > 1) {
+  if (a.variant == 10 && batched) {
     if (!adj) return forces_fwd_r_cfg<8, false>(a, st);
     forces_adjpair_r_cfg<8>(a, st);
     return 1;
   }
-  if (a.variant == 11 && a.nev > 1) {
+  if (a.variant == 11 && batched) {
     if (!adj) return a.m.ncolour > 0 ? forces_fwd_r_cfg<8, true>(a, st)
                                      : forces_fwd_r_cfg<8, false>(a, st);
     forces_adjpair_r_cfg<8>(a, st);
     return 1;
   }
-  if (a.variant == 13 && a.nev > 1) {
+  if (a.variant == 13 && batched) {
     if (!adj) return forces_fwd_r_cfg<8, false>(a, st);
     forces_adjpair_r3_cfg(a, st);
     return 1;
   }
-  if (a.variant == 14 && a.nev > 1) {
+  if (a.variant == 14 && batched) {
     if (!adj) return forces_fwd_r5_cfg(a, st);
     forces_adjpair_r_cfg<8>(a, st);
     return 1;
   }
-  if ((a.variant >= 6 && a.variant <= 9) && a.nev > 1) {
+  if ((a.variant >= 6 && a.variant <= 9) && batched) {
     if (!adj)
       forces_vec_cfg<8, 2, false>(a, st);
     else if (a.variant == 6)
@@ -3488,21 +3492,21 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
       forces_adjpair_r_cfg<8>(a, st);
     return 1;
   }
-  if (a.variant == 4 && a.nev > 1) {
+  if (a.variant == 4 && batched) {
     if (adj)
       forces_vec_cfg<4, 2, true>(a, st);
     else
       forces_vec_cfg<8, 2, false>(a, st);
     return 1;
   }
-  if (a.variant == 5 && a.nev > 1) {
+  if (a.variant == 5 && batched) {
     if (adj)
       forces_vec_cfg<8, 2, true>(a, st);
     else
       forces_vec_cfg<8, 4, false>(a, st);
     return 1;
   }
-  if (a.variant == 3 && a.nev > 1) {
+  if (a.variant == 3 && batched) {
     if (adj)
       forces_piped_cfg<2, 2, 25, true>(a, st);
     else
@@ -3510,7 +3514,7 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
     return 1;
   }
   if (a.variant == 2 || a.variant == 3) {
-    if (a.nev == 1) {
+    if (!batched) {
       if (adj)
         forces_piped_cfg<1, 4, 32, true>(a, st);
       else
@@ -3529,7 +3533,7 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
     return 1;
   }
   if (a.variant == 1) {
-    if (a.nev == 1) {
+    if (!batched) {
       if (adj)
         forces_pencil_cfg<1, 5, true>(a, st);
       else
@@ -3547,7 +3551,7 @@ int launch_forces(const StepArgs& a, bool adj, cudaStream_t st) {
     }
     return 1;
   }
-  if (a.nev == 1) {
+  if (!batched) {
     if (adj)
       forces_cfg<1, 128, true>(a, st);
     else

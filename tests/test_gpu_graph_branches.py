@@ -8,7 +8,9 @@ runs on one stream over all lanes. The two must agree for every lane:
   accumulators or the lane table breaks its lanes by far more than the
   order of the atomic scatter-adds does (about 1e-6 relative between two
   runs);
-- a partly filled last group must not touch lanes past the batch.
+- a partly filled last group must not touch lanes past the batch, and a
+  last group of one event still runs the batch's kernels (variants 2 and 3
+  have separate one-event kernels for the one-event layout).
 
 Distinct events per lane, so that lanes of different groups cannot stand in
 for one another.
@@ -45,7 +47,7 @@ def _batch(mesh, rec, srcs, obs, nstep, graph, variant):
     return seis, kern, ksum, hess
 
 
-@pytest.mark.parametrize("nev,variant", [(20, 11), (17, 5)])
+@pytest.mark.parametrize("nev,variant", [(20, 11), (17, 5), (17, 3), (9, 2)])
 def test_group_branches_match_step_launches(gpu, nev, variant):
     db = D.build("mini")
     rec = D.surface_receivers(db.box, 3)
