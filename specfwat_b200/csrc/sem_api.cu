@@ -1350,7 +1350,6 @@ static int ring_after(sem_run* r, bool adjoint, int g, bool save) {
   return SEM_OK;
 }
 
-// Queue the step loop of one phase (graphs or per-step launches).
 // Step arguments of lane group g (lanes 8g .. 8g+7) of a batched run as a
 // run of its own: every per-lane array starts at the group's block of the
 // lane-group layout, so the kernels see lanes 0..7 of one group.
@@ -1393,6 +1392,7 @@ static int ensure_chains(sem_run* r, int G) {
   return SEM_OK;
 }
 
+// Queue the step loop of one phase (graphs or per-step launches).
 static int run_loop(sem_run* r, bool adjoint) {
   long long launches = 0;
   StepArgs a = r->args(adjoint);
