@@ -88,5 +88,18 @@ def test_entry_points_take_their_python_arguments():
         lambda: L.sem_lane_finish(None, 0, f32.ctypes.data, f64.ctypes.data, None),
         lambda: L.sem_lane_status(None, 0, C.byref(i1), C.byref(i2), C.byref(i3)),
     ]
+    desc = _lib.GridDesc((C.c_double * 3)(0.0, 0.0, 0.0), (C.c_double * 3)(1.0, 1.0, 1.0),
+                         (C.c_int * 3)(2, 2, 2), 8)
+    bad = _lib.GridDesc((C.c_double * 3)(0.0, 0.0, 0.0), (C.c_double * 3)(0.0, 1.0, 1.0),
+                        (C.c_int * 3)(2, 2, 2), 8)
+    tap = _lib.GridTaperCfg(1.0, 1.0, 1.0, 1.0)
+    z = np.zeros(2)
+    calls += [
+        lambda: L.sem_grid_project(None, C.byref(desc), 1, f32.ctypes.data, f32.ctypes.data),
+        lambda: L.sem_grid_taper(None, C.byref(desc), C.byref(tap), 1, f32.ctypes.data, None),
+        lambda: L.sem_grid_zprecond(C.byref(desc), z.ctypes.data, 1, 1, f32.ctypes.data),
+        lambda: L.sem_grid_zprecond(C.byref(desc), z.ctypes.data, 2, 0, f32.ctypes.data),
+        lambda: L.sem_grid_zprecond(C.byref(bad), z.ctypes.data, 2, 1, f32.ctypes.data),
+    ]
     for k, call in enumerate(calls):
         assert call() == -1, k
