@@ -482,6 +482,8 @@ void coswin(int n, int opt, double* out) {
 // t2, one inside
 int taper_window(int n, double h, double t1, double t2, bool both, std::vector<double>& w) {
   w.assign((size_t)n, 0.0);
+  if (t1 / h > (double)n || t2 / h > (double)n)
+    return report_error(SEM_ERR_ARG, "taper widths (%g + %g m) exceed the mesh", t1, t2);
   const long long nh1 = (long long)std::floor(t1 / h), nh2 = (long long)std::floor(t2 / h);
   const long long a = nh1, b = nh1 + nh2;
   const long long c = both ? (long long)n - nh1 - nh2 : (long long)n;
