@@ -25,6 +25,24 @@ def nvcc_path():
     raise RuntimeError("nvcc not found")
 
 
+HOST_LIB = os.path.join(HERE, "host", "libspecfwat_host.so")
+
+
+def build_host(verbose: bool = False) -> str:
+    """The C++ host side (``host/prepare_fwd.cpp``, the PrepareFWD driver
+    over the C ABI) as ``host/libspecfwat_host.so``, linked against the
+    CUDA library beside it."""
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall",
+           "-I", os.path.join(ROOT, "include"),
+           os.path.join(HERE, "host", "prepare_fwd.cpp"),
+           "-L", HERE, "-l:libsem_b200.so", "-Wl,-rpath,$ORIGIN/..", "-o", HOST_LIB]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return HOST_LIB
+
+
 def build(verbose: bool = False, extra=()) -> str:
     srcs = [os.path.join(HERE, "csrc", s) for s in SOURCES]
     cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17",
@@ -35,6 +53,7 @@ def build(verbose: bool = False, extra=()) -> str:
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    build_host(verbose)
     return LIB
 
 

@@ -1,0 +1,136 @@
+// Test driver of the C++ host side: reads a case directory written by
+// tests/test_gpu_host_cpp.py, runs one PrepareFWD pass and writes the
+// results beside the inputs.
+//
+// case.txt: nspec nglob nf nev nrec nstep dt xix jac run_mode taper_pct
+// arrays (little-endian, C order): ibool.i32 [nspec*125], x/y/z.f32
+// [nglob], kappa/mu/rho/rho_vp/rho_vs.f32 [nspec*125], rmass.f32 [nglob],
+// f_ispec.i32 [nf], f_ijk.i32 [nf*75], f_jw.f32 [nf*25], f_n.f32 [nf*75],
+// sources.f64 [nev][11] (sem_source fields), stations.f64 [nrec][3],
+// obs.f64 [nev][nrec][3][nstep].
+// Writes misfits.f64, kernels.f64 [nev][6][nspec*125], sum.f64,
+// seis.f32 [nev][nrec][3][nstep] and errors.txt (the status of a refused
+// call).
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "prepare_fwd.hpp"
+
+template <class T>
+static std::vector<T> load(const std::string& dir, const std::string& name, size_t n) {
+  std::vector<T> v(n);
+  std::ifstream f(dir + "/" + name, std::ios::binary);
+  if (!f || !f.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(n * sizeof(T))))
+    throw std::runtime_error("cannot read " + name);
+  return v;
+}
+
+template <class T>
+static void save(const std::string& dir, const std::string& name, const std::vector<T>& v) {
+  std::ofstream f(dir + "/" + name, std::ios::binary);
+  f.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(T)));
+}
+
+int main(int argc, char** argv) {
+  if (argc != 2) {
+    std::cerr << "usage: run_case <case dir>\n";
+    return 2;
+  }
+  const std::string dir = argv[1];
+  try {
+    std::ifstream h(dir + "/case.txt");
+    int nspec, nglob, nf, nev, nrec, nstep, mode;
+    double dt, xix, jac, taper;
+    if (!(h >> nspec >> nglob >> nf >> nev >> nrec >> nstep >> dt >> xix >> jac >> mode >> taper))
+      throw std::runtime_error("bad case.txt");
+    const size_t ne = (size_t)nspec * 125;
+    auto ibool = load<int>(dir, "ibool.i32", ne);
+    auto x = load<float>(dir, "x.f32", nglob), y = load<float>(dir, "y.f32", nglob),
+         z = load<float>(dir, "z.f32", nglob);
+    auto kappa = load<float>(dir, "kappa.f32", ne), mu = load<float>(dir, "mu.f32", ne),
+         rho = load<float>(dir, "rho.f32", ne), rvp = load<float>(dir, "rho_vp.f32", ne),
+         rvs = load<float>(dir, "rho_vs.f32", ne);
+    auto rmass = load<float>(dir, "rmass.f32", nglob);
+    auto fisp = load<int>(dir, "f_ispec.i32", nf), fijk = load<int>(dir, "f_ijk.i32", nf * 75);
+    auto fjw = load<float>(dir, "f_jw.f32", nf * 25), fn = load<float>(dir, "f_n.f32", nf * 75);
+    auto srcs = load<double>(dir, "sources.f64", (size_t)nev * 11);
+    auto sta = load<double>(dir, "stations.f64", (size_t)nrec * 3);
+    const size_t per = (size_t)nrec * 3 * nstep;
+    auto obs = load<double>(dir, "obs.f64", (size_t)nev * per);
+
+    sem_mesh_desc d{};
+    d.nspec = nspec;
+    d.nglob = nglob;
+    d.index_base = 0;
+    d.ibool = ibool.data();
+    d.xstore = x.data();
+    d.ystore = y.data();
+    d.zstore = z.data();
+    d.xix_regular = (float)xix;
+    d.jacobian_regular = (float)jac;
+    d.kappastore = kappa.data();
+    d.mustore = mu.data();
+    d.rhostore = rho.data();
+    d.rmass = rmass.data();
+    d.rho_vp = rvp.data();
+    d.rho_vs = rvs.data();
+    d.num_abs_boundary_faces = nf;
+    d.abs_boundary_ispec = fisp.data();
+    d.abs_boundary_ijk = fijk.data();
+    d.abs_boundary_jacobian2Dw = fjw.data();
+    d.abs_boundary_normal = fn.data();
+    specfwat::Mesh mesh(d);
+
+    specfwat::PrepareFWD::Config cfg;
+    cfg.nstep = nstep;
+    cfg.dt = dt;
+    cfg.max_receivers = nrec;
+    cfg.taper_pct = taper;
+    specfwat::PrepareFWD fwd(mesh, cfg, (specfwat::RunMode)mode, nev);
+    std::vector<specfwat::EventData> events((size_t)nev);
+    for (int e = 0; e < nev; ++e) {
+      const double* s = srcs.data() + (size_t)e * 11;
+      events[(size_t)e].source = sem_source{s[0], s[1], s[2], s[3], s[4], s[5],
+                                            s[6], s[7], s[8], s[9], s[10]};
+      events[(size_t)e].stations = sta;
+      events[(size_t)e].observed.assign(obs.begin() + (long)(e * per),
+                                        obs.begin() + (long)((e + 1) * per));
+    }
+    fwd.prepare_for_event(events);
+    fwd.simulation();
+
+    save(dir, "misfits.f64", fwd.misfits());
+    std::vector<float> seis;
+    std::vector<double> kern;
+    for (int e = 0; e < nev; ++e) {
+      auto s = fwd.seismograms(e);
+      seis.insert(seis.end(), s.begin(), s.end());
+      const auto& k = fwd.event_kernels(e);
+      kern.insert(kern.end(), k.begin(), k.end());
+    }
+    save(dir, "seis.f32", seis);
+    save(dir, "kernels.f64", kern);
+    save(dir, "sum.f64", fwd.sum_kernels());
+
+    // a refused call reaches the caller as SemError with the status
+    int status = 0;
+    try {
+      fwd.set_adjoint_sources(nev, std::vector<double>(per, 0.0));
+    } catch (const specfwat::SemError& e) {
+      status = e.status();
+    }
+    std::ofstream out(dir + "/errors.txt");
+    out.precision(17);
+    out << status << " " << fwd.obj_func() << "\n";
+  } catch (const specfwat::SemError& e) {
+    std::cerr << "SemError " << e.status() << ": " << e.what() << "\n";
+    return 3;
+  } catch (const std::exception& e) {
+    std::cerr << e.what() << "\n";
+    return 4;
+  }
+  return 0;
+}

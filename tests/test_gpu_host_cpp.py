@@ -1,0 +1,110 @@
+"""The C++ host side (``specfwat_b200/host``: PrepareFWD over the C ABI).
+
+- CPU: the test driver ``tests/host/run_case.cpp`` compiles and links
+  against ``libspecfwat_host.so`` and the CUDA library.
+- GPU: a FORWARD_ADJOINT pass of three distinct events on the mini box
+  through the C++ driver gives the Python PrepareFWD's misfits,
+  seismograms and kernels on the same inputs. Both use the FP16 store and
+  graphs; their autotuned kernels may differ, so they agree to the
+  scatter-add order (about 1e-6). A refused call (an event past the batch)
+  reaches the C++ caller as SemError with SEM_ERR_ARG.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from specfwat_b200 import build as B
+from specfwat_b200 import database as D
+from specfwat_b200 import solver as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "host", "run_case.cpp")
+
+
+def compile_driver(out_dir):
+    if not os.path.exists(B.HOST_LIB):
+        B.build_host()
+    exe = os.path.join(out_dir, "run_case")
+    host_dir, lib_dir = os.path.dirname(B.HOST_LIB), B.HERE
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"),
+           "-I", host_dir, SRC, "-L", host_dir, "-l:libspecfwat_host.so", "-L", lib_dir,
+           "-l:libsem_b200.so", f"-Wl,-rpath,{host_dir}:{lib_dir}", "-o", exe]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def test_driver_builds(tmp_path):
+    exe = compile_driver(str(tmp_path))
+    assert os.access(exe, os.X_OK)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+@pytest.mark.gpu
+def test_cpp_prepare_fwd_matches_python(gpu, tmp_path):
+    d = str(tmp_path)
+    db = D.build("mini")
+    rec = D.surface_receivers(db.box, 3)
+    nev, nstep, dt = 3, 300, 0.02
+    rng = np.random.default_rng(90)
+    box = db.box
+    ev = [(rng.uniform(0.3, 0.7) * box.lx, rng.uniform(0.3, 0.7) * box.ly,
+           -rng.uniform(0.2, 0.5) * box.lz, D.random_moment_tensor(rng),
+           rng.uniform(0.8, 1.2)) for _ in range(nev)]
+    srcs = [S.make_source(*e) for e in ev]
+    obs = 1e-5 * rng.standard_normal((nev, len(rec), 3, nstep))
+
+    # the case directory the C++ driver reads
+    with open(os.path.join(d, "case.txt"), "w") as f:
+        f.write(f"{db.nspec} {db.nglob} {db.nfaces} {nev} {len(rec)} {nstep} {dt!r} "
+                f"{float(db.xix_regular)!r} {float(db.jacobian_regular)!r} 3 0.05\n")
+    arrays = {
+        "ibool.i32": (db.ibool, np.int32), "x.f32": (db.xstore, np.float32),
+        "y.f32": (db.ystore, np.float32), "z.f32": (db.zstore, np.float32),
+        "kappa.f32": (db.kappa, np.float32), "mu.f32": (db.mu, np.float32),
+        "rho.f32": (db.rho, np.float32), "rho_vp.f32": (db.rho_vp, np.float32),
+        "rho_vs.f32": (db.rho_vs, np.float32), "rmass.f32": (db.rmass, np.float32),
+        "f_ispec.i32": (db.abs_ispec, np.int32), "f_ijk.i32": (db.abs_ijk, np.int32),
+        "f_jw.f32": (db.abs_jw, np.float32), "f_n.f32": (db.abs_normal, np.float32),
+        "sources.f64": (np.array([[s.x, s.y, s.z, s.Mrr, s.Mtt, s.Mpp, s.Mrt, s.Mrp, s.Mtp,
+                                   s.f0, s.tshift] for s in srcs]), np.float64),
+        "stations.f64": (rec, np.float64), "obs.f64": (obs, np.float64),
+    }
+    for name, (a, dtype) in arrays.items():
+        np.ascontiguousarray(a, dtype).tofile(os.path.join(d, name))
+    exe = compile_driver(d)
+    r = subprocess.run([exe, d], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+
+    ne = db.nspec * 125
+    mis = np.fromfile(os.path.join(d, "misfits.f64"))
+    kern = np.fromfile(os.path.join(d, "kernels.f64")).reshape(nev, 6, ne)
+    ksum = np.fromfile(os.path.join(d, "sum.f64")).reshape(6, ne)
+    seis = np.fromfile(os.path.join(d, "seis.f32"), np.float32).reshape(nev, len(rec), 3, nstep)
+    status, obj = open(os.path.join(d, "errors.txt")).read().split()
+    assert int(status) == -1
+    assert float(obj) == pytest.approx(mis.sum(), rel=1e-12)
+
+    # the Python PrepareFWD on the same inputs
+    mesh = S.Mesh(db)
+    p = S.PrepareFWD(mesh, nstep, dt, nev=nev, store="fp16", use_graph=True,
+                     max_receivers=len(rec))
+    p.setup(srcs, rec)
+    p.simulation([obs[e] for e in range(nev)], run_mode=S.FORWARD_ADJOINT)
+    py_seis = [p.sim.seismograms(e) for e in range(nev)]
+    py_kern = [p.sim.save_adjoint_kernels(e).reshape(6, ne) for e in range(nev)]
+    py_sum = p.sim.sum_kernels().reshape(6, ne)
+    py_mis = p.misfits.copy()
+    p.close()
+    mesh.close()
+    for e in range(nev):
+        assert mis[e] == pytest.approx(py_mis[e], rel=1e-5)
+        assert rel(seis[e], py_seis[e]) < 1e-5
+        for q in range(6):
+            assert rel(kern[e, q], py_kern[e][q]) < 1e-4, (e, q)
+    for q in range(6):
+        assert rel(ksum[q], py_sum[q]) < 1e-4
