@@ -88,11 +88,19 @@ void PrepareFWD::set_adjoint_sources(int ev, const std::vector<double>& adj) {
   check(sem_set_adjoint_sources(run_, ev, adj.data()), "sem_set_adjoint_sources");
 }
 
+void PrepareFWD::set_run_mode(RunMode mode) {
+  require(mode >= FORWARD_ONLY && mode <= ADJOINT_ONLY, "run_mode must be 1..5");
+  mode_ = mode;
+}
+
 void PrepareFWD::simulation() {
   require(run_ != nullptr, "the run was destroyed");
   if (mode_ <= FORWARD_SAVE) run_simulation(1);
   if (mode_ == FORWARD_MEASADJ || mode_ == FORWARD_ADJOINT) measure_adj();
   if (mode_ == FORWARD_ADJOINT || mode_ == ADJOINT_ONLY) {
+    if (!saved_)
+      throw SemError(SEM_ERR_STATE, "the adjoint run needs a saved forward run "
+                                    "(FORWARD_ADJOINT, or FORWARD_SAVE before ADJOINT_ONLY)");
     run_simulation(3);
     postproc_adjoint();
   }

@@ -101,6 +101,11 @@ class PrepareFWD {
   // adjoint sources of event ev in forward time order [nrec][3][nstep],
   // for ADJOINT_ONLY passes whose sources come from elsewhere
   void set_adjoint_sources(int ev, const std::vector<double>& adj);
+  // the mode of the next pass: a FORWARD_SAVE pass keeps the forward state
+  // on the device, and an ADJOINT_ONLY pass of the same object runs the
+  // adjoint of it (the reference does the two in separate runs through
+  // save_forward_arrays.bin and absorb_field.bin)
+  void set_run_mode(RunMode mode);
 
   // results of the last pass
   double obj_func() const { return obj_func_; }                     // sum of the misfits

@@ -10,7 +10,8 @@
 // obs.f64 [nev][nrec][3][nstep].
 // Writes misfits.f64, kernels.f64 [nev][6][nspec*125], sum.f64,
 // seis.f32 [nev][nrec][3][nstep] and errors.txt (the status of a refused
-// call).
+// call).  With a second argument "save-adjoint" the pass is FORWARD_SAVE,
+// then ADJOINT_ONLY with the adjoint sources synthetics - observed.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -35,11 +36,12 @@ static void save(const std::string& dir, const std::string& name, const std::vec
 }
 
 int main(int argc, char** argv) {
-  if (argc != 2) {
-    std::cerr << "usage: run_case <case dir>\n";
+  if (argc != 2 && argc != 3) {
+    std::cerr << "usage: run_case <case dir> [save-adjoint]\n";
     return 2;
   }
   const std::string dir = argv[1];
+  const bool two_pass = argc == 3 && std::string(argv[2]) == "save-adjoint";
   try {
     std::ifstream h(dir + "/case.txt");
     int nspec, nglob, nf, nev, nrec, nstep, mode;
@@ -100,6 +102,26 @@ int main(int argc, char** argv) {
                                         obs.begin() + (long)((e + 1) * per));
     }
     fwd.prepare_for_event(events);
+    if (two_pass) {
+      // an adjoint pass before any saved forward is refused
+      fwd.set_run_mode(specfwat::ADJOINT_ONLY);
+      int early = 0;
+      try {
+        fwd.simulation();
+      } catch (const specfwat::SemError& e) {
+        early = e.status();
+      }
+      if (early != SEM_ERR_STATE) throw std::runtime_error("adjoint before forward not refused");
+      fwd.set_run_mode(specfwat::FORWARD_SAVE);
+      fwd.simulation();
+      for (int e = 0; e < nev; ++e) {
+        const auto s = fwd.seismograms(e);
+        std::vector<double> adj(per);
+        for (size_t i = 0; i < per; ++i) adj[i] = (double)s[i] - events[(size_t)e].observed[i];
+        fwd.set_adjoint_sources(e, adj);
+      }
+      fwd.set_run_mode(specfwat::ADJOINT_ONLY);
+    }
     fwd.simulation();
 
     save(dir, "misfits.f64", fwd.misfits());

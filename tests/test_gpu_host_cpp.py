@@ -4,7 +4,8 @@
   against ``libspecfwat_host.so`` and the CUDA library.
 - GPU: a FORWARD_ADJOINT pass of three distinct events on the mini box
   through the C++ driver gives the Python PrepareFWD's misfits,
-  seismograms and kernels on the same inputs. Both use the FP16 store and
+  seismograms and kernels on the same inputs; so does a FORWARD_SAVE pass
+  followed by ADJOINT_ONLY with the caller's adjoint sources. Both use the FP16 store and
   graphs; their autotuned kernels may differ, so they agree to the
   scatter-add order (about 1e-6). A refused call (an event past the batch)
   reaches the C++ caller as SemError with SEM_ERR_ARG.
@@ -44,24 +45,22 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
 
 
-@pytest.mark.gpu
-def test_cpp_prepare_fwd_matches_python(gpu, tmp_path):
+def _case(tmp_path, mode, seed):
+    """A three-event case on the mini box written for the C++ driver."""
     d = str(tmp_path)
     db = D.build("mini")
     rec = D.surface_receivers(db.box, 3)
     nev, nstep, dt = 3, 300, 0.02
-    rng = np.random.default_rng(90)
+    rng = np.random.default_rng(seed)
     box = db.box
     ev = [(rng.uniform(0.3, 0.7) * box.lx, rng.uniform(0.3, 0.7) * box.ly,
            -rng.uniform(0.2, 0.5) * box.lz, D.random_moment_tensor(rng),
            rng.uniform(0.8, 1.2)) for _ in range(nev)]
     srcs = [S.make_source(*e) for e in ev]
     obs = 1e-5 * rng.standard_normal((nev, len(rec), 3, nstep))
-
-    # the case directory the C++ driver reads
     with open(os.path.join(d, "case.txt"), "w") as f:
         f.write(f"{db.nspec} {db.nglob} {db.nfaces} {nev} {len(rec)} {nstep} {dt!r} "
-                f"{float(db.xix_regular)!r} {float(db.jacobian_regular)!r} 3 0.05\n")
+                f"{float(db.xix_regular)!r} {float(db.jacobian_regular)!r} {mode} 0.05\n")
     arrays = {
         "ibool.i32": (db.ibool, np.int32), "x.f32": (db.xstore, np.float32),
         "y.f32": (db.ystore, np.float32), "z.f32": (db.zstore, np.float32),
@@ -76,20 +75,31 @@ def test_cpp_prepare_fwd_matches_python(gpu, tmp_path):
     }
     for name, (a, dtype) in arrays.items():
         np.ascontiguousarray(a, dtype).tofile(os.path.join(d, name))
-    exe = compile_driver(d)
-    r = subprocess.run([exe, d], capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stderr
+    return d, db, rec, srcs, obs, nev, nstep, dt
 
+
+def _results(d, db, nev, nrec, nstep):
     ne = db.nspec * 125
     mis = np.fromfile(os.path.join(d, "misfits.f64"))
     kern = np.fromfile(os.path.join(d, "kernels.f64")).reshape(nev, 6, ne)
     ksum = np.fromfile(os.path.join(d, "sum.f64")).reshape(6, ne)
-    seis = np.fromfile(os.path.join(d, "seis.f32"), np.float32).reshape(nev, len(rec), 3, nstep)
+    seis = np.fromfile(os.path.join(d, "seis.f32"), np.float32).reshape(nev, nrec, 3, nstep)
     status, obj = open(os.path.join(d, "errors.txt")).read().split()
-    assert int(status) == -1
-    assert float(obj) == pytest.approx(mis.sum(), rel=1e-12)
+    return mis, kern, ksum, seis, int(status), float(obj)
+
+
+@pytest.mark.gpu
+def test_cpp_prepare_fwd_matches_python(gpu, tmp_path):
+    d, db, rec, srcs, obs, nev, nstep, dt = _case(tmp_path, 3, 90)
+    exe = compile_driver(d)
+    r = subprocess.run([exe, d], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    mis, kern, ksum, seis, status, obj = _results(d, db, nev, len(rec), nstep)
+    assert status == -1
+    assert obj == pytest.approx(mis.sum(), rel=1e-12)
 
     # the Python PrepareFWD on the same inputs
+    ne = db.nspec * 125
     mesh = S.Mesh(db)
     p = S.PrepareFWD(mesh, nstep, dt, nev=nev, store="fp16", use_graph=True,
                      max_receivers=len(rec))
@@ -108,3 +118,36 @@ def test_cpp_prepare_fwd_matches_python(gpu, tmp_path):
             assert rel(kern[e, q], py_kern[e][q]) < 1e-4, (e, q)
     for q in range(6):
         assert rel(ksum[q], py_sum[q]) < 1e-4
+
+
+@pytest.mark.gpu
+def test_cpp_save_then_adjoint_only(gpu, tmp_path):
+    """FORWARD_SAVE, then ADJOINT_ONLY on the kept state with the caller's
+    adjoint sources (synthetics - observed); an ADJOINT_ONLY pass before
+    any saved forward is refused with SEM_ERR_STATE (checked in the
+    driver)."""
+    d, db, rec, srcs, obs, nev, nstep, dt = _case(tmp_path, 3, 91)
+    exe = compile_driver(d)
+    r = subprocess.run([exe, d, "save-adjoint"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    _, kern, ksum, seis, status, _ = _results(d, db, nev, len(rec), nstep)
+    assert status == -1
+    ne = db.nspec * 125
+    mesh = S.Mesh(db)
+    sim = S.Simulation(mesh, nstep, dt, nev=nev, store="fp16", use_graph=True,
+                       max_receivers=len(rec))
+    sim.set_sources(srcs)
+    sim.set_receivers(rec)
+    sim.iterate_time(1, save_forward=True)
+    py_seis = [sim.seismograms(e) for e in range(nev)]
+    for e in range(nev):
+        sim.set_adjoint_sources(e, py_seis[e].astype(np.float64) - obs[e])
+    sim.iterate_time(3)
+    py_kern = [sim.save_adjoint_kernels(e).reshape(6, ne) for e in range(nev)]
+    sim.close()
+    mesh.close()
+    for e in range(nev):
+        assert rel(seis[e], py_seis[e]) < 1e-5
+        for q in range(6):
+            assert rel(kern[e, q], py_kern[e][q]) < 1e-4, (e, q)
+    assert rel(ksum[1], np.sum([k[1] for k in py_kern], axis=0)) < 1e-4
