@@ -1,7 +1,9 @@
 """The C++ host side (``specfwat_b200/host``: PrepareFWD over the C ABI).
 
 - CPU: the test driver ``tests/host/run_case.cpp`` compiles and links
-  against ``libspecfwat_host.so`` and the CUDA library.
+  against ``libspecfwat_host.so`` and the CUDA library, and a refused call
+  (an empty database) reaches a C++ caller as ``SemError`` with the
+  library's status.
 - GPU: a FORWARD_ADJOINT pass of three distinct events on the mini box
   through the C++ driver gives the Python PrepareFWD's misfits,
   seismograms and kernels on the same inputs; so does a FORWARD_SAVE pass
@@ -24,13 +26,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = os.path.join(ROOT, "tests", "host", "run_case.cpp")
 
 
-def compile_driver(out_dir):
+def compile_driver(out_dir, src=SRC, name="run_case"):
     if not os.path.exists(B.HOST_LIB):
         B.build_host()
-    exe = os.path.join(out_dir, "run_case")
+    exe = os.path.join(out_dir, name)
     host_dir, lib_dir = os.path.dirname(B.HOST_LIB), B.HERE
     cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"),
-           "-I", host_dir, SRC, "-L", host_dir, "-l:libspecfwat_host.so", "-L", lib_dir,
+           "-I", host_dir, src, "-L", host_dir, "-l:libspecfwat_host.so", "-L", lib_dir,
            "-l:libsem_b200.so", f"-Wl,-rpath,{host_dir}:{lib_dir}", "-o", exe]
     subprocess.run(cmd, check=True)
     return exe
@@ -39,6 +41,17 @@ def compile_driver(out_dir):
 def test_driver_builds(tmp_path):
     exe = compile_driver(str(tmp_path))
     assert os.access(exe, os.X_OK)
+
+
+def test_refused_call_is_a_sem_error(tmp_path):
+    """No device needed: sem_prepare_mesh refuses an empty database before
+    touching the GPU, and the C++ Mesh turns that into SemError(-1)."""
+    exe = compile_driver(str(tmp_path), os.path.join(ROOT, "tests", "host", "refuse_mesh.cpp"),
+                         "refuse_mesh")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    status, msg = r.stdout.split("\n", 1)
+    assert int(status) == -1 and "nspec" in msg
 
 
 def rel(a, b):
