@@ -150,4 +150,37 @@ const std::vector<double>& PrepareFWD::event_kernels(int ev) const {
   return kernels_[(size_t)ev];
 }
 
+std::vector<float> gradient_on_grid(const Mesh& mesh, const std::vector<double>& kernels,
+                                    const std::vector<float>* precond,
+                                    const GradientConfig& cfg) {
+  const size_t ne = (size_t)mesh.nspec() * 125;
+  require(kernels.size() == 6 * ne, "kernels are [6][nspec][125]");
+  require(!precond || precond->size() == ne, "the preconditioner is [nspec][125]");
+  const int iso[3] = {5, 4, 3};  // alpha, beta, rhop in rho, mu, kappa, rhop, beta, alpha
+  const int nsm = cfg.rho_scaling ? 2 : 3;
+  std::vector<float> in((size_t)nsm * ne), sm((size_t)nsm * ne);
+  for (int f = 0; f < nsm; ++f)
+    for (size_t i = 0; i < ne; ++i) {
+      double v = kernels[(size_t)iso[f] * ne + i];
+      if (precond) v *= (double)(*precond)[i];
+      in[(size_t)f * ne + i] = (float)v;
+    }
+  sem_smooth_cfg sc{};
+  sc.sigma_h = cfg.sigma_h;
+  sc.sigma_v = cfg.sigma_v;
+  sc.mapping = SEM_SMOOTH_MAP_CUBE;
+  check(sem_smooth_pde(mesh.handle(), &sc, nsm, in.data(), nullptr, sm.data(), nullptr),
+        "sem_smooth_pde");
+  const size_t ng = (size_t)cfg.grid.n[0] * cfg.grid.n[1] * cfg.grid.n[2];
+  std::vector<float> grid(3 * ng);
+  check(sem_grid_project(mesh.handle(), &cfg.grid, nsm, sm.data(), grid.data()),
+        "sem_grid_project");
+  if (cfg.rho_scaling)
+    for (size_t i = 0; i < ng; ++i) grid[2 * ng + i] = grid[ng + i] * 0.33f;
+  if (cfg.taper)
+    check(sem_grid_taper(mesh.handle(), &cfg.grid, &cfg.taper_widths, 3, grid.data(), nullptr),
+          "sem_grid_taper");
+  return grid;
+}
+
 }  // namespace specfwat

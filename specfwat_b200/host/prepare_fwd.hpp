@@ -14,6 +14,10 @@
 //   destroy                :127-140      destroy() / destructor
 //   obj_func                             obj_func()
 //
+//   xfwat_post_proc for an isotropic model (src/postproc/fwat_post_proc.f90:
+//   29-46; PostFlow%apply_precond, pde_smooth, taper_kernel_grid of
+//   post_processing.f90:164-325)         gradient_on_grid(mesh, kernels, ...)
+//
 // read_mesh_databases_fwat (+ the mesh part of prepare_GPU) is Mesh, built
 // from the database arrays the reference reads (sem_mesh_desc).  The run
 // modes are the reference's (src/shared/config.f90:52-56).  Where the
@@ -135,5 +139,26 @@ class PrepareFWD {
   std::vector<std::vector<double>> kernels_;
   std::vector<double> sum_;
 };
+
+// The model-grid gradient of fwat_post_proc: the KERNEL_ISO kernels
+// (alpha, beta, rhop; src/shared/config.f90:35) of summed kernels
+// [6][nspec][125] (rho, mu, kappa, rhop, beta, alpha), times the
+// preconditioner [nspec][125] when given (apply_precond), each smoothed
+// (pde_smooth: sem_smooth_pde, the cube mapping), projected onto the grid
+// (gll2grid: sem_grid_project); with rho_scaling the rhop grid is the beta
+// grid times 0.33 (USE_RHO_SCALING, post_processing.f90:262-264); then
+// tapered when `taper` is set (taper_kernel_grid: sem_grid_taper).
+// Returns [3][nx][ny][nz] in KERNEL_ISO order.
+struct GradientConfig {
+  sem_grid_desc grid{};
+  double sigma_h = 0.0, sigma_v = 0.0;
+  bool rho_scaling = false;
+  bool taper = false;
+  sem_grid_taper_cfg taper_widths{};
+};
+
+std::vector<float> gradient_on_grid(const Mesh& mesh, const std::vector<double>& kernels,
+                                    const std::vector<float>* precond,
+                                    const GradientConfig& cfg);
 
 }  // namespace specfwat

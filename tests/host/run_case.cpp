@@ -12,28 +12,13 @@
 // seis.f32 [nev][nrec][3][nstep] and errors.txt (the status of a refused
 // call).  With a second argument "save-adjoint" the pass is FORWARD_SAVE,
 // then ADJOINT_ONLY with the adjoint sources synthetics - observed.
-#include <cstdio>
 #include <fstream>
 #include <iostream>
 #include <string>
 #include <vector>
 
+#include "case_mesh.hpp"
 #include "prepare_fwd.hpp"
-
-template <class T>
-static std::vector<T> load(const std::string& dir, const std::string& name, size_t n) {
-  std::vector<T> v(n);
-  std::ifstream f(dir + "/" + name, std::ios::binary);
-  if (!f || !f.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(n * sizeof(T))))
-    throw std::runtime_error("cannot read " + name);
-  return v;
-}
-
-template <class T>
-static void save(const std::string& dir, const std::string& name, const std::vector<T>& v) {
-  std::ofstream f(dir + "/" + name, std::ios::binary);
-  f.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(T)));
-}
 
 int main(int argc, char** argv) {
   if (argc != 2 && argc != 3) {
@@ -48,42 +33,12 @@ int main(int argc, char** argv) {
     double dt, xix, jac, taper;
     if (!(h >> nspec >> nglob >> nf >> nev >> nrec >> nstep >> dt >> xix >> jac >> mode >> taper))
       throw std::runtime_error("bad case.txt");
-    const size_t ne = (size_t)nspec * 125;
-    auto ibool = load<int>(dir, "ibool.i32", ne);
-    auto x = load<float>(dir, "x.f32", nglob), y = load<float>(dir, "y.f32", nglob),
-         z = load<float>(dir, "z.f32", nglob);
-    auto kappa = load<float>(dir, "kappa.f32", ne), mu = load<float>(dir, "mu.f32", ne),
-         rho = load<float>(dir, "rho.f32", ne), rvp = load<float>(dir, "rho_vp.f32", ne),
-         rvs = load<float>(dir, "rho_vs.f32", ne);
-    auto rmass = load<float>(dir, "rmass.f32", nglob);
-    auto fisp = load<int>(dir, "f_ispec.i32", nf), fijk = load<int>(dir, "f_ijk.i32", nf * 75);
-    auto fjw = load<float>(dir, "f_jw.f32", nf * 25), fn = load<float>(dir, "f_n.f32", nf * 75);
-    auto srcs = load<double>(dir, "sources.f64", (size_t)nev * 11);
-    auto sta = load<double>(dir, "stations.f64", (size_t)nrec * 3);
+    CaseMesh cm(dir, nspec, nglob, nf, xix, jac);
+    auto srcs = load_array<double>(dir, "sources.f64", (size_t)nev * 11);
+    auto sta = load_array<double>(dir, "stations.f64", (size_t)nrec * 3);
     const size_t per = (size_t)nrec * 3 * nstep;
-    auto obs = load<double>(dir, "obs.f64", (size_t)nev * per);
-
-    sem_mesh_desc d{};
-    d.nspec = nspec;
-    d.nglob = nglob;
-    d.index_base = 0;
-    d.ibool = ibool.data();
-    d.xstore = x.data();
-    d.ystore = y.data();
-    d.zstore = z.data();
-    d.xix_regular = (float)xix;
-    d.jacobian_regular = (float)jac;
-    d.kappastore = kappa.data();
-    d.mustore = mu.data();
-    d.rhostore = rho.data();
-    d.rmass = rmass.data();
-    d.rho_vp = rvp.data();
-    d.rho_vs = rvs.data();
-    d.num_abs_boundary_faces = nf;
-    d.abs_boundary_ispec = fisp.data();
-    d.abs_boundary_ijk = fijk.data();
-    d.abs_boundary_jacobian2Dw = fjw.data();
-    d.abs_boundary_normal = fn.data();
+    auto obs = load_array<double>(dir, "obs.f64", (size_t)nev * per);
+    const sem_mesh_desc& d = cm.desc;
     specfwat::Mesh mesh(d);
 
     specfwat::PrepareFWD::Config cfg;
@@ -124,7 +79,7 @@ int main(int argc, char** argv) {
     }
     fwd.simulation();
 
-    save(dir, "misfits.f64", fwd.misfits());
+    save_array(dir, "misfits.f64", fwd.misfits());
     std::vector<float> seis;
     std::vector<double> kern;
     for (int e = 0; e < nev; ++e) {
@@ -133,9 +88,9 @@ int main(int argc, char** argv) {
       const auto& k = fwd.event_kernels(e);
       kern.insert(kern.end(), k.begin(), k.end());
     }
-    save(dir, "seis.f32", seis);
-    save(dir, "kernels.f64", kern);
-    save(dir, "sum.f64", fwd.sum_kernels());
+    save_array(dir, "seis.f32", seis);
+    save_array(dir, "kernels.f64", kern);
+    save_array(dir, "sum.f64", fwd.sum_kernels());
 
     // a refused call reaches the caller as SemError with the status
     int status = 0;

@@ -7,7 +7,8 @@
 - GPU: a FORWARD_ADJOINT pass of three distinct events on the mini box
   through the C++ driver gives the Python PrepareFWD's misfits,
   seismograms and kernels on the same inputs; so does a FORWARD_SAVE pass
-  followed by ADJOINT_ONLY with the caller's adjoint sources. Both use the FP16 store and
+  followed by ADJOINT_ONLY with the caller's adjoint sources, and the C++
+  gradient_on_grid gives postproc.gradient_on_grid's grids. Both use the FP16 store and
   graphs; their autotuned kernels may differ, so they agree to the
   scatter-add order (about 1e-6). A refused call (an event past the batch)
   reaches the C++ caller as SemError with SEM_ERR_ARG.
@@ -32,7 +33,7 @@ def compile_driver(out_dir, src=SRC, name="run_case"):
     exe = os.path.join(out_dir, name)
     host_dir, lib_dir = os.path.dirname(B.HOST_LIB), B.HERE
     cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"),
-           "-I", host_dir, src, "-L", host_dir, "-l:libspecfwat_host.so", "-L", lib_dir,
+           "-I", host_dir, "-I", os.path.join(ROOT, "tests", "host"), src, "-L", host_dir, "-l:libspecfwat_host.so", "-L", lib_dir,
            "-l:libsem_b200.so", f"-Wl,-rpath,{host_dir}:{lib_dir}", "-o", exe]
     subprocess.run(cmd, check=True)
     return exe
@@ -58,6 +59,20 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
 
 
+def _write_mesh(d, db):
+    arrays = {
+        "ibool.i32": (db.ibool, np.int32), "x.f32": (db.xstore, np.float32),
+        "y.f32": (db.ystore, np.float32), "z.f32": (db.zstore, np.float32),
+        "kappa.f32": (db.kappa, np.float32), "mu.f32": (db.mu, np.float32),
+        "rho.f32": (db.rho, np.float32), "rho_vp.f32": (db.rho_vp, np.float32),
+        "rho_vs.f32": (db.rho_vs, np.float32), "rmass.f32": (db.rmass, np.float32),
+        "f_ispec.i32": (db.abs_ispec, np.int32), "f_ijk.i32": (db.abs_ijk, np.int32),
+        "f_jw.f32": (db.abs_jw, np.float32), "f_n.f32": (db.abs_normal, np.float32),
+    }
+    for name, (a, dtype) in arrays.items():
+        np.ascontiguousarray(a, dtype).tofile(os.path.join(d, name))
+
+
 def _case(tmp_path, mode, seed):
     """A three-event case on the mini box written for the C++ driver."""
     d = str(tmp_path)
@@ -74,14 +89,8 @@ def _case(tmp_path, mode, seed):
     with open(os.path.join(d, "case.txt"), "w") as f:
         f.write(f"{db.nspec} {db.nglob} {db.nfaces} {nev} {len(rec)} {nstep} {dt!r} "
                 f"{float(db.xix_regular)!r} {float(db.jacobian_regular)!r} {mode} 0.05\n")
+    _write_mesh(d, db)
     arrays = {
-        "ibool.i32": (db.ibool, np.int32), "x.f32": (db.xstore, np.float32),
-        "y.f32": (db.ystore, np.float32), "z.f32": (db.zstore, np.float32),
-        "kappa.f32": (db.kappa, np.float32), "mu.f32": (db.mu, np.float32),
-        "rho.f32": (db.rho, np.float32), "rho_vp.f32": (db.rho_vp, np.float32),
-        "rho_vs.f32": (db.rho_vs, np.float32), "rmass.f32": (db.rmass, np.float32),
-        "f_ispec.i32": (db.abs_ispec, np.int32), "f_ijk.i32": (db.abs_ijk, np.int32),
-        "f_jw.f32": (db.abs_jw, np.float32), "f_n.f32": (db.abs_normal, np.float32),
         "sources.f64": (np.array([[s.x, s.y, s.z, s.Mrr, s.Mtt, s.Mpp, s.Mrt, s.Mrp, s.Mtp,
                                    s.f0, s.tshift] for s in srcs]), np.float64),
         "stations.f64": (rec, np.float64), "obs.f64": (obs, np.float64),
@@ -164,3 +173,42 @@ def test_cpp_save_then_adjoint_only(gpu, tmp_path):
         for q in range(6):
             assert rel(kern[e, q], py_kern[e][q]) < 1e-4, (e, q)
     assert rel(ksum[1], np.sum([k[1] for k in py_kern], axis=0)) < 1e-4
+
+
+@pytest.mark.gpu
+def test_cpp_gradient_on_grid_matches_python(gpu, tmp_path):
+    """The C++ gradient_on_grid (precondition, smooth, project, rhop from
+    beta, taper) against postproc.gradient_on_grid on the same kernels: the
+    same device calls in the same order, so they agree to the smoother's
+    scatter-add order."""
+    from specfwat_b200.postproc import gradient_on_grid
+    d = str(tmp_path)
+    db = D.build("mini")
+    rng = np.random.default_rng(92)
+    k6 = rng.standard_normal((6, db.nspec, 5, 5, 5))
+    pre = rng.uniform(0.5, 1.5, (db.nspec, 5, 5, 5)).astype(np.float32)
+    box = db.box
+    x0, h, n = (0.0, 0.0, -box.lz), (1000.0, 1000.0, 1000.0), (
+        int(box.lx // 1000) + 1, int(box.ly // 1000) + 1, int(box.lz // 1000) + 1)
+    sig = (6000.0, 3000.0)
+    tap = (1000.0, 2000.0, 1000.0, 2000.0)
+    _write_mesh(d, db)
+    k6.tofile(os.path.join(d, "kernels.f64"))
+    pre.tofile(os.path.join(d, "precond.f32"))
+    with open(os.path.join(d, "case.txt"), "w") as f:
+        f.write(f"{db.nspec} {db.nglob} {db.nfaces} {float(db.xix_regular)!r} "
+                f"{float(db.jacobian_regular)!r} {' '.join(map(repr, x0))} "
+                f"{' '.join(map(repr, h))} {' '.join(map(str, n))} {sig[0]!r} {sig[1]!r} 1 1 "
+                f"{' '.join(map(repr, tap))}\n")
+    exe = compile_driver(d, os.path.join(ROOT, "tests", "host", "run_gradient.cpp"),
+                         "run_gradient")
+    r = subprocess.run([exe, d], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    grad = np.fromfile(os.path.join(d, "grad.f32"), np.float32).reshape((3,) + n)
+    mesh = S.Mesh(db)
+    ref = gradient_on_grid(mesh, db, k6, x0, h, n, *sig, precond=pre.astype(np.float64),
+                           rho_scaling=True, taper=tap)
+    mesh.close()
+    assert np.count_nonzero(grad[1]) > 0.3 * grad[1].size
+    for q in range(3):
+        assert rel(grad[q], ref[q]) < 1e-5, q
